@@ -1,0 +1,232 @@
+/*
+ * msbg_cuda.h -- C ABI of the B200 (sm_100a) sparse-grid hot path.
+ *
+ * Drop-in boundary for the msbg-rs crate's sparse-grid path: the functions
+ * below replace, one for one, the crate entry points cited beside each
+ * declaration (paths relative to the msbg-rs source tree).  A Rust host binds
+ * them with `extern "C"` declarations; the Python package in msbg-rs_b200/
+ * binds them with ctypes.
+ *
+ * Conventions
+ *  - Every function returns an int status: MSBG_OK (0) or an MSBG_ERR_* code.
+ *    No exception or panic crosses the ABI.  msbg_status_string() names a code;
+ *    msbg_last_error() returns the message of the last failure on this thread.
+ *  - Handles are opaque.  A context owns one CUDA stream on one device; every
+ *    call on objects of a context is ordered on that stream.  Calls are
+ *    thread-safe per context object only if the caller serialises them.
+ *  - Host-pointer entry points copy their inputs to the device and their
+ *    results back (they synchronise the stream before returning).  The
+ *    `_device` variants take device pointers, enqueue work and return without
+ *    synchronising.
+ *  - Block ids (bids) are 64-bit: bid = bx + by*nx + bz*nx*ny
+ *    (sparse_grid.rs:157-165); voxel-in-block index vid = x | y<<log2(bsx) |
+ *    z<<2*log2(bsx) (sparse_grid.rs:167-175).
+ */
+#ifndef MSBG_CUDA_H
+#define MSBG_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define MSBG_OK 0
+#define MSBG_ERR_ARG 1     /* invalid argument (size, id, enum, alignment)  */
+#define MSBG_ERR_OOM 2     /* device or host allocation failed              */
+#define MSBG_ERR_TIMEOUT 3 /* a bounded device-side wait gave up            */
+#define MSBG_ERR_CUDA 4    /* a CUDA runtime call failed                    */
+#define MSBG_ERR_STATE 5   /* object used in the wrong state                */
+#define MSBG_ERR_NUMERIC 6 /* solver breakdown (NaN / stall)                */
+
+/* ---- enums ----------------------------------------------------------- */
+/* Storage element of a grid channel (channel.rs:31-116, stencil.rs:142-192). */
+#define MSBG_F32 0  /* f32 payload                                          */
+#define MSBG_U16 1  /* `Density`: u16, value = q / 65535, store rounds      */
+                    /* half away from zero (stencil.rs:160-174)            */
+#define MSBG_BF16 2 /* bf16 payload, store rounds to nearest even           */
+
+/* Stencil of a sweep (solver.rs:44-51). */
+#define MSBG_LAPLACIAN 0       /* 7-tap,  laplacian.rs:16-70               */
+#define MSBG_MEAN_CURVATURE 1  /* 19-tap, meancurv.rs:17-107               */
+#define MSBG_BILAPLACIAN 2     /* 25-tap, bilaplacian.rs:15-97             */
+
+/* Boundary condition (math/boundary.rs:7-16). */
+#define MSBG_CLAMP 0
+#define MSBG_NEUMANN 1
+#define MSBG_DIRICHLET 2
+
+typedef struct msbg_ctx msbg_ctx;
+typedef struct msbg_grid msbg_grid;
+typedef struct msbg_mac msbg_mac;
+typedef struct msbg_poisson msbg_poisson;
+
+/* ---- context ---------------------------------------------------------- */
+const char* msbg_status_string(int status);
+const char* msbg_last_error(void);
+/* Creates a context on CUDA device `device` with its own stream.
+ * (No crate counterpart: the crate runs on the rayon global pool,
+ * thread_pool.rs:1-40.) */
+int msbg_ctx_create(int device, msbg_ctx** out);
+int msbg_ctx_destroy(msbg_ctx* ctx);
+int msbg_ctx_synchronize(msbg_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for interop. */
+int msbg_ctx_stream(msbg_ctx* ctx, void** stream_out);
+/* Number of kernels this library launched on the context since creation. */
+int msbg_ctx_kernel_launches(msbg_ctx* ctx, uint64_t* out);
+/* Per-kernel timing with CUDA events on the context stream (SURVEY-style
+ * phase profiling; no crate counterpart beyond MSBG_BUCKET_PROFILE,
+ * particles/sort.rs:184-262).  While enabled every kernel launch is bracketed
+ * by two events.  The report lists "name launches total_ms" per kernel; it
+ * synchronises the stream.  reset != 0 clears the totals after reporting. */
+int msbg_ctx_set_timing(msbg_ctx* ctx, int enable);
+int msbg_ctx_timing_report(msbg_ctx* ctx, int reset, char* buf, size_t cap, size_t* len_out);
+/* Bytes of device scratch currently held by the context's arena. */
+int msbg_ctx_scratch_bytes(msbg_ctx* ctx, uint64_t* out);
+
+/* ---- sparse grid (sparse_grid.rs:61-435, blockmap.rs:35-209) ----------- */
+/* SparseGrid::new(name, sx, sy, sz, empty_value, full_value, pool)
+ * (sparse_grid.rs:109-156).  bsx is a power of two in [1, 32]. */
+int msbg_grid_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, int dtype,
+                     float empty_value, float full_value, msbg_grid** out);
+int msbg_grid_destroy(msbg_grid* grid);
+/* out[0..7] = sx, sy, sz, nx, ny, nz, n_blocks, n_value_blocks */
+int msbg_grid_dims(const msbg_grid* grid, uint64_t out[8]);
+/* ensure_blocks_parallel (sparse_grid.rs:326-355): allocate value blocks for
+ * `bids` not yet allocated (a full dummy is replaced), filled with the empty
+ * value; existing value blocks are kept. */
+int msbg_grid_ensure_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
+/* set_full_block / set_empty_block (sparse_grid.rs:248-262): only for bids
+ * that are not value blocks (MSBG_ERR_ARG otherwise). */
+int msbg_grid_set_full_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
+int msbg_grid_set_empty_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
+/* set_empty_value / set_full_value (sparse_grid.rs:232-245). */
+int msbg_grid_set_values(msbg_grid* grid, float empty_value, float full_value);
+/* Ensure + write whole blocks: payload is [n][bsx^3] elements of the grid's
+ * dtype (get_block_data_mut + copy). */
+int msbg_grid_write_blocks(msbg_grid* grid, const uint64_t* bids, size_t n, const void* payload);
+int msbg_grid_write_blocks_device(msbg_grid* grid, const uint64_t* bids, size_t n, const void* d_payload);
+/* Read whole blocks (get_value_in_block over the block, sparse_grid.rs:296-305):
+ * value blocks give their data, the full dummy its full value, anything else
+ * the empty value. */
+int msbg_grid_read_blocks(msbg_grid* grid, const uint64_t* bids, size_t n, void* payload);
+int msbg_grid_read_blocks_device(msbg_grid* grid, const uint64_t* bids, size_t n, void* d_payload);
+/* fill_blocks_parallel (sparse_grid.rs:359-369): fill value blocks among
+ * `bids` with `value`; dummies are skipped. */
+int msbg_grid_fill_blocks(msbg_grid* grid, const uint64_t* bids, size_t n, float value);
+/* Value-block ids in ascending order (active_block_ids, sparse_grid.rs:432).
+ * Writes min(count, cap) ids, returns the count in *n_out. */
+int msbg_grid_value_block_ids(const msbg_grid* grid, uint64_t* out, size_t cap, size_t* n_out);
+/* Device pointer to the payload arena and the slot of each listed bid (-1 if
+ * not a value block): zero-copy access for callers that keep data on device. */
+int msbg_grid_payload(msbg_grid* grid, void** d_payload, uint64_t* n_slots);
+int msbg_grid_slots(const msbg_grid* grid, const uint64_t* bids, size_t n, int32_t* slots_out);
+
+/* ---- halo gather (multires/halo.rs:31-170) ------------------------------ */
+/* HaloBlock::fill::<HALO, FULL>(grid, bid, bc) for each listed bid.  out is
+ * [n][(bsx+2*halo)^3] f32; halo in {1, 2}.  With full == 0 only the centre,
+ * the six faces and the x-edges are written (the rest is 0), as in the
+ * reference. */
+int msbg_halo_gather(msbg_grid* grid, const uint64_t* bids, size_t n, int halo, int full, int bc,
+                     float* out);
+int msbg_halo_gather_device(msbg_grid* grid, const uint64_t* d_bids, size_t n, int halo, int full,
+                            int bc, float* d_out);
+
+/* ---- 8-colour in-place smoother (solver.rs:141-267) -------------------- */
+/* Sweeper::new(grid, ..).sweep(active, stencil, &PdeParams{dt, iterations,
+ * do_constr_zero_one}) (solver.rs:154-185) and apply_pde (solver.rs:228-240).
+ * Blocks of `active` that are not value blocks are skipped (solver.rs:196-199).
+ * The boundary condition is Neumann (solver.rs:205-209).  The plan (colour
+ * buckets, neighbour table) is cached per grid and rebuilt only when the
+ * active list or the grid's block set changes. */
+int msbg_sweep(msbg_grid* grid, const uint64_t* active, size_t n, int stencil, float dt,
+               int iterations, int clamp01);
+/* Multiresolution sweep: the halo of each fine block reads coarser
+ * neighbours (levels[b] > levels[bid]) from `coarse` at the fine coordinate
+ * >> 1 (fill_multires, multires/halo.rs:187-358); absent blocks read 0.
+ * levels is [n_blocks] u8 on the host; coarse.bsx == fine.bsx / 2. */
+int msbg_sweep_multires(msbg_grid* fine, msbg_grid* coarse, const uint8_t* levels,
+                        const uint64_t* active, size_t n, int stencil, float dt, int iterations,
+                        int clamp01);
+
+/* ---- Morton keys and sorts --------------------------------------------- */
+/* morton3 (multires/sort.rs:20-22) for n coordinate triples (u64 xyz). */
+int msbg_morton3(msbg_ctx* ctx, const uint64_t* xyz, size_t n, uint64_t* keys_out);
+/* sort_block_list_morton (multires/sort.rs:35-57): sorts `blocks` in place on
+ * the device by the level-scaled Morton key. */
+int msbg_sort_block_list_morton(msbg_ctx* ctx, uint64_t* blocks, size_t n, uint64_t nx, uint64_t ny,
+                                const uint8_t* levels, size_t n_levels_array, int n_levels);
+/* Per-particle Morton sort: key = morton3(trunc(p)) (21 bits per axis), a
+ * stable LSD radix sort of (key, index).  keys_out[i] is the i-th smallest key,
+ * perm_out[i] the original index of the i-th particle (bit-exact against a
+ * stable CPU sort).  pos is [n][3] f32; coordinates must be >= 0 and < 2^21. */
+int msbg_morton_sort(msbg_ctx* ctx, const float* pos, size_t n, uint64_t* keys_out, uint32_t* perm_out);
+int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out,
+                            uint32_t* d_perm_out);
+/* Applies a sort permutation to per-particle data: dst[i] = src[perm[i]] for
+ * items of `width` floats (the payload gather of bucket_particles,
+ * fluid/mod.rs:71-91, and bucket_by_block, particles/sort.rs:274-285). */
+int msbg_permute_device(msbg_ctx* ctx, const uint32_t* d_perm, size_t n, int width, const float* d_src, float* d_dst);
+/* bucket_indices (particles/sort.rs:174-269): block-major permutation of
+ * particle block ids.  particle_blocks (capacity n) receives the distinct bids
+ * ascending, starts (capacity n + 1) the CSR offsets, perm (n) the particle
+ * indices grouped by block; *n_blocks_out the number of distinct blocks.  The
+ * order inside a block is the input order (the stable order of the dense
+ * counting sort, particles/sort.rs:455-490). */
+int msbg_bucket_indices(msbg_ctx* ctx, const uint64_t* bids, size_t n, uint64_t* particle_blocks,
+                        uint64_t* starts, uint32_t* perm, size_t* n_blocks_out);
+int msbg_bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n,
+                               uint64_t* d_particle_blocks, uint64_t* d_starts, uint32_t* d_perm,
+                               size_t* n_blocks_out);
+
+/* ---- staggered MAC grid (fluid/mac.rs) ---------------------------------- */
+/* MacGrid::new(sx, sy, sz, pool) (mac.rs:35-45): three face-velocity and three
+ * face-mass f32 channels, empty = full = 0. */
+int msbg_mac_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, msbg_mac** out);
+int msbg_mac_destroy(msbg_mac* mac);
+/* Borrowed channel handle: which = 0..2 velocity[X..Z], 3..5 mass[X..Z]. */
+int msbg_mac_channel(msbg_mac* mac, int which, msbg_grid** out);
+/* MacGrid::zero_blocks (mac.rs:95-102). */
+int msbg_mac_zero_blocks(msbg_mac* mac, const uint64_t* bids, size_t n);
+/* particles_to_grid (fluid/p2g.rs:141-164): bucket, active_blocks(r_p+1),
+ * zero_blocks, splat of mass and momentum to the right faces with
+ * w = max(1 - d^2/r_p^2, 0)^3, then normalize_velocity.  pos, vel are [n][3],
+ * mass [n] (f32).  Sums are accumulated per particle block in FP64 and
+ * combined across blocks in a fixed order: deterministic, no float atomics.
+ * Domain extents must be multiples of bsx; 0 < r_p <= bsx / 2.
+ * *n_active_out (may be NULL) receives the size of the active block set. */
+int msbg_p2g(msbg_mac* mac, const float* pos, const float* vel, const float* mass, size_t n, float r_p,
+             size_t* n_active_out);
+int msbg_p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass, size_t n,
+                    float r_p, size_t* n_active_out);
+/* Active block set of the last P2G (ascending bids). */
+int msbg_mac_active_blocks(const msbg_mac* mac, uint64_t* out, size_t cap, size_t* n_out);
+/* MacGrid::normalize_velocity (mac.rs:106-132) over the listed blocks. */
+int msbg_mac_normalize_velocity(msbg_mac* mac, const uint64_t* bids, size_t n);
+/* MacGrid::divergence (mac.rs:137-171) into `dst` (an f32 grid of the same
+ * dims; blocks are ensured). */
+int msbg_mac_divergence(msbg_mac* mac, msbg_grid* dst, const uint64_t* active, size_t n);
+/* MacSampler::sample::<Linear> (fluid/g2p.rs:15-32): per face component a
+ * trilinear cell-centred sample at p - 1/2 e_a (gather_map, math/gather.rs:54-158;
+ * trilinear_value, math/sample.rs:203-211).  vel_out is [n][3]. */
+int msbg_g2p(msbg_mac* mac, const float* pos, size_t n, int bc, float* vel_out);
+int msbg_g2p_device(msbg_mac* mac, const float* d_pos, size_t n, int bc, float* d_vel_out);
+/* g2p_blend (fluid/g2p.rs:42-45) on [n][3] arrays. */
+int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u, const float* d_u_tilde,
+                          size_t n, float alpha, float* d_out);
+/* Scalar trilinear Sampler::sample::<Linear> (math/sample.rs:494-512);
+ * align 0 = Corner, 1 = CellCentered. */
+int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, int bc, float* out);
+
+/* ---- multiresolution transfers (multires/downsample.rs) ----------------- */
+/* downsample_channel_avg (downsample.rs:13-59): every value block of `src`
+ * (block size b) gets a block in `dst` (block size b/2, same block grid) set
+ * to the 2^3 mean. */
+int msbg_downsample_avg(msbg_grid* dst, msbg_grid* src);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSBG_CUDA_H */

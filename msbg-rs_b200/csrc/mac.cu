@@ -1,0 +1,453 @@
+// mac.cu -- MAC grid channels, normalize_velocity, divergence (fluid/mac.rs),
+// trilinear sampling and G2P (fluid/g2p.rs, math/gather.rs, math/sample.rs),
+// the FLIP/PIC blend and the 2^3 downsample (multires/downsample.rs).
+//
+// Built with --fmad=false: every sample is the reference's f32 arithmetic
+// (three-level fmaf lerp of gather_map's corners), bit-identical to the CPU
+// restatement.
+#include <algorithm>
+
+#include "mac.cuh"
+
+msbg_mac::~msbg_mac() {
+    for (auto* c : ch) delete c;
+}
+
+namespace msbg {
+
+void mac_ensure(msbg_mac* m, const uint64_t* bids, size_t n, int32_t* slots) {
+    for (int c = 0; c < 6; ++c) grid_ensure(m->ch[c], bids, n, c == 0 ? slots : nullptr);
+}
+
+struct SampleGrid {
+    const float* payload;
+    DevHash hash;
+    int64_t nx, ny, nz;
+    int32_t sx, sy, sz;
+    int lg;
+    float empty, full;
+};
+
+static SampleGrid sample_grid(msbg_grid* g) {
+    MSBG_REQUIRE(g->dtype == MSBG_F32, "sampling needs an f32 grid");
+    SampleGrid s;
+    s.payload = g->payload.as<float>();
+    s.hash = device_hash(g);
+    s.nx = (int64_t)g->nx; s.ny = (int64_t)g->ny; s.nz = (int64_t)g->nz;
+    s.sx = (int32_t)g->sx; s.sy = (int32_t)g->sy; s.sz = (int32_t)g->sz;
+    s.lg = g->lg;
+    s.empty = g->empty_value;
+    s.full = g->full_value;
+    return s;
+}
+
+__device__ __forceinline__ float code_value(const SampleGrid& g, int32_t code, int vid) {
+    if (code >= 0) return g.payload[((size_t)code << (3 * g.lg)) + vid];
+    return code == kCodeFull ? g.full : g.empty;
+}
+
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(b - a, t, a); }
+
+// gather_map (math/gather.rs:54-158, dmax = 1) + trilinear_value (sample.rs:203-211)
+// at a position already in the grid's node frame.
+__device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float z, int bc) {
+    const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const int32_t ix0 = (int32_t)fx, iy0 = (int32_t)fy, iz0 = (int32_t)fz;
+    float c[8];
+    bool fast = false;
+    if (ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + 1 < g.sx && iy0 + 1 < g.sy && iz0 + 1 < g.sz) {
+        const int vx0 = ix0 & mask, vy0 = iy0 & mask, vz0 = iz0 & mask;
+        if (vx0 + 1 < bsx && vy0 + 1 < bsx && vz0 + 1 < bsx) {
+            const uint64_t bid = (uint64_t)(ix0 >> lg) + (uint64_t)(iy0 >> lg) * g.nx + (uint64_t)(iz0 >> lg) * g.nx * g.ny;
+            const int32_t code = hash_find(g.hash, bid);
+            int s = 0;
+            for (int k = 0; k < 2; ++k)
+                for (int j = 0; j < 2; ++j)
+                    for (int i = 0; i < 2; ++i)
+                        c[s++] = code_value(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
+            fast = true;
+        }
+    }
+    if (!fast) {
+        const int64_t bx0 = min(max((int64_t)(ix0 >> lg), (int64_t)0), g.nx - 1);
+        const int64_t by0 = min(max((int64_t)(iy0 >> lg), (int64_t)0), g.ny - 1);
+        const int64_t bz0 = min(max((int64_t)(iz0 >> lg), (int64_t)0), g.nz - 1);
+        int32_t codes[8];
+        for (int s = 0; s < 8; ++s) {
+            const int64_t bxx = min(bx0 + (s & 1), g.nx - 1), byy = min(by0 + ((s >> 1) & 1), g.ny - 1),
+                          bzz = min(bz0 + (s >> 2), g.nz - 1);
+            codes[s] = hash_find(g.hash, (uint64_t)bxx + (uint64_t)byy * g.nx + (uint64_t)bzz * g.nx * g.ny);
+        }
+        int s = 0;
+        for (int k = 0; k < 2; ++k) {
+            int32_t rz;
+            const bool okz = resolve_axis(iz0 + k, g.sz - 1, bc, &rz);
+            for (int j = 0; j < 2; ++j) {
+                int32_t ry;
+                const bool oky = resolve_axis(iy0 + j, g.sy - 1, bc, &ry);
+                for (int i = 0; i < 2; ++i) {
+                    int32_t rx;
+                    const bool okx = resolve_axis(ix0 + i, g.sx - 1, bc, &rx);
+                    if (okx && oky && okz) {
+                        const int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) |
+                                             ((((rz >> lg) - bz0) & 1) << 2));
+                        c[s] = code_value(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
+                    } else {
+                        c[s] = g.empty;
+                    }
+                    ++s;
+                }
+            }
+        }
+    }
+    const float u = x - fx, v = y - fy, w = z - fz;
+    const float c00 = lerpf(c[0], c[1], u), c10 = lerpf(c[2], c[3], u), c01 = lerpf(c[4], c[5], u),
+                c11 = lerpf(c[6], c[7], u);
+    const float c0 = lerpf(c00, c10, v), c1 = lerpf(c01, c11, v);
+    return lerpf(c0, c1, w);
+}
+
+__global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, int align, int bc, float* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        if (align == 1) { x = x - 0.5f; y = y - 0.5f; z = z - 0.5f; }
+        out[i] = sample_linear_dev(g, x, y, z, bc);
+    }
+}
+
+// MacSampler::sample::<Linear> (fluid/g2p.rs:26-32): component a is a
+// cell-centred sample of velocity[a] at p - 1/2 e_a.
+__global__ void g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz, const float* __restrict__ pos, size_t n, int bc,
+                           float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+        const float cx = px - 0.5f, cy = py - 0.5f, cz = pz - 0.5f;
+        out[3 * i + 0] = sample_linear_dev(gx, (px - 0.5f) - 0.5f, cy, cz, bc);
+        out[3 * i + 1] = sample_linear_dev(gy, cx, (py - 0.5f) - 0.5f, cz, bc);
+        out[3 * i + 2] = sample_linear_dev(gz, cx, cy, (pz - 0.5f) - 0.5f, bc);
+    }
+}
+
+// g2p_blend (fluid/g2p.rs:42-45), component-wise.
+__global__ void g2p_blend_kernel(const float* u_old, const float* u, const float* ut, size_t n3, float alpha, float* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+        const float delta = u[i] - ut[i];
+        out[i] = (u_old[i] + delta) * alpha + u[i] * (1.0f - alpha);
+    }
+}
+
+// MacGrid::normalize_velocity (mac.rs:106-132) over the given slots.
+__global__ void normalize_kernel(float* vel, const float* mass, const int32_t* slots, size_t n, size_t be) {
+    for (size_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const int32_t s = slots[k];
+        if (s < 0) continue;
+        float* v = vel + (size_t)s * be;
+        const float* m = mass + (size_t)s * be;
+        for (size_t i = threadIdx.x; i < be; i += blockDim.x) {
+            const float mm = m[i];
+            v[i] = mm > 0.0f ? v[i] / mm : 0.0f;
+        }
+    }
+}
+
+// MacGrid::divergence (mac.rs:137-171).  nb[k][0..3] = codes of the block
+// itself and its -x, -y, -z neighbours in each channel (same block set).
+struct DivArgs {
+    const float* u[3];
+    float* dst;
+    int64_t nx, ny;
+    int32_t sx, sy, sz;
+    int lg;
+    float empty, full;
+};
+
+__global__ void divergence_kernel(DivArgs a, const uint64_t* bids, const int32_t* codes, const int32_t* dst_slots, size_t n) {
+    const int bsx = 1 << a.lg, mask = bsx - 1;
+    const size_t be = (size_t)bsx * bsx * bsx;
+    for (size_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const int32_t ds = dst_slots[k];
+        if (ds < 0) continue;
+        const uint64_t bid = bids[k];
+        const int64_t bx = (int64_t)(bid % a.nx), by = (int64_t)((bid / a.nx) % a.ny), bz = (int64_t)(bid / (a.nx * a.ny));
+        const int32_t gx0 = (int32_t)(bx * bsx), gy0 = (int32_t)(by * bsx), gz0 = (int32_t)(bz * bsx);
+        const int32_t gx1 = min(gx0 + bsx, a.sx), gy1 = min(gy0 + bsx, a.sy), gz1 = min(gz0 + bsx, a.sz);
+        const int32_t lx = gx1 - gx0, ly = gy1 - gy0, lz = gz1 - gz0;
+        const int32_t* c = codes + k * 4;
+        for (int i = threadIdx.x; i < lx * ly * lz; i += blockDim.x) {
+            const int x = i % lx, y = (i / lx) % ly, z = i / (lx * ly);
+            const int vid = x | (y << a.lg) | (z << (2 * a.lg));
+            auto val = [&](int ch, int32_t code, int v) -> float {
+                if (code >= 0) return a.u[ch][(size_t)code * be + v];
+                return code == kCodeFull ? a.full : a.empty;
+            };
+            const float ux1 = val(0, c[0], vid);
+            const float ux0 = (gx0 + x == 0) ? 0.0f
+                              : x > 0 ? val(0, c[0], vid - 1) : val(0, c[1], (mask) | (y << a.lg) | (z << (2 * a.lg)));
+            const float vy1 = val(1, c[0], vid);
+            const float vy0 = (gy0 + y == 0) ? 0.0f
+                              : y > 0 ? val(1, c[0], vid - bsx) : val(1, c[2], x | (mask << a.lg) | (z << (2 * a.lg)));
+            const float wz1 = val(2, c[0], vid);
+            const float wz0 = (gz0 + z == 0) ? 0.0f
+                              : z > 0 ? val(2, c[0], vid - bsx * bsx) : val(2, c[3], x | (y << a.lg) | (mask << (2 * a.lg)));
+            // The reference writes a compact running index over the in-domain
+            // cells of the block (mac.rs:151-168).
+            a.dst[(size_t)ds * be + i] = ((ux1 - ux0) + (vy1 - vy0)) + (wz1 - wz0);
+        }
+    }
+}
+
+// downsample_channel_avg (downsample.rs:13-59): coarse cell = mean of its 8
+// children, summed z-major as the reference.
+__global__ void downsample_kernel(const float* src, const int32_t* src_slots, float* dst, const int32_t* dst_slots, size_t n,
+                                  int lg) {
+    const int bsx = 1 << lg, bsc = bsx >> 1, clg = lg - 1;
+    const size_t be = (size_t)bsx * bsx * bsx, bc = (size_t)bsc * bsc * bsc;
+    for (size_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const float* sp = src + (size_t)src_slots[k] * be;
+        float* dp = dst + (size_t)dst_slots[k] * bc;
+        for (int i = threadIdx.x; i < (int)bc; i += blockDim.x) {
+            const int cx = i & (bsc - 1), cy = (i >> clg) & (bsc - 1), cz = i >> (2 * clg);
+            float sum = 0.0f;
+            for (int dz = 0; dz < 2; ++dz)
+                for (int dy = 0; dy < 2; ++dy)
+                    for (int dx = 0; dx < 2; ++dx)
+                        sum += sp[(2 * cx + dx) | ((2 * cy + dy) << lg) | ((2 * cz + dz) << (2 * lg))];
+            dp[i] = sum / 8.0f;
+        }
+    }
+}
+
+static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 8192); }
+
+void g2p_device(msbg_mac* m, const float* d_pos, size_t n, int bc, float* d_out) {
+    MSBG_REQUIRE(bc >= 0 && bc <= 2, "bad boundary condition");
+    if (!n) return;
+    SampleGrid gx = sample_grid(m->ch[0]), gy = sample_grid(m->ch[1]), gz = sample_grid(m->ch[2]);
+    begin_launch(m->ctx);
+    g2p_kernel<<<grid_for(n), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, d_out);
+    after_launch(m->ctx, "g2p_kernel");
+}
+
+}  // namespace msbg
+
+using namespace msbg;
+
+extern "C" {
+
+int msbg_mac_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, msbg_mac** out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && out, "null argument");
+    auto* m = new msbg_mac;
+    m->ctx = ctx;
+    for (int c = 0; c < 6; ++c) {
+        int st = msbg_grid_create(ctx, sx, sy, sz, bsx, MSBG_F32, 0.0f, 0.0f, &m->ch[c]);
+        if (st != MSBG_OK) {
+            std::string msg = msbg_last_error();
+            delete m;
+            MSBG_THROW(st, msg);
+        }
+    }
+    *out = m;
+    MSBG_API_END
+}
+
+int msbg_mac_destroy(msbg_mac* m) {
+    MSBG_API_BEGIN
+    if (!m) return MSBG_OK;
+    cudaSetDevice(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+    delete m;
+    MSBG_API_END
+}
+
+int msbg_mac_channel(msbg_mac* m, int which, msbg_grid** out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && out, "null argument");
+    MSBG_REQUIRE(which >= 0 && which < 6, "channel index must be 0..5");
+    *out = m->ch[which];
+    MSBG_API_END
+}
+
+int msbg_mac_zero_blocks(msbg_mac* m, const uint64_t* bids, size_t n) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && (bids || !n), "null argument");
+    set_device(m->ctx);
+    std::vector<int32_t> slots(n);
+    mac_ensure(m, bids, n, slots.data());
+    if (n) {
+        ScratchLayout L;
+        size_t o = L.add<int32_t>(n);
+        char* base = scratch(m->ctx, L);
+        int32_t* d = ScratchLayout::at<int32_t>(base, o);
+        CUDA_CHECK(cudaMemcpyAsync(d, slots.data(), n * 4, cudaMemcpyHostToDevice, m->ctx->stream));
+        for (int c = 0; c < 6; ++c) grid_fill_slots(m->ch[c], d, n, 0.0f);
+        sync(m->ctx);
+    }
+    MSBG_API_END
+}
+
+int msbg_mac_active_blocks(const msbg_mac* m, uint64_t* out, size_t cap, size_t* n_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && n_out, "null argument");
+    for (size_t k = 0; k < m->active.size() && k < cap; ++k) out[k] = m->active[k];
+    *n_out = m->active.size();
+    MSBG_API_END
+}
+
+int msbg_mac_normalize_velocity(msbg_mac* m, const uint64_t* bids, size_t n) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && (bids || !n), "null argument");
+    if (!n) return MSBG_OK;
+    set_device(m->ctx);
+    std::vector<int32_t> slots(n);
+    for (size_t k = 0; k < n; ++k) {
+        int32_t c = bids[k] < m->ch[0]->n_blocks ? grid_code(m->ch[0], bids[k]) : kCodeEmpty;
+        slots[k] = c >= 0 ? c : -1;
+    }
+    ScratchLayout L;
+    size_t o = L.add<int32_t>(n);
+    char* base = scratch(m->ctx, L);
+    int32_t* d = ScratchLayout::at<int32_t>(base, o);
+    CUDA_CHECK(cudaMemcpyAsync(d, slots.data(), n * 4, cudaMemcpyHostToDevice, m->ctx->stream));
+    for (int a = 0; a < 3; ++a) {
+        begin_launch(m->ctx);
+        normalize_kernel<<<(unsigned)std::min<size_t>(n, 65535), 256, 0, m->ctx->stream>>>(
+            m->ch[a]->payload.as<float>(), m->ch[3 + a]->payload.as<float>(), d, n, m->ch[a]->block_elems);
+        after_launch(m->ctx, "normalize_kernel");
+    }
+    sync(m->ctx);
+    MSBG_API_END
+}
+
+int msbg_mac_divergence(msbg_mac* m, msbg_grid* dst, const uint64_t* active, size_t n) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && dst && (active || !n), "null argument");
+    msbg_grid* u = m->ch[0];
+    MSBG_REQUIRE(dst->dtype == MSBG_F32 && dst->bsx == u->bsx && dst->sx == u->sx && dst->sy == u->sy && dst->sz == u->sz,
+                 "divergence target must be an f32 grid with the MAC grid's dims");
+    if (!n) return MSBG_OK;
+    set_device(m->ctx);
+    std::vector<int32_t> dslots(n);
+    grid_ensure(dst, active, n, dslots.data());
+    std::vector<int32_t> codes(4 * n);
+    for (size_t k = 0; k < n; ++k) {
+        int64_t bx, by, bz;
+        block_coords(u, active[k], &bx, &by, &bz);
+        codes[4 * k + 0] = grid_code(u, active[k]);
+        codes[4 * k + 1] = bx > 0 ? grid_code(u, active[k] - 1) : kCodeEmpty;
+        codes[4 * k + 2] = by > 0 ? grid_code(u, active[k] - u->nx) : kCodeEmpty;
+        codes[4 * k + 3] = bz > 0 ? grid_code(u, active[k] - u->nxy) : kCodeEmpty;
+    }
+    ScratchLayout L;
+    size_t ob = L.add<uint64_t>(n), oc = L.add<int32_t>(4 * n), od = L.add<int32_t>(n);
+    char* base = scratch(m->ctx, L);
+    uint64_t* db = ScratchLayout::at<uint64_t>(base, ob);
+    int32_t* dc = ScratchLayout::at<int32_t>(base, oc);
+    int32_t* dd = ScratchLayout::at<int32_t>(base, od);
+    CUDA_CHECK(cudaMemcpyAsync(db, active, n * 8, cudaMemcpyHostToDevice, m->ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(dc, codes.data(), 16 * n, cudaMemcpyHostToDevice, m->ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(dd, dslots.data(), 4 * n, cudaMemcpyHostToDevice, m->ctx->stream));
+    DivArgs a;
+    for (int c = 0; c < 3; ++c) a.u[c] = m->ch[c]->payload.as<float>();
+    a.dst = dst->payload.as<float>();
+    a.nx = (int64_t)u->nx; a.ny = (int64_t)u->ny;
+    a.sx = (int32_t)u->sx; a.sy = (int32_t)u->sy; a.sz = (int32_t)u->sz;
+    a.lg = u->lg;
+    a.empty = u->empty_value;
+    a.full = u->full_value;
+    begin_launch(m->ctx);
+    divergence_kernel<<<(unsigned)std::min<size_t>(n, 65535), 256, 0, m->ctx->stream>>>(a, db, dc, dd, n);
+    after_launch(m->ctx, "divergence_kernel");
+    sync(m->ctx);
+    MSBG_API_END
+}
+
+int msbg_g2p_device(msbg_mac* m, const float* d_pos, size_t n, int bc, float* d_vel_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((d_pos && d_vel_out) || !n), "null argument");
+    set_device(m->ctx);
+    g2p_device(m, d_pos, n, bc, d_vel_out);
+    MSBG_API_END
+}
+
+int msbg_g2p(msbg_mac* m, const float* pos, size_t n, int bc, float* vel_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((pos && vel_out) || !n), "null argument");
+    if (!n) return MSBG_OK;
+    set_device(m->ctx);
+    DevBuf io;
+    io.reserve(2 * ((n * 12 + 255) & ~size_t(255)));
+    float* dp = io.as<float>();
+    float* dv = (float*)((char*)io.p + ((n * 12 + 255) & ~size_t(255)));
+    CUDA_CHECK(cudaMemcpyAsync(dp, pos, n * 12, cudaMemcpyHostToDevice, m->ctx->stream));
+    g2p_device(m, dp, n, bc, dv);
+    CUDA_CHECK(cudaMemcpyAsync(vel_out, dv, n * 12, cudaMemcpyDeviceToHost, m->ctx->stream));
+    sync(m->ctx);
+    MSBG_API_END
+}
+
+int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u, const float* d_u_tilde, size_t n,
+                          float alpha, float* d_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((d_u_old && d_u && d_u_tilde && d_out) || !n), "null argument");
+    if (!n) return MSBG_OK;
+    set_device(ctx);
+    begin_launch(ctx);
+    g2p_blend_kernel<<<grid_for(3 * n), 256, 0, ctx->stream>>>(d_u_old, d_u, d_u_tilde, 3 * n, alpha, d_out);
+    after_launch(ctx, "g2p_blend_kernel");
+    MSBG_API_END
+}
+
+int msbg_sample_linear(msbg_grid* g, const float* pos, size_t n, int align, int bc, float* out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(g && ((pos && out) || !n), "null argument");
+    MSBG_REQUIRE(align == 0 || align == 1, "align must be 0 (Corner) or 1 (CellCentered)");
+    MSBG_REQUIRE(bc >= 0 && bc <= 2, "bad boundary condition");
+    if (!n) return MSBG_OK;
+    set_device(g->ctx);
+    SampleGrid s = sample_grid(g);
+    ScratchLayout L;
+    size_t op = L.add<float>(3 * n), oo = L.add<float>(n);
+    char* base = scratch(g->ctx, L);
+    float* dp = ScratchLayout::at<float>(base, op);
+    float* dout = ScratchLayout::at<float>(base, oo);
+    CUDA_CHECK(cudaMemcpyAsync(dp, pos, 12 * n, cudaMemcpyHostToDevice, g->ctx->stream));
+    begin_launch(g->ctx);
+    sample_linear_kernel<<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout);
+    after_launch(g->ctx, "sample_linear_kernel");
+    CUDA_CHECK(cudaMemcpyAsync(out, dout, 4 * n, cudaMemcpyDeviceToHost, g->ctx->stream));
+    sync(g->ctx);
+    MSBG_API_END
+}
+
+int msbg_downsample_avg(msbg_grid* dst, msbg_grid* src) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(dst && src, "null argument");
+    MSBG_REQUIRE(dst->dtype == MSBG_F32 && src->dtype == MSBG_F32, "downsample needs f32 levels");
+    MSBG_REQUIRE(src->bsx >= 2 && dst->bsx * 2 == src->bsx && dst->nx == src->nx && dst->ny == src->ny && dst->nz == src->nz,
+                 "dst must have half the block size of src on the same block grid");
+    MSBG_REQUIRE(dst->ctx == src->ctx, "levels on different contexts");
+    set_device(src->ctx);
+    const size_t n = src->n_slots();
+    if (!n) return MSBG_OK;
+    std::vector<uint64_t> bids(src->slot_bid);
+    std::vector<int32_t> sslots(n), dslots(n);
+    for (size_t k = 0; k < n; ++k) sslots[k] = (int32_t)k;
+    grid_ensure(dst, bids.data(), n, dslots.data());
+    ScratchLayout L;
+    size_t os = L.add<int32_t>(n), od = L.add<int32_t>(n);
+    char* base = scratch(src->ctx, L);
+    int32_t* ds = ScratchLayout::at<int32_t>(base, os);
+    int32_t* dd = ScratchLayout::at<int32_t>(base, od);
+    CUDA_CHECK(cudaMemcpyAsync(ds, sslots.data(), 4 * n, cudaMemcpyHostToDevice, src->ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(dd, dslots.data(), 4 * n, cudaMemcpyHostToDevice, src->ctx->stream));
+    begin_launch(src->ctx);
+    downsample_kernel<<<(unsigned)std::min<size_t>(n, 65535), 256, 0, src->ctx->stream>>>(
+        src->payload.as<float>(), ds, dst->payload.as<float>(), dd, n, src->lg);
+    after_launch(src->ctx, "downsample_kernel");
+    sync(src->ctx);
+    MSBG_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,509 @@
+// p2g.cu -- particles_to_grid (fluid/p2g.rs:141-412): deterministic,
+// atomic-free sum-splat of mass and momentum to the right MAC faces.
+//
+// Pipeline (all on the context stream):
+//  1. Morton key of every particle's cell, stable radix sort -> permutation;
+//     payloads gathered into cell-sorted SoA arrays.  A 16^3 block is one
+//     contiguous Morton range, so particles end up grouped by block ("particle
+//     blocks") and by cell inside a block.
+//  2. Per particle block: CSR of its cells, and the union of its particles'
+//     footprint blocks (active_blocks, p2g.rs:104-136, reach r_p + 1) as a
+//     27-bit mask; the active set is the sorted union over particle blocks.
+//  3. Splat: one CTA per (particle block, face direction) accumulates into a
+//     (bsx + 2M)^3 staging window in shared memory (M = ceil(r_p)), in FP64.
+//     Cells are visited in (2M+1)^3 colour phases: cells of one phase are
+//     2M+1 apart, so their face windows are disjoint and each warp owns its
+//     cell's faces -- no atomics, a fixed summation order.  A warp handles a
+//     cell: lanes take the cell's (2M+1)^3 candidate faces, loop over the
+//     cell's particles, and evaluate the reference's per-face weight
+//     w = max(1 - d^2/r_p^2, 0)^3 with its exact f32 operation order and its
+//     exact clamped footprint (p2g.rs:263-330).
+//  4. Combine: one CTA per (active block, direction) sums, in the reference's
+//     commit order (colour of the contributing particle block, p2g.rs:186-216),
+//     the staging windows of the <= 27 neighbouring particle blocks, rounds to
+//     f32 and applies normalize_velocity (mac.rs:106-132).
+// FP64 accumulation makes the result the correctly rounded sum of the f32
+// per-particle terms up to a few ulp; the reference's own f32 sums differ from
+// that by their rounding error.
+#include <algorithm>
+
+#include "mac.cuh"
+#include "sort.cuh"
+
+namespace msbg {
+
+struct SplatArgs {
+    const float *px, *py, *pz, *pm, *pv[3];  // cell-sorted particle SoA
+    const int32_t* cell_begin;               // [npb][bsx^3] by local Morton code
+    const int32_t* cell_end;
+    const uint64_t* pb_key;                  // block Morton key per particle block
+    double* partial;                         // [npb][3][2][W^3]
+    float r_p, inv_r2;
+};
+
+template <int BSX> struct P2GLg { static constexpr int v = BSX == 8 ? 3 : BSX == 16 ? 4 : 5; };
+
+template <int BSX, int M>
+__global__ void __launch_bounds__(1024, 1) p2g_splat_kernel(SplatArgs a) {
+    constexpr int W = BSX + 2 * M;
+    constexpr int WW = W * W * W;
+    constexpr int WIN = 2 * M + 1;
+    constexpr int NF = WIN * WIN * WIN;
+    constexpr int Q = (NF + 31) / 32;
+    constexpr int LG = P2GLg<BSX>::v;
+    extern __shared__ double st[];  // [2][W^3]: mass, momentum
+    const int k = blockIdx.x, dir = blockIdx.y;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
+    const uint64_t key = a.pb_key[k];
+    const int32_t b0x = (int32_t)compact3(key) * BSX, b0y = (int32_t)compact3(key >> 1) * BSX,
+                  b0z = (int32_t)compact3(key >> 2) * BSX;
+    const float ofx = dir == 0 ? 1.0f : 0.5f, ofy = dir == 1 ? 1.0f : 0.5f, ofz = dir == 2 ? 1.0f : 0.5f;
+    // Candidate face offsets relative to the cell: the face axis reaches
+    // [-M-1, M-1], the other axes [-M, M].
+    const int lox = dir == 0 ? -M - 1 : -M, loy = dir == 1 ? -M - 1 : -M, loz = dir == 2 ? -M - 1 : -M;
+    const float* __restrict__ pv = a.pv[dir];
+    const int32_t* cb = a.cell_begin + (size_t)k * BSX * BSX * BSX;
+    const int32_t* ce = a.cell_end + (size_t)k * BSX * BSX * BSX;
+    const float r_p = a.r_p, inv_r2 = a.inv_r2;
+    __syncthreads();
+    for (int ph = 0; ph < WIN * WIN * WIN; ++ph) {
+        const int ox = ph % WIN, oy = (ph / WIN) % WIN, oz = ph / (WIN * WIN);
+        const int ncx = ox < BSX ? (BSX - ox + WIN - 1) / WIN : 0;
+        const int ncy = oy < BSX ? (BSX - oy + WIN - 1) / WIN : 0;
+        const int ncz = oz < BSX ? (BSX - oz + WIN - 1) / WIN : 0;
+        const int total = ncx * ncy * ncz;
+        for (int c = warp; c < total; c += nwarp) {
+            const int lx = ox + WIN * (c % ncx), ly = oy + WIN * ((c / ncx) % ncy), lz = oz + WIN * (c / (ncx * ncy));
+            const uint32_t lm = (uint32_t)morton3(lx, ly, lz);
+            const int b = cb[lm], e = ce[lm];
+            if (b >= e) continue;
+            double am[Q], av[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) am[q] = av[q] = 0.0;
+            for (int p = b; p < e; ++p) {
+                const float x = a.px[p], y = a.py[p], z = a.pz[p], m_p = a.pm[p], u_a = pv[p];
+                const float scale_mass = m_p, scale_mom = m_p * u_a;
+                const float px0 = x - 0.5f, py0 = y - 0.5f, pz0 = z - 0.5f;
+                // Footprint clipped to the staging window (p2g.rs:263-270).
+                const int32_t ix1 = min(max((int32_t)ceilf((x - r_p) - ofx), b0x - M), b0x + BSX + M - 1);
+                const int32_t ix2 = min(max((int32_t)floorf((x + r_p) - ofx), b0x - M), b0x + BSX + M - 1);
+                const int32_t iy1 = min(max((int32_t)ceilf((y - r_p) - ofy), b0y - M), b0y + BSX + M - 1);
+                const int32_t iy2 = min(max((int32_t)floorf((y + r_p) - ofy), b0y - M), b0y + BSX + M - 1);
+                const int32_t iz1 = min(max((int32_t)ceilf((z - r_p) - ofz), b0z - M), b0z + BSX + M - 1);
+                const int32_t iz2 = min(max((int32_t)floorf((z + r_p) - ofz), b0z - M), b0z + BSX + M - 1);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int f = lane + 32 * q;
+                    if (f >= NF) continue;
+                    const int32_t gx = b0x + lx + lox + f % WIN, gy = b0y + ly + loy + (f / WIN) % WIN,
+                                  gz = b0z + lz + loz + f / (WIN * WIN);
+                    if (gx < ix1 || gx > ix2 || gy < iy1 || gy > iy2 || gz < iz1 || gz > iz2) continue;
+                    // p2g.rs:287-325, operation by operation.
+                    const float dz = (float)gz - pz0;
+                    const float dz2 = dz * dz;
+                    const float dy = (float)gy - py0;
+                    const float dyz = dz2 + dy * dy;
+                    const float dx = (float)gx - px0;
+                    const float dist_sq = dx * dx + dyz;
+                    const float d_a = dir == 0 ? dx : (dir == 1 ? dy : dz);
+                    const float df2 = (dist_sq + d_a) + 0.25f;
+                    float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
+                    w = (w * w) * w;
+                    am[q] += (double)(w * scale_mass);
+                    av[q] += (double)(w * scale_mom);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int f = lane + 32 * q;
+                if (f >= NF) continue;
+                const int sx = lx + M + lox + f % WIN, sy = ly + M + loy + (f / WIN) % WIN, sz = lz + M + loz + f / (WIN * WIN);
+                if (sx < 0 || sy < 0 || sz < 0 || sx >= W || sy >= W || sz >= W) continue;
+                const int si = (sz * W + sy) * W + sx;
+                st[si] += am[q];
+                st[WW + si] += av[q];
+            }
+        }
+        __syncthreads();
+    }
+    double* out = a.partial + ((size_t)k * 3 + dir) * 2 * WW;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
+    (void)LG;
+}
+
+struct CombineArgs {
+    const double* partial;
+    const int32_t* nbr_rank;  // [n_active][27] particle-block rank or -1
+    const uint64_t* active;   // sorted active bids
+    const int32_t* slots;     // MAC slot per active block
+    float* mass[3];
+    float* vel[3];
+    int64_t nx, ny;
+};
+
+template <int BSX, int M>
+__global__ void __launch_bounds__(256) p2g_combine_kernel(CombineArgs a) {
+    constexpr int W = BSX + 2 * M;
+    constexpr int WW = W * W * W;
+    constexpr int N = BSX * BSX * BSX;
+    constexpr int LG = P2GLg<BSX>::v;
+    __shared__ int32_t rank[27];
+    __shared__ int8_t order[27];
+    const int j = blockIdx.x, dir = blockIdx.y;
+    const uint64_t bid = a.active[j];
+    const int64_t bx = (int64_t)(bid % a.nx), by = (int64_t)((bid / a.nx) % a.ny), bz = (int64_t)(bid / (a.nx * a.ny));
+    if (threadIdx.x < 27) rank[threadIdx.x] = a.nbr_rank[(size_t)j * 27 + threadIdx.x];
+    if (threadIdx.x == 0) {
+        // Contributions are added in the colour order of the contributing
+        // particle block (the reference commits colour by colour).
+        int t = 0;
+        for (int c = 0; c < 8; ++c)
+            for (int d = 0; d < 27; ++d) {
+                const int64_t X = bx + d % 3 - 1, Y = by + (d / 3) % 3 - 1, Z = bz + d / 9 - 1;
+                if ((int)((X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2)) == c) order[t++] = (int8_t)d;
+            }
+    }
+    __syncthreads();
+    const int32_t slot = a.slots[j];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int lx = i & (BSX - 1), ly = (i >> LG) & (BSX - 1), lz = i >> (2 * LG);
+        double sm = 0.0, sv = 0.0;
+        for (int t = 0; t < 27; ++t) {
+            const int d = order[t];
+            const int r = rank[d];
+            if (r < 0) continue;
+            const int sx = lx - BSX * (d % 3 - 1) + M, sy = ly - BSX * ((d / 3) % 3 - 1) + M, sz = lz - BSX * (d / 9 - 1) + M;
+            if (sx < 0 || sy < 0 || sz < 0 || sx >= W || sy >= W || sz >= W) continue;
+            const double* p = a.partial + ((size_t)r * 3 + dir) * 2 * WW + (sz * W + sy) * W + sx;
+            sm += p[0];
+            sv += p[WW];
+        }
+        const float mf = (float)sm, pf = (float)sv;
+        a.mass[dir][(size_t)slot * N + i] = mf;
+        a.vel[dir][(size_t)slot * N + i] = mf > 0.0f ? pf / mf : 0.0f;
+    }
+}
+
+// Cell CSR of one particle block: begin/end index of every cell (by local
+// Morton code) in the sorted particle order.
+__global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts, int lg, int32_t* cell_begin,
+                                int32_t* cell_end) {
+    const int k = blockIdx.x;
+    const int n_cells = 1 << (3 * lg);
+    const uint64_t cmask = (uint64_t)n_cells - 1;
+    int32_t* cb = cell_begin + (size_t)k * n_cells;
+    int32_t* ce = cell_end + (size_t)k * n_cells;
+    for (int i = threadIdx.x; i < n_cells; i += blockDim.x) cb[i] = ce[i] = 0;
+    __syncthreads();
+    const int64_t s = (int64_t)pb_starts[k], e = (int64_t)pb_starts[k + 1];
+    for (int64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
+        const uint64_t c = skeys[i] & cmask;
+        if (i == s || (skeys[i - 1] & cmask) != c) cb[c] = (int32_t)i;
+        if (i == e - 1 || (skeys[i + 1] & cmask) != c) ce[c] = (int32_t)(i + 1);
+    }
+}
+
+// Payload gather into cell-sorted SoA, and each particle's footprint mask
+// (particles/mod.rs:207-212 footprint_axis with r_scan = (r_p + 1) / bsx,
+// relative to its own block).
+__global__ void p2g_gather_kernel(const float* pos, const float* vel, const float* mass, const uint32_t* perm, size_t n,
+                                  int lg, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz, float* px, float* py,
+                                  float* pz, float* pm, float* v0, float* v1, float* v2, uint32_t* fmask, int* bad) {
+    const float bsx = (float)(1 << lg);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t s = perm[i];
+        const float x = pos[3 * (size_t)s], y = pos[3 * (size_t)s + 1], z = pos[3 * (size_t)s + 2];
+        px[i] = x; py[i] = y; pz[i] = z;
+        pm[i] = mass[s];
+        v0[i] = vel[3 * (size_t)s]; v1[i] = vel[3 * (size_t)s + 1]; v2[i] = vel[3 * (size_t)s + 2];
+        const float p[3] = {x, y, z};
+        const int64_t nn[3] = {nx, ny, nz};
+        uint32_t lo[3], hi[3];
+        bool out = false;
+        for (int ax = 0; ax < 3; ++ax) {
+            const int64_t cb = p[ax] > 0.0f ? (int64_t)p[ax] >> lg : 0;  // the particle's block (p as usize >> lg)
+            if (cb >= nn[ax]) out = true;
+            const float b = p[ax] / bsx;
+            const int64_t l = max((int64_t)(int32_t)truncf(b - r_scan_bsx), (int64_t)0);
+            const int64_t h = min((int64_t)(int32_t)truncf(b + r_scan_bsx), nn[ax] - 1);
+            lo[ax] = (uint32_t)(min(max(l - cb, (int64_t)-1), (int64_t)1) + 1);
+            hi[ax] = (uint32_t)(min(max(h - cb, (int64_t)-1), (int64_t)1) + 1);
+        }
+        if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
+        uint32_t m = 0;
+        for (uint32_t dz = lo[2]; dz <= hi[2]; ++dz)
+            for (uint32_t dy = lo[1]; dy <= hi[1]; ++dy)
+                for (uint32_t dx = lo[0]; dx <= hi[0]; ++dx) m |= 1u << (dx + 3 * dy + 9 * dz);
+        fmask[i] = m;
+    }
+}
+
+// OR of the footprint masks over each particle block's particles, expanded to
+// candidate block ids (n_blocks = "none").
+__global__ void pb_candidates_kernel(const uint32_t* fmask, const uint64_t* pb_starts, const uint64_t* pb_key, size_t npb,
+                                     int64_t nx, int64_t ny, int64_t nz, uint64_t* cand) {
+    for (size_t k = blockIdx.x; k < npb; k += gridDim.x) {
+        uint32_t m = 0;
+        for (uint64_t i = pb_starts[k] + threadIdx.x; i < pb_starts[k + 1]; i += blockDim.x) m |= fmask[i];
+        for (int o = 16; o; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
+        __shared__ uint32_t wm[32];
+        if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 27) {
+            uint32_t all = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) all |= wm[w];
+            const uint64_t key = pb_key[k];
+            const int64_t X = (int64_t)compact3(key) + threadIdx.x % 3 - 1, Y = (int64_t)compact3(key >> 1) + (threadIdx.x / 3) % 3 - 1,
+                          Z = (int64_t)compact3(key >> 2) + threadIdx.x / 9 - 1;
+            const bool on = (all >> threadIdx.x) & 1u;
+            cand[k * 27 + threadIdx.x] = on && X >= 0 && Y >= 0 && Z >= 0 && X < nx && Y < ny && Z < nz
+                                             ? (uint64_t)X + (uint64_t)Y * nx + (uint64_t)Z * nx * ny
+                                             : (uint64_t)(nx * ny * nz);
+        }
+        __syncthreads();
+    }
+}
+
+// For every active block, the particle-block rank of each of its 27
+// neighbours (binary search of the neighbour's Morton key among the sorted
+// particle-block keys), or -1.
+__global__ void active_nbr_kernel(const uint64_t* active, size_t n_active, const uint64_t* pb_key, size_t npb, int64_t nx,
+                                  int64_t ny, int64_t nz, int32_t* nbr_rank) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_active * 27; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t j = t / 27;
+        const int d = (int)(t % 27);
+        const uint64_t bid = active[j];
+        const int64_t X = (int64_t)(bid % nx) + d % 3 - 1, Y = (int64_t)((bid / nx) % ny) + (d / 3) % 3 - 1,
+                      Z = (int64_t)(bid / (nx * ny)) + d / 9 - 1;
+        int32_t r = -1;
+        if (X >= 0 && Y >= 0 && Z >= 0 && X < nx && Y < ny && Z < nz) {
+            const uint64_t key = morton3(X, Y, Z);
+            size_t lo = 0, hi = npb;
+            while (lo < hi) {
+                const size_t mid = (lo + hi) / 2;
+                if (pb_key[mid] < key) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < npb && pb_key[lo] == key) r = (int32_t)lo;
+        }
+        nbr_rank[t] = r;
+    }
+}
+
+static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 8192); }
+
+template <int BSX, int M>
+static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
+    constexpr int W = BSX + 2 * M;
+    const size_t smem = 2 * sizeof(double) * W * W * W;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(p2g_splat_kernel<BSX, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    begin_launch(ctx);
+    p2g_splat_kernel<BSX, M><<<dim3((unsigned)npb, 3), 1024, smem, ctx->stream>>>(a);
+    after_launch(ctx, "p2g_splat_kernel");
+}
+
+template <int BSX, int M>
+static void launch_combine(msbg_ctx* ctx, const CombineArgs& a, size_t n_active) {
+    begin_launch(ctx);
+    p2g_combine_kernel<BSX, M><<<dim3((unsigned)n_active, 3), 256, 0, ctx->stream>>>(a);
+    after_launch(ctx, "p2g_combine_kernel");
+}
+
+template <int BSX>
+static void dispatch_m(msbg_ctx* ctx, int M, const SplatArgs* s, size_t npb, const CombineArgs* c, size_t na) {
+    switch (M) {
+        case 1: if (s) launch_splat<BSX, 1>(ctx, *s, npb); else launch_combine<BSX, 1>(ctx, *c, na); break;
+        case 2: if (s) launch_splat<BSX, 2>(ctx, *s, npb); else launch_combine<BSX, 2>(ctx, *c, na); break;
+        default: if (s) launch_splat<BSX, 3>(ctx, *s, npb); else launch_combine<BSX, 3>(ctx, *c, na); break;
+    }
+}
+
+static void dispatch(msbg_ctx* ctx, int bsx, int M, const SplatArgs* s, size_t npb, const CombineArgs* c, size_t na) {
+    if (bsx == 8) dispatch_m<8>(ctx, M, s, npb, c, na);
+    else dispatch_m<16>(ctx, M, s, npb, c, na);
+}
+
+static size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass, size_t n, float r_p,
+                size_t* n_active_out) {
+    msbg_ctx* ctx = mac->ctx;
+    msbg_grid* u = mac->ch[0];
+    const int bsx = u->bsx, lg = u->lg;
+    MSBG_REQUIRE(bsx == 8 || bsx == 16, "P2G supports bsx 8 and 16");
+    MSBG_REQUIRE(u->sx % bsx == 0 && u->sy % bsx == 0 && u->sz % bsx == 0, "P2G needs domain extents that are multiples of bsx");
+    MSBG_REQUIRE(r_p > 0.0f && r_p <= 3.0f, "P2G supports 0 < r_p <= 3");
+    const int M = (int)ceilf(r_p);
+    MSBG_REQUIRE(2 * M <= bsx, "r_p too large for the block size");
+    MSBG_REQUIRE(n < (1ULL << 31), "P2G supports < 2^31 particles");
+    MSBG_REQUIRE(u->sx <= (1u << 21) && u->sy <= (1u << 21) && u->sz <= (1u << 21), "domain exceeds 21-bit Morton keys");
+    const uint64_t smax = std::max(u->sx, std::max(u->sy, u->sz));
+    const int key_bits = 3 * ilog2i(smax);
+    const int W = bsx + 2 * M;
+    const size_t WW = (size_t)W * W * W, NC = (size_t)bsx * bsx * bsx;
+    if (n == 0) {
+        mac->active.clear();
+        if (n_active_out) *n_active_out = 0;
+        return;
+    }
+    // ---- phase 1: sort, gather, particle blocks -------------------------------
+    ScratchLayout L1;
+    const size_t o_keys = L1.add<uint64_t>(n), o_skeys = L1.add<uint64_t>(n), o_perm = L1.add<uint32_t>(n),
+                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_pbk = L1.add<uint64_t>(n + 1),
+                 o_pbs = L1.add<uint64_t>(n + 2), o_tmp = L1.add<char>(std::max(radix_sort_scratch_bytes(n), segment_scratch_bytes(n))),
+                 o_bad = L1.add<int>(4);
+    // phase-2 buffers go after phase 1's (sized once npb is known)
+    char* base = scratch(ctx, L1);
+    uint64_t* keys = ScratchLayout::at<uint64_t>(base, o_keys);
+    uint64_t* skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    uint32_t* perm = ScratchLayout::at<uint32_t>(base, o_perm);
+    float* soa = ScratchLayout::at<float>(base, o_soa);
+    uint32_t* fmask = ScratchLayout::at<uint32_t>(base, o_fm);
+    uint64_t* pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
+    uint64_t* pb_starts = ScratchLayout::at<uint64_t>(base, o_pbs);
+    int* bad = ScratchLayout::at<int>(base, o_bad);
+    CUDA_CHECK(cudaMemsetAsync(bad, 0, 4, ctx->stream));
+    morton_keys(ctx, d_pos, n, keys);
+    radix_sort_pairs(ctx, keys, nullptr, skeys, perm, n, key_bits, ScratchLayout::at<char>(base, o_tmp));
+    float *px = soa, *py = soa + n, *pz = soa + 2 * n, *pm = soa + 3 * n, *v0 = soa + 4 * n, *v1 = soa + 5 * n, *v2 = soa + 6 * n;
+    begin_launch(ctx);
+    p2g_gather_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, (r_p + 1.0f) / (float)bsx,
+                                                            (int64_t)u->nx, (int64_t)u->ny, (int64_t)u->nz, px, py, pz, pm,
+                                                            v0, v1, v2, fmask, bad);
+    after_launch(ctx, "p2g_gather_kernel");
+    const size_t npb = sorted_segments(ctx, skeys, n, (uint64_t)(3 * lg), pb_key, pb_starts, ScratchLayout::at<char>(base, o_tmp));
+    int hbad = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    MSBG_REQUIRE(!hbad, "a particle lies outside the domain");
+
+    // ---- phase 2: active set ------------------------------------------------
+    ScratchLayout L2 = L1;
+    const size_t o_cand = L2.add<uint64_t>(npb * 27), o_csort = L2.add<uint64_t>(npb * 27), o_cperm = L2.add<uint32_t>(npb * 27),
+                 o_act = L2.add<uint64_t>(npb * 27 + 1), o_ast = L2.add<uint64_t>(npb * 27 + 2),
+                 o_ctmp = L2.add<char>(std::max(radix_sort_scratch_bytes(npb * 27), segment_scratch_bytes(npb * 27))),
+                 o_cb = L2.add<int32_t>(npb * NC), o_ce = L2.add<int32_t>(npb * NC), o_part = L2.add<double>(npb * 6 * WW);
+    base = scratch(ctx, L2);  // may move: re-derive phase-1 pointers
+    skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    soa = ScratchLayout::at<float>(base, o_soa);
+    fmask = ScratchLayout::at<uint32_t>(base, o_fm);
+    pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
+    pb_starts = ScratchLayout::at<uint64_t>(base, o_pbs);
+    px = soa; py = soa + n; pz = soa + 2 * n; pm = soa + 3 * n; v0 = soa + 4 * n; v1 = soa + 5 * n; v2 = soa + 6 * n;
+    uint64_t* cand = ScratchLayout::at<uint64_t>(base, o_cand);
+    uint64_t* csort = ScratchLayout::at<uint64_t>(base, o_csort);
+    uint32_t* cperm = ScratchLayout::at<uint32_t>(base, o_cperm);
+    uint64_t* act = ScratchLayout::at<uint64_t>(base, o_act);
+    uint64_t* ast = ScratchLayout::at<uint64_t>(base, o_ast);
+    int32_t* cell_begin = ScratchLayout::at<int32_t>(base, o_cb);
+    int32_t* cell_end = ScratchLayout::at<int32_t>(base, o_ce);
+    double* partial = ScratchLayout::at<double>(base, o_part);
+
+    begin_launch(ctx);
+    pb_candidates_kernel<<<(unsigned)std::min<size_t>(npb, 65535), 256, 0, ctx->stream>>>(
+        fmask, pb_starts, pb_key, npb, (int64_t)u->nx, (int64_t)u->ny, (int64_t)u->nz, cand);
+    after_launch(ctx, "pb_candidates_kernel");
+    const int cbits = ilog2i(u->n_blocks + 1) + 1;
+    radix_sort_pairs(ctx, cand, nullptr, csort, cperm, npb * 27, cbits, ScratchLayout::at<char>(base, o_ctmp));
+    size_t nuniq = sorted_segments(ctx, csort, npb * 27, 0, act, ast, ScratchLayout::at<char>(base, o_ctmp));
+    std::vector<uint64_t> active(nuniq);
+    CUDA_CHECK(cudaMemcpyAsync(active.data(), act, nuniq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (!active.empty() && active.back() == u->n_blocks) active.pop_back();  // the "none" sentinel
+    const size_t na = active.size();
+    std::vector<int32_t> slots(na);
+    mac_ensure(mac, active.data(), na, slots.data());  // may grow the six payloads
+    mac->active = active;
+
+    // ---- phase 3: splat + combine -------------------------------------------
+    ScratchLayout L3 = L2;
+    const size_t o_nr = L3.add<int32_t>(na * 27), o_sl = L3.add<int32_t>(na);
+    base = scratch(ctx, L3);
+    skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    soa = ScratchLayout::at<float>(base, o_soa);
+    pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
+    pb_starts = ScratchLayout::at<uint64_t>(base, o_pbs);
+    px = soa; py = soa + n; pz = soa + 2 * n; pm = soa + 3 * n; v0 = soa + 4 * n; v1 = soa + 5 * n; v2 = soa + 6 * n;
+    act = ScratchLayout::at<uint64_t>(base, o_act);
+    cell_begin = ScratchLayout::at<int32_t>(base, o_cb);
+    cell_end = ScratchLayout::at<int32_t>(base, o_ce);
+    partial = ScratchLayout::at<double>(base, o_part);
+    int32_t* nbr_rank = ScratchLayout::at<int32_t>(base, o_nr);
+    int32_t* d_slots = ScratchLayout::at<int32_t>(base, o_sl);
+    CUDA_CHECK(cudaMemcpyAsync(d_slots, slots.data(), na * 4, cudaMemcpyHostToDevice, ctx->stream));
+
+    begin_launch(ctx);
+    cell_csr_kernel<<<(unsigned)npb, 256, 0, ctx->stream>>>(skeys, pb_starts, lg, cell_begin, cell_end);
+    after_launch(ctx, "cell_csr_kernel");
+    begin_launch(ctx);
+    active_nbr_kernel<<<grid_for(na * 27), 256, 0, ctx->stream>>>(act, na, pb_key, npb, (int64_t)u->nx, (int64_t)u->ny,
+                                                                  (int64_t)u->nz, nbr_rank);
+    after_launch(ctx, "active_nbr_kernel");
+    SplatArgs s;
+    s.px = px; s.py = py; s.pz = pz; s.pm = pm;
+    s.pv[0] = v0; s.pv[1] = v1; s.pv[2] = v2;
+    s.cell_begin = cell_begin;
+    s.cell_end = cell_end;
+    s.pb_key = pb_key;
+    s.partial = partial;
+    s.r_p = r_p;
+    s.inv_r2 = 1.0f / (r_p * r_p);
+    dispatch(ctx, bsx, M, &s, npb, nullptr, 0);
+    CombineArgs c;
+    c.partial = partial;
+    c.nbr_rank = nbr_rank;
+    c.active = act;
+    c.slots = d_slots;
+    for (int a = 0; a < 3; ++a) {
+        c.vel[a] = mac->ch[a]->payload.as<float>();
+        c.mass[a] = mac->ch[3 + a]->payload.as<float>();
+    }
+    c.nx = (int64_t)u->nx;
+    c.ny = (int64_t)u->ny;
+    if (na) dispatch(ctx, bsx, M, nullptr, 0, &c, na);
+    sync(ctx);  // `slots` (host) and the scratch layout end here
+    if (n_active_out) *n_active_out = na;
+    (void)a256;
+}
+
+}  // namespace msbg
+
+using namespace msbg;
+
+extern "C" {
+
+int msbg_p2g_device(msbg_mac* m, const float* d_pos, const float* d_vel, const float* d_mass, size_t n, float r_p,
+                    size_t* n_active_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass) || !n), "null argument");
+    set_device(m->ctx);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out);
+    MSBG_API_END
+}
+
+int msbg_p2g(msbg_mac* m, const float* pos, const float* vel, const float* mass, size_t n, float r_p, size_t* n_active_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((pos && vel && mass) || !n), "null argument");
+    set_device(m->ctx);
+    DevBuf io;
+    const size_t b3 = (n * 12 + 255) & ~size_t(255), b1 = (n * 4 + 255) & ~size_t(255);
+    io.reserve(2 * b3 + b1 + 256);
+    float* dp = io.as<float>();
+    float* dv = (float*)((char*)io.p + b3);
+    float* dm = (float*)((char*)io.p + 2 * b3);
+    if (n) {
+        CUDA_CHECK(cudaMemcpyAsync(dp, pos, n * 12, cudaMemcpyHostToDevice, m->ctx->stream));
+        CUDA_CHECK(cudaMemcpyAsync(dv, vel, n * 12, cudaMemcpyHostToDevice, m->ctx->stream));
+        CUDA_CHECK(cudaMemcpyAsync(dm, mass, n * 4, cudaMemcpyHostToDevice, m->ctx->stream));
+    }
+    p2g_device(m, dp, dv, dm, n, r_p, n_active_out);
+    sync(m->ctx);
+    MSBG_API_END
+}
+
+}  // extern "C"

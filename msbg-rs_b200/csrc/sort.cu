@@ -1,0 +1,528 @@
+// sort.cu -- stable LSD radix sort (8-bit digits, reduce-then-scan), device
+// scans, per-particle Morton keys (multires/sort.rs:5-22), bucket_indices
+// (particles/sort.rs:174-269) and sort_block_list_morton (multires/sort.rs:35-57).
+//
+// Each pass: (1) per-tile digit histograms, (2) a digit-major exclusive scan of
+// those histograms, (3) a scatter in which every tile ranks its keys stably
+// (warp __match_any_sync + a running per-digit prefix across the tile's rounds)
+// and writes them to digit base + tile prefix + rank.  Stable, so sorting
+// (key, index) pairs reproduces a stable CPU sort exactly.
+#include <algorithm>
+
+#include "sort.cuh"
+
+namespace msbg {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024, a
+// multiple of 32).  Returns the exclusive prefix; *total gets the block sum.
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;  // inclusive prefix over warps
+    }
+    __syncthreads();
+    uint32_t warp_ex = warp ? wsum[warp - 1] : 0;
+    *total = wsum[nw - 1];
+    __syncthreads();
+    return warp_ex + x - v;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) rs_hist_kernel(const uint64_t* keys, size_t n, int shift, uint32_t* counts,
+                                                              unsigned n_tiles) {
+    __shared__ uint32_t c[256];
+    c[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t base = (size_t)blockIdx.x * RS_TILE;
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) {
+        size_t i = base + (size_t)j * RS_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&c[(keys[i] >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    counts[(size_t)threadIdx.x * n_tiles + blockIdx.x] = c[threadIdx.x];
+}
+
+// One CTA per row: exclusive scan of the row in place, row total to totals.
+__global__ void __launch_bounds__(1024) scan_rows_kernel(uint32_t* data, size_t row_len, uint32_t* totals) {
+    uint32_t* row = data + (size_t)blockIdx.x * row_len;
+    uint32_t carry = 0;
+    for (size_t b = 0; b < row_len; b += blockDim.x) {
+        size_t i = b + threadIdx.x;
+        uint32_t v = i < row_len ? row[i] : 0, tot;
+        uint32_t ex = block_exclusive_scan(v, &tot);
+        if (i < row_len) row[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && totals) totals[blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                                 uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, size_t n,
+                                                                 int shift, const uint32_t* __restrict__ counts,
+                                                                 const uint32_t* __restrict__ totals, unsigned n_tiles) {
+    __shared__ uint32_t base_d[256];
+    __shared__ uint32_t wcnt[RS_THREADS / 32][256];
+    __shared__ uint32_t run[256];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan(totals[tid], &tot);
+    base_d[tid] = ex + counts[(size_t)tid * n_tiles + blockIdx.x];
+    run[tid] = 0;
+    const size_t base = (size_t)blockIdx.x * RS_TILE;
+    for (int j = 0; j < RS_ITEMS; ++j) {
+        const size_t i = base + (size_t)j * RS_THREADS + tid;
+        const bool valid = i < n;
+        const uint64_t key = valid ? kin[i] : 0;
+        const uint32_t d = valid ? (uint32_t)((key >> shift) & 255) : 256u;
+#pragma unroll
+        for (int w = 0; w < RS_THREADS / 32; ++w) wcnt[w][tid] = 0;
+        __syncthreads();
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t lt = __popc(peers & lanemask_lt());
+        if (valid && lt == 0) wcnt[warp][d] = __popc(peers);
+        __syncthreads();
+        uint32_t acc = run[tid];
+#pragma unroll
+        for (int w = 0; w < RS_THREADS / 32; ++w) {
+            uint32_t t = wcnt[w][tid];
+            wcnt[w][tid] = acc;
+            acc += t;
+        }
+        run[tid] = acc;
+        __syncthreads();
+        if (valid) {
+            const uint32_t pos = base_d[d] + wcnt[warp][d] + lt;
+            kout[pos] = key;
+            vout[pos] = vin ? vin[i] : (uint32_t)i;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void iota_copy_kernel(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        kout[i] = kin[i];
+        vout[i] = vin ? vin[i] : (uint32_t)i;
+    }
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t radix_sort_scratch_bytes(size_t n) {
+    size_t tiles = (n + RS_TILE - 1) / RS_TILE;
+    return align256(n * 8) + align256(n * 4) + align256(256 * std::max<size_t>(tiles, 1) * 4) + align256(256 * 4);
+}
+
+void radix_sort_pairs(msbg_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                      uint32_t* vals_out, size_t n, int end_bit, void* tmp) {
+    if (!n) return;
+    MSBG_REQUIRE(n < (1ULL << 32), "radix sort supports < 2^32 items");
+    const int passes = (end_bit + 7) / 8;
+    const unsigned tiles = (unsigned)((n + RS_TILE - 1) / RS_TILE);
+    if (passes == 0) {
+        begin_launch(ctx);
+        iota_copy_kernel<<<std::min<size_t>(div_up(n, 256), 4096), 256, 0, ctx->stream>>>(keys_in, vals_in, keys_out, vals_out, n);
+        after_launch(ctx, "iota_copy_kernel");
+        return;
+    }
+    char* t = (char*)tmp;
+    uint64_t* kt = (uint64_t*)t;
+    t += align256(n * 8);
+    uint32_t* vt = (uint32_t*)t;
+    t += align256(n * 4);
+    uint32_t* counts = (uint32_t*)t;
+    t += align256(256 * (size_t)tiles * 4);
+    uint32_t* totals = (uint32_t*)t;
+    const uint64_t* ki = keys_in;
+    const uint32_t* vi = vals_in;
+    for (int p = 0; p < passes; ++p) {
+        const bool to_out = ((passes - 1 - p) % 2) == 0;
+        uint64_t* ko = to_out ? keys_out : kt;
+        uint32_t* vo = to_out ? vals_out : vt;
+        begin_launch(ctx);
+        rs_hist_kernel<<<tiles, RS_THREADS, 0, ctx->stream>>>(ki, n, 8 * p, counts, tiles);
+        after_launch(ctx, "rs_hist_kernel");
+        begin_launch(ctx);
+        scan_rows_kernel<<<256, 1024, 0, ctx->stream>>>(counts, tiles, totals);
+        after_launch(ctx, "scan_rows_kernel");
+        begin_launch(ctx);
+        rs_scatter_kernel<<<tiles, RS_THREADS, 0, ctx->stream>>>(ki, vi, ko, vo, n, 8 * p, counts, totals, tiles);
+        after_launch(ctx, "rs_scatter_kernel");
+        ki = ko;
+        vi = vo;
+    }
+}
+
+// ---- exclusive scan of u32 --------------------------------------------------
+constexpr int SC_THREADS = 1024;
+constexpr int SC_ITEMS = 4;
+constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
+
+__global__ void __launch_bounds__(SC_THREADS) scan_tile_sums_kernel(const uint32_t* in, size_t n, uint32_t* sums) {
+    const size_t base = (size_t)blockIdx.x * SC_TILE;
+    uint32_t s = 0;
+    for (int j = 0; j < SC_ITEMS; ++j) {
+        size_t i = base + (size_t)threadIdx.x * SC_ITEMS + j;
+        if (i < n) s += in[i];
+    }
+    uint32_t tot;
+    block_exclusive_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) scan_tiles_kernel(const uint32_t* in, uint32_t* out, size_t n, const uint32_t* offs) {
+    const size_t base = (size_t)blockIdx.x * SC_TILE;
+    uint32_t v[SC_ITEMS], s = 0;
+    for (int j = 0; j < SC_ITEMS; ++j) {
+        size_t i = base + (size_t)threadIdx.x * SC_ITEMS + j;
+        v[j] = i < n ? in[i] : 0;
+        s += v[j];
+    }
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan(s, &tot) + offs[blockIdx.x];
+    for (int j = 0; j < SC_ITEMS; ++j) {
+        size_t i = base + (size_t)threadIdx.x * SC_ITEMS + j;
+        if (i < n) out[i] = ex;
+        ex += v[j];
+    }
+}
+
+size_t scan_scratch_bytes(size_t n) { return align256(((n + SC_TILE - 1) / SC_TILE + 1) * 4) + 256; }
+
+__global__ void copy_u32_kernel(const uint32_t* a, uint32_t* b) { *b = *a; }
+
+void exclusive_scan_u32(msbg_ctx* ctx, const uint32_t* in, uint32_t* out, size_t n, uint32_t* d_total, void* tmp) {
+    if (!n) return;
+    const unsigned tiles = (unsigned)((n + SC_TILE - 1) / SC_TILE);
+    uint32_t* sums = (uint32_t*)tmp;
+    uint32_t* total = sums + tiles;  // scan_rows writes the row total here
+    begin_launch(ctx);
+    scan_tile_sums_kernel<<<tiles, SC_THREADS, 0, ctx->stream>>>(in, n, sums);
+    after_launch(ctx, "scan_tile_sums_kernel");
+    begin_launch(ctx);
+    scan_rows_kernel<<<1, 1024, 0, ctx->stream>>>(sums, tiles, total);
+    after_launch(ctx, "scan_rows_kernel");
+    begin_launch(ctx);
+    scan_tiles_kernel<<<tiles, SC_THREADS, 0, ctx->stream>>>(in, out, n, sums);
+    after_launch(ctx, "scan_tiles_kernel");
+    if (d_total) {
+        begin_launch(ctx);
+        copy_u32_kernel<<<1, 1, 0, ctx->stream>>>(total, d_total);
+        after_launch(ctx, "copy_u32_kernel");
+    }
+}
+
+__global__ void max_u64_kernel(const uint64_t* k, size_t n, unsigned long long* out) {
+    unsigned long long m = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = max(m, (unsigned long long)k[i]);
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+int key_bits(msbg_ctx* ctx, const uint64_t* d_keys, size_t n, void* tmp8) {
+    if (!n) return 0;
+    CUDA_CHECK(cudaMemsetAsync(tmp8, 0, 8, ctx->stream));
+    begin_launch(ctx);
+    max_u64_kernel<<<std::min<size_t>(div_up(n, 256), 1184), 256, 0, ctx->stream>>>(d_keys, n, (unsigned long long*)tmp8);
+    after_launch(ctx, "max_u64_kernel");
+    uint64_t m = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&m, tmp8, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    int b = 0;
+    while (b < 64 && (m >> b)) ++b;
+    return b;
+}
+
+__global__ void seg_flags_kernel(const uint64_t* k, size_t n, uint64_t shift, uint32_t* f) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        f[i] = (i == 0 || (k[i] >> shift) != (k[i - 1] >> shift)) ? 1u : 0u;
+}
+
+__global__ void seg_write_kernel(const uint64_t* k, size_t n, uint64_t shift, const uint32_t* f, const uint32_t* idx,
+                                 uint64_t* uniq, uint64_t* starts, const uint32_t* count) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (f[i]) {
+            uniq[idx[i]] = k[i] >> shift;
+            starts[idx[i]] = i;
+        }
+        if (i == 0) starts[*count] = n;
+    }
+}
+
+size_t segment_scratch_bytes(size_t n) { return align256(n * 4) * 2 + scan_scratch_bytes(n) + 256; }
+
+size_t sorted_segments(msbg_ctx* ctx, const uint64_t* d_sorted, size_t n, uint64_t shift, uint64_t* d_uniq,
+                       uint64_t* d_starts, void* tmp) {
+    if (!n) {
+        uint64_t z = 0;
+        CUDA_CHECK(cudaMemcpyAsync(d_starts, &z, 8, cudaMemcpyHostToDevice, ctx->stream));
+        sync(ctx);
+        return 0;
+    }
+    char* t = (char*)tmp;
+    uint32_t* f = (uint32_t*)t;
+    t += align256(n * 4);
+    uint32_t* idx = (uint32_t*)t;
+    t += align256(n * 4);
+    uint32_t* count = (uint32_t*)t;
+    t += 256;
+    unsigned g = std::min<size_t>(div_up(n, 256), 8192);
+    begin_launch(ctx);
+    seg_flags_kernel<<<g, 256, 0, ctx->stream>>>(d_sorted, n, shift, f);
+    after_launch(ctx, "seg_flags_kernel");
+    exclusive_scan_u32(ctx, f, idx, n, count, t);
+    begin_launch(ctx);
+    seg_write_kernel<<<g, 256, 0, ctx->stream>>>(d_sorted, n, shift, f, idx, d_uniq, d_starts, count);
+    after_launch(ctx, "seg_write_kernel");
+    uint32_t c = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&c, count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    return c;
+}
+
+// ---- Morton keys ------------------------------------------------------------
+// `p as usize` (p2g.rs:149-157): truncation toward zero, negatives and NaN to 0.
+__device__ __forceinline__ uint64_t trunc_coord(float p) { return p > 0.0f ? (uint64_t)p : 0; }
+
+__global__ void morton_keys_kernel(const float* pos, size_t n, uint64_t* keys) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        keys[i] = morton3(trunc_coord(pos[3 * i]), trunc_coord(pos[3 * i + 1]), trunc_coord(pos[3 * i + 2]));
+}
+
+__global__ void morton3_kernel(const uint64_t* xyz, size_t n, uint64_t* keys) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        keys[i] = morton3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+}
+
+// multires/sort.rs:35-57 key.
+__global__ void block_list_key_kernel(const uint64_t* blocks, size_t n, uint64_t nx, uint64_t ny, const uint8_t* levels,
+                                      int n_levels, uint64_t* keys) {
+    const uint64_t ref_shift = (uint64_t)(n_levels - 1);
+    const uint64_t mask = (1ULL << ref_shift) - 1;
+    const uint64_t fine_bits = 3 * ref_shift;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t bid = blocks[i];
+        uint64_t bx = bid % nx, by = (bid / nx) % ny, bz = bid / (nx * ny);
+        uint64_t lvl = levels[i];
+        uint64_t coarse = morton3(bx >> ref_shift, by >> ref_shift, bz >> ref_shift);
+        uint64_t priority = ref_shift - lvl;
+        uint64_t fine = morton3(bx & mask, by & mask, bz & mask);
+        keys[i] = (coarse << (fine_bits + ref_shift)) | (priority << fine_bits) | fine;
+    }
+}
+
+__global__ void gather_u64_kernel(const uint64_t* src, const uint32_t* perm, uint64_t* dst, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[perm[i]];
+}
+
+// dst[i] = src[perm[i]] for items of `width` floats.
+__global__ void permute_kernel(const uint32_t* perm, size_t n, int width, const float* src, float* dst) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n * width; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = t / width, c = t % width;
+        dst[t] = src[(size_t)perm[i] * width + c];
+    }
+}
+
+static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 8192); }
+
+void morton_keys(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys) {
+    if (!n) return;
+    begin_launch(ctx);
+    morton_keys_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, n, d_keys);
+    after_launch(ctx, "morton_keys_kernel");
+}
+
+void morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out, uint32_t* d_perm_out) {
+    if (!n) return;
+    ScratchLayout L;
+    size_t ok = L.add<uint64_t>(n), ot = L.add<char>(radix_sort_scratch_bytes(n)), o8 = L.add<uint64_t>(1);
+    char* base = scratch(ctx, L);
+    uint64_t* keys = ScratchLayout::at<uint64_t>(base, ok);
+    morton_keys(ctx, d_pos, n, keys);
+    int bits = key_bits(ctx, keys, n, ScratchLayout::at<char>(base, o8));
+    radix_sort_pairs(ctx, keys, nullptr, d_keys_out, d_perm_out, n, bits, ScratchLayout::at<char>(base, ot));
+}
+
+size_t bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n, uint64_t* d_blocks, uint64_t* d_starts,
+                             uint32_t* d_perm) {
+    if (!n) {
+        uint64_t z = 0;
+        CUDA_CHECK(cudaMemcpyAsync(d_starts, &z, 8, cudaMemcpyHostToDevice, ctx->stream));
+        sync(ctx);
+        return 0;
+    }
+    ScratchLayout L;
+    size_t osk = L.add<uint64_t>(n), ot = L.add<char>(std::max(radix_sort_scratch_bytes(n), segment_scratch_bytes(n))),
+           o8 = L.add<uint64_t>(1);
+    char* base = scratch(ctx, L);
+    uint64_t* sk = ScratchLayout::at<uint64_t>(base, osk);
+    int bits = key_bits(ctx, d_bids, n, ScratchLayout::at<char>(base, o8));
+    radix_sort_pairs(ctx, d_bids, nullptr, sk, d_perm, n, bits, ScratchLayout::at<char>(base, ot));
+    return sorted_segments(ctx, sk, n, 0, d_blocks, d_starts, ScratchLayout::at<char>(base, ot));
+}
+
+}  // namespace msbg
+
+using namespace msbg;
+
+extern "C" {
+
+int msbg_morton3(msbg_ctx* ctx, const uint64_t* xyz, size_t n, uint64_t* keys_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((xyz && keys_out) || !n), "null argument");
+    if (!n) return MSBG_OK;
+    set_device(ctx);
+    ScratchLayout L;
+    size_t oi = L.add<uint64_t>(3 * n), oo = L.add<uint64_t>(n);
+    char* base = scratch(ctx, L);
+    uint64_t* di = ScratchLayout::at<uint64_t>(base, oi);
+    uint64_t* dout = ScratchLayout::at<uint64_t>(base, oo);
+    CUDA_CHECK(cudaMemcpyAsync(di, xyz, 3 * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    begin_launch(ctx);
+    morton3_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(di, n, dout);
+    after_launch(ctx, "morton3_kernel");
+    CUDA_CHECK(cudaMemcpyAsync(keys_out, dout, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    MSBG_API_END
+}
+
+int msbg_sort_block_list_morton(msbg_ctx* ctx, uint64_t* blocks, size_t n, uint64_t nx, uint64_t ny,
+                                const uint8_t* levels, size_t n_levels_array, int n_levels) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((blocks && levels) || !n), "null argument");
+    MSBG_REQUIRE(n_levels >= 1 && n_levels <= 8, "n_levels out of range");
+    if (!n) return MSBG_OK;
+    set_device(ctx);
+    std::vector<uint8_t> lv(n);
+    for (size_t i = 0; i < n; ++i) {
+        MSBG_REQUIRE(blocks[i] < n_levels_array, "block id outside the levels array");
+        lv[i] = levels[blocks[i]];
+        MSBG_REQUIRE(lv[i] < n_levels, "block level >= n_levels");
+    }
+    ScratchLayout L;
+    size_t ob = L.add<uint64_t>(n), ol = L.add<uint8_t>(n), ok = L.add<uint64_t>(n), osk = L.add<uint64_t>(n),
+           op = L.add<uint32_t>(n), ot = L.add<char>(radix_sort_scratch_bytes(n)), o8 = L.add<uint64_t>(1);
+    char* base = scratch(ctx, L);
+    uint64_t* db = ScratchLayout::at<uint64_t>(base, ob);
+    uint8_t* dl = ScratchLayout::at<uint8_t>(base, ol);
+    uint64_t* dk = ScratchLayout::at<uint64_t>(base, ok);
+    uint64_t* dsk = ScratchLayout::at<uint64_t>(base, osk);
+    uint32_t* dp = ScratchLayout::at<uint32_t>(base, op);
+    CUDA_CHECK(cudaMemcpyAsync(db, blocks, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(dl, lv.data(), n, cudaMemcpyHostToDevice, ctx->stream));
+    begin_launch(ctx);
+    block_list_key_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(db, n, nx, ny, dl, n_levels, dk);
+    after_launch(ctx, "block_list_key_kernel");
+    int bits = key_bits(ctx, dk, n, ScratchLayout::at<char>(base, o8));
+    radix_sort_pairs(ctx, dk, nullptr, dsk, dp, n, bits, ScratchLayout::at<char>(base, ot));
+    begin_launch(ctx);
+    gather_u64_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(db, dp, dk, n);
+    after_launch(ctx, "gather_u64_kernel");
+    CUDA_CHECK(cudaMemcpyAsync(blocks, dk, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    MSBG_API_END
+}
+
+int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out, uint32_t* d_perm_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((d_pos && d_keys_out && d_perm_out) || !n), "null argument");
+    set_device(ctx);
+    morton_sort_device(ctx, d_pos, n, d_keys_out, d_perm_out);
+    MSBG_API_END
+}
+
+int msbg_morton_sort(msbg_ctx* ctx, const float* pos, size_t n, uint64_t* keys_out, uint32_t* perm_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((pos && keys_out && perm_out) || !n), "null argument");
+    if (!n) return MSBG_OK;
+    set_device(ctx);
+    DevBuf io;
+    io.reserve(n * 12 + n * 8 + n * 4 + 1024);
+    float* dpos = io.as<float>();
+    uint64_t* dk = (uint64_t*)((char*)io.p + ((n * 12 + 255) & ~size_t(255)));
+    uint32_t* dp = (uint32_t*)((char*)dk + ((n * 8 + 255) & ~size_t(255)));
+    CUDA_CHECK(cudaMemcpyAsync(dpos, pos, n * 12, cudaMemcpyHostToDevice, ctx->stream));
+    morton_sort_device(ctx, dpos, n, dk, dp);
+    CUDA_CHECK(cudaMemcpyAsync(keys_out, dk, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(perm_out, dp, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    MSBG_API_END
+}
+
+int msbg_permute_device(msbg_ctx* ctx, const uint32_t* d_perm, size_t n, int width, const float* d_src, float* d_dst) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((d_perm && d_src && d_dst) || !n), "null argument");
+    MSBG_REQUIRE(width >= 1 && width <= 16, "width must be 1..16");
+    MSBG_REQUIRE(d_src != d_dst, "permute cannot run in place");
+    if (!n) return MSBG_OK;
+    set_device(ctx);
+    begin_launch(ctx);
+    permute_kernel<<<grid_for(n * width), 256, 0, ctx->stream>>>(d_perm, n, width, d_src, d_dst);
+    after_launch(ctx, "permute_kernel");
+    MSBG_API_END
+}
+
+int msbg_bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n, uint64_t* d_particle_blocks,
+                               uint64_t* d_starts, uint32_t* d_perm, size_t* n_blocks_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && d_starts && n_blocks_out && ((d_bids && d_particle_blocks && d_perm) || !n), "null argument");
+    set_device(ctx);
+    *n_blocks_out = bucket_indices_device(ctx, d_bids, n, d_particle_blocks, d_starts, d_perm);
+    MSBG_API_END
+}
+
+int msbg_bucket_indices(msbg_ctx* ctx, const uint64_t* bids, size_t n, uint64_t* particle_blocks, uint64_t* starts,
+                        uint32_t* perm, size_t* n_blocks_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && starts && n_blocks_out && ((bids && particle_blocks && perm) || !n), "null argument");
+    set_device(ctx);
+    if (!n) {
+        starts[0] = 0;
+        *n_blocks_out = 0;
+        return MSBG_OK;
+    }
+    DevBuf io;
+    size_t a = (n * 8 + 255) & ~size_t(255), p = (n * 4 + 255) & ~size_t(255);
+    io.reserve(a * 3 + p + 512);
+    uint64_t* db = io.as<uint64_t>();
+    uint64_t* dblk = (uint64_t*)((char*)io.p + a);
+    uint64_t* dst = (uint64_t*)((char*)io.p + 2 * a);
+    uint32_t* dp = (uint32_t*)((char*)io.p + 3 * a + 256);
+    CUDA_CHECK(cudaMemcpyAsync(db, bids, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    size_t nb = bucket_indices_device(ctx, db, n, dblk, dst, dp);
+    CUDA_CHECK(cudaMemcpyAsync(particle_blocks, dblk, nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(starts, dst, (nb + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(perm, dp, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    *n_blocks_out = nb;
+    MSBG_API_END
+}
+
+}  // extern "C"

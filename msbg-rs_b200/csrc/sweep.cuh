@@ -1,0 +1,23 @@
+// sweep.cuh -- the cached plan of an 8-colour in-place sweep (solver.rs:141-267).
+#pragma once
+
+#include "grid.cuh"
+
+namespace msbg {
+
+// Everything a sweep needs besides the payload: the blocks of the active list
+// that are value blocks, grouped by colour (solver.rs:247-267: colour =
+// bx&1 | (by&1)<<1 | (bz&1)<<2, Morton order inside a colour), and for each
+// of them the 27 neighbour codes (slot, empty, full or coarse slot) and the
+// block coordinates.  Rebuilt when the list, the grid's block set or (for a
+// multiresolution sweep) the coarse level changes.
+struct SweepPlan {
+    uint64_t key = 0;
+    size_t n = 0;
+    int color_off[9] = {0};
+    DevBuf nbr;    // int32 [n][27]
+    DevBuf bxyz;   // int32 [n][3]
+    DevBuf order;  // int32 [n] plan indices grouped by colour
+};
+
+}  // namespace msbg

@@ -1,0 +1,106 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+There is no public dataset for this path: every input is generated here from a
+seed (numpy PCG64, seed = configuration index + 1), following the
+configuration rules stated beside each generator.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def shell_active_blocks(n_per_axis: int, bsx: int, radius: float, thickness: float) -> np.ndarray:
+    """Blocks whose bounding box meets the spherical shell
+    | |x - c| - radius | <= thickness / 2, c = the domain centre."""
+    c = n_per_axis * bsx / 2.0
+    b = np.arange(n_per_axis)
+    bz, by, bx = np.meshgrid(b, b, b, indexing="ij")
+    lo = np.stack([bx, by, bz], -1).astype(np.float64) * bsx
+    hi = lo + bsx
+    dmin = np.linalg.norm(np.clip(c, lo, hi) - c, axis=-1)
+    dmax = np.linalg.norm(np.maximum(np.abs(lo - c), np.abs(hi - c)), axis=-1)
+    hit = (dmin <= radius + thickness / 2) & (dmax >= radius - thickness / 2)
+    return np.nonzero(hit.reshape(-1))[0].astype(np.uint64)
+
+
+@dataclass
+class ShellProblem:
+    """Single-level shell: 16^3 blocks of a size^3 domain intersecting the
+    shell of radius 0.35*size and thickness 12 cells, U[-1, 1] values."""
+
+    size: int
+    bsx: int
+    active: np.ndarray
+    values: np.ndarray  # [n_active][bsx^3] f32
+
+
+def shell_problem(size: int = 128, bsx: int = 16, seed: int = 1, radius_frac: float = 0.35, thickness: float = 12.0,
+                  values: bool = True) -> ShellProblem:
+    n = size // bsx
+    active = shell_active_blocks(n, bsx, radius_frac * size, thickness)
+    vals = None
+    if values:
+        rng = np.random.default_rng(seed)
+        vals = rng.uniform(-1.0, 1.0, (len(active), bsx ** 3)).astype(np.float32)
+    return ShellProblem(size, bsx, active, vals)
+
+
+@dataclass
+class FlipTransfer:
+    """FLIP transfer workload: size^3 domain of bsx^3 blocks, 3 levels by the
+    distance of a block centre to the sphere |x - c| = 0.35*size (< 16 cells
+    -> level 0, < 48 -> level 1, else 2); 8 particles per level-0 cell,
+    uniformly jittered inside the cell; velocities N(0, 1), mass 1."""
+
+    size: int
+    bsx: int
+    levels: np.ndarray      # [n_blocks] u8
+    fine_blocks: np.ndarray  # level-0 block ids
+    pos: np.ndarray          # [n][3] f32
+    vel: np.ndarray          # [n][3] f32
+    mass: np.ndarray         # [n] f32
+
+    @property
+    def n(self) -> int:
+        return len(self.mass)
+
+
+def block_levels(size: int, bsx: int, radius: float, bands=(16.0, 48.0)) -> np.ndarray:
+    n = size // bsx
+    b = np.arange(n)
+    bz, by, bx = np.meshgrid(b, b, b, indexing="ij")
+    centre = (np.stack([bx, by, bz], -1).astype(np.float64) + 0.5) * bsx
+    d = np.abs(np.linalg.norm(centre - size / 2.0, axis=-1) - radius).reshape(-1)
+    lv = np.full(d.shape, 2, np.uint8)
+    lv[d < bands[1]] = 1
+    lv[d < bands[0]] = 0
+    return lv
+
+
+def flip_transfer(size: int = 256, bsx: int = 16, seed: int = 2, ppc: int = 8, radius_frac: float = 0.35,
+                  particles: bool = True) -> FlipTransfer:
+    levels = block_levels(size, bsx, radius_frac * size)
+    fine = np.nonzero(levels == 0)[0].astype(np.uint64)
+    if not particles:
+        e = np.empty((0, 3), np.float32)
+        return FlipTransfer(size, bsx, levels, fine, e, e, np.empty(0, np.float32))
+    n_per_axis = size // bsx
+    rng = np.random.default_rng(seed)
+    cells = np.arange(bsx ** 3)
+    lx, ly, lz = cells % bsx, (cells // bsx) % bsx, cells // (bsx * bsx)
+    bx = (fine % n_per_axis).astype(np.int64)
+    by = ((fine // n_per_axis) % n_per_axis).astype(np.int64)
+    bz = (fine // (n_per_axis * n_per_axis)).astype(np.int64)
+    cx = (bx[:, None] * bsx + lx[None, :]).reshape(-1)
+    cy = (by[:, None] * bsx + ly[None, :]).reshape(-1)
+    cz = (bz[:, None] * bsx + lz[None, :]).reshape(-1)
+    origin = np.repeat(np.stack([cx, cy, cz], -1).astype(np.float32), ppc, axis=0)
+    jitter = rng.random(origin.shape, dtype=np.float32)
+    pos = origin + jitter
+    # origin + jitter can round up to the next cell in f32: keep it inside
+    pos = np.minimum(pos, np.nextafter(origin + 1, origin, dtype=np.float32))
+    vel = rng.standard_normal(origin.shape, dtype=np.float32)
+    mass = np.ones(len(pos), np.float32)
+    return FlipTransfer(size, bsx, levels, fine, pos.astype(np.float32), vel, mass)
