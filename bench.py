@@ -201,7 +201,7 @@ def run_ours(args, world, rank, local):
         call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(vel), ptr(svel))
         call("msbg_permute_device", ctx.handle, ptr(perm), n, 1, ptr(mass), ptr(smass))
         mark("sort")
-        msbg.particles_to_grid_device(mac, spos, svel, smass, n, R_P)
+        msbg.particles_to_grid_sorted_device(mac, spos, svel, smass, keys, n, R_P)
         mark("p2g")
         act = mac.active_blocks()
         fine = act[levels[act.astype(np.int64)] == 0]
@@ -332,14 +332,14 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, steps):
     per particle for G2P; 24 B per element per radix pass)."""
     if kernel == "sweep_phase_kernel":
         return 8.0 * n_fine * 4096 * SWEEPS * steps
-    if kernel == "p2g_splat_kernel":
+    if kernel == "p2g_cells_kernel":
         return 28.0 * n * steps
     if kernel == "p2g_combine_kernel":
         return 24.0 * n_active * 4096 * steps
     if kernel == "g2p_kernel":
         return 24.0 * n * steps
     if kernel in ("rs_scatter_kernel",):
-        return 24.0 * n * steps * 3 * 2  # two sorts of 3 passes each
+        return 24.0 * n * steps * 3  # one sort of 3 passes
     if kernel == "permute_kernel":
         return 2 * 28.0 * n * steps
     return None
@@ -433,7 +433,7 @@ def run_reference(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=256)

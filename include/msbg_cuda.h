@@ -201,6 +201,12 @@ int msbg_p2g(msbg_mac* mac, const float* pos, const float* vel, const float* mas
              size_t* n_active_out);
 int msbg_p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass, size_t n,
                     float r_p, size_t* n_active_out);
+/* particles_to_grid for particles already in Morton order: d_keys are their
+ * sorted keys as msbg_morton_sort_device returns them (the caller applied the
+ * permutation with msbg_permute_device); the internal sort is skipped.  The
+ * result is identical to msbg_p2g_device on the same particles. */
+int msbg_p2g_sorted_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass,
+                           const uint64_t* d_keys, size_t n, float r_p, size_t* n_active_out);
 /* Active block set of the last P2G (ascending bids). */
 int msbg_mac_active_blocks(const msbg_mac* mac, uint64_t* out, size_t cap, size_t* n_out);
 /* MacGrid::normalize_velocity (mac.rs:106-132) over the listed blocks. */

@@ -93,6 +93,19 @@ DevHash device_hash(msbg_grid* g) {
     return DevHash{g->hkeys.as<uint64_t>(), g->hvals.as<int32_t>(), g->hmask, g->hshift};
 }
 
+const int32_t* device_dense(msbg_grid* g) {
+    if (g->n_blocks > kDenseMaxBlocks) return nullptr;
+    if (g->dense_dirty || g->hash_dirty) {
+        std::vector<int32_t> t(g->n_blocks, kCodeEmpty);
+        for (const auto& kv : g->map) t[kv.first] = kv.second;
+        g->dense.reserve(t.size() * 4);
+        CUDA_CHECK(cudaMemcpyAsync(g->dense.p, t.data(), t.size() * 4, cudaMemcpyHostToDevice, g->ctx->stream));
+        sync(g->ctx);
+        g->dense_dirty = false;
+    }
+    return g->dense.as<int32_t>();
+}
+
 int32_t grid_code(const msbg_grid* g, uint64_t bid) {
     auto it = g->map.find(bid);
     return it == g->map.end() ? kCodeEmpty : it->second;
@@ -166,6 +179,7 @@ void grid_ensure(msbg_grid* g, const uint64_t* bids, size_t n, int32_t* slots) {
     if (!fresh.empty()) {
         g->version++;
         g->hash_dirty = true;
+        g->dense_dirty = true;
         grid_reserve(g, g->n_slots());
         // A private buffer, not the context arena: pipelines call this while
         // their own temporaries live in the arena.
@@ -567,7 +581,7 @@ int msbg_grid_set_full_blocks(msbg_grid* g, const uint64_t* bids, size_t n) {
         MSBG_REQUIRE(grid_code(g, bids[k]) < 0, "set_full_block on a value block");
     }
     for (size_t k = 0; k < n; ++k) g->map[bids[k]] = kCodeFull;
-    if (n) { g->hash_dirty = true; g->version++; }
+    if (n) { g->hash_dirty = true; g->dense_dirty = true; g->version++; }
     MSBG_API_END
 }
 
@@ -579,7 +593,7 @@ int msbg_grid_set_empty_blocks(msbg_grid* g, const uint64_t* bids, size_t n) {
         MSBG_REQUIRE(grid_code(g, bids[k]) < 0, "set_empty_block on a value block");
     }
     for (size_t k = 0; k < n; ++k) g->map.erase(bids[k]);
-    if (n) { g->hash_dirty = true; g->version++; }
+    if (n) { g->hash_dirty = true; g->dense_dirty = true; g->version++; }
     MSBG_API_END
 }
 

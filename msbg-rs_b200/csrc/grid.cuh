@@ -77,6 +77,8 @@ struct msbg_grid {
     uint32_t hmask = 0;
     int hshift = 64;
     bool hash_dirty = true;
+    msbg::DevBuf dense;  // int32 code per block id, for grids of <= kDenseMaxBlocks blocks
+    bool dense_dirty = true;
 
     msbg::SweepPlan* plan = nullptr;  // cached sweep plan
 
@@ -89,6 +91,10 @@ namespace msbg {
 
 // Makes sure the device table mirrors the host map.
 DevHash device_hash(msbg_grid* g);
+// A dense bid -> code table (null when the grid has more than kDenseMaxBlocks
+// blocks): one load instead of a hash probe for small and medium domains.
+constexpr uint64_t kDenseMaxBlocks = 1ull << 24;
+const int32_t* device_dense(msbg_grid* g);
 // Materialises value blocks for `bids` (new ones filled with the empty value);
 // returns the slot of each bid in `slots` (may be null).
 void grid_ensure(msbg_grid* g, const uint64_t* bids, size_t n, int32_t* slots);

@@ -21,6 +21,7 @@ void mac_ensure(msbg_mac* m, const uint64_t* bids, size_t n, int32_t* slots) {
 
 struct SampleGrid {
     const float* payload;
+    const int32_t* dense;  // bid -> code, or null (use the hash)
     DevHash hash;
     int64_t nx, ny, nz;
     int32_t sx, sy, sz;
@@ -33,6 +34,7 @@ static SampleGrid sample_grid(msbg_grid* g) {
     SampleGrid s;
     s.payload = g->payload.as<float>();
     s.hash = device_hash(g);
+    s.dense = device_dense(g);
     s.nx = (int64_t)g->nx; s.ny = (int64_t)g->ny; s.nz = (int64_t)g->nz;
     s.sx = (int32_t)g->sx; s.sy = (int32_t)g->sy; s.sz = (int32_t)g->sz;
     s.lg = g->lg;
@@ -44,6 +46,10 @@ static SampleGrid sample_grid(msbg_grid* g) {
 __device__ __forceinline__ float code_value(const SampleGrid& g, int32_t code, int vid) {
     if (code >= 0) return g.payload[((size_t)code << (3 * g.lg)) + vid];
     return code == kCodeFull ? g.full : g.empty;
+}
+
+__device__ __forceinline__ int32_t block_code(const SampleGrid& g, uint64_t bid) {
+    return g.dense ? __ldg(g.dense + bid) : hash_find(g.hash, bid);
 }
 
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(b - a, t, a); }
@@ -60,7 +66,7 @@ __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float 
         const int vx0 = ix0 & mask, vy0 = iy0 & mask, vz0 = iz0 & mask;
         if (vx0 + 1 < bsx && vy0 + 1 < bsx && vz0 + 1 < bsx) {
             const uint64_t bid = (uint64_t)(ix0 >> lg) + (uint64_t)(iy0 >> lg) * g.nx + (uint64_t)(iz0 >> lg) * g.nx * g.ny;
-            const int32_t code = hash_find(g.hash, bid);
+            const int32_t code = block_code(g, bid);
             int s = 0;
             for (int k = 0; k < 2; ++k)
                 for (int j = 0; j < 2; ++j)
@@ -77,7 +83,7 @@ __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float 
         for (int s = 0; s < 8; ++s) {
             const int64_t bxx = min(bx0 + (s & 1), g.nx - 1), byy = min(by0 + ((s >> 1) & 1), g.ny - 1),
                           bzz = min(bz0 + (s >> 2), g.nz - 1);
-            codes[s] = hash_find(g.hash, (uint64_t)bxx + (uint64_t)byy * g.nx + (uint64_t)bzz * g.nx * g.ny);
+            codes[s] = block_code(g, (uint64_t)bxx + (uint64_t)byy * g.nx + (uint64_t)bzz * g.nx * g.ny);
         }
         int s = 0;
         for (int k = 0; k < 2; ++k) {

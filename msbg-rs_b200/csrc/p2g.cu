@@ -37,100 +37,12 @@ struct SplatArgs {
     const int32_t* cell_begin;               // [npb][bsx^3] by local Morton code
     const int32_t* cell_end;
     const uint64_t* pb_key;                  // block Morton key per particle block
+    const uint64_t* fp;                      // packed clipped footprints per particle
     double* partial;                         // [npb][3][2][W^3]
     float r_p, inv_r2;
 };
 
 template <int BSX> struct P2GLg { static constexpr int v = BSX == 8 ? 3 : BSX == 16 ? 4 : 5; };
-
-template <int BSX, int M>
-__global__ void __launch_bounds__(1024, 1) p2g_splat_kernel(SplatArgs a) {
-    constexpr int W = BSX + 2 * M;
-    constexpr int WW = W * W * W;
-    constexpr int WIN = 2 * M + 1;
-    constexpr int NF = WIN * WIN * WIN;
-    constexpr int Q = (NF + 31) / 32;
-    constexpr int LG = P2GLg<BSX>::v;
-    extern __shared__ double st[];  // [2][W^3]: mass, momentum
-    const int k = blockIdx.x, dir = blockIdx.y;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-    for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
-    const uint64_t key = a.pb_key[k];
-    const int32_t b0x = (int32_t)compact3(key) * BSX, b0y = (int32_t)compact3(key >> 1) * BSX,
-                  b0z = (int32_t)compact3(key >> 2) * BSX;
-    const float ofx = dir == 0 ? 1.0f : 0.5f, ofy = dir == 1 ? 1.0f : 0.5f, ofz = dir == 2 ? 1.0f : 0.5f;
-    // Candidate face offsets relative to the cell: the face axis reaches
-    // [-M-1, M-1], the other axes [-M, M].
-    const int lox = dir == 0 ? -M - 1 : -M, loy = dir == 1 ? -M - 1 : -M, loz = dir == 2 ? -M - 1 : -M;
-    const float* __restrict__ pv = a.pv[dir];
-    const int32_t* cb = a.cell_begin + (size_t)k * BSX * BSX * BSX;
-    const int32_t* ce = a.cell_end + (size_t)k * BSX * BSX * BSX;
-    const float r_p = a.r_p, inv_r2 = a.inv_r2;
-    __syncthreads();
-    for (int ph = 0; ph < WIN * WIN * WIN; ++ph) {
-        const int ox = ph % WIN, oy = (ph / WIN) % WIN, oz = ph / (WIN * WIN);
-        const int ncx = ox < BSX ? (BSX - ox + WIN - 1) / WIN : 0;
-        const int ncy = oy < BSX ? (BSX - oy + WIN - 1) / WIN : 0;
-        const int ncz = oz < BSX ? (BSX - oz + WIN - 1) / WIN : 0;
-        const int total = ncx * ncy * ncz;
-        for (int c = warp; c < total; c += nwarp) {
-            const int lx = ox + WIN * (c % ncx), ly = oy + WIN * ((c / ncx) % ncy), lz = oz + WIN * (c / (ncx * ncy));
-            const uint32_t lm = (uint32_t)morton3(lx, ly, lz);
-            const int b = cb[lm], e = ce[lm];
-            if (b >= e) continue;
-            double am[Q], av[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) am[q] = av[q] = 0.0;
-            for (int p = b; p < e; ++p) {
-                const float x = a.px[p], y = a.py[p], z = a.pz[p], m_p = a.pm[p], u_a = pv[p];
-                const float scale_mass = m_p, scale_mom = m_p * u_a;
-                const float px0 = x - 0.5f, py0 = y - 0.5f, pz0 = z - 0.5f;
-                // Footprint clipped to the staging window (p2g.rs:263-270).
-                const int32_t ix1 = min(max((int32_t)ceilf((x - r_p) - ofx), b0x - M), b0x + BSX + M - 1);
-                const int32_t ix2 = min(max((int32_t)floorf((x + r_p) - ofx), b0x - M), b0x + BSX + M - 1);
-                const int32_t iy1 = min(max((int32_t)ceilf((y - r_p) - ofy), b0y - M), b0y + BSX + M - 1);
-                const int32_t iy2 = min(max((int32_t)floorf((y + r_p) - ofy), b0y - M), b0y + BSX + M - 1);
-                const int32_t iz1 = min(max((int32_t)ceilf((z - r_p) - ofz), b0z - M), b0z + BSX + M - 1);
-                const int32_t iz2 = min(max((int32_t)floorf((z + r_p) - ofz), b0z - M), b0z + BSX + M - 1);
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    const int f = lane + 32 * q;
-                    if (f >= NF) continue;
-                    const int32_t gx = b0x + lx + lox + f % WIN, gy = b0y + ly + loy + (f / WIN) % WIN,
-                                  gz = b0z + lz + loz + f / (WIN * WIN);
-                    if (gx < ix1 || gx > ix2 || gy < iy1 || gy > iy2 || gz < iz1 || gz > iz2) continue;
-                    // p2g.rs:287-325, operation by operation.
-                    const float dz = (float)gz - pz0;
-                    const float dz2 = dz * dz;
-                    const float dy = (float)gy - py0;
-                    const float dyz = dz2 + dy * dy;
-                    const float dx = (float)gx - px0;
-                    const float dist_sq = dx * dx + dyz;
-                    const float d_a = dir == 0 ? dx : (dir == 1 ? dy : dz);
-                    const float df2 = (dist_sq + d_a) + 0.25f;
-                    float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
-                    w = (w * w) * w;
-                    am[q] += (double)(w * scale_mass);
-                    av[q] += (double)(w * scale_mom);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int f = lane + 32 * q;
-                if (f >= NF) continue;
-                const int sx = lx + M + lox + f % WIN, sy = ly + M + loy + (f / WIN) % WIN, sz = lz + M + loz + f / (WIN * WIN);
-                if (sx < 0 || sy < 0 || sz < 0 || sx >= W || sy >= W || sz >= W) continue;
-                const int si = (sz * W + sy) * W + sx;
-                st[si] += am[q];
-                st[WW + si] += av[q];
-            }
-        }
-        __syncthreads();
-    }
-    double* out = a.partial + ((size_t)k * 3 + dir) * 2 * WW;
-    for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
-    (void)LG;
-}
 
 struct CombineArgs {
     const double* partial;
@@ -204,22 +116,28 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
     }
 }
 
-// Payload gather into cell-sorted SoA, and each particle's footprint mask
-// (particles/mod.rs:207-212 footprint_axis with r_scan = (r_p + 1) / bsx,
-// relative to its own block).
+// Payload gather into cell-sorted SoA (perm == null: already sorted), each
+// particle's block-footprint mask (particles/mod.rs:207-212 footprint_axis
+// with r_scan = (r_p + 1) / bsx, relative to its own block) and its clipped
+// face footprints in staging coordinates of its block (p2g.rs:263-270): per
+// axis, for the cell-centred offset (0.5) and the face offset (1.0), lo and hi
+// as 5-bit fields of a u64 (bits ((axis*2 + face)*2 + hi)*5).
 __global__ void p2g_gather_kernel(const float* pos, const float* vel, const float* mass, const uint32_t* perm, size_t n,
-                                  int lg, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz, float* px, float* py,
-                                  float* pz, float* pm, float* v0, float* v1, float* v2, uint32_t* fmask, int* bad) {
+                                  int lg, int M, float r_p, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz,
+                                  float* px, float* py, float* pz, float* pm, float* v0, float* v1, float* v2,
+                                  uint32_t* fmask, uint64_t* fp, int* bad) {
     const float bsx = (float)(1 << lg);
+    const int32_t B = 1 << lg;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t s = perm[i];
-        const float x = pos[3 * (size_t)s], y = pos[3 * (size_t)s + 1], z = pos[3 * (size_t)s + 2];
+        const size_t s = perm ? perm[i] : i;
+        const float x = pos[3 * s], y = pos[3 * s + 1], z = pos[3 * s + 2];
         px[i] = x; py[i] = y; pz[i] = z;
         pm[i] = mass[s];
-        v0[i] = vel[3 * (size_t)s]; v1[i] = vel[3 * (size_t)s + 1]; v2[i] = vel[3 * (size_t)s + 2];
+        v0[i] = vel[3 * s]; v1[i] = vel[3 * s + 1]; v2[i] = vel[3 * s + 2];
         const float p[3] = {x, y, z};
         const int64_t nn[3] = {nx, ny, nz};
         uint32_t lo[3], hi[3];
+        uint64_t f = 0;
         bool out = false;
         for (int ax = 0; ax < 3; ++ax) {
             const int64_t cb = p[ax] > 0.0f ? (int64_t)p[ax] >> lg : 0;  // the particle's block (p as usize >> lg)
@@ -229,7 +147,16 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             const int64_t h = min((int64_t)(int32_t)truncf(b + r_scan_bsx), nn[ax] - 1);
             lo[ax] = (uint32_t)(min(max(l - cb, (int64_t)-1), (int64_t)1) + 1);
             hi[ax] = (uint32_t)(min(max(h - cb, (int64_t)-1), (int64_t)1) + 1);
+            const int32_t b0 = (int32_t)cb * B;
+            for (int face = 0; face < 2; ++face) {
+                const float of = face ? 1.0f : 0.5f;
+                const int32_t a1 = min(max((int32_t)ceilf((p[ax] - r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
+                const int32_t a2 = min(max((int32_t)floorf((p[ax] + r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
+                f |= (uint64_t)(a1 & 31) << (((ax * 2 + face) * 2) * 5);
+                f |= (uint64_t)(a2 & 31) << (((ax * 2 + face) * 2 + 1) * 5);
+            }
         }
+        fp[i] = f;
         if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
         uint32_t m = 0;
         for (uint32_t dz = lo[2]; dz <= hi[2]; ++dz)
@@ -237,6 +164,120 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
                 for (uint32_t dx = lo[0]; dx <= hi[0]; ++dx) m |= 1u << (dx + 3 * dy + 9 * dz);
         fmask[i] = m;
     }
+}
+
+__device__ __forceinline__ int fp_field(uint64_t f, int ax, int face, int hi) {
+    return (int)((f >> (((ax * 2 + face) * 2 + hi) * 5)) & 31);
+}
+
+// Splat kernel: one CTA per (particle block, direction DIR).  The block's
+// (bsx + 2M)^3 staging window of face sums lives in shared memory in FP64.
+// Cells are visited in (2M+1)^3 colour phases (cells of a phase are 2M+1
+// apart, so their candidate face windows are disjoint) with a barrier between
+// phases; inside a phase one warp handles one cell.  The lanes of the warp
+// take the (2M+1)^2 positions of the cell's face window across the two axes
+// other than the face axis, and each lane keeps the 2M+1 faces along the face
+// axis in FP64 registers.  For every particle of the cell (sorted order) a
+// lane evaluates the reference's f32 term for each of its faces that lies in
+// the particle's clipped footprint (p2g.rs:263-330, operation by operation),
+// then adds its register sums to the staging window: a fixed summation order,
+// no atomics.
+template <int BSX, int M, int DIR>
+__global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
+    constexpr int W = BSX + 2 * M;
+    constexpr int WW = W * W * W;
+    constexpr int WIN = 2 * M + 1;
+    constexpr int NUV = WIN * WIN;       // lane positions
+    constexpr int Q = (NUV + 31) / 32;   // lane rounds
+    extern __shared__ double st[];       // [2][W^3]: mass, momentum
+    const int k_pb = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
+    const uint64_t key = a.pb_key[k_pb];
+    const int32_t b0[3] = {(int32_t)compact3(key) * BSX, (int32_t)compact3(key >> 1) * BSX,
+                           (int32_t)compact3(key >> 2) * BSX};
+    // axes: F = face axis (registers), U and V = lane axes
+    constexpr int F = DIR, U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2;
+    const int32_t* cb = a.cell_begin + (size_t)k_pb * BSX * BSX * BSX;
+    const int32_t* ce = a.cell_end + (size_t)k_pb * BSX * BSX * BSX;
+    const float* __restrict__ pv = a.pv[DIR];
+    const float inv_r2 = a.inv_r2;
+    __syncthreads();
+    for (int ph = 0; ph < WIN * WIN * WIN; ++ph) {
+        const int ox = ph % WIN, oy = (ph / WIN) % WIN, oz = ph / (WIN * WIN);
+        const int ncx = ox < BSX ? (BSX - ox + WIN - 1) / WIN : 0;
+        const int ncy = oy < BSX ? (BSX - oy + WIN - 1) / WIN : 0;
+        const int ncz = oz < BSX ? (BSX - oz + WIN - 1) / WIN : 0;
+        const int total = ncx * ncy * ncz;
+        for (int c = warp; c < total; c += nwarp) {
+            int cell[3];
+            cell[0] = ox + WIN * (c % ncx);
+            cell[1] = oy + WIN * ((c / ncx) % ncy);
+            cell[2] = oz + WIN * (c / (ncx * ncy));
+            const uint32_t lm = (uint32_t)morton3(cell[0], cell[1], cell[2]);
+            const int b = cb[lm], e = ce[lm];
+            if (b >= e) continue;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int uv = lane + 32 * q;
+                const bool on = uv < NUV;
+                // staging coordinates of this lane's row: U, V offsets in [-M, M]
+                const int su = cell[U] + M + (uv % WIN) - M, sv = cell[V] + M + (uv / WIN) - M;
+                const float gu = (float)(b0[U] - M + su), gv = (float)(b0[V] - M + sv);
+                double am[WIN], av[WIN];
+#pragma unroll
+                for (int s = 0; s < WIN; ++s) am[s] = av[s] = 0.0;
+                for (int p = b; p < e; ++p) {
+                    const uint64_t f = a.fp[p];
+                    if (!on || su < fp_field(f, U, 0, 0) || su > fp_field(f, U, 0, 1) || sv < fp_field(f, V, 0, 0) ||
+                        sv > fp_field(f, V, 0, 1))
+                        continue;
+                    const int sf1 = fp_field(f, F, 1, 0), sf2 = fp_field(f, F, 1, 1);
+                    const float m_p = a.pm[p];
+                    const float scale_mom = m_p * pv[p];
+                    const float pc[3] = {a.px[p] - 0.5f, a.py[p] - 0.5f, a.pz[p] - 0.5f};
+                    const float du = gu - pc[U], dv = gv - pc[V];
+#pragma unroll
+                    for (int s = 0; s < WIN; ++s) {
+                        // face-axis offset in [-M-1, M-1] -> staging cell[F] + s - 1
+                        const int sf = cell[F] + s - 1;
+                        if (sf < sf1 || sf > sf2) continue;
+                        const float df = (float)(b0[F] - M + sf) - pc[F];
+                        // p2g.rs:287-325: dz2 = dz*dz; dyz = dz2 + dy*dy; dist_sq = dx*dx + dyz
+                        float dx, dy, dz;
+                        if (DIR == 0) { dx = df; dy = du; dz = dv; }
+                        else if (DIR == 1) { dx = du; dy = df; dz = dv; }
+                        else { dx = du; dy = dv; dz = df; }
+                        const float dz2 = dz * dz;
+                        const float dyz = dz2 + dy * dy;
+                        const float dist_sq = dx * dx + dyz;
+                        const float df2 = (dist_sq + df) + 0.25f;
+                        float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
+                        w = (w * w) * w;
+                        am[s] += (double)(w * m_p);
+                        av[s] += (double)(w * scale_mom);
+                    }
+                }
+                if (on) {
+#pragma unroll
+                    for (int s = 0; s < WIN; ++s) {
+                        const int sf = cell[F] + s - 1;
+                        if (sf < 0 || sf >= W) continue;
+                        int sc[3];
+                        sc[F] = sf;
+                        sc[U] = su;
+                        sc[V] = sv;
+                        const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                        st[si] += am[s];
+                        st[WW + si] += av[s];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    double* out = a.partial + ((size_t)k_pb * 3 + DIR) * 2 * WW;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
 }
 
 // OR of the footprint masks over each particle block's particles, expanded to
@@ -293,18 +334,25 @@ __global__ void active_nbr_kernel(const uint64_t* active, size_t n_active, const
 
 static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 8192); }
 
-template <int BSX, int M>
-static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
+template <int BSX, int M, int DIR>
+static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     constexpr int W = BSX + 2 * M;
     const size_t smem = 2 * sizeof(double) * W * W * W;
     static bool attr = false;
     if (!attr) {
-        CUDA_CHECK(cudaFuncSetAttribute(p2g_splat_kernel<BSX, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_CHECK(cudaFuncSetAttribute(p2g_cells_kernel<BSX, M, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     begin_launch(ctx);
-    p2g_splat_kernel<BSX, M><<<dim3((unsigned)npb, 3), 1024, smem, ctx->stream>>>(a);
-    after_launch(ctx, "p2g_splat_kernel");
+    p2g_cells_kernel<BSX, M, DIR><<<(unsigned)npb, 1024, smem, ctx->stream>>>(a);
+    after_launch(ctx, "p2g_cells_kernel");
+}
+
+template <int BSX, int M>
+static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
+    launch_splat_dir<BSX, M, 0>(ctx, a, npb);
+    launch_splat_dir<BSX, M, 1>(ctx, a, npb);
+    launch_splat_dir<BSX, M, 2>(ctx, a, npb);
 }
 
 template <int BSX, int M>
@@ -330,8 +378,10 @@ static void dispatch(msbg_ctx* ctx, int bsx, int M, const SplatArgs* s, size_t n
 
 static size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// d_sorted_keys: optional Morton keys of particles that are already sorted
+// by them (msbg_morton_sort_device + msbg_permute_device); skips the sort.
 void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass, size_t n, float r_p,
-                size_t* n_active_out) {
+                size_t* n_active_out, const uint64_t* d_sorted_keys) {
     msbg_ctx* ctx = mac->ctx;
     msbg_grid* u = mac->ch[0];
     const int bsx = u->bsx, lg = u->lg;
@@ -354,27 +404,35 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     // ---- phase 1: sort, gather, particle blocks -------------------------------
     ScratchLayout L1;
     const size_t o_keys = L1.add<uint64_t>(n), o_skeys = L1.add<uint64_t>(n), o_perm = L1.add<uint32_t>(n),
-                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_pbk = L1.add<uint64_t>(n + 1),
+                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_fp = L1.add<uint64_t>(n),
+                 o_pbk = L1.add<uint64_t>(n + 1),
                  o_pbs = L1.add<uint64_t>(n + 2), o_tmp = L1.add<char>(std::max(radix_sort_scratch_bytes(n), segment_scratch_bytes(n))),
                  o_bad = L1.add<int>(4);
     // phase-2 buffers go after phase 1's (sized once npb is known)
     char* base = scratch(ctx, L1);
     uint64_t* keys = ScratchLayout::at<uint64_t>(base, o_keys);
-    uint64_t* skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    const uint64_t* skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
     uint32_t* perm = ScratchLayout::at<uint32_t>(base, o_perm);
     float* soa = ScratchLayout::at<float>(base, o_soa);
     uint32_t* fmask = ScratchLayout::at<uint32_t>(base, o_fm);
+    uint64_t* fpk = ScratchLayout::at<uint64_t>(base, o_fp);
     uint64_t* pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
     uint64_t* pb_starts = ScratchLayout::at<uint64_t>(base, o_pbs);
     int* bad = ScratchLayout::at<int>(base, o_bad);
     CUDA_CHECK(cudaMemsetAsync(bad, 0, 4, ctx->stream));
-    morton_keys(ctx, d_pos, n, keys);
-    radix_sort_pairs(ctx, keys, nullptr, skeys, perm, n, key_bits, ScratchLayout::at<char>(base, o_tmp));
+    if (d_sorted_keys) {
+        skeys = d_sorted_keys;
+        perm = nullptr;
+    } else {
+        morton_keys(ctx, d_pos, n, keys);
+        radix_sort_pairs(ctx, keys, nullptr, ScratchLayout::at<uint64_t>(base, o_skeys), perm, n, key_bits,
+                         ScratchLayout::at<char>(base, o_tmp));
+    }
     float *px = soa, *py = soa + n, *pz = soa + 2 * n, *pm = soa + 3 * n, *v0 = soa + 4 * n, *v1 = soa + 5 * n, *v2 = soa + 6 * n;
     begin_launch(ctx);
-    p2g_gather_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, (r_p + 1.0f) / (float)bsx,
-                                                            (int64_t)u->nx, (int64_t)u->ny, (int64_t)u->nz, px, py, pz, pm,
-                                                            v0, v1, v2, fmask, bad);
+    p2g_gather_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, M, r_p,
+                                                            (r_p + 1.0f) / (float)bsx, (int64_t)u->nx, (int64_t)u->ny,
+                                                            (int64_t)u->nz, px, py, pz, pm, v0, v1, v2, fmask, fpk, bad);
     after_launch(ctx, "p2g_gather_kernel");
     const size_t npb = sorted_segments(ctx, skeys, n, (uint64_t)(3 * lg), pb_key, pb_starts, ScratchLayout::at<char>(base, o_tmp));
     int hbad = 0;
@@ -389,7 +447,8 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
                  o_ctmp = L2.add<char>(std::max(radix_sort_scratch_bytes(npb * 27), segment_scratch_bytes(npb * 27))),
                  o_cb = L2.add<int32_t>(npb * NC), o_ce = L2.add<int32_t>(npb * NC), o_part = L2.add<double>(npb * 6 * WW);
     base = scratch(ctx, L2);  // may move: re-derive phase-1 pointers
-    skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    if (!d_sorted_keys) skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    fpk = ScratchLayout::at<uint64_t>(base, o_fp);
     soa = ScratchLayout::at<float>(base, o_soa);
     fmask = ScratchLayout::at<uint32_t>(base, o_fm);
     pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
@@ -424,7 +483,8 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     ScratchLayout L3 = L2;
     const size_t o_nr = L3.add<int32_t>(na * 27), o_sl = L3.add<int32_t>(na);
     base = scratch(ctx, L3);
-    skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    if (!d_sorted_keys) skeys = ScratchLayout::at<uint64_t>(base, o_skeys);
+    fpk = ScratchLayout::at<uint64_t>(base, o_fp);
     soa = ScratchLayout::at<float>(base, o_soa);
     pb_key = ScratchLayout::at<uint64_t>(base, o_pbk);
     pb_starts = ScratchLayout::at<uint64_t>(base, o_pbs);
@@ -450,6 +510,7 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     s.cell_begin = cell_begin;
     s.cell_end = cell_end;
     s.pb_key = pb_key;
+    s.fp = fpk;
     s.partial = partial;
     s.r_p = r_p;
     s.inv_r2 = 1.0f / (r_p * r_p);
@@ -482,7 +543,16 @@ int msbg_p2g_device(msbg_mac* m, const float* d_pos, const float* d_vel, const f
     MSBG_API_BEGIN
     MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass) || !n), "null argument");
     set_device(m->ctx);
-    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, nullptr);
+    MSBG_API_END
+}
+
+int msbg_p2g_sorted_device(msbg_mac* m, const float* d_pos, const float* d_vel, const float* d_mass,
+                           const uint64_t* d_keys, size_t n, float r_p, size_t* n_active_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass && d_keys) || !n), "null argument");
+    set_device(m->ctx);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, d_keys);
     MSBG_API_END
 }
 
@@ -501,7 +571,7 @@ int msbg_p2g(msbg_mac* m, const float* pos, const float* vel, const float* mass,
         CUDA_CHECK(cudaMemcpyAsync(dv, vel, n * 12, cudaMemcpyHostToDevice, m->ctx->stream));
         CUDA_CHECK(cudaMemcpyAsync(dm, mass, n * 4, cudaMemcpyHostToDevice, m->ctx->stream));
     }
-    p2g_device(m, dp, dv, dm, n, r_p, n_active_out);
+    p2g_device(m, dp, dv, dm, n, r_p, n_active_out, nullptr);
     sync(m->ctx);
     MSBG_API_END
 }

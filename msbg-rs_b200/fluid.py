@@ -87,6 +87,14 @@ def particles_to_grid_device(mac: MacGrid, d_pos, d_vel, d_mass, n: int, r_p: fl
     return na.value
 
 
+def particles_to_grid_sorted_device(mac: MacGrid, d_pos, d_vel, d_mass, d_keys, n: int, r_p: float) -> int:
+    """particles_to_grid for Morton-sorted device arrays with their sorted keys."""
+    na = C.c_size_t()
+    call("msbg_p2g_sorted_device", mac.handle, ptr(d_pos), ptr(d_vel), ptr(d_mass), ptr(d_keys), int(n), float(r_p),
+         C.byref(na))
+    return na.value
+
+
 class MacSampler:
     """MacSampler::new(mac, bc) + sample::<Linear> (fluid/g2p.rs:15-32)."""
 

@@ -116,11 +116,14 @@ def check_p2g(msbg, ctx, oracle, pos, vel, mass, s, bsx, r_p):
         assert np.all((ulp_diff(got[3 + a], v_want) <= 3.0) | ~well_conditioned), ("velocity ulp", a)
         mom = got[3 + a].astype(np.float64) * got[a].astype(np.float64)
         assert np.all(np.abs(mom - terms64[3 + a]) <= 4 * EPS * absum[3 + a] + 1e-30), ("momentum", a)
-        # (2) against exact weights, (3) against the reference's f32 sums
-        for name, want in (("exact", exact[a]), ("f32 staged", ref32[a])):
-            err = np.abs(got[a].astype(np.float64) - want)
-            tol = (P2G_EXACT_TOL if name == "exact" else P2G_F32_TOL) * absum[a] + 1e-30
-            assert np.all(err <= tol), (name, a, (err / np.maximum(absum[a], 1e-30)).max())
+        # (3) against the reference's own f32 staged sums
+        err = np.abs(got[a].astype(np.float64) - ref32[a])
+        assert np.all(err <= P2G_F32_TOL * absum[a] + 1e-30), ("f32 staged", a, (err / np.maximum(absum[a], 1e-30)).max())
+        # (2) against exact-weight FP64: the reference's f32 weight near the
+        # edge of the support, w = (1 - d^2/r^2)^3, carries a cancellation
+        # error of ~eps * m per term, so the bound has an absolute part.
+        err = np.abs(got[a].astype(np.float64) - exact[a])
+        assert np.all(err <= P2G_EXACT_TOL * absum[a] + 8 * EPS * mass.max()), ("exact", a, err.max())
     return mac, got
 
 
@@ -148,6 +151,23 @@ def test_p2g_deterministic(msbg, ctx):
         msbg.particles_to_grid(mac, pos, vel, mass, 2.0)
         runs.append(device_channels(mac, mac.active_blocks()))
     assert np.array_equal(runs[0], runs[1])
+
+
+def test_p2g_sorted_input_identical(msbg, ctx):
+    """msbg_p2g_sorted_device on Morton-sorted particles == msbg_p2g."""
+    import torch
+    pos, vel, mass = make_particles(40000, 64, 13)
+    mac = msbg.MacGrid(ctx, 64, 64, 64, 16)
+    msbg.particles_to_grid(mac, pos, vel, mass, 2.0)
+    ref = device_channels(mac, mac.active_blocks())
+    keys, perm = msbg.morton_sort(ctx, pos)
+    tp, tv, tm = (torch.from_numpy(np.ascontiguousarray(x[perm])).cuda() for x in (pos, vel, mass))
+    tk = torch.from_numpy(keys.view(np.int64)).cuda()
+    mac2 = msbg.MacGrid(ctx, 64, 64, 64, 16)
+    msbg.particles_to_grid_sorted_device(mac2, tp, tv, tm, tk, len(pos), 2.0)
+    ctx.synchronize()
+    assert np.array_equal(mac2.active_blocks(), mac.active_blocks())
+    assert np.array_equal(device_channels(mac2, mac2.active_blocks()), ref)
 
 
 def test_p2g_rejects_out_of_domain(msbg, ctx):
