@@ -86,7 +86,7 @@ struct SweepArgs {
     void* payload;              // fine payload (grid dtype)
     const float* coarse;        // coarse payload (f32) for multiresolution halos
     const int32_t* nbr;         // [n][27]
-    const int32_t* bxyz;        // [n][3]
+    const int32_t* bxyz;        // [n][4]: block coords + flags (bit h-1: interior for halo h)
     int32_t sx, sy, sz;
     float empty, full, dt;
     int clamp01;
@@ -94,15 +94,58 @@ struct SweepArgs {
 
 template <int BSX> struct Lg { static constexpr int v = BSX == 4 ? 2 : BSX == 8 ? 3 : BSX == 16 ? 4 : 5; };
 
+// Vector load of 4 consecutive stored elements as floats.
+template <class E> struct Quad;
+template <> struct Quad<ElemF32> {
+    __device__ static float4 load(const float* p) { return *reinterpret_cast<const float4*>(p); }
+};
+template <> struct Quad<ElemU16> {
+    __device__ static float4 load(const uint16_t* p) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        return make_float4(ElemU16::load((uint16_t)(u.x & 0xffff)), ElemU16::load((uint16_t)(u.x >> 16)),
+                           ElemU16::load((uint16_t)(u.y & 0xffff)), ElemU16::load((uint16_t)(u.y >> 16)));
+    }
+};
+template <> struct Quad<ElemBF16> {
+    __device__ static float4 load(const uint16_t* p) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u), __uint_as_float(u.y << 16),
+                           __uint_as_float(u.y & 0xffff0000u));
+    }
+};
+
+// Shared-memory layout of the staged halo block: rows of RS floats with the
+// block's x = 0 at column 4 (16-byte aligned), HSX rows per plane.
+template <int BSX> struct Stage { static constexpr int RS = BSX + 8; };
+
+// Which staged cells a stencil reads: depth of a halo coordinate is 0 inside
+// the block, 1 or 2 outside.
+template <int ST> __device__ __forceinline__ bool row_needed(int dy, int dz) {
+    if (ST == MSBG_LAPLACIAN) return dy == 0 || dz == 0;
+    if (ST == MSBG_MEAN_CURVATURE) return true;
+    return dy == 0 || dz == 0 || (dy == 1 && dz == 1);
+}
+template <int ST> __device__ __forceinline__ bool xhalo_needed(int dx, int dy, int dz) {
+    if (ST == MSBG_LAPLACIAN) return dy == 0 && dz == 0;
+    if (ST == MSBG_MEAN_CURVATURE) return (dy == 0 && dz == 0) || (dy + dz == 1);
+    return (dy == 0 && dz == 0) || (dx == 1 && dy + dz == 1 && (dy == 1 || dz == 1));
+}
+
 template <class E, int BSX, int ST>
 __global__ void __launch_bounds__(BSX * BSX < 32 ? 32 : BSX * BSX)
 sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
     constexpr int HSX = BSX + 2 * HALO;
+    constexpr int RS = Stage<BSX>::RS;
+    constexpr int PL = HSX * RS;
+    constexpr int X0 = 4 - HALO;  // column of halo x = 0
     constexpr int LG = Lg<BSX>::v;
     constexpr int N = BSX * BSX * BSX;
-    extern __shared__ float h[];  // HSX^3 staged halo block
+    constexpr int QR = BSX / 4;  // float4 quads per row
+    extern __shared__ float4 h4[];
+    float* h = reinterpret_cast<float*>(h4);
     __shared__ int32_t nb[27];
+    __shared__ int32_t flags;
     __shared__ int8_t ok[3][HSX], dd[3][HSX], ll[3][HSX];
     typename E::T* payload = (typename E::T*)a.payload;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
@@ -110,54 +153,197 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const int pi = order[t];
         __syncthreads();  // the previous block's compute is done with h
-        for (int i = tid; i < 27 + 3 * HSX; i += nthr) {
-            if (i < 27) {
-                nb[i] = a.nbr[(size_t)pi * 27 + i];
-            } else {
-                int ax = (i - 27) / HSX, hh = (i - 27) % HSX;
+        if (tid < 27) nb[tid] = a.nbr[(size_t)pi * 27 + tid];
+        if (tid == 32 || (nthr <= 32 && tid == 31)) flags = a.bxyz[(size_t)pi * 4 + 3];
+        __syncthreads();
+        const bool interior = (flags >> (HALO - 1)) & 1;
+        if (interior) {
+            // Fast path: the block and its needed halo lie inside the domain,
+            // so every staged cell comes from one of the 27 neighbour slots
+            // without boundary resolution.  Centre and face rows move as
+            // 16-byte quads; all loads of a category are issued before its
+            // shared-memory stores.
+            constexpr int NT = BSX * BSX < 32 ? 32 : BSX * BSX;
+            constexpr int NC4 = N / 4;
+            constexpr int KC = (NC4 + NT - 1) / NT;
+            const int c13 = nb[13];
+            float4 vq[KC];
+#pragma unroll
+            for (int k = 0; k < KC; ++k) {
+                const int it = tid + k * NT;
+                if (it < NC4) vq[k] = Quad<E>::load(payload + (size_t)c13 * N + 4 * it);
+            }
+#pragma unroll
+            for (int k = 0; k < KC; ++k) {
+                const int it = tid + k * NT;
+                if (it < NC4) {
+                    const int q = it % QR, r = it / QR, y = r % BSX, z = r / BSX;
+                    h4[(((z + HALO) * HSX + y + HALO) * RS + 4 + 4 * q) >> 2] = vq[k];
+                }
+            }
+            // face rows: y and z planes at depth 1..HALO on both sides, and
+            // (19/25 taps) the four x-edge rows at depth 1
+            constexpr int NFACE = 4 * HALO * BSX * QR;
+            constexpr int NEDGE = ST == MSBG_LAPLACIAN ? 0 : 4 * QR;
+            constexpr int KF = (NFACE + NEDGE + NT - 1) / NT;
+            float4 vf[KF];
+            int df[KF];
+#pragma unroll
+            for (int k = 0; k < KF; ++k) {
+                const int it = tid + k * NT;
+                df[k] = -1;
+                if (it < NFACE) {
+                    const int q = it % QR, rr = it / QR;
+                    const int row = rr % BSX, pd = rr / BSX;        // pd: plane descriptor
+                    const int axis = pd / (2 * HALO), sd = pd % (2 * HALO);
+                    const int side = sd < HALO ? -1 : 1, d = sd < HALO ? sd + 1 : sd - HALO + 1;
+                    const int l = side < 0 ? BSX - d : d - 1;        // source coordinate
+                    const int hh = side < 0 ? HALO - d : HALO + BSX - 1 + d;
+                    int c, src, dst;
+                    if (axis == 0) {  // y plane: rows over z
+                        c = nb[13 + 3 * side];
+                        src = (l << LG) + (row << (2 * LG));
+                        dst = ((row + HALO) * HSX + hh) * RS + 4;
+                    } else {          // z plane: rows over y
+                        c = nb[13 + 9 * side];
+                        src = (row << LG) + (l << (2 * LG));
+                        dst = (hh * HSX + row + HALO) * RS + 4;
+                    }
+                    df[k] = dst + 4 * q;
+                    if (c >= 0) {
+                        vf[k] = Quad<E>::load(payload + (size_t)c * N + src + 4 * q);
+                    } else if (c <= kCodeCoarse0) {
+                        constexpr int CLG = LG > 0 ? LG - 1 : 0;
+                        const int lx = 4 * q, ly = axis == 0 ? l : row, lz = axis == 0 ? row : l;
+                        const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((ly >> 1) << CLG) + ((lz >> 1) << (2 * CLG));
+                        vf[k] = make_float4(cp[lx >> 1], cp[(lx + 1) >> 1], cp[(lx + 2) >> 1], cp[(lx + 3) >> 1]);
+                    } else {
+                        const float f = c == kCodeFull ? a.full : a.empty;
+                        vf[k] = make_float4(f, f, f, f);
+                    }
+                } else if (it < NFACE + NEDGE) {
+                    const int e = it - NFACE, q = e % QR, corner = e / QR;
+                    const int sy = (corner & 1) ? 1 : -1, sz = (corner & 2) ? 1 : -1;
+                    const int ly = sy < 0 ? BSX - 1 : 0, lz = sz < 0 ? BSX - 1 : 0;
+                    const int hy = sy < 0 ? HALO - 1 : HALO + BSX, hz = sz < 0 ? HALO - 1 : HALO + BSX;
+                    const int c = nb[13 + 3 * sy + 9 * sz];
+                    df[k] = (hz * HSX + hy) * RS + 4 + 4 * q;
+                    if (c >= 0) {
+                        vf[k] = Quad<E>::load(payload + (size_t)c * N + (ly << LG) + (lz << (2 * LG)) + 4 * q);
+                    } else if (c <= kCodeCoarse0) {
+                        constexpr int CLG = LG > 0 ? LG - 1 : 0;
+                        const int lx = 4 * q;
+                        const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((ly >> 1) << CLG) + ((lz >> 1) << (2 * CLG));
+                        vf[k] = make_float4(cp[lx >> 1], cp[(lx + 1) >> 1], cp[(lx + 2) >> 1], cp[(lx + 3) >> 1]);
+                    } else {
+                        const float f = c == kCodeFull ? a.full : a.empty;
+                        vf[k] = make_float4(f, f, f, f);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KF; ++k)
+                if (df[k] >= 0) h4[df[k] >> 2] = vf[k];
+            // x-halo cells: the x planes at depth 1..HALO (rows over y, z) and
+            // (19/25 taps) the y- and z-edges at x depth 1
+            constexpr int NXF = 2 * HALO * BSX * BSX;
+            constexpr int NXE = ST == MSBG_LAPLACIAN ? 0 : 8 * BSX;
+            constexpr int KX = (NXF + NXE + NT - 1) / NT;
+            float vx[KX];
+            int dx[KX];
+#pragma unroll
+            for (int k = 0; k < KX; ++k) {
+                const int it = tid + k * NT;
+                dx[k] = -1;
+                int c = kCodeEmpty, lx = 0, ly = 0, lz = 0;
+                if (it < NXF) {
+                    const int y = it % BSX, z = (it / BSX) % BSX, sd = it / (BSX * BSX);
+                    const int side = sd < HALO ? -1 : 1, d = sd < HALO ? sd + 1 : sd - HALO + 1;
+                    lx = side < 0 ? BSX - d : d - 1;
+                    ly = y;
+                    lz = z;
+                    const int hx = side < 0 ? HALO - d : HALO + BSX - 1 + d;
+                    c = nb[13 + side];
+                    dx[k] = ((z + HALO) * HSX + y + HALO) * RS + X0 + hx;
+                } else if (it < NXF + NXE) {
+                    const int e = it - NXF, j = e % BSX, kind = e / BSX;  // kind 0..3: y-edges, 4..7: z-edges
+                    const int sx = (kind & 1) ? 1 : -1, so = (kind & 2) ? 1 : -1;
+                    lx = sx < 0 ? BSX - 1 : 0;
+                    const int hx = sx < 0 ? HALO - 1 : HALO + BSX;
+                    const int ho = so < 0 ? HALO - 1 : HALO + BSX, lo = so < 0 ? BSX - 1 : 0;
+                    if (kind < 4) {  // edge along y at (x side, z side)
+                        ly = j;
+                        lz = lo;
+                        c = nb[13 + sx + 9 * so];
+                        dx[k] = (ho * HSX + j + HALO) * RS + X0 + hx;
+                    } else {         // edge along z at (x side, y side)
+                        ly = lo;
+                        lz = j;
+                        c = nb[13 + sx + 3 * so];
+                        dx[k] = ((j + HALO) * HSX + ho) * RS + X0 + hx;
+                    }
+                }
+                if (dx[k] >= 0) {
+                    if (c >= 0) {
+                        vx[k] = E::load(payload[(size_t)c * N + lx + (ly << LG) + (lz << (2 * LG))]);
+                    } else if (c <= kCodeCoarse0) {
+                        constexpr int CLG = LG > 0 ? LG - 1 : 0;
+                        vx[k] = a.coarse[(size_t)(kCodeCoarse0 - c) * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
+                    } else {
+                        vx[k] = c == kCodeFull ? a.full : a.empty;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KX; ++k)
+                if (dx[k] >= 0) h[dx[k]] = vx[k];
+        } else {
+            // General path (blocks at the domain edge): resolve every staged
+            // coordinate with the Neumann rule (solver.rs:205-209).
+            for (int i = tid; i < 3 * HSX; i += nthr) {
+                int ax = i / HSX, hh = i % HSX;
                 int32_t smax = ax == 0 ? a.sx : ax == 1 ? a.sy : a.sz;
-                int32_t b0 = a.bxyz[(size_t)pi * 3 + ax];
+                int32_t b0 = a.bxyz[(size_t)pi * 4 + ax];
                 int32_t g = b0 * BSX + hh - HALO, r;
-                bool o = resolve_axis(g, smax - 1, MSBG_NEUMANN, &r);  // solver.rs:205-209
+                bool o = resolve_axis(g, smax - 1, MSBG_NEUMANN, &r);
                 ok[ax][hh] = o;
                 dd[ax][hh] = (int8_t)((r >> LG) - b0 + 1);
                 ll[ax][hh] = (int8_t)(r & (BSX - 1));
             }
-        }
-        __syncthreads();
-        // Stage the halo block: one warp per (hz, hy) row, lanes along x.
-        for (int r = warp; r < HSX * HSX; r += nwarp) {
-            const int hz = r / HSX, hy = r % HSX;
-            const bool midy = hy >= HALO && hy < HALO + BSX, midz = hz >= HALO && hz < HALO + BSX;
-            for (int hx = lane; hx < HSX; hx += 32) {
-                const bool midx = hx >= HALO && hx < HALO + BSX;
-                const int nout = (!midx) + (!midy) + (!midz);
-                bool need;
-                if (ST == MSBG_LAPLACIAN) {
-                    need = nout <= 1;
-                } else if (ST == MSBG_MEAN_CURVATURE) {
-                    need = nout <= 2;
-                } else {
-                    const bool d1x = hx == HALO - 1 || hx == HALO + BSX, d1y = hy == HALO - 1 || hy == HALO + BSX,
-                               d1z = hz == HALO - 1 || hz == HALO + BSX;
-                    need = nout <= 1 || (nout == 2 && (midx || d1x) && (midy || d1y) && (midz || d1z));
-                }
-                if (!need) continue;
-                float v = a.empty;
-                if (ok[0][hx] && ok[1][hy] && ok[2][hz]) {
-                    const int c = nb[dd[0][hx] + 3 * dd[1][hy] + 9 * dd[2][hz]];
-                    const int lx = ll[0][hx], ly = ll[1][hy], lz = ll[2][hz];
-                    if (c >= 0) {
-                        v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
-                    } else if (c == kCodeFull) {
-                        v = a.full;
-                    } else if (c <= kCodeCoarse0) {
-                        constexpr int CLG = LG - 1;
-                        const int cs = kCodeCoarse0 - c;
-                        v = a.coarse[(size_t)cs * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
+            __syncthreads();
+            for (int r = warp; r < HSX * HSX; r += nwarp) {
+                const int hz = r / HSX, hy = r % HSX;
+                const bool midy = hy >= HALO && hy < HALO + BSX, midz = hz >= HALO && hz < HALO + BSX;
+                for (int hx = lane; hx < HSX; hx += 32) {
+                    const bool midx = hx >= HALO && hx < HALO + BSX;
+                    const int nout = (!midx) + (!midy) + (!midz);
+                    bool need;
+                    if (ST == MSBG_LAPLACIAN) {
+                        need = nout <= 1;
+                    } else if (ST == MSBG_MEAN_CURVATURE) {
+                        need = nout <= 2;
+                    } else {
+                        const bool d1x = hx == HALO - 1 || hx == HALO + BSX, d1y = hy == HALO - 1 || hy == HALO + BSX,
+                                   d1z = hz == HALO - 1 || hz == HALO + BSX;
+                        need = nout <= 1 || (nout == 2 && (midx || d1x) && (midy || d1y) && (midz || d1z));
                     }
+                    if (!need) continue;
+                    float v = a.empty;
+                    if (ok[0][hx] && ok[1][hy] && ok[2][hz]) {
+                        const int c = nb[dd[0][hx] + 3 * dd[1][hy] + 9 * dd[2][hz]];
+                        const int lx = ll[0][hx], ly = ll[1][hy], lz = ll[2][hz];
+                        if (c >= 0) {
+                            v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
+                        } else if (c == kCodeFull) {
+                            v = a.full;
+                        } else if (c <= kCodeCoarse0) {
+                            constexpr int CLG = LG - 1;
+                            const int cs = kCodeCoarse0 - c;
+                            v = a.coarse[(size_t)cs * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
+                        }
+                    }
+                    h[(hz * HSX + hy) * RS + X0 + hx] = v;
                 }
-                h[(hz * HSX + hy) * HSX + hx] = v;
             }
         }
         __syncthreads();
@@ -165,14 +351,69 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
             const int x = tid % BSX, y = tid / BSX;
             const int slot = nb[13];
             typename E::T* out = payload + (size_t)slot * N + x + y * BSX;
+            const int i0 = (HALO * HSX + (y + HALO)) * RS + X0 + x + HALO;  // z = 0
+            const float dt = a.dt;
+            const int clamp01 = a.clamp01;
+            if (ST == MSBG_LAPLACIAN) {
+                // taps along z slide through registers: 5 shared loads per output
+                float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
 #pragma unroll 4
-            for (int z = 0; z < BSX; ++z) {
-                const int i = ((z + HALO) * HSX + (y + HALO)) * HSX + (x + HALO);
-                float v;
-                if (ST == MSBG_LAPLACIAN) v = stencil_laplacian(h, i, HSX, HSX * HSX, a.dt, a.clamp01);
-                else if (ST == MSBG_MEAN_CURVATURE) v = stencil_meancurv(h, i, HSX, HSX * HSX, a.dt, a.clamp01);
-                else v = stencil_bilaplacian(h, i, HSX, HSX * HSX, a.dt, a.clamp01);
-                out[z * BSX * BSX] = E::store(v);
+                for (int z = 0; z < BSX; ++z) {
+                    const int i = i0 + z * PL;
+                    const float lx = h[i - 1], rx = h[i + 1], dyu = h[i - RS], dyd = h[i + RS];
+                    float nbs = lx + rx;
+                    nbs = nbs + dyu;
+                    nbs = nbs + dyd;
+                    nbs = nbs + zb;
+                    nbs = nbs + zf;
+                    const float lap = fmaf(c, -6.0f, nbs);
+                    const float fx = (rx - lx) * 0.5f, fy = (dyd - dyu) * 0.5f, fz = (zf - zb) * 0.5f;
+                    const float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
+                    const float nv = fmaf(dt * lap, g, c);
+                    out[z * BSX * BSX] = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                    zb = c;
+                    c = zf;
+                    if (z + 1 < BSX) zf = h[i + 2 * PL];
+                }
+            } else if (ST == MSBG_MEAN_CURVATURE) {
+                // plane z-1: cross (c, x-, x+, y-, y+); plane z: 3x3; plane z+1: cross
+                float pc = h[i0 - PL], pxm = h[i0 - PL - 1], pxp = h[i0 - PL + 1], pym = h[i0 - PL - RS], pyp = h[i0 - PL + RS];
+                float c = h[i0], cxm = h[i0 - 1], cxp = h[i0 + 1], cym = h[i0 - RS], cyp = h[i0 + RS];
+                float nc = h[i0 + PL], nxm = h[i0 + PL - 1], nxp = h[i0 + PL + 1], nym = h[i0 + PL - RS], nyp = h[i0 + PL + RS];
+#pragma unroll 2
+                for (int z = 0; z < BSX; ++z) {
+                    const int i = i0 + z * PL;
+                    const float xpyp = h[i + 1 + RS], xpym = h[i + 1 - RS], xmyp = h[i - 1 + RS], xmym = h[i - 1 - RS];
+                    // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
+                    const float f0 = c, f1 = cxm, f2 = cxp, f3 = cym, f4 = cyp, f5 = pc, f6 = nc;
+                    const float fx = (f2 - f1) * 0.5f, fy = (f4 - f3) * 0.5f, fz = (f6 - f5) * 0.5f;
+                    const float fxx = (f1 + f2) - 2.0f * f0, fyy = (f3 + f4) - 2.0f * f0, fzz = (f5 + f6) - 2.0f * f0;
+                    const float d1 = xpyp, d2 = xpym, d3 = xmyp, d4 = xmym;
+                    const float d5 = nxp, d6 = pxp, d7 = nxm, d8 = pxm;
+                    const float d9 = nyp, d10 = pyp, d11 = nym, d12 = pym;
+                    const float fyx = (((d1 - d2) - d3) + d4) * 0.25f;
+                    const float fzx = (((d5 - d6) - d7) + d8) * 0.25f;
+                    const float fzy = (((d9 - d10) - d11) + d12) * 0.25f;
+                    const float cross = (fx * (fy * fyx) + fx * (fz * fzx)) + fy * (fz * fzy);
+                    const float hnum = fmaf(fy * fy + fz * fz, fxx, fmaf(fx * fx + fz * fz, fyy, fmaf(fx * fx + fy * fy, fzz, -2.0f * cross)));
+                    const float grad = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+                    const float hc = grad > 1e-7f ? hnum / grad : 0.0f;
+                    const float d = clampf(dt * hc, -0.1f, 0.1f);
+                    const float nv = f0 + d;
+                    out[z * BSX * BSX] = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                    pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
+                    c = nc; cxm = nxm; cxp = nxp; cym = nym; cyp = nyp;
+                    if (z + 1 < BSX) {
+                        const int j = i + 2 * PL;
+                        nc = h[j]; nxm = h[j - 1]; nxp = h[j + 1]; nym = h[j - RS]; nyp = h[j + RS];
+                    }
+                }
+            } else {
+#pragma unroll 4
+                for (int z = 0; z < BSX; ++z) {
+                    const int i = i0 + z * PL;
+                    out[z * BSX * BSX] = E::store(stencil_bilaplacian(h, i, RS, PL, dt, clamp01));
+                }
             }
         }
     }
@@ -182,7 +423,7 @@ template <class E, int BSX, int ST>
 static void launch_phase(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
     constexpr int HSX = BSX + 2 * HALO;
-    const size_t smem = sizeof(float) * HSX * HSX * HSX;
+    const size_t smem = sizeof(float) * HSX * HSX * Stage<BSX>::RS;
     static bool attr_set = false;  // per instantiation
     if (!attr_set) {
         CUDA_CHECK(cudaFuncSetAttribute(sweep_phase_kernel<E, BSX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -261,6 +502,15 @@ static SweepPlan* get_plan(msbg_grid* g, msbg_grid* coarse, const uint8_t* level
             bxyz.push_back((int32_t)bx);
             bxyz.push_back((int32_t)by);
             bxyz.push_back((int32_t)bz);
+            // interior: the block and a halo of h cells lie inside the domain
+            int32_t fl = 0;
+            for (int hh = 1; hh <= 2; ++hh) {
+                const int64_t B = g->bsx;
+                bool in = bx * B - hh >= 0 && by * B - hh >= 0 && bz * B - hh >= 0 && (bx + 1) * B + hh <= (int64_t)g->sx &&
+                          (by + 1) * B + hh <= (int64_t)g->sy && (bz + 1) * B + hh <= (int64_t)g->sz;
+                if (in) fl |= 1 << (hh - 1);
+            }
+            bxyz.push_back(fl);
             for (int k = 0; k < 27; ++k) {
                 int64_t X = bx + k % 3 - 1, Y = by + (k / 3) % 3 - 1, Z = bz + k / 9 - 1;
                 int32_t code = kCodeEmpty;
