@@ -232,6 +232,39 @@ int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, i
  * to the 2^3 mean. */
 int msbg_downsample_avg(msbg_grid* dst, msbg_grid* src);
 
+/* ---- Poisson pressure solve (no crate counterpart) ------------------------
+ * The crate's roadmap specifies but does not implement the pressure solve
+ * (docs/roadmap.md:608-702): the 7-point operator y = D x - sum_nb x and the
+ * relaxation y = w (b + sum_nb x) D^-1 + (1 - w) x, D = 6, zero Dirichlet
+ * values outside the active blocks.  Unknowns are the cells of the active
+ * blocks in ascending block-id order, [n_active][bsx^3] f32 (the block
+ * payload layout).  The multigrid hierarchy halves the block size down to 2,
+ * then halves the block grid, down to <= 1024 cells solved by a dense FP64
+ * inverse; level operators are the Galerkin products (0.5^l times the 7-point
+ * stencil).  Dot products and norms are FP64. */
+int msbg_poisson_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, const uint64_t* active,
+                        size_t n, msbg_poisson** out);
+int msbg_poisson_destroy(msbg_poisson* p);
+/* Cells per level (finest first). */
+int msbg_poisson_levels(const msbg_poisson* p, uint64_t* cells_out, size_t cap, size_t* n_levels);
+/* Pre/post weighted-Jacobi sweeps of the V-cycle and their weight (default 2, 2, 2/3). */
+int msbg_poisson_set_smoother(msbg_poisson* p, int nu1, int nu2, float omega);
+int msbg_poisson_matvec_device(msbg_poisson* p, const float* d_x, float* d_y);
+/* `sweeps` weighted-Jacobi sweeps of A x = b on the finest level, in place. */
+int msbg_poisson_jacobi_device(msbg_poisson* p, float* d_x, const float* d_b, float omega, int sweeps);
+/* r = b - A x; *norm_out (optional, host) = ||r||_2 in FP64. */
+int msbg_poisson_residual_device(msbg_poisson* p, const float* d_x, const float* d_b, float* d_r, double* norm_out);
+/* One V-cycle for A x = b, x updated in place. */
+int msbg_poisson_vcycle_device(msbg_poisson* p, float* d_x, const float* d_b);
+int msbg_poisson_dot_device(msbg_poisson* p, const float* d_a, const float* d_b, double* out);
+/* method 0: V-cycles; 1: V-cycle-preconditioned CG.  Iterates from x until
+ * ||b - A x|| <= tol ||b|| or max_iter.  history (optional, max_iter entries)
+ * receives the relative residual after each iteration. */
+int msbg_poisson_solve_device(msbg_poisson* p, int method, float* d_x, const float* d_b, double tol, int max_iter,
+                              int* iters_out, double* rel_res_out, double* history);
+int msbg_poisson_solve(msbg_poisson* p, int method, float* x, const float* b, double tol, int max_iter,
+                       int* iters_out, double* rel_res_out, double* history);
+
 #ifdef __cplusplus
 }
 #endif

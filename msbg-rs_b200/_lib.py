@@ -92,6 +92,17 @@ SIGNATURES = {
     "msbg_g2p_blend_device": [_P, _P, _P, _P, _SZ, _F, _P],
     "msbg_sample_linear": [_P, _P, _SZ, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_poisson_create": [_P, _U64, _U64, _U64, _I, _P, _SZ, C.POINTER(_P)],
+    "msbg_poisson_destroy": [_P],
+    "msbg_poisson_levels": [_P, _P, _SZ, _SZP],
+    "msbg_poisson_set_smoother": [_P, _I, _I, _F],
+    "msbg_poisson_matvec_device": [_P, _P, _P],
+    "msbg_poisson_jacobi_device": [_P, _P, _P, _F, _I],
+    "msbg_poisson_residual_device": [_P, _P, _P, _P, C.POINTER(C.c_double)],
+    "msbg_poisson_vcycle_device": [_P, _P, _P],
+    "msbg_poisson_dot_device": [_P, _P, _P, C.POINTER(C.c_double)],
+    "msbg_poisson_solve_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
+    "msbg_poisson_solve": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
 }
 
 _lib = None

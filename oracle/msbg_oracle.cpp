@@ -924,38 +924,52 @@ void or_downsample_avg(const float* fine, int64_t n_blocks, int bsx, float* coar
 
 // ===========================================================================
 // FP64 Poisson oracle (no reference implementation: parity unpinned).
-// Problem: unknowns are the cells of the active blocks of one level (block
-// size bs, `active` = block ids on an nx*ny*nz block grid); cells outside the
-// active blocks are zero (Dirichlet).  Operator at level l:
-//   (A x)_c = s_l * (6 x_c - sum_{6 nb} x_nb),  s_l = 0.5^l
-// which is the Galerkin operator R A P for piecewise-constant prolongation P
-// and averaging restriction R = P^T / 8 (docs/roadmap.md:618-627 gives the
-// matvec `y = D x - sum nb` and relax `y = w (b + sum nb) D^-1 + (1-w) x`).
+//
+// Problem: the unknowns are the cells of the active blocks (block size bs on
+// an nx*ny*nz block grid); every other cell is zero (Dirichlet).  At level l
+//   (A_l x)_c = s_l * (6 x_c - sum of the x of its active face neighbours),
+//   s_l = 0.5^l,
+// the Galerkin operator R A P for piecewise-constant prolongation P and
+// averaging restriction R = P^T / 8 (docs/roadmap.md:618-627 states the
+// matvec `y = D x - sum nb` and relaxation `y = w (b + sum nb) D^-1 + (1-w) x`).
+// Hierarchy: level l+1 has cells of twice the size.  While bs_l >= 4 the
+// block grid is kept and the block size halves ("same grid" levels); from
+// bs_l == 2 on, the block grid halves and the block size stays 2 (a coarse
+// block is active when any of its 8 child blocks is).  Coarsening stops at
+// <= kPoissonDirect cells, which are solved directly (dense Cholesky, FP64).
+// V-cycle: nu1 weighted-Jacobi sweeps, residual, restriction, recursion,
+// prolongation-correction, nu2 sweeps.
 // ===========================================================================
+static const int64_t kPoissonDirect = 1024;
+static double g_corr = 1.0;  // coarse-correction scale of the V-cycle
+
 struct PLevel {
     int bs, lg;
-    int64_t n_active;
-    std::vector<int64_t> nbr;  // [n_active][6] slot of -x,+x,-y,+y,-z,+z neighbour block or -1
+    int64_t nx, ny, nz;
+    std::vector<int64_t> bids;  // sorted active block ids
+    std::vector<int64_t> nbr;   // [n][6] slot of the -x,+x,-y,+y,-z,+z neighbour block or -1
+    std::vector<int64_t> parent;  // [n] slot of the parent block at level l+1
     double scale;
+    int64_t n() const { return (int64_t)bids.size(); }
+    int64_t cells() const { return n() * bs * bs * bs; }
 };
 
-static void build_nbr(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz,
-                      std::vector<int64_t>& nbr) {
-    std::vector<int64_t> slot((size_t)(nx * ny * nz), -1);
-    for (int64_t k = 0; k < n_active; ++k) slot[active[k]] = k;
-    nbr.assign((size_t)n_active * 6, -1);
-    for (int64_t k = 0; k < n_active; ++k) {
-        int64_t b = active[k], bx = b % nx, by = (b / nx) % ny, bz = b / (nx * ny);
+static void build_nbr(PLevel& L) {
+    std::vector<int64_t> slot((size_t)(L.nx * L.ny * L.nz), -1);
+    for (int64_t k = 0; k < L.n(); ++k) slot[L.bids[k]] = k;
+    L.nbr.assign((size_t)L.n() * 6, -1);
+    for (int64_t k = 0; k < L.n(); ++k) {
+        int64_t b = L.bids[k], bx = b % L.nx, by = (b / L.nx) % L.ny, bz = b / (L.nx * L.ny);
         const int64_t d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
         for (int f = 0; f < 6; ++f) {
             int64_t X = bx + d[f][0], Y = by + d[f][1], Z = bz + d[f][2];
-            if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
-            nbr[k * 6 + f] = slot[X + Y * nx + Z * nx * ny];
+            if (X < 0 || Y < 0 || Z < 0 || X >= L.nx || Y >= L.ny || Z >= L.nz) continue;
+            L.nbr[k * 6 + f] = slot[X + Y * L.nx + Z * L.nx * L.ny];
         }
     }
 }
 
-// value of cell (x,y,z) relative to block k, where each coordinate may be -1 or bs
+// value of cell (cx,cy,cz) relative to block k, where one coordinate may be -1 or bs
 static inline double cell_at(const PLevel& L, const double* x, int64_t k, int cx, int cy, int cz) {
     int64_t kk = k;
     if (cx < 0) { kk = L.nbr[k * 6 + 0]; cx += L.bs; }
@@ -982,7 +996,7 @@ static inline double nbsum(const PLevel& L, const double* x, int64_t k, int cx, 
 static void p_matvec(const PLevel& L, const double* x, double* y) {
     const size_t N = (size_t)L.bs * L.bs * L.bs;
 #pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < L.n_active; ++k)
+    for (int64_t k = 0; k < L.n(); ++k)
         for (int cz = 0; cz < L.bs; ++cz)
             for (int cy = 0; cy < L.bs; ++cy)
                 for (int cx = 0; cx < L.bs; ++cx) {
@@ -992,11 +1006,11 @@ static void p_matvec(const PLevel& L, const double* x, double* y) {
 }
 
 static void p_jacobi(const PLevel& L, double* x, const double* b, double omega, int sweeps, std::vector<double>& tmp) {
-    const size_t N = (size_t)L.bs * L.bs * L.bs, tot = N * L.n_active;
+    const size_t N = (size_t)L.bs * L.bs * L.bs, tot = N * L.n();
     tmp.resize(tot);
     for (int s = 0; s < sweeps; ++s) {
 #pragma omp parallel for schedule(static)
-        for (int64_t k = 0; k < L.n_active; ++k)
+        for (int64_t k = 0; k < L.n(); ++k)
             for (int cz = 0; cz < L.bs; ++cz)
                 for (int cy = 0; cy < L.bs; ++cy)
                     for (int cx = 0; cx < L.bs; ++cx) {
@@ -1008,27 +1022,63 @@ static void p_jacobi(const PLevel& L, double* x, const double* b, double omega, 
     }
 }
 
+// global cell (gx,gy,gz) -> index into the level's array, or -1
+static inline int64_t cell_index(const PLevel& L, const std::vector<int64_t>& slot, int64_t gx, int64_t gy, int64_t gz) {
+    int64_t bx = gx >> L.lg, by = gy >> L.lg, bz = gz >> L.lg;
+    if (bx >= L.nx || by >= L.ny || bz >= L.nz) return -1;
+    int64_t s = slot[bx + by * L.nx + bz * L.nx * L.ny];
+    if (s < 0) return -1;
+    int m = L.bs - 1;
+    return s * L.bs * L.bs * L.bs + ((gx & m) | ((gy & m) << L.lg) | ((gz & m) << (2 * L.lg)));
+}
+
 struct PHier {
     std::vector<PLevel> lv;
-    std::vector<double> chol;  // dense Cholesky of the coarsest operator (row-major lower)
-    int64_t nc;
+    std::vector<std::vector<int64_t>> slot;  // per level: dense bid -> slot
+    std::vector<double> chol;
+    int64_t nc = 0;
 };
 
-static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz,
-                       int bs, int max_levels) {
+static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs,
+                       int max_levels) {
     H.lv.clear();
-    for (int l = 0; l < max_levels && (bs >> l) >= 1; ++l) {
-        PLevel L;
-        L.bs = bs >> l; L.lg = ilog2(L.bs); L.n_active = n_active; L.scale = std::ldexp(1.0, -l);
-        build_nbr(active, n_active, nx, ny, nz, L.nbr);
-        H.lv.push_back(L);
+    H.slot.clear();
+    PLevel L0;
+    L0.bs = bs; L0.lg = ilog2(bs); L0.nx = nx; L0.ny = ny; L0.nz = nz; L0.scale = 1.0;
+    L0.bids.assign(active, active + n_active);
+    std::sort(L0.bids.begin(), L0.bids.end());
+    L0.bids.erase(std::unique(L0.bids.begin(), L0.bids.end()), L0.bids.end());
+    H.lv.push_back(L0);
+    while ((int)H.lv.size() < max_levels && H.lv.back().cells() > kPoissonDirect) {
+        const PLevel& F = H.lv.back();
+        PLevel C;
+        C.scale = F.scale * 0.5;
+        if (F.bs >= 4) {
+            C.bs = F.bs / 2; C.nx = F.nx; C.ny = F.ny; C.nz = F.nz;
+            C.bids = F.bids;
+        } else {
+            C.bs = F.bs; C.nx = (F.nx + 1) / 2; C.ny = (F.ny + 1) / 2; C.nz = (F.nz + 1) / 2;
+            for (int64_t b : F.bids) {
+                int64_t bx = b % F.nx, by = (b / F.nx) % F.ny, bz = b / (F.nx * F.ny);
+                C.bids.push_back((bx >> 1) + (by >> 1) * C.nx + (bz >> 1) * C.nx * C.ny);
+            }
+            std::sort(C.bids.begin(), C.bids.end());
+            C.bids.erase(std::unique(C.bids.begin(), C.bids.end()), C.bids.end());
+        }
+        C.lg = ilog2(C.bs);
+        H.lv.push_back(C);
     }
-    // Dense Cholesky of the coarsest level when it is small enough.
+    for (auto& L : H.lv) {
+        build_nbr(L);
+        std::vector<int64_t> sl((size_t)(L.nx * L.ny * L.nz), -1);
+        for (int64_t k = 0; k < L.n(); ++k) sl[L.bids[k]] = k;
+        H.slot.push_back(sl);
+    }
     const PLevel& C = H.lv.back();
-    const int64_t n = C.n_active * C.bs * C.bs * C.bs;
+    const int64_t n = C.cells();
     H.nc = n;
     H.chol.clear();
-    if (n > 6000) return;
+    if (n > 4 * kPoissonDirect) return;  // max_levels cut the hierarchy short: iterate instead
     std::vector<double> A((size_t)n * n, 0.0), e(n, 0.0), col(n);
     for (int64_t j = 0; j < n; ++j) {
         e[j] = 1.0;
@@ -1042,9 +1092,9 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
         d = std::sqrt(d);
         A[(size_t)j * n + j] = d;
         for (int64_t i = j + 1; i < n; ++i) {
-            double s = A[(size_t)i * n + j];
-            for (int64_t k = 0; k < j; ++k) s -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
-            A[(size_t)i * n + j] = s / d;
+            double s2 = A[(size_t)i * n + j];
+            for (int64_t k = 0; k < j; ++k) s2 -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
+            A[(size_t)i * n + j] = s2 / d;
         }
     }
     H.chol.swap(A);
@@ -1053,7 +1103,7 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
 static void coarse_solve(const PHier& H, double* x, const double* b) {
     const int64_t n = H.nc;
     const PLevel& C = H.lv.back();
-    if (H.chol.empty()) {  // fall back to many Jacobi sweeps (large coarsest level)
+    if (H.chol.empty()) {
         std::vector<double> tmp;
         std::fill(x, x + n, 0.0);
         p_jacobi(C, x, b, 2.0 / 3.0, 400, tmp);
@@ -1077,30 +1127,35 @@ static void vcycle(const PHier& H, int l, double* x, const double* b, int nu1, i
     if (l == (int)H.lv.size() - 1) { coarse_solve(H, x, b); return; }
     const PLevel& F = H.lv[l];
     const PLevel& C = H.lv[l + 1];
-    const size_t N = (size_t)F.bs * F.bs * F.bs, NC = (size_t)C.bs * C.bs * C.bs;
-    const size_t tot = N * F.n_active, totc = NC * C.n_active;
-    std::vector<double> tmp, r(tot), bc(totc), xc(totc, 0.0);
+    const size_t N = (size_t)F.bs * F.bs * F.bs;
+    const size_t tot = F.cells(), totc = C.cells();
+    std::vector<double> tmp, r(tot), bc(totc, 0.0), xc(totc, 0.0);
     p_jacobi(F, x, b, omega, nu1, tmp);
     p_matvec(F, x, r.data());
     for (size_t i = 0; i < tot; ++i) r[i] = b[i] - r[i];
-    for (int64_t k = 0; k < F.n_active; ++k)  // restriction: 2^3 average
-        for (int cz = 0; cz < C.bs; ++cz)
-            for (int cy = 0; cy < C.bs; ++cy)
-                for (int cx = 0; cx < C.bs; ++cx) {
-                    double s = 0.0;
-                    for (int dz = 0; dz < 2; ++dz)
-                        for (int dy = 0; dy < 2; ++dy)
-                            for (int dx = 0; dx < 2; ++dx)
-                                s += r[k * N + ((size_t)(2 * cx + dx) | ((size_t)(2 * cy + dy) << F.lg) | ((size_t)(2 * cz + dz) << (2 * F.lg)))];
-                    bc[k * NC + ((size_t)cx | ((size_t)cy << C.lg) | ((size_t)cz << (2 * C.lg)))] = s / 8.0;
-                }
-    vcycle(H, l + 1, xc.data(), bc.data(), nu1, nu2, omega);
-    for (int64_t k = 0; k < F.n_active; ++k)  // prolongation: injection
+    // restriction: each fine cell adds 1/8 of its residual to its parent cell
+    for (int64_t k = 0; k < F.n(); ++k) {
+        int64_t bid = F.bids[k], bx = bid % F.nx, by = (bid / F.nx) % F.ny, bz = bid / (F.nx * F.ny);
         for (int cz = 0; cz < F.bs; ++cz)
             for (int cy = 0; cy < F.bs; ++cy)
-                for (int cx = 0; cx < F.bs; ++cx)
-                    x[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))] +=
-                        xc[k * NC + ((size_t)(cx >> 1) | ((size_t)(cy >> 1) << C.lg) | ((size_t)(cz >> 1) << (2 * C.lg)))];
+                for (int cx = 0; cx < F.bs; ++cx) {
+                    int64_t gx = bx * F.bs + cx, gy = by * F.bs + cy, gz = bz * F.bs + cz;
+                    int64_t ci = cell_index(C, H.slot[l + 1], gx >> 1, gy >> 1, gz >> 1);
+                    bc[ci] += r[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))];
+                }
+    }
+    for (size_t i = 0; i < totc; ++i) bc[i] /= 8.0;
+    vcycle(H, l + 1, xc.data(), bc.data(), nu1, nu2, omega);
+    for (int64_t k = 0; k < F.n(); ++k) {  // prolongation: injection
+        int64_t bid = F.bids[k], bx = bid % F.nx, by = (bid / F.nx) % F.ny, bz = bid / (F.nx * F.ny);
+        for (int cz = 0; cz < F.bs; ++cz)
+            for (int cy = 0; cy < F.bs; ++cy)
+                for (int cx = 0; cx < F.bs; ++cx) {
+                    int64_t gx = bx * F.bs + cx, gy = by * F.bs + cy, gz = bz * F.bs + cz;
+                    int64_t ci = cell_index(C, H.slot[l + 1], gx >> 1, gy >> 1, gz >> 1);
+                    x[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))] += g_corr * xc[ci];
+                }
+    }
     p_jacobi(F, x, b, omega, nu2, tmp);
 }
 
@@ -1111,33 +1166,52 @@ static double dot(const double* a, const double* b, size_t n) {
     return s;
 }
 
+static PLevel single_level(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs, double scale) {
+    PLevel L;
+    L.bs = bs; L.lg = ilog2(bs); L.nx = nx; L.ny = ny; L.nz = nz; L.scale = scale;
+    L.bids.assign(active, active + n_active);  // caller order = slot order
+    build_nbr(L);
+    return L;
+}
+
+}  // extern "C" (reopened below)
+extern "C" {
+
 void or_poisson_matvec(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs,
                        double scale, const double* x, double* y) {
-    PLevel L;
-    L.bs = bs; L.lg = ilog2(bs); L.n_active = n_active; L.scale = scale;
-    build_nbr(active, n_active, nx, ny, nz, L.nbr);
+    PLevel L = single_level(active, n_active, nx, ny, nz, bs, scale);
     p_matvec(L, x, y);
 }
 
 void or_poisson_jacobi(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs,
                        double scale, double omega, int sweeps, double* x, const double* b) {
-    PLevel L;
-    L.bs = bs; L.lg = ilog2(bs); L.n_active = n_active; L.scale = scale;
-    build_nbr(active, n_active, nx, ny, nz, L.nbr);
+    PLevel L = single_level(active, n_active, nx, ny, nz, bs, scale);
     std::vector<double> tmp;
     p_jacobi(L, x, b, omega, sweeps, tmp);
 }
 
-// mode 0: plain V-cycles; mode 1: V-cycle-preconditioned CG.  Iterates until
-// ||b - A x|| <= tol ||b|| or max_iter; writes the residual history, returns
-// the iteration count.
+void or_poisson_set_correction(double c) { g_corr = c; }
+
+// Number of levels and cells per level of the hierarchy (for tests).
+int or_poisson_levels(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs, int max_levels,
+                      int64_t* cells_out) {
+    PHier H;
+    build_hier(H, active, n_active, nx, ny, nz, bs, max_levels);
+    for (size_t l = 0; l < H.lv.size(); ++l) cells_out[l] = H.lv[l].cells();
+    return (int)H.lv.size();
+}
+
+// mode 0: plain V-cycles; mode 1: V-cycle-preconditioned CG.  The unknowns
+// are ordered by ascending block id (x, b are [n_active][bs^3]).  Iterates
+// until ||b - A x|| <= tol ||b|| or max_iter; writes the relative residual
+// history, returns the iteration count.
 int or_poisson_solve(const int64_t* active, int64_t n_active, int64_t nx, int64_t ny, int64_t nz, int bs,
                      int max_levels, int nu1, int nu2, double omega, int mode, double tol, int max_iter,
                      double* x, const double* b, double* hist) {
     PHier H;
     build_hier(H, active, n_active, nx, ny, nz, bs, max_levels);
     const PLevel& F = H.lv[0];
-    const size_t tot = (size_t)F.n_active * F.bs * F.bs * F.bs;
+    const size_t tot = F.cells();
     std::vector<double> r(tot), z(tot), p(tot), q(tot);
     const double bn = std::sqrt(dot(b, b, tot));
     if (bn == 0.0) { std::fill(x, x + tot, 0.0); return 0; }

@@ -71,6 +71,8 @@ def lib() -> C.CDLL:
         _lib.or_poisson_solve.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.or_poisson_solve.restype = C.c_int
+        _lib.or_poisson_levels.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_void_p]
+        _lib.or_poisson_levels.restype = C.c_int
         _lib.or_num_threads.restype = C.c_int
     return _lib
 
@@ -291,9 +293,18 @@ def poisson_jacobi(active, nx, ny, nz, bs, x, b, omega, sweeps, scale=1.0):
     return xx
 
 
+def poisson_levels(active, nx, ny, nz, bs, max_levels=32):
+    a = np.ascontiguousarray(np.unique(np.asarray(active, np.int64)))
+    cells = np.zeros(64, np.int64)
+    n = lib().or_poisson_levels(_p(a), len(a), nx, ny, nz, bs, max_levels, _p(cells))
+    return cells[:n]
+
+
 def poisson_solve(active, nx, ny, nz, bs, b, mode=0, tol=1e-6, max_iter=200, nu1=2, nu2=2, omega=2.0 / 3.0,
-                  max_levels=8):
-    a = np.ascontiguousarray(active, np.int64)
+                  max_levels=32):
+    """FP64 V-cycle (mode 0) or MG-preconditioned CG (mode 1); unknowns in
+    ascending block-id order."""
+    a = np.ascontiguousarray(np.unique(np.asarray(active, np.int64)))
     bb = np.ascontiguousarray(b, np.float64)
     x = np.zeros_like(bb)
     hist = np.zeros(max_iter + 1, np.float64)

@@ -320,3 +320,7 @@ def test_poisson_oracle_converges(oracle):
         assert hist[-1] <= 1e-8, (mode, hist)
         ax = oracle.poisson_matvec(active, nx, nx, nx, 8, x)
         assert np.linalg.norm(ax - b) <= 1e-7 * np.linalg.norm(b)
+    # hierarchy: 8^3 blocks halve to 4, 2, then the block grid halves
+    cells = oracle.poisson_levels(active, nx, nx, nx, 8)
+    assert list(cells[:3]) == [len(active) * 512, len(active) * 64, len(active) * 8]
+    assert cells[-1] <= 1024
