@@ -76,8 +76,8 @@ int msbg_ctx_synchronize(msbg_ctx* ctx);
 int msbg_ctx_stream(msbg_ctx* ctx, void** stream_out);
 /* Number of kernels this library launched on the context since creation. */
 int msbg_ctx_kernel_launches(msbg_ctx* ctx, uint64_t* out);
-/* Per-kernel timing with CUDA events on the context stream (SURVEY-style
- * phase profiling; no crate counterpart beyond MSBG_BUCKET_PROFILE,
+/* Per-kernel timing with CUDA events on the context stream (phase profiling;
+ * no crate counterpart beyond MSBG_BUCKET_PROFILE,
  * particles/sort.rs:184-262).  While enabled every kernel launch is bracketed
  * by two events.  The report lists "name launches total_ms" per kernel; it
  * synchronises the stream.  reset != 0 clears the totals after reporting. */
@@ -195,7 +195,8 @@ int msbg_mac_zero_blocks(msbg_mac* mac, const uint64_t* bids, size_t n);
  * w = max(1 - d^2/r_p^2, 0)^3, then normalize_velocity.  pos, vel are [n][3],
  * mass [n] (f32).  Sums are accumulated per particle block in FP64 and
  * combined across blocks in a fixed order: deterministic, no float atomics.
- * Domain extents must be multiples of bsx; 0 < r_p <= bsx / 2.
+ * bsx is 8 or 16, domain extents are multiples of bsx, 0 < r_p <= 3 and
+ * ceil(r_p) <= bsx / 2.
  * *n_active_out (may be NULL) receives the size of the active block set. */
 int msbg_p2g(msbg_mac* mac, const float* pos, const float* vel, const float* mass, size_t n, float r_p,
              size_t* n_active_out);
