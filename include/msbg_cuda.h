@@ -165,6 +165,19 @@ int msbg_sort_block_list_morton(msbg_ctx* ctx, uint64_t* blocks, size_t n, uint6
 int msbg_morton_sort(msbg_ctx* ctx, const float* pos, size_t n, uint64_t* keys_out, uint32_t* perm_out);
 int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out,
                             uint32_t* d_perm_out);
+/* No counterpart in the reference.  msbg_morton_sort_device without any
+ * device allocation, for callers that cannot allocate on the calling path
+ * (real-time loops, allocator callbacks, processes whose device memory is
+ * reserved up front).  Its temporaries live in a fixed scratch array built
+ * into the library (about 5 MB, held by every device that loads the library
+ * until exit), so n is limited to 262144 particles; larger n returns
+ * MSBG_ERR_ARG.  The first call on a device looks up the array's device
+ * address: make it before any stream capture.  Calls share the array, so
+ * calls whose GPU work overlaps in time race; calls ordered on one stream do
+ * not.  Returns MSBG_ERR_STATE while per-kernel timing is enabled (timing
+ * creates CUDA events). */
+int msbg_morton_sort_noalloc_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out,
+                                    uint32_t* d_perm_out);
 /* Applies a sort permutation to per-particle data: dst[i] = src[perm[i]] for
  * items of `width` floats (the payload gather of bucket_particles,
  * fluid/mod.rs:71-91, and bucket_by_block, particles/sort.rs:274-285). */

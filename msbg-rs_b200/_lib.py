@@ -74,6 +74,7 @@ SIGNATURES = {
     "msbg_sort_block_list_morton": [_P, _P, _SZ, _U64, _U64, _P, _SZ, _I],
     "msbg_morton_sort": [_P, _P, _SZ, _P, _P],
     "msbg_morton_sort_device": [_P, _P, _SZ, _P, _P],
+    "msbg_morton_sort_noalloc_device": [_P, _P, _SZ, _P, _P],
     "msbg_permute_device": [_P, _P, _SZ, _I, _P, _P],
     "msbg_bucket_indices": [_P, _P, _SZ, _P, _P, _P, _SZP],
     "msbg_bucket_indices_device": [_P, _P, _SZ, _P, _P, _P, _SZP],

@@ -8,6 +8,7 @@
 // and writes them to digit base + tile prefix + rank.  Stable, so sorting
 // (key, index) pairs reproduces a stable CPU sort exactly.
 #include <algorithm>
+#include <mutex>
 
 #include "sort.cuh"
 
@@ -388,6 +389,41 @@ size_t bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n, ui
     return sorted_segments(ctx, sk, n, 0, d_blocks, d_starts, ScratchLayout::at<char>(base, ot));
 }
 
+// ---- Morton sort without device allocation ----------------------------------
+// Some callers cannot allocate device memory on the calling path: hosts that
+// embed the library in a real-time loop, inside a memory-pool-managed
+// allocator callback, or in a process whose device memory is fully reserved
+// up front.  For them msbg_morton_sort_noalloc_device sorts up to
+// kNoAllocMaxParticles particles using a fixed scratch area that is part of
+// the library image: a file-scope device array, allocated by the CUDA driver
+// when the library's module is loaded on a device and held by every device
+// that loads the library until the process exits (about 5 MB).
+constexpr size_t kNoAllocMaxParticles = size_t(1) << 18;
+constexpr size_t a256c(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kNoAllocKeysBytes = a256c(kNoAllocMaxParticles * 8);
+constexpr size_t kNoAllocSortBytes = a256c(kNoAllocMaxParticles * 8) + a256c(kNoAllocMaxParticles * 4) +
+                                     a256c(256 * ((kNoAllocMaxParticles + RS_TILE - 1) / RS_TILE) * 4) + a256c(256 * 4);
+constexpr size_t kNoAllocScratchBytes = kNoAllocKeysBytes + kNoAllocSortBytes + 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current (the host-side name of the array is not a device address).
+static std::mutex g_noalloc_mu;
+static char* g_noalloc_ptr[128] = {};
+
+static char* noalloc_scratch(int device) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    MSBG_REQUIRE(device >= 0 && device < 128, "device ordinal out of range for the fixed scratch table");
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            MSBG_THROW(MSBG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = (char*)p;
+    }
+    return g_noalloc_ptr[device];
+}
+
 }  // namespace msbg
 
 using namespace msbg;
@@ -455,6 +491,39 @@ int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_
     MSBG_REQUIRE(ctx && ((d_pos && d_keys_out && d_perm_out) || !n), "null argument");
     set_device(ctx);
     morton_sort_device(ctx, d_pos, n, d_keys_out, d_perm_out);
+    MSBG_API_END
+}
+
+// Same result as msbg_morton_sort_device for n <= 262144 particles, without
+// allocating: the temporaries live in the library's fixed device scratch
+// array.  The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress), so make that first call before capturing the
+// stream into a CUDA graph.  All calls share the one array: calls whose GPU
+// work overlaps in time (different streams or contexts on one device) race on
+// it; calls ordered on one stream do not.  Every scratch word is written
+// before it is read in a call (the key-bits word is cleared on the stream),
+// so nothing depends on what a previous call left there.
+int msbg_morton_sort_noalloc_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out,
+                                    uint32_t* d_perm_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && ((d_pos && d_keys_out && d_perm_out) || !n), "null argument");
+    if (n > kNoAllocMaxParticles)
+        MSBG_THROW(MSBG_ERR_ARG, "msbg_morton_sort_noalloc_device: n = " + std::to_string(n) +
+                                     " exceeds the maximum of " + std::to_string(kNoAllocMaxParticles) +
+                                     " particles of the fixed scratch area; use msbg_morton_sort_device");
+    if (ctx->timing)
+        MSBG_THROW(MSBG_ERR_STATE, "msbg_morton_sort_noalloc_device: per-kernel timing is on and would create CUDA events");
+    set_device(ctx);
+    if (!n) return MSBG_OK;
+    char* base = noalloc_scratch(ctx->device);
+    uint64_t* keys = reinterpret_cast<uint64_t*>(base);
+    char* sort_tmp = base + kNoAllocKeysBytes;
+    char* bits_word = base + kNoAllocKeysBytes + kNoAllocSortBytes;
+    if (radix_sort_scratch_bytes(n) > kNoAllocSortBytes)
+        MSBG_THROW(MSBG_ERR_STATE, "fixed scratch area smaller than the radix sort needs");
+    morton_keys(ctx, d_pos, n, keys);
+    const int bits = key_bits(ctx, keys, n, bits_word);
+    radix_sort_pairs(ctx, keys, nullptr, d_keys_out, d_perm_out, n, bits, sort_tmp);
     MSBG_API_END
 }
 
