@@ -1,22 +1,36 @@
 #!/usr/bin/env python
-"""Benchmark: one FLIP transfer step of the msbg-rs sparse-grid hot path on B200.
+"""Benchmark of the msbg-rs sparse-grid hot path on B200.
 
-Workload (the FLIP transfer configuration): 256^3 domain, 16^3 blocks, three
-resolution levels chosen per block by the distance of its centre to the
-sphere |x - c| = 89.6 (< 16 cells: level 0, < 48: level 1, else level 2), 8
-particles per level-0 cell uniformly jittered inside the cell (25,427,968
-particles), velocities N(0, 1), mass 1, all from a fixed seed, in shuffled
-order.  One step:
-  1. Morton sort of the particles by morton3 of their cell (21 bits per axis)
-     and the payload gather into sorted order,
-  2. P2G: splat of mass and momentum to the MAC faces (r_p = 2) + normalise,
-  3. 2^3 downsample of the splatted x-face mass to the coarse level and 10
-     sweeps of the 19-tap mean-curvature smoother (dt 0.025) over the level-0
-     blocks, halos of coarser neighbours sampled from the coarse level,
-  4. G2P: trilinear MAC sample at every particle + FLIP/PIC blend (alpha 0.95).
-metric = particles through the whole step per second.  Inputs are resident in
-HBM when the timed region starts and are far larger than L2 (713 MB of
-particle data), so no L2 flush is needed.
+Workloads (--workload; every input is seeded synthetic data, no dataset
+exists for this path):
+
+flip (default): one FLIP transfer step.  256^3 domain, 16^3 blocks, three
+  resolution levels chosen per block by the distance of its centre to the
+  sphere |x - c| = 89.6 (< 16 cells: level 0, < 48: level 1, else level 2), 8
+  particles per level-0 cell uniformly jittered inside the cell (25,427,968
+  particles), velocities N(0, 1), mass 1, in shuffled order.  One step:
+    1. Morton sort of the particles by morton3 of their cell (21 bits per axis)
+       and the payload gather into sorted order,
+    2. P2G: splat of mass and momentum to the MAC faces (r_p = 2) + normalise,
+    3. 2^3 downsample of the splatted x-face mass to the coarse level and 10
+       sweeps of the 19-tap mean-curvature smoother (dt 0.025) over the level-0
+       blocks, halos of coarser neighbours sampled from the coarse level,
+    4. G2P: trilinear MAC sample at every particle + FLIP/PIC blend (alpha 0.95).
+  metric = particles through the whole step per second.  Inputs (713 MB of
+  particle data) are larger than L2: no flush needed.
+
+smoother: the single-level shell (blocks meeting |‖x - c‖ - 0.35 size| <= 6),
+  U[-1, 1] values; one step = 10 in-place 8-colour sweeps of the 7-tap stencil
+  (dt 0.025).  Default size 2048 (56,056 blocks, 918 MB, larger than L2).
+  metric = cell-updates per second; the 19- and 25-tap stencils and 10 sweeps
+  of the weighted-Jacobi Poisson relaxation (w = 2/3) are reported beside it.
+
+poisson: the pressure solve on the level-0 blocks of the FLIP layout (776
+  blocks, 3.18 M unknowns, zero Dirichlet outside), right-hand side the
+  divergence of a random smooth velocity field (32 Gaussian blobs).  One step =
+  one solve from x = 0 to 1e-6 relative residual; metric = milliseconds per
+  solve (lower is better); plain multigrid V-cycles and MG-preconditioned CG
+  are both timed.
 
 --impl reference times the reference algorithm on the host CPU (the C++
 restatement in oracle/, all host threads) on a bounded sample of the same
@@ -84,7 +98,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -217,8 +231,6 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     ctx.synchronize()
-    call("msbg_ctx_set_timing", ctx.handle, 1)
-    timing_report(msbg, ctx, reset=True)
     clocks = ClockSampler(local)
     if dist:
         dist.barrier()
@@ -243,12 +255,15 @@ def run_ours(args, world, rank, local):
     for ev in all_events:
         for (a, ea), (b, eb) in zip(ev[:-1], ev[1:]):
             phase_ms[b] = phase_ms.get(b, 0.0) + ea.elapsed_time(eb) / args.steps
+    ms = _max_over_ranks(dist, ms, dev)
+    # per-kernel device times: a separate pass with an event pair around every
+    # library launch (kept out of the timed region above)
+    prof_steps = max(1, min(args.steps, 5))
+    call_timing(msbg, ctx, True)
+    for _ in range(prof_steps):
+        step()
     kernels = timing_report(msbg, ctx, reset=True)
-    call("msbg_ctx_set_timing", ctx.handle, 0)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    call_timing(msbg, ctx, False)
 
     # ---- end to end through the C ABI with host buffers ----------------------
     pin_pos = torch.from_numpy(pos_h).pin_memory()
@@ -281,17 +296,20 @@ def run_ours(args, world, rank, local):
     dom = max(kernels.items(), key=lambda kv: kv[1][1]) if kernels else ("none", (1, 1.0))
     n_fine = len(state["fine"])
     n_active = len(state["active"])
-    algo = algorithmic_bytes(dom[0], n=n, n_fine=n_fine, n_active=n_active, steps=args.steps)
+    algo = algorithmic_bytes(dom[0], n=n, n_fine=n_fine, n_active=n_active, launches=dom[1][0])
     roof = None
     if algo is not None:
         achieved = algo / (dom[1][1] * 1e-3) / 1e9
+        per_launch = algo / dom[1][0]
+        traffic = measured_traffic(dom[0], n=n)
         roof = {"kernel": dom[0], "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "traffic": None, "launches": dom[1][0], "avg_launch_us": round(dom[1][1] / dom[1][0] * 1e3, 2)}
+                "traffic": traffic, "algorithmic_bytes_per_launch": per_launch, "launches": dom[1][0],
+                "avg_launch_us": round(dom[1][1] / dom[1][0] * 1e3, 2)}
     sweep_k = kernels.get("sweep_phase_kernel")
     smoother = None
     if sweep_k:
-        cells = n_fine * 4096 * SWEEPS * args.steps
+        cells = n_fine * 4096 * SWEEPS * prof_steps
         smoother = {"cell_updates_per_s": cells / (sweep_k[1] * 1e-3), "gbs_algorithmic": 8 * cells / (sweep_k[1] * 1e-3) / 1e9,
                     "frac_of_hbm": 8 * cells / (sweep_k[1] * 1e-3) / 1e9 / peak}
 
@@ -309,7 +327,7 @@ def run_ours(args, world, rank, local):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
-        "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])},
+        "kernels_ms_per_step": {k: round(v[1] / prof_steps, 4) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])},
         "submetrics": {"p2g_particles_per_s": n / (phase_ms.get("p2g", float("nan")) * 1e-3),
                        "smoother": smoother},
         "roofline": roof,
@@ -324,25 +342,40 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
-def algorithmic_bytes(kernel, n, n_fine, n_active, steps):
-    """Algorithmic HBM bytes moved by all launches of `kernel` in the timed
-    region (the per-unit figures: 8 B per f32 cell-update for the in-place
-    smoother; 28 B read per particle for the P2G splat plus 24 B written per
-    face-cell of the active blocks for the combine; 12 B read + 12 B written
-    per particle for G2P; 24 B per element per radix pass)."""
+def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
+    """Algorithmic HBM bytes moved by `launches` launches of `kernel` in one
+    FLIP transfer step's accounting: 8 B per f32 cell-update for the in-place
+    smoother; 28 B read per particle per face direction for the P2G splat (x,
+    y, z, velocity component, mass, packed footprint; one launch per
+    direction); 24 B written per face-cell of the active blocks for the
+    combine; 12 B read + 12 B written per particle for G2P; 24 B per element
+    per radix pass (3 passes per sort)."""
     if kernel == "sweep_phase_kernel":
-        return 8.0 * n_fine * 4096 * SWEEPS * steps
+        return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
-        return 28.0 * n * steps
+        return 28.0 * n * launches
     if kernel == "p2g_combine_kernel":
-        return 24.0 * n_active * 4096 * steps
+        return 24.0 * n_active * 4096 * launches
     if kernel == "g2p_kernel":
-        return 24.0 * n * steps
-    if kernel in ("rs_scatter_kernel",):
-        return 24.0 * n * steps * 3  # one sort of 3 passes
+        return 24.0 * n * launches
+    if kernel == "rs_scatter_kernel":
+        return 24.0 * n * launches
     if kernel == "permute_kernel":
-        return 2 * 28.0 * n * steps
+        return 28.0 * n * launches
     return None
+
+
+# DRAM bytes (read + write) per launch measured by ncu on a smaller case of
+# the same kernel, per unit of work: p2g_cells_kernel at 128^3 (5,767,168
+# particles, one direction per launch) read 168.23 MB and wrote 4.79 MB
+# (profiles/p2g_cells_kernel_flip128.txt); traffic grows with the particle
+# count, so it is scaled by particles.
+TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (168.23e6 + 4.79e6) / 5767168}
+
+
+def measured_traffic(kernel, n):
+    per = TRAFFIC_PER_UNIT.get(kernel)
+    return None if per is None else per * n
 
 
 def cpu_baseline(ft, pos_h, vel_h, mass_h, budget_s=20.0):
@@ -430,21 +463,394 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def _dist_init(world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    if world <= 1:
+        return None
+    import torch.distributed as dist_mod
+    from datetime import timedelta
+
+    dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return dist_mod
+
+
+def _max_over_ranks(dist, v, dev):
+    import torch
+
+    if not dist:
+        return v
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _finish(dist):
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# DRAM bytes per launch of the 7-tap sweep phase on the 2048^3 shell (7,007
+# blocks per colour), mean of two ncu-captured launches
+# (profiles/sweep_phase_kernel_shell2048.txt): 263.76 MB read + 79.98 MB written.
+SWEEP_TRAFFIC_2048 = 263.76e6 + 79.98e6
+
+SMOOTHER_STENCILS = {0: "7-tap laplacian", 1: "19-tap mean curvature", 2: "25-tap bilaplacian"}
+
+
+def run_smoother(args, world, rank, local):
+    """10 in-place sweeps of the 7-tap stencil over the shell per step."""
+    import torch
+
+    msbg = load_package()
+    from msbg_rs_b200 import workloads
+
+    dist = _dist_init(world, local)
+    dev = torch.device("cuda", local)
+    size = args.size or 2048
+    sp = workloads.shell_problem(size, 16, seed=1)
+    nb = len(sp.active)
+    ctx = msbg.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    grid = msbg.SparseGrid(ctx, size, size, size, 0.0, 1.0, 16)
+    grid.write_blocks(sp.active, sp.values)
+    sw = msbg.Sweeper(grid)
+    params = msbg.PdeParams(DT, SWEEPS, False)
+    ctx.synchronize()
+
+    def timed(stencil, steps, warmup):
+        """Device time per step (no per-launch events), then the per-kernel
+        times of a separate pass of `steps` steps with an event pair around
+        every launch."""
+        for _ in range(warmup):
+            sw.sweep(sp.active, stencil, params)
+        ctx.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            sw.sweep(sp.active, stencil, params)
+        t1.record(stream)
+        ctx.synchronize()
+        call_timing(msbg, ctx, True)
+        for _ in range(steps):
+            sw.sweep(sp.active, stencil, params)
+        kern = timing_report(msbg, ctx, reset=True)
+        call_timing(msbg, ctx, False)
+        return t0.elapsed_time(t1) / steps, kern
+
+    stencil = {"laplacian": 0, "meancurv": 1, "bilaplacian": 2}[args.stencil]
+    for _ in range(args.warmup):
+        sw.sweep(sp.active, stencil, params)
+    ctx.synchronize()
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.kernel_launches()
+    ms, kern = timed(stencil, args.steps, 0)
+    clk = clocks.stop()
+    launches = (ctx.kernel_launches() - launches0) // 2
+    ms = _max_over_ranks(dist, ms, dev)
+    cells = nb * 4096 * SWEEPS
+    peak, peak_kind = load_peaks()
+    sk = kern.get("sweep_phase_kernel", (0, float("nan")))
+    k_ms = sk[1] / args.steps
+    achieved = 8.0 * cells / (k_ms * 1e-3) / 1e9
+    roof = {"kernel": "sweep_phase_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": SWEEP_TRAFFIC_2048 if size == 2048 and stencil == 0 else None,
+            "algorithmic_bytes_per_launch": 8.0 * cells / max(sk[0] / args.steps, 1),
+            "launches": sk[0], "avg_launch_us": round(sk[1] / max(sk[0], 1) * 1e3, 2),
+            "algorithmic": "8 B per f32 cell-update (read + in-place write)"}
+    others = {}
+    for st in (0, 1, 2):
+        if st == stencil:
+            continue
+        o_ms, o_k = timed(st, 2, 1)
+        ok = o_k.get("sweep_phase_kernel", (1, float("nan")))
+        others[SMOOTHER_STENCILS[st]] = {"ms_per_10_sweeps": o_ms, "cell_updates_per_s": cells / (o_ms * 1e-3),
+                                         "kernel_gbs_algorithmic": 8.0 * cells / (ok[1] / 2 * 1e-3) / 1e9}
+    # weighted-Jacobi relaxation of the Poisson operator on the same blocks
+    P = msbg.Poisson(ctx, size, size, size, 16, sp.active)
+    x = torch.empty(P.n, device=dev)
+    b = torch.empty(P.n, device=dev)
+    x.uniform_(-1, 1)
+    b.uniform_(-1, 1)
+    torch.cuda.synchronize()
+    P.jacobi(x, b, 2.0 / 3.0, 2)
+    ctx.synchronize()
+    call_timing(msbg, ctx, True)
+    P.jacobi(x, b, 2.0 / 3.0, SWEEPS)
+    jk = timing_report(msbg, ctx, reset=True)
+    call_timing(msbg, ctx, False)
+    jac = jk.get("pk_jacobi", (1, float("nan")))
+    jacobi = {"sweeps": SWEEPS, "kernel_ms": jac[1], "cell_updates_per_s": P.n * SWEEPS / (jac[1] * 1e-3),
+              "gbs_algorithmic": 12.0 * P.n * SWEEPS / (jac[1] * 1e-3) / 1e9,
+              "frac_of_hbm": 12.0 * P.n * SWEEPS / (jac[1] * 1e-3) / 1e9 / peak,
+              "algorithmic": "12 B per cell-update (x, b read, x written)"}
+    P.close()
+    # end to end through the C ABI: host payload in, 10 sweeps, host payload out
+    e2e_steps = max(1, min(args.steps, 3))
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        grid.write_blocks(sp.active, sp.values)
+        sw.sweep(sp.active, stencil, params)
+        out = grid.read_blocks(sp.active)
+    e2e_ms = (time.perf_counter() - t) * 1e3 / e2e_steps
+    e2e_ms = _max_over_ranks(dist, e2e_ms, dev)
+    value = world * cells / (ms * 1e-3)
+    line = {
+        "metric": "smoother cell-updates per second (10 in-place 8-colour sweeps)", "value": value,
+        "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded U[-1,1] values; no dataset exists for this path)",
+        "config": {"workload": f"shell {size}^3, 16^3 blocks, radius 0.35*size, thickness 12", "blocks": nb,
+                   "stencil": SMOOTHER_STENCILS[stencil], "sweeps": SWEEPS, "dt": DT,
+                   "parallelism": f"replicas x{world}", "l2": f"grid payload {nb * 16384 / 1e6:.0f} MB; larger than L2, no flush" if nb * 16384 > 126e6 else "grid fits in L2"},
+        "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(sp.values.nbytes), "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": launches,
+        "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in kern.items()},
+        "submetrics": {"gbs_algorithmic": achieved, "other_stencils": others, "jacobi": jacobi},
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_smoother(sp, stencil, args.cpu_budget)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    _finish(dist)
+
+
+def call_timing(msbg, ctx, on):
+    from msbg_rs_b200._lib import call
+
+    call("msbg_ctx_set_timing", ctx.handle, 1 if on else 0)
+    if on:
+        timing_report(msbg, ctx, reset=True)
+
+
+def run_cpu_smoother(oracle, sp, stencil, budget_s):
+    """The oracle's colour-ordered sweep (10 sweeps) on the first k shell
+    blocks, k doubling until the run takes a quarter of the budget."""
+    msbg = load_package()
+    threads = oracle.num_threads()
+    k = 64
+    while True:
+        sel = sp.active[:k]
+        g = msbg.HostGrid("shell", sp.size, sp.size, sp.size, 0.0, 1.0, 16)
+        for j, bid in enumerate(sel):
+            g.ensure_block(int(bid))
+            g.blocks[int(bid)][:] = sp.values[j]
+        t = time.perf_counter()
+        oracle.sweep(g, sel.astype(np.int64), stencil, DT, SWEEPS, False, threads=threads)
+        el = time.perf_counter() - t
+        cells = k * 4096 * SWEEPS
+        res = {"value": cells / el, "threads": threads, "seconds": el,
+               "sample": f"{k} of {len(sp.active)} shell blocks, 10 sweeps, {el:.1f} s"}
+        if el > budget_s / 4 or k * 2 > len(sp.active):
+            return res
+        k *= 2
+
+
+def cpu_baseline_smoother(sp, stencil, budget_s):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    r = run_cpu_smoother(oracle, sp, stencil, budget_s)
+    return {"value": r["value"], "unit": "cell-updates/s", "cores": r["threads"], "kind": "port", "sample": r["sample"]}
+
+
+def poisson_problem(size=256):
+    from msbg_rs_b200 import workloads
+
+    ft = workloads.flip_transfer(size=size, bsx=16, particles=False)
+    active = np.unique(ft.fine_blocks)
+    b = workloads.smooth_divergence_rhs(size, 16, active, seed=4)
+    return active, b
+
+
+def run_poisson(args, world, rank, local):
+    """Time to 1e-6 relative residual, plain V-cycles and MG-PCG."""
+    import torch
+
+    msbg = load_package()
+    dist = _dist_init(world, local)
+    dev = torch.device("cuda", local)
+    size = args.size or 256
+    active, bh = poisson_problem(size)
+    ctx = msbg.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    P = msbg.Poisson(ctx, size, size, size, 16, active)
+    b = torch.from_numpy(bh.reshape(-1)).to(dev)
+    x = torch.zeros(P.n, device=dev)
+    torch.cuda.synchronize()
+    methods = {"plain_mg": msbg.MG, "mg_pcg": msbg.PCG}
+    head = "mg_pcg"
+
+    def one(method):
+        x.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        it, rel, hist = P.solve_device(x, b, method=method, tol=1e-6, max_iter=400)
+        e1.record(stream)
+        ctx.synchronize()
+        return e0.elapsed_time(e1), it, rel
+
+    for _ in range(args.warmup):
+        one(methods[head])
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.kernel_launches()
+    times, its = [], []
+    for _ in range(args.steps):
+        t, it, rel = one(methods[head])
+        times.append(t)
+        its.append(it)
+    clk = clocks.stop()
+    launches = ctx.kernel_launches() - launches0
+    call_timing(msbg, ctx, True)
+    prof_steps = max(1, min(args.steps, 3))
+    for _ in range(prof_steps):
+        one(methods[head])
+    kern = timing_report(msbg, ctx, reset=True)
+    call_timing(msbg, ctx, False)
+    ms = _max_over_ranks(dist, statistics.mean(times), dev)
+    per_method = {}
+    for name, m in methods.items():
+        one(m)
+        t, it, rel = one(m)
+        per_method[name] = {"ms": t, "iterations": it, "rel_residual": rel}
+    # end to end through the C ABI with host arrays
+    t = time.perf_counter()
+    _, it_h, rel_h, _ = P.solve(bh.reshape(-1), method=methods[head], tol=1e-6, max_iter=400)
+    e2e_ms = (time.perf_counter() - t) * 1e3
+    peak, peak_kind = load_peaks()
+    jac = kern.get("pk_jacobi", (1, float("nan")))
+    n_cells = P.n
+    # one V-cycle per PCG iteration plus the initial one; 2 + 2 sweeps per level
+    level_cells = [int(c) for c in P.levels()[:-1]]
+    jac_bytes = prof_steps * (its[0] + 1) * sum(4 * 12.0 * c for c in level_cells)
+    jac_gbs = jac_bytes / (jac[1] * 1e-3) / 1e9
+    line = {
+        "metric": "time to 1e-6 relative residual (Poisson, 7-point, MG-preconditioned CG)", "value": ms, "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 dots and coarsest solve)",
+        "data": "synthetic (seeded smooth-divergence right-hand side; no dataset exists for this path)",
+        "config": {"workload": f"Poisson on the level-0 blocks of the {size}^3 3-level layout, 16^3 blocks",
+                   "blocks": int(len(active)), "unknowns": int(n_cells), "tol": 1e-6,
+                   "smoother": "weighted Jacobi w=2/3, 2+2 sweeps", "parallelism": f"replicas x{world}",
+                   "l2": "working set (~64 MB) fits in L2; solves run back to back"},
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(bh.nbytes) * 2, "d2h_bytes_per_step": int(bh.nbytes)},
+        "gpu_launches": launches,
+        "iterations": its[0],
+        "methods": per_method,
+        "kernels_ms_per_step": {k: round(v[1] / prof_steps, 4) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][1])},
+        "roofline": {"kernel": "pk_jacobi", "bound": "hbm", "achieved": round(jac_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(jac_gbs / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": None, "algorithmic": "12 B per cell-update, (nu1 + nu2) sweeps on every level per V-cycle",
+                     "launches": jac[0], "avg_launch_us": round(jac[1] / max(jac[0], 1) * 1e3, 2)},
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_poisson(active, bh, size)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    P.close()
+    _finish(dist)
+
+
+def cpu_baseline_poisson(active, bh, size):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    n = size // 16
+    t = time.perf_counter()
+    _, hist = oracle.poisson_solve(np.asarray(active, np.int64), n, n, n, 16, bh.reshape(-1).astype(np.float64), mode=1,
+                                   tol=1e-6, max_iter=400)
+    el = time.perf_counter() - t
+    return {"value": el * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+            "sample": f"the whole solve ({len(hist)} MG-PCG iterations, FP64, one thread)"}
+
+
+def run_reference_smoother(args, world, rank, local):
+    """Reference arm of the smoother workload: the oracle sweep on the host."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    load_package()
+    from msbg_rs_b200 import workloads
+
+    sp = workloads.shell_problem(args.size, 16, seed=1)
+    stencil = {"laplacian": 0, "meancurv": 1, "bilaplacian": 2}[args.stencil]
+    for _ in range(args.warmup):
+        run_cpu_smoother(oracle, sp, stencil, budget_s=2.0)
+    vals = [run_cpu_smoother(oracle, sp, stencil, budget_s=args.cpu_budget) for _ in range(args.steps)]
+    v = statistics.median(r["value"] for r in vals)
+    cells = len(sp.active) * 4096 * SWEEPS
+    print(json.dumps({
+        "impl": "reference", "metric": "smoother cell-updates per second (10 in-place 8-colour sweeps)", "value": v,
+        "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": cells / v * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"shell {args.size}^3, 16^3 blocks, radius 0.35*size, thickness 12",
+                   "blocks": len(sp.active), "stencil": SMOOTHER_STENCILS[stencil], "parallelism": "host CPU"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": vals[0]["threads"], "kind": "port",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_reference_poisson(args, world, rank, local):
+    """Reference arm of the Poisson workload: the FP64 oracle MG-PCG solve."""
+    if rank != 0:
+        return
+    load_package()
+    active, bh = poisson_problem(args.size)
+    steps = max(1, min(args.steps, 3))
+    vals = [cpu_baseline_poisson(active, bh, args.size) for _ in range(steps)]
+    v = statistics.median(r["value"] for r in vals)
+    print(json.dumps({
+        "impl": "reference", "metric": "time to 1e-6 relative residual (Poisson, 7-point, MG-preconditioned CG)",
+        "value": v, "unit": "ms", "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": v,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"Poisson on the level-0 blocks of the {args.size}^3 3-level layout, 16^3 blocks",
+                   "blocks": int(len(active)), "parallelism": "host CPU"},
+        "cpu_baseline": dict(vals[0], value=v),
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--workload", choices=["flip", "smoother", "poisson"], default="flip")
+    ap.add_argument("--stencil", choices=["laplacian", "meancurv", "bilaplacian"], default="laplacian")
+    ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.size is None:
+        args.size = {"flip": 256, "smoother": 2048, "poisson": 256}[args.workload]
     world, rank, local = dist_setup()
     if args.impl == "reference":
-        run_reference(args, world, rank, local)
+        {"flip": run_reference, "smoother": run_reference_smoother, "poisson": run_reference_poisson}[args.workload](
+            args, world, rank, local)
     else:
-        run_ours(args, world, rank, local)
+        {"flip": run_ours, "smoother": run_smoother, "poisson": run_poisson}[args.workload](args, world, rank, local)
 
 
 if __name__ == "__main__":

@@ -104,3 +104,43 @@ def flip_transfer(size: int = 256, bsx: int = 16, seed: int = 2, ppc: int = 8, r
     vel = rng.standard_normal(origin.shape, dtype=np.float32)
     mass = np.ones(len(pos), np.float32)
     return FlipTransfer(size, bsx, levels, fine, pos.astype(np.float32), vel, mass)
+
+
+def block_cell_centres(size: int, bsx: int, bids: np.ndarray) -> np.ndarray:
+    """Cell-centre coordinates [n_blocks][bsx^3][3] (f64) of the given blocks in
+    the payload order x | y<<lg | z<<2lg."""
+    n = size // bsx
+    bids = np.asarray(bids, np.int64)
+    cells = np.arange(bsx ** 3)
+    lx, ly, lz = cells % bsx, (cells // bsx) % bsx, cells // (bsx * bsx)
+    bx, by, bz = bids % n, (bids // n) % n, bids // (n * n)
+    return np.stack([(bx[:, None] * bsx + lx[None, :]) + 0.5, (by[:, None] * bsx + ly[None, :]) + 0.5,
+                     (bz[:, None] * bsx + lz[None, :]) + 0.5], -1)
+
+
+def smooth_divergence_rhs(size: int, bsx: int, active: np.ndarray, seed: int = 4, n_blobs: int = 32,
+                          sigma=(4.0, 16.0)) -> np.ndarray:
+    """Right-hand side of the learned-preconditioner configuration: the
+    divergence of a random smooth velocity field u = sum_i a_i g_i(x),
+    g_i = exp(-|x - c_i|^2 / (2 sigma_i^2)), amplitudes a_i ~ N(0, 1)^3, sigma_i
+    uniform in [4, 16] cells, centres at random cells of the active blocks.
+    div u = sum_i -(a_i . (x - c_i)) / sigma_i^2 g_i(x), evaluated at cell
+    centres.  Returns [n_active][bsx^3] f32 for the active blocks in ascending
+    block-id order (the Poisson vector layout)."""
+    rng = np.random.default_rng(seed)
+    bids = np.unique(np.asarray(active, np.uint64)).astype(np.int64)
+    x = block_cell_centres(size, bsx, bids).reshape(-1, 3)
+    centres = x[rng.integers(0, len(x), n_blobs)]
+    sig = rng.uniform(sigma[0], sigma[1], n_blobs)
+    amp = rng.standard_normal((n_blobs, 3))
+    out = np.zeros(len(x), np.float64)
+    chunk = 1 << 20
+    for s in range(0, len(x), chunk):
+        xs = x[s:s + chunk]
+        acc = np.zeros(len(xs), np.float64)
+        for i in range(n_blobs):
+            d = xs - centres[i]
+            r2 = np.einsum("ij,ij->i", d, d)
+            acc += -(d @ amp[i]) / sig[i] ** 2 * np.exp(-r2 / (2.0 * sig[i] ** 2))
+        out[s:s + chunk] = acc
+    return out.astype(np.float32).reshape(len(bids), bsx ** 3)
