@@ -279,6 +279,23 @@ int msbg_poisson_solve_device(msbg_poisson* p, int method, float* d_x, const flo
 int msbg_poisson_solve(msbg_poisson* p, int method, float* x, const float* b, double tol, int max_iter,
                        int* iters_out, double* rel_res_out, double* history);
 
+/* ---- block-sparse 3x3x3 convolution on the tensor cores ------------------
+ * No counterpart in the reference (the learned preconditioner of the pressure
+ * solve).  A level's feature map is bf16 [cells][C], cells in block order
+ * (block k = cells k*bs^3 .. (k+1)*bs^3-1, payload order), zero outside the
+ * active blocks; nbr27 is int32 [n_blocks][27] (slot of neighbour block
+ * (dx,dy,dz) at (dx+1)+3(dy+1)+9(dz+1), -1 if absent).  Weights are bf16
+ * [27][cout][cin]; cin, cout in {16, 32, 64}; lg = log2(bs) in [1, 5].
+ * msbg_conv3_forward_device: y = relu?(conv(x) + bias), y bf16 or f32
+ * (out_f32) [cells][cout]; bias f32 [cout] or NULL.
+ * msbg_conv3_wgrad_device: dw = sum_c x[c + d(t)] dy[c]^T, f32 [27][cout][cin].
+ * Both synchronise and return MSBG_ERR_TIMEOUT if a bounded wait gave up. */
+int msbg_conv3_forward_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blocks, int lg, int cin, int cout,
+                              const uint16_t* d_x, const uint16_t* d_w, const float* d_bias, int relu, int out_f32,
+                              void* d_y);
+int msbg_conv3_wgrad_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blocks, int lg, int cin, int cout,
+                            const uint16_t* d_x, const uint16_t* d_dy, float* d_dw);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,8 @@ SIGNATURES = {
     "msbg_g2p_blend_device": [_P, _P, _P, _P, _SZ, _F, _P],
     "msbg_sample_linear": [_P, _P, _SZ, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_conv3_forward_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P, _I, _I, _P],
+    "msbg_conv3_wgrad_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P],
     "msbg_poisson_create": [_P, _U64, _U64, _U64, _I, _P, _SZ, C.POINTER(_P)],
     "msbg_poisson_destroy": [_P],
     "msbg_poisson_levels": [_P, _P, _SZ, _SZP],

@@ -1,0 +1,348 @@
+// conv.cu -- block-sparse 3x3x3 convolutions on tcgen05 (see conv.cuh).
+#include <algorithm>
+
+#include "conv.cuh"
+#include "tc.cuh"
+
+namespace msbg {
+
+constexpr int kConvStages = 3;
+constexpr int kWgCells = 64;  // cells (K) per weight-gradient stage
+
+__device__ __forceinline__ uint16_t bf16_rne(float v) { return ElemBF16::store(v); }
+
+// Source row of cell `cell` shifted by tap t, or null when it falls outside
+// the active blocks (zero padding).
+template <int C>
+__device__ __forceinline__ const uint4* tap_row(const ConvLevel& L, const uint16_t* __restrict__ x, int64_t cell, int t) {
+    const int lg = L.lg, m = (1 << lg) - 1;
+    const int64_t k = cell >> (3 * lg);
+    const int v = (int)(cell & ((1 << (3 * lg)) - 1));
+    const int gx = (v & m) + t % 3 - 1, gy = ((v >> lg) & m) + (t / 3) % 3 - 1, gz = (v >> (2 * lg)) + t / 9 - 1;
+    const int ox = gx < 0 ? 0 : (gx > m ? 2 : 1), oy = gy < 0 ? 0 : (gy > m ? 2 : 1), oz = gz < 0 ? 0 : (gz > m ? 2 : 1);
+    const int code = ox + 3 * oy + 9 * oz;
+    const int32_t kk = code == 13 ? (int32_t)k : L.nbr27[k * 27 + code];
+    if (kk < 0 || kk >= L.n_blocks) return nullptr;  // absent (or a corrupt table entry: read as zero)
+    const int64_t c2 = ((int64_t)kk << (3 * lg)) + ((gx & m) | ((gy & m) << lg) | ((gz & m) << (2 * lg)));
+    return reinterpret_cast<const uint4*>(x + c2 * C);
+}
+
+template <int CIN, int COUT>
+struct FwdSmem {
+    static constexpr int A_BYTES = 128 * CIN * 2;
+    static constexpr int B_BYTES = COUT * CIN * 2;
+    static constexpr int OFF_B = kConvStages * A_BYTES;
+    static constexpr int OFF_BAR = OFF_B + kConvStages * B_BYTES;
+    static constexpr int BYTES = OFF_BAR + 64;
+    // At least 32 KB per CTA: at most 7 CTAs share an SM, so their TMEM
+    // columns (<= 64 each) never exceed the 512 an SM has.
+    static constexpr int ALLOC = BYTES < 32768 ? 32768 : BYTES;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvLevel L, const uint16_t* __restrict__ x,
+                                                        const uint16_t* __restrict__ w, const float* __restrict__ bias,
+                                                        int relu, int out_f32, void* __restrict__ y, int* __restrict__ status) {
+    using S = FwdSmem<CIN, COUT>;
+    constexpr int TCOLS = COUT < 32 ? 32 : COUT;
+    constexpr int KCH = CIN / 8;
+    constexpr uint32_t SBO = KCH * 128;
+    constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, 0, 0);
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::OFF_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kConvStages);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) tc::tmem_alloc(tslot, TCOLS);
+    if (tid == 0) {
+        for (int s = 0; s < kConvStages; ++s) tc::mbar_init(&bars[s], 1);
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    const int64_t cell = (int64_t)blockIdx.x * 128 + tid;
+    const bool valid = cell < L.cells();
+    bool ok = true;
+    for (int t = 0; t < 27; ++t) {
+        const int s = t % kConvStages;
+        if (t >= kConvStages) ok &= tc::mbar_wait(&bars[s], ((t / kConvStages) - 1) & 1);
+        const uint4* src = valid ? tap_row<CIN>(L, x, cell, t) : nullptr;
+        uint8_t* arow = smem + s * S::A_BYTES + (tid >> 3) * SBO + (tid & 7) * 16;
+#pragma unroll
+        for (int j = 0; j < KCH; ++j)
+            *reinterpret_cast<uint4*>(arow + j * 128) = src ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
+        uint8_t* bst = smem + S::OFF_B + s * S::B_BYTES;
+        const uint4* wt = reinterpret_cast<const uint4*>(w + (int64_t)t * COUT * CIN);
+        for (int q = tid; q < COUT * KCH; q += 128) {
+            const int n = q / KCH, j = q % KCH;
+            *reinterpret_cast<uint4*>(bst + (n >> 3) * SBO + j * 128 + (n & 7) * 16) = __ldg(wt + q);
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(smem + s * S::A_BYTES), b0 = tc::smem_u32(bst);
+#pragma unroll
+            for (int kk = 0; kk < CIN / 16; ++kk)
+                tc::mma_bf16(tmem, tc::sdesc(a0 + kk * 256, 128, SBO), tc::sdesc(b0 + kk * 256, 128, SBO), IDESC,
+                             (t | kk) != 0);
+            tc::mma_commit(&bars[s]);
+        }
+    }
+    ok &= tc::mbar_wait(&bars[26 % kConvStages], (26 / kConvStages) & 1);
+    tc::fence_after_sync();
+    float acc[16];
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, acc);
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float v = acc[i] + (bias ? __ldg(bias + c0 + i) : 0.0f);
+                acc[i] = relu ? fmaxf(v, 0.0f) : v;
+            }
+            if (out_f32) {
+                float4* yo = reinterpret_cast<float4*>(static_cast<float*>(y) + cell * COUT + c0);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) yo[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
+            } else {
+                uint32_t pk[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) pk[i] = (uint32_t)bf16_rne(acc[2 * i]) | ((uint32_t)bf16_rne(acc[2 * i + 1]) << 16);
+                uint4* yo = reinterpret_cast<uint4*>(static_cast<uint16_t*>(y) + cell * COUT + c0);
+                yo[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                yo[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+    if (!ok && tid == 0) atomicOr(status, 1);
+}
+
+template <int CIN, int COUT>
+struct WgSmem {
+    static constexpr int A_BYTES = 128 * kWgCells * 2;
+    static constexpr int B_BYTES = COUT * kWgCells * 2;
+    static constexpr int OFF_B = kConvStages * A_BYTES;
+    static constexpr int OFF_BAR = OFF_B + kConvStages * B_BYTES;
+    static constexpr int BYTES = OFF_BAR + 64;
+    static constexpr int ALLOC = BYTES < 32768 ? 32768 : BYTES;
+};
+
+// partial[part][q][o], q = tap * CIN + i over tiles of 128 (rows past
+// 27 * CIN are zero).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) conv3_wgrad_kernel(ConvLevel L, const uint16_t* __restrict__ x,
+                                                          const uint16_t* __restrict__ dy, int64_t cells_per_part,
+                                                          float* __restrict__ partial, int* __restrict__ status) {
+    using S = WgSmem<CIN, COUT>;
+    constexpr int TCOLS = COUT < 32 ? 32 : COUT;
+    constexpr uint32_t SBO = (kWgCells / 8) * 128;
+    constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, 1, 1);
+    constexpr int TPT = 128 / CIN;  // taps per M tile
+    constexpr int MROWS = ((27 * CIN + 127) / 128) * 128;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::OFF_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kConvStages);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) tc::tmem_alloc(tslot, TCOLS);
+    if (tid == 0) {
+        for (int s = 0; s < kConvStages; ++s) tc::mbar_init(&bars[s], 1);
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    const int mt = blockIdx.x, part = blockIdx.y;
+    const int tap0 = mt * TPT;
+    const int64_t total = L.cells();
+    const int64_t c_begin = (int64_t)part * cells_per_part;
+    const int64_t c_end = std::min<int64_t>(total, c_begin + cells_per_part);
+    const int nchunks = c_end > c_begin ? (int)((c_end - c_begin + kWgCells - 1) / kWgCells) : 0;
+    bool ok = true;
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const int s = ch % kConvStages;
+        if (ch >= kConvStages) ok &= tc::mbar_wait(&bars[s], ((ch / kConvStages) - 1) & 1);
+        const int64_t cbase = c_begin + (int64_t)ch * kWgCells;
+        uint8_t* ast = smem + s * S::A_BYTES;
+#pragma unroll 4
+        for (int r = 0; r < (kWgCells * 16) / 128; ++r) {
+            const int item = tid + 128 * r;
+            const int c = item % kWgCells, mg = item / kWgCells;
+            const int64_t cell = cbase + c;
+            const int q0 = mg * 8;
+            const int tap = tap0 + q0 / CIN, ci0 = q0 % CIN;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (cell < c_end && tap < 27) {
+                const uint4* src = tap_row<CIN>(L, x, cell, tap);
+                if (src) v = __ldg(src + ci0 / 8);
+            }
+            *reinterpret_cast<uint4*>(ast + mg * SBO + (c >> 3) * 128 + (c & 7) * 16) = v;
+        }
+        uint8_t* bst = smem + S::OFF_B + s * S::B_BYTES;
+        for (int item = tid; item < kWgCells * (COUT / 8); item += 128) {
+            const int c = item % kWgCells, ng = item / kWgCells;
+            const int64_t cell = cbase + c;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (cell < c_end) v = __ldg(reinterpret_cast<const uint4*>(dy + cell * COUT) + ng);
+            *reinterpret_cast<uint4*>(bst + ng * SBO + (c >> 3) * 128 + (c & 7) * 16) = v;
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(ast), b0 = tc::smem_u32(bst);
+#pragma unroll
+            for (int kk = 0; kk < kWgCells / 16; ++kk)
+                tc::mma_bf16(tmem, tc::sdesc(a0 + kk * 256, 128, SBO), tc::sdesc(b0 + kk * 256, 128, SBO), IDESC,
+                             (ch | kk) != 0);
+            tc::mma_commit(&bars[s]);
+        }
+    }
+    if (nchunks > 0) {
+        ok &= tc::mbar_wait(&bars[(nchunks - 1) % kConvStages], ((nchunks - 1) / kConvStages) & 1);
+        tc::fence_after_sync();
+    }
+    float acc[16];
+    const int q = mt * 128 + tid;
+    float* out = partial + ((int64_t)part * MROWS + q) * COUT;
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+        if (nchunks > 0) {
+            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, acc);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] = 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            reinterpret_cast<float4*>(out + c0)[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+    if (!ok && tid == 0) atomicOr(status, 1);
+}
+
+// dw[t][o][i] (+)= sum over parts (in order) of partial[part][t * CIN + i][o]
+__global__ void conv3_wgrad_reduce_kernel(const float* __restrict__ partial, int parts, int cin, int cout, int mrows,
+                                          float* __restrict__ dw, int acc) {
+    const int n = 27 * cin * cout;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int i = e % cin, o = (e / cin) % cout, t = e / (cin * cout);
+        const int q = t * cin + i;
+        float s = 0.0f;
+        for (int p = 0; p < parts; ++p) s += partial[((int64_t)p * mrows + q) * cout + o];
+        dw[e] = acc ? dw[e] + s : s;
+    }
+}
+
+template <int CIN, int COUT>
+static void launch_fwd(msbg_ctx* ctx, const ConvLevel& L, const uint16_t* x, const uint16_t* w, const float* bias, bool relu,
+                       bool out_f32, void* y) {
+    using S = FwdSmem<CIN, COUT>;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(conv3_fwd_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::ALLOC));
+        attr = true;
+    }
+    const int64_t cells = L.cells();
+    if (!cells) return;
+    begin_launch(ctx);
+    conv3_fwd_kernel<CIN, COUT><<<(unsigned)((cells + 127) / 128), 128, S::ALLOC, ctx->stream>>>(
+        L, x, w, bias, relu ? 1 : 0, out_f32 ? 1 : 0, y, ctx->status.as<int>());
+    after_launch(ctx, "conv3_fwd_kernel");
+}
+
+template <int CIN, int COUT>
+static void launch_wgrad(msbg_ctx* ctx, const ConvLevel& L, const uint16_t* x, const uint16_t* dy, float* dw, bool acc) {
+    using S = WgSmem<CIN, COUT>;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(conv3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::ALLOC));
+        attr = true;
+    }
+    constexpr int MT = (27 * CIN + 127) / 128;
+    constexpr int MROWS = MT * 128;
+    const int64_t cells = L.cells();
+    // about 4 CTAs per SM in total, each over a contiguous range of whole 64-cell chunks
+    const int64_t chunks = std::max<int64_t>(1, (cells + kWgCells - 1) / kWgCells);
+    const int parts = (int)std::min<int64_t>(chunks, std::max<int64_t>(1, 592 / MT));
+    const int64_t cells_per_part = ((chunks + parts - 1) / parts) * kWgCells;
+    ScratchLayout SL;
+    const size_t op = SL.add<float>((size_t)parts * MROWS * COUT);
+    float* partial = ScratchLayout::at<float>(scratch(ctx, SL), op);
+    begin_launch(ctx);
+    conv3_wgrad_kernel<CIN, COUT><<<dim3(MT, parts), 128, S::ALLOC, ctx->stream>>>(L, x, dy, cells_per_part, partial,
+                                                                                  ctx->status.as<int>());
+    after_launch(ctx, "conv3_wgrad_kernel");
+    begin_launch(ctx);
+    conv3_wgrad_reduce_kernel<<<(27 * CIN * COUT + 255) / 256, 256, 0, ctx->stream>>>(partial, parts, CIN, COUT, MROWS, dw,
+                                                                                       acc ? 1 : 0);
+    after_launch(ctx, "conv3_wgrad_reduce_kernel");
+}
+
+#define MSBG_CONV_PAIRS(X) X(16, 32) X(32, 16) X(32, 32) X(32, 64) X(64, 32) X(64, 64) X(16, 16) X(64, 16) X(16, 64)
+
+void conv3_forward(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uint16_t* x, const uint16_t* w,
+                   const float* bias, bool relu, bool out_f32, void* y) {
+#define MSBG_FWD_CASE(A, B) \
+    if (cin == A && cout == B) return launch_fwd<A, B>(ctx, L, x, w, bias, relu, out_f32, y);
+    MSBG_CONV_PAIRS(MSBG_FWD_CASE)
+#undef MSBG_FWD_CASE
+    MSBG_THROW(MSBG_ERR_ARG, "conv3: channel counts must be 16, 32 or 64");
+}
+
+void conv3_wgrad(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uint16_t* x, const uint16_t* dy, float* dw,
+                 bool acc) {
+#define MSBG_WG_CASE(A, B) \
+    if (cin == A && cout == B) return launch_wgrad<A, B>(ctx, L, x, dy, dw, acc);
+    MSBG_CONV_PAIRS(MSBG_WG_CASE)
+#undef MSBG_WG_CASE
+    MSBG_THROW(MSBG_ERR_ARG, "conv3: channel counts must be 16, 32 or 64");
+}
+
+void check_device_status(msbg_ctx* ctx) {
+    int h = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&h, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (h) {
+        CUDA_CHECK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->stream));
+        MSBG_THROW(MSBG_ERR_TIMEOUT, "a bounded wait inside a tensor-core kernel gave up");
+    }
+}
+
+}  // namespace msbg
+
+using namespace msbg;
+
+extern "C" {
+
+int msbg_conv3_forward_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blocks, int lg, int cin, int cout,
+                              const uint16_t* d_x, const uint16_t* d_w, const float* d_bias, int relu, int out_f32,
+                              void* d_y) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && d_nbr27 && d_x && d_w && d_y && n_blocks >= 0 && lg >= 1 && lg <= 5, "bad argument");
+    set_device(ctx);
+    conv3_forward(ctx, ConvLevel{d_nbr27, lg, n_blocks}, cin, cout, d_x, d_w, d_bias, relu != 0, out_f32 != 0, d_y);
+    check_device_status(ctx);
+    MSBG_API_END
+}
+
+int msbg_conv3_wgrad_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blocks, int lg, int cin, int cout,
+                            const uint16_t* d_x, const uint16_t* d_dy, float* d_dw) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && d_nbr27 && d_x && d_dy && d_dw && n_blocks >= 0 && lg >= 1 && lg <= 5, "bad argument");
+    set_device(ctx);
+    conv3_wgrad(ctx, ConvLevel{d_nbr27, lg, n_blocks}, cin, cout, d_x, d_dy, d_dw, false);
+    check_device_status(ctx);
+    MSBG_API_END
+}
+
+}  // extern "C"
