@@ -296,6 +296,33 @@ int msbg_conv3_forward_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_b
 int msbg_conv3_wgrad_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blocks, int lg, int cin, int cout,
                             const uint16_t* d_x, const uint16_t* d_dy, float* d_dw);
 
+/* ---- learned preconditioner: block-sparse 3D U-Net ------------------------
+ * No counterpart in the reference.  Three levels on the same blocks (16^3,
+ * 8^3, 4^3 cells), 16/32/64 channels, 3x3x3 convolutions with bf16 weights
+ * and activations and f32 accumulation on the tensor cores; forward and
+ * backward run on the device, Adam updates f32 master weights.  The network
+ * acts on level-0 vectors of a Poisson solve (f32 [n_blocks][4096], blocks
+ * in ascending id order): z = rms(r) * out_scale * N(r / rms(r)).
+ * Parameters are one flat f32 array; msbg_unet_layers lists per layer
+ * (level, cin, cout, cin_real, cout_real, relu, w_offset, b_offset), weights
+ * [27][cout][cin] (padded channels stay zero).  A train step returns the loss
+ * sum((out_scale y - e/rms(r))^2) / sum((e/rms(r))^2) and leaves the
+ * gradient readable with msbg_unet_get_grads; update != 0 applies Adam. */
+typedef struct msbg_unet msbg_unet;
+int msbg_unet_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, const uint64_t* active, size_t n,
+                     uint64_t seed, msbg_unet** out);
+int msbg_unet_destroy(msbg_unet* net);
+int msbg_unet_num_params(const msbg_unet* net, size_t* out);
+int msbg_unet_layers(const msbg_unet* net, int64_t* out, size_t cap, size_t* n_out);
+int msbg_unet_get_params(msbg_unet* net, float* out);
+int msbg_unet_set_params(msbg_unet* net, const float* in);
+int msbg_unet_get_grads(msbg_unet* net, float* out);
+int msbg_unet_set_output_scale(msbg_unet* net, float s);
+int msbg_unet_apply_device(msbg_unet* net, const float* d_r, float* d_z);
+int msbg_unet_forward_raw_device(msbg_unet* net, const float* d_r, float* d_y);
+int msbg_unet_train_step_device(msbg_unet* net, const float* d_r, const float* d_e, float lr, int update,
+                                double* loss_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,17 @@ SIGNATURES = {
     "msbg_downsample_avg": [_P, _P],
     "msbg_conv3_forward_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P, _I, _I, _P],
     "msbg_conv3_wgrad_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P],
+    "msbg_unet_create": [_P, _U64, _U64, _U64, _P, _SZ, _U64, C.POINTER(_P)],
+    "msbg_unet_destroy": [_P],
+    "msbg_unet_num_params": [_P, _SZP],
+    "msbg_unet_layers": [_P, _P, _SZ, _SZP],
+    "msbg_unet_get_params": [_P, _P],
+    "msbg_unet_set_params": [_P, _P],
+    "msbg_unet_get_grads": [_P, _P],
+    "msbg_unet_set_output_scale": [_P, _F],
+    "msbg_unet_apply_device": [_P, _P, _P],
+    "msbg_unet_forward_raw_device": [_P, _P, _P],
+    "msbg_unet_train_step_device": [_P, _P, _P, _F, _I, C.POINTER(C.c_double)],
     "msbg_poisson_create": [_P, _U64, _U64, _U64, _I, _P, _SZ, C.POINTER(_P)],
     "msbg_poisson_destroy": [_P],
     "msbg_poisson_levels": [_P, _P, _SZ, _SZP],

@@ -42,7 +42,8 @@ struct FwdSmem {
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvLevel L, const uint16_t* __restrict__ x,
                                                         const uint16_t* __restrict__ w, const float* __restrict__ bias,
-                                                        int relu, int out_f32, void* __restrict__ y, int* __restrict__ status) {
+                                                        int relu, const uint16_t* __restrict__ mask, int out_f32,
+                                                        int out_ch, void* __restrict__ y, int* __restrict__ status) {
     using S = FwdSmem<CIN, COUT>;
     constexpr int TCOLS = COUT < 32 ? 32 : COUT;
     constexpr int KCH = CIN / 8;
@@ -97,13 +98,27 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvLevel L, const uint1
 #pragma unroll
     for (int c0 = 0; c0 < COUT; c0 += 16) {
         tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, acc);
-        if (valid) {
+        if (valid && c0 < out_ch) {
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 float v = acc[i] + (bias ? __ldg(bias + c0 + i) : 0.0f);
                 acc[i] = relu ? fmaxf(v, 0.0f) : v;
             }
-            if (out_f32) {
+            if (mask) {  // ReLU backward: zero where the layer's stored activation is not positive
+                const uint4* mk = reinterpret_cast<const uint4*>(mask + cell * COUT + c0);
+                uint32_t mw[8];
+                *reinterpret_cast<uint4*>(mw) = __ldg(mk);
+                *reinterpret_cast<uint4*>(mw + 4) = __ldg(mk + 1);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const uint32_t h = (mw[i >> 1] >> (16 * (i & 1))) & 0xFFFFu;
+                    if (!(h != 0u && !(h & 0x8000u))) acc[i] = 0.0f;  // bf16 > 0: nonzero, sign clear
+                }
+            }
+            if (out_f32 && out_ch < COUT) {
+                float* yo = static_cast<float*>(y) + cell * out_ch + c0;
+                for (int i = 0; i < 16 && c0 + i < out_ch; ++i) yo[i] = acc[i];
+            } else if (out_f32) {
                 float4* yo = reinterpret_cast<float4*>(static_cast<float*>(y) + cell * COUT + c0);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) yo[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
@@ -245,7 +260,7 @@ __global__ void conv3_wgrad_reduce_kernel(const float* __restrict__ partial, int
 
 template <int CIN, int COUT>
 static void launch_fwd(msbg_ctx* ctx, const ConvLevel& L, const uint16_t* x, const uint16_t* w, const float* bias, bool relu,
-                       bool out_f32, void* y) {
+                       const uint16_t* mask, bool out_f32, int out_ch, void* y) {
     using S = FwdSmem<CIN, COUT>;
     static bool attr = false;
     if (!attr) {
@@ -256,7 +271,7 @@ static void launch_fwd(msbg_ctx* ctx, const ConvLevel& L, const uint16_t* x, con
     if (!cells) return;
     begin_launch(ctx);
     conv3_fwd_kernel<CIN, COUT><<<(unsigned)((cells + 127) / 128), 128, S::ALLOC, ctx->stream>>>(
-        L, x, w, bias, relu ? 1 : 0, out_f32 ? 1 : 0, y, ctx->status.as<int>());
+        L, x, w, bias, relu ? 1 : 0, mask, out_f32 ? 1 : 0, out_ch > 0 ? out_ch : COUT, y, ctx->status.as<int>());
     after_launch(ctx, "conv3_fwd_kernel");
 }
 
@@ -291,9 +306,10 @@ static void launch_wgrad(msbg_ctx* ctx, const ConvLevel& L, const uint16_t* x, c
 #define MSBG_CONV_PAIRS(X) X(16, 32) X(32, 16) X(32, 32) X(32, 64) X(64, 32) X(64, 64) X(16, 16) X(64, 16) X(16, 64)
 
 void conv3_forward(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uint16_t* x, const uint16_t* w,
-                   const float* bias, bool relu, bool out_f32, void* y) {
+                   const float* bias, bool relu, bool out_f32, void* y, const uint16_t* mask, int out_ch) {
+    MSBG_REQUIRE(out_ch >= 0 && out_ch <= cout && (out_f32 || out_ch == 0 || out_ch == cout), "conv3: bad output width");
 #define MSBG_FWD_CASE(A, B) \
-    if (cin == A && cout == B) return launch_fwd<A, B>(ctx, L, x, w, bias, relu, out_f32, y);
+    if (cin == A && cout == B) return launch_fwd<A, B>(ctx, L, x, w, bias, relu, mask, out_f32, out_ch, y);
     MSBG_CONV_PAIRS(MSBG_FWD_CASE)
 #undef MSBG_FWD_CASE
     MSBG_THROW(MSBG_ERR_ARG, "conv3: channel counts must be 16, 32 or 64");

@@ -34,9 +34,12 @@ struct ConvLevel {
 };
 
 // y = conv(x) (+ bias) (ReLU): x bf16 [cells][cin], w bf16 [27][cout][cin],
-// y bf16 or f32 [cells][cout].  cin, cout in {16, 32, 64}.
+// y bf16 or f32 [cells][cout].  cin, cout in {16, 32, 64}.  mask (bf16
+// [cells][cout], optional) zeroes outputs where it is not positive (the ReLU
+// derivative of the data gradient).  out_ch (f32 output only, 0 = cout)
+// writes the first out_ch channels as rows of out_ch.
 void conv3_forward(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uint16_t* x, const uint16_t* w,
-                   const float* bias, bool relu, bool out_f32, void* y);
+                   const float* bias, bool relu, bool out_f32, void* y, const uint16_t* mask = nullptr, int out_ch = 0);
 
 // dw = sum over cells of x[c + d(t)] dy[c]^T as f32 [27][cout][cin]; `acc`
 // adds to dw instead of overwriting.
