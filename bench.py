@@ -30,7 +30,10 @@ poisson: the pressure solve on the level-0 blocks of the FLIP layout (776
   divergence of a random smooth velocity field (32 Gaussian blobs).  One step =
   one solve from x = 0 to 1e-6 relative residual; metric = milliseconds per
   solve (lower is better); plain multigrid V-cycles and MG-preconditioned CG
-  are both timed.
+  are timed beside the learned-preconditioned CG (the network alone, and a
+  V-cycle plus the network's correction of its error, the headline), whose
+  network is first trained on the device on (residual, multigrid error)
+  pairs the solver generates for other right-hand sides.
 
 --impl reference times the reference algorithm on the host CPU (the C++
 restatement in oracle/, all host threads) on a bounded sample of the same
@@ -687,10 +690,21 @@ def run_poisson(args, world, rank, local):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     P = msbg.Poisson(ctx, size, size, size, 16, active)
     b = torch.from_numpy(bh.reshape(-1)).to(dev)
-    x = torch.zeros(P.n, device=dev)
+    x = torch.zeros(P.n, device=dev, dtype=torch.float64)
     torch.cuda.synchronize()
-    methods = {"plain_mg": msbg.MG, "mg_pcg": msbg.PCG}
-    head = "mg_pcg"
+    # the learned preconditioner, trained on pairs the solver generates on
+    # this geometry (right-hand sides of other seeds than the timed one)
+    net = msbg.UNet(ctx, size, size, size, active, seed=1)
+    P.set_preconditioner(net)
+    t_train = time.perf_counter()
+    hist = P.train_preconditioner(n_rhs=args.train_rhs, mg_iters=args.train_iters, steps_per_rhs=args.train_iters,
+                                  pool=64, lr=1e-3, target=1, seed=7)
+    ctx.synchronize()
+    t_train = time.perf_counter() - t_train
+    ev = P.eval_preconditioner(n_rhs=2, mg_iters=10, seed=99)
+    methods = {"plain_mg": msbg.MG, "mg_pcg": msbg.PCG, "learned_pcg": msbg.LEARNED, "hybrid_pcg": msbg.HYBRID,
+               "learned_mg": msbg.LEARNED_MG}
+    head = "hybrid_pcg"
 
     def one(method):
         x.zero_()
@@ -728,10 +742,17 @@ def run_poisson(args, world, rank, local):
     for name, m in methods.items():
         one(m)
         t, it, rel = one(m)
-        per_method[name] = {"ms": t, "iterations": it, "rel_residual": rel}
+        per_method[name] = {"ms": t, "iterations": it, "rel_residual": rel, **P.solve_stats(),
+                            "history": [float("%.3g" % v) for v in P.last_history[:12]]}
     # end to end through the C ABI with host arrays
     t = time.perf_counter()
     _, it_h, rel_h, _ = P.solve(bh.reshape(-1), method=methods[head], tol=1e-6, max_iter=400)
+    learned = {"pairs": args.train_rhs * args.train_iters, "adam_steps": int(len(hist)), "train_s": t_train,
+               "loss_first": float(np.mean(hist[:20])) if len(hist) else None,
+               "loss_last": float(np.mean(hist[-20:])) if len(hist) else None,
+               "rel_error_fresh_pairs": ev,
+               "speedup_vs_plain_mg": per_method["plain_mg"]["ms"] / per_method[head]["ms"],
+               "speedup_vs_mg_pcg": per_method["mg_pcg"]["ms"] / per_method[head]["ms"]}
     e2e_ms = (time.perf_counter() - t) * 1e3
     peak, peak_kind = load_peaks()
     jac = kern.get("pk_jacobi", (1, float("nan")))
@@ -741,7 +762,7 @@ def run_poisson(args, world, rank, local):
     jac_bytes = prof_steps * (its[0] + 1) * sum(4 * 12.0 * c for c in level_cells)
     jac_gbs = jac_bytes / (jac[1] * 1e-3) / 1e9
     line = {
-        "metric": "time to 1e-6 relative residual (Poisson, 7-point, MG-preconditioned CG)", "value": ms, "unit": "ms",
+        "metric": "time to 1e-6 relative residual (Poisson, 7-point, learned-preconditioned CG)", "value": ms, "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 dots and coarsest solve)",
         "data": "synthetic (seeded smooth-divergence right-hand side; no dataset exists for this path)",
@@ -753,6 +774,7 @@ def run_poisson(args, world, rank, local):
         "gpu_launches": launches,
         "iterations": its[0],
         "methods": per_method,
+        "learned": learned,
         "kernels_ms_per_step": {k: round(v[1] / prof_steps, 4) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][1])},
         "roofline": {"kernel": "pk_jacobi", "bound": "hbm", "achieved": round(jac_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(jac_gbs / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -842,6 +864,8 @@ def main():
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--train-rhs", type=int, default=100, help="poisson: right-hand sides generating training pairs")
+    ap.add_argument("--train-iters", type=int, default=40, help="poisson: V-cycles (pairs) and Adam steps per rhs")
     args = ap.parse_args()
     if args.size is None:
         args.size = {"flip": 256, "smoother": 2048, "poisson": 256}[args.workload]

@@ -62,6 +62,7 @@ typedef struct msbg_ctx msbg_ctx;
 typedef struct msbg_grid msbg_grid;
 typedef struct msbg_mac msbg_mac;
 typedef struct msbg_poisson msbg_poisson;
+typedef struct msbg_unet msbg_unet;
 
 /* ---- context ---------------------------------------------------------- */
 const char* msbg_status_string(int status);
@@ -278,6 +279,47 @@ int msbg_poisson_solve_device(msbg_poisson* p, int method, float* d_x, const flo
                               int* iters_out, double* rel_res_out, double* history);
 int msbg_poisson_solve(msbg_poisson* p, int method, float* x, const float* b, double tol, int max_iter,
                        int* iters_out, double* rel_res_out, double* history);
+/* Learned preconditioner of methods 2 and 3 (not owned; NULL clears).  The
+ * network must be built on the same level-0 blocks (bsx 16) and context.
+ * method 2: flexible CG preconditioned by the network followed by a V-cycle
+ * on its residual, z = N r + V(r - A N r); method 3: flexible CG
+ * preconditioned by V-cycle, network, V-cycle: t = V r + N(r - A V r),
+ * z = t + V(r - A t).  Both fall back to the V-cycle (and restart)
+ * when the residual stalls for three iterations or a direction loses
+ * positivity (method 4, the stationary iteration x += z with the method-3 z,
+ * falls back to plain V-cycles when an iteration fails to halve the
+ * residual).  msbg_poisson_solve_stats gives, for the last solve (int[4]),
+ * V-cycle applications, network applications, the fallback reason (0 none,
+ * 1 stall, 2 p.Ap <= 0, 3 r.z <= 0) and the iteration it happened at. */
+int msbg_poisson_set_preconditioner(msbg_poisson* p, msbg_unet* net);
+/* msbg_poisson_solve_device with the solution in FP64 (d_x: initial guess in,
+ * solution out).  The f32 entry points round the FP64 solution on return; on
+ * smooth right-hand sides that rounding alone can leave a relative residual
+ * of order 6 eps / lambda_min (about 1e-5 on thin shells), so callers that
+ * need the 1e-6 residual in the stored solution use this one. */
+int msbg_poisson_solve_f64_device(msbg_poisson* p, int method, double* d_x, const float* d_b, double tol,
+                                  int max_iter, int* iters_out, double* rel_res_out, double* history);
+int msbg_poisson_solve_stats(const msbg_poisson* p, int* out);
+/* Right-hand side of the learned-preconditioner workload on the device: the
+ * divergence of a random smooth velocity field (n_blobs Gaussian blobs,
+ * sigma uniform in [4, 16] cells, amplitudes N(0,1)^3, centres in random
+ * active blocks) at the level-0 cell centres; `seed` selects the field. */
+int msbg_poisson_rhs_device(msbg_poisson* p, uint64_t seed, int n_blobs, float* d_b);
+/* Trains the network on pairs the solver generates: per right-hand side
+ * (seeds seed*1000003 + i), the MG-PCG solution x* to 1e-7, then plain
+ * V-cycles from zero giving (residual r_k, error x* - x_k) after each cycle
+ * (target 0), or (r_k - A V r_k, x* - x_k - V r_k) (target 1, for method 3).
+ * Pairs fill a device pool of `pool` slots; after each right-hand side,
+ * steps_per_rhs Adam steps (learning rate lr) on random pool slots.  The
+ * network's output scale is set from the first right-hand side's pairs.
+ * loss_hist (may be NULL) receives up to hist_cap per-step losses. */
+int msbg_poisson_train_preconditioner(msbg_poisson* p, int n_rhs, int mg_iters, int steps_per_rhs, int pool, float lr,
+                                      int target, uint64_t seed, double* loss_hist, int64_t hist_cap,
+                                      int64_t* steps_out);
+/* Mean relative L2 errors over fresh pairs (as above, seeds from `seed`):
+ * out[0] network alone ||N r - e|| / ||e||, out[1] one V-cycle
+ * ||V r - e|| / ||e||, out[2] V-cycle plus network correction. */
+int msbg_poisson_eval_preconditioner(msbg_poisson* p, int n_rhs, int mg_iters, uint64_t seed, double* out3);
 
 /* ---- block-sparse 3x3x3 convolution on the tensor cores ------------------
  * No counterpart in the reference (the learned preconditioner of the pressure
@@ -308,7 +350,6 @@ int msbg_conv3_wgrad_device(msbg_ctx* ctx, const int32_t* d_nbr27, int64_t n_blo
  * [27][cout][cin] (padded channels stay zero).  A train step returns the loss
  * sum((out_scale y - e/rms(r))^2) / sum((e/rms(r))^2) and leaves the
  * gradient readable with msbg_unet_get_grads; update != 0 applies Adam. */
-typedef struct msbg_unet msbg_unet;
 int msbg_unet_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, const uint64_t* active, size_t n,
                      uint64_t seed, msbg_unet** out);
 int msbg_unet_destroy(msbg_unet* net);

@@ -117,6 +117,12 @@ SIGNATURES = {
     "msbg_poisson_dot_device": [_P, _P, _P, C.POINTER(C.c_double)],
     "msbg_poisson_solve_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_solve": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
+    "msbg_poisson_set_preconditioner": [_P, _P],
+    "msbg_poisson_solve_f64_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
+    "msbg_poisson_solve_stats": [_P, _P],
+    "msbg_poisson_rhs_device": [_P, _U64, _I, _P],
+    "msbg_poisson_train_preconditioner": [_P, _I, _I, _I, _I, _F, _I, _U64, _P, C.c_int64, C.POINTER(C.c_int64)],
+    "msbg_poisson_eval_preconditioner": [_P, _I, _I, _U64, _P],
 }
 
 _lib = None

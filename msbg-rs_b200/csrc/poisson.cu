@@ -22,8 +22,10 @@
 // with a fixed two-stage reduction order (deterministic).
 #include <algorithm>
 #include <cmath>
+#include <random>
 
 #include "common.cuh"
+#include "unet.cuh"
 
 namespace msbg {
 
@@ -60,6 +62,10 @@ struct msbg_poisson {
     int nu1 = 2, nu2 = 2;
     float omega = 2.0f / 3.0f;
     msbg::DevBuf work;   // PCG vectors + dot partials
+    msbg_unet* net = nullptr;  // learned preconditioner (not owned)
+    // PCG statistics of the last solve: preconditioner applications of each
+    // kind and whether the learned preconditioner fell back to multigrid
+    int n_net = 0, n_vcycle = 0, fell_back = 0, fallback_iter = -1;
 };
 
 namespace msbg {
@@ -205,12 +211,20 @@ __global__ void pk_prolong(TransferArgs T, const float* __restrict__ xc, float* 
     }
 }
 
-// x_c = A^-1 b_c with the FP64 inverse (column-major).
+// x_c = A^-1 b_c with the FP64 inverse, one warp per row.  The inverse of
+// the symmetric operator is symmetric, so row i is column i: its n entries
+// are contiguous and the warp reads them coalesced.  Lane partial sums are
+// combined in a fixed butterfly order (deterministic).
 __global__ void pk_dense_solve(const double* __restrict__ ainv, int64_t n, const float* __restrict__ b, float* __restrict__ x) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const double* row = ainv + i * n;
         double s = 0.0;
-        for (int64_t j = 0; j < n; ++j) s += ainv[j * n + i] * (double)b[j];
-        x[i] = (float)s;
+        for (int64_t j = lane; j < n; j += 32) s += row[j] * (double)b[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) x[i] = (float)s;
     }
 }
 
@@ -401,7 +415,7 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
     }
     upload(ctx, P->ainv, inv.data(), inv.size() * 8);
     const int64_t n0 = P->lv[0].cells();
-    P->work.reserve((size_t)n0 * (4 * 4 + 8) + (DOT_BLOCKS + 16) * 8 + 1024);
+    P->work.reserve((size_t)n0 * (7 * 4 + 8) + (DOT_BLOCKS + 16) * 8 + 1024);
     sync(ctx);
 }
 
@@ -438,7 +452,7 @@ static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps,
 static void vcycle(msbg_poisson* P, int l, float* x, const float* b, bool x_zero) {
     if (l == (int)P->lv.size() - 1) {
         begin_launch(P->ctx);
-        pk_dense_solve<<<grid_for(P->nc), 256, 0, P->ctx->stream>>>(P->ainv.as<double>(), P->nc, b, x);
+        pk_dense_solve<<<grid_for(P->nc * 32), 256, 0, P->ctx->stream>>>(P->ainv.as<double>(), P->nc, b, x);
         after_launch(P->ctx, "pk_dense_solve");
         return;
     }
@@ -492,56 +506,149 @@ static void add64(msbg_poisson* P, int64_t n, double a, const float* d, double* 
     after_launch(P->ctx, "pk_add64");
 }
 
-// method 0: V-cycles (x += V(b - A x)); 1: MG-preconditioned CG.  The solution
-// accumulates in FP64 and convergence is judged on the true residual
-// b - A x of that FP64 solution; PCG's recursively updated residual is
-// replaced by the true one when it reaches the tolerance (and the iteration
-// restarts from it if the true residual is still above).  Returns iterations.
+// Preconditioners of the CG solve.
+enum { PC_MG = 0, PC_NET = 1, PC_HYBRID = 2 };
+
+// z += V (r - A z).  The network's correction removes smooth error that
+// V-cycles with piecewise-constant prolongation reduce slowly, and leaves
+// high-frequency error that the operator amplifies in the residual; a
+// V-cycle on the residual equation removes that.
+static void post_smooth(msbg_poisson* P, float* z, const float* r, float* s, float* u) {
+    const int64_t n = P->lv[0].cells();
+    launch_residual(P, 0, z, r, s);
+    vcycle(P, 0, u, s, true);
+    axpby(P, n, 1.0, u, 1.0, z);
+}
+
+// z = V r, then the network's correction of the remaining error,
+// z += N(r - A z), then post_smooth (V-cycle, network, V-cycle).
+static void learned_cycle(msbg_poisson* P, float* z, const float* r, float* s, float* u) {
+    const int64_t n = P->lv[0].cells();
+    vcycle(P, 0, z, r, true);
+    launch_residual(P, 0, z, r, s);
+    unet_apply(P->net, s, u);
+    axpby(P, n, 1.0, u, 1.0, z);
+    post_smooth(P, z, r, s, u);
+}
+
+// method 0: V-cycles (x += V(b - A x)); 1: MG-preconditioned CG; 2: flexible
+// CG preconditioned by the learned network; 3: flexible CG preconditioned by
+// a V-cycle plus the network's correction of the V-cycle's remaining error,
+// z = V r + N(r - A V r).  Methods 2 and 3 fall back to the V-cycle
+// preconditioner (and restart) when the residual stalls (three iterations in
+// a row without a 5 % decrease) or a search direction loses positivity.  The
+// solution accumulates in FP64 and convergence is judged on the true
+// residual b - A x of that FP64 solution; CG's recursively updated residual
+// is replaced by the true one when it reaches the tolerance (and the
+// iteration restarts from it if the true residual is still above).  Returns
+// iterations.
 static int solve(msbg_poisson* P, int method, float* x, const float* b, double tol, int max_iter, double* rel_out,
-                 double* hist) {
+                 double* hist, double* x64_ext = nullptr) {
     PLevelDev& F = P->lv[0];
     const int64_t n = F.cells();
     float* r = (float*)P->work.p;
     float* z = r + n;
     float* p = z + n;
     float* q = p + n;
-    double* x64 = (double*)(q + n);
+    double* x64 = x64_ext ? x64_ext : (double*)(q + n);
+    float* r_old = (float*)((double*)(q + n) + n);
+    float* sv = r_old + n;
+    float* uv = sv + n;
+    P->n_net = P->n_vcycle = P->fell_back = 0;
+    P->fallback_iter = -1;
+    if (method >= 2) MSBG_REQUIRE(P->net != nullptr, "learned preconditioner not set (msbg_poisson_set_preconditioner)");
     const double bn = std::sqrt(dot(P, b, b, n));
     if (bn == 0.0) {
-        CUDA_CHECK(cudaMemsetAsync(x, 0, n * 4, P->ctx->stream));
+        if (x64_ext) CUDA_CHECK(cudaMemsetAsync(x64_ext, 0, n * 8, P->ctx->stream));
+        else CUDA_CHECK(cudaMemsetAsync(x, 0, n * 4, P->ctx->stream));
         if (rel_out) *rel_out = 0.0;
         return 0;
     }
-    begin_launch(P->ctx);
-    pk_widen<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, x, x64);
-    after_launch(P->ctx, "pk_widen");
+    if (!x64_ext) {
+        begin_launch(P->ctx);
+        pk_widen<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, x, x64);
+        after_launch(P->ctx, "pk_widen");
+    }
     launch_residual64(P, x64, b, r);
     double rn = std::sqrt(dot(P, r, r, n));
     int it = 0;
-    if (method == 0) {
+    if (method == 0 || method == 4) {
+        // stationary iteration x += M r with M = V (method 0) or the hybrid
+        // M r = V r + N(r - A V r) (method 4); the learned one falls back to
+        // V when an iteration fails to halve the residual
+        bool learned = method == 4;
+        double rn_prev = rn;
         while (rn > tol * bn && it < max_iter) {
-            vcycle(P, 0, z, r, true);
+            if (learned) {
+                learned_cycle(P, z, r, sv, uv);
+                P->n_net++;
+                P->n_vcycle++;
+            } else {
+                vcycle(P, 0, z, r, true);
+            }
+            P->n_vcycle++;
             add64(P, n, 1.0, z, x64);
             launch_residual64(P, x64, b, r);
             rn = std::sqrt(dot(P, r, r, n));
             if (!std::isfinite(rn)) MSBG_THROW(MSBG_ERR_NUMERIC, "multigrid residual is not finite");
             if (hist) hist[it] = rn / bn;
             ++it;
+            if (learned && rn > 0.5 * rn_prev) {
+                learned = false;
+                P->fell_back = 1;
+                P->fallback_iter = it;
+            }
+            rn_prev = rn;
         }
     } else {
+        int pc = method == 1 ? PC_MG : (method == 2 ? PC_NET : PC_HYBRID);
+        const bool flexible = method >= 2;
+        auto precondition = [&](const float* rr, float* zz) {
+            if (pc == PC_MG) {
+                vcycle(P, 0, zz, rr, true);
+                P->n_vcycle++;
+            } else if (pc == PC_NET) {
+                unet_apply(P->net, rr, zz);
+                post_smooth(P, zz, rr, sv, uv);
+                P->n_net++;
+                P->n_vcycle++;
+            } else {
+                learned_cycle(P, zz, rr, sv, uv);
+                P->n_vcycle += 2;
+                P->n_net++;
+            }
+        };
         double rz = 0.0;
         auto restart = [&]() {
-            vcycle(P, 0, z, r, true);
+            precondition(r, z);
             CUDA_CHECK(cudaMemcpyAsync(p, z, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
             rz = dot(P, r, z, n);
         };
+        int since = 0;  // iterations since the last (re)start
+        std::vector<double> rn_hist;
+        auto fall_back = [&](int reason) {
+            pc = PC_MG;
+            P->fell_back = reason;
+            P->fallback_iter = it;
+            restart();
+            since = 0;
+        };
+        rn_hist.push_back(rn);  // the window below always holds the start
         restart();
+        if (flexible && !(rz > 0.0)) fall_back(3);
         while (rn > tol * bn && it < max_iter) {
             launch_matvec(P, 0, p, q);
             const double pq = dot(P, p, q, n);
-            if (!(pq > 0.0) || !std::isfinite(rz)) MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
+            if (!(pq > 0.0) || !std::isfinite(rz)) {
+                if (flexible && pc != PC_MG) {
+                    fall_back(2);
+                    continue;
+                }
+                MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
+            }
             const double alpha = rz / pq;
             add64(P, n, alpha, p, x64);
+            if (flexible) CUDA_CHECK(cudaMemcpyAsync(r_old, r, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
             axpby(P, n, -alpha, q, 1.0, r);
             rn = std::sqrt(dot(P, r, r, n));
             ++it;
@@ -551,21 +658,232 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                 if (hist) hist[it - 1] = rn / bn;
                 if (rn <= tol * bn) break;
                 restart();
+                since = 0;
                 continue;
             }
             if (hist) hist[it - 1] = rn / bn;
-            vcycle(P, 0, z, r, true);
+            rn_hist.push_back(rn);
+            ++since;
+            // stall: the residual norm of CG is not monotone, so the test is
+            // over a window: less than a halving in the last 4 iterations
+            if (flexible && pc != PC_MG && since >= 4 && rn > 0.5 * rn_hist[rn_hist.size() - 5]) {
+                fall_back(1);
+                continue;
+            }
+            precondition(r, z);
             const double rz2 = dot(P, r, z, n);
-            const double beta = rz2 / rz;
+            double beta = rz2 / rz;
+            if (flexible) beta = (rz2 - dot(P, z, r_old, n)) / rz;
+            if (flexible && pc != PC_MG && !(rz2 > 0.0)) {
+                fall_back(3);
+                continue;
+            }
             rz = rz2;
             axpby(P, n, 1.0, z, beta, p);
         }
     }
-    begin_launch(P->ctx);
-    pk_narrow<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, x64, x);
-    after_launch(P->ctx, "pk_narrow");
+    if (!x64_ext) {
+        begin_launch(P->ctx);
+        pk_narrow<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, x64, x);
+        after_launch(P->ctx, "pk_narrow");
+    }
     if (rel_out) *rel_out = rn / bn;
     return it;
+}
+
+// ---- training data: solver-generated (residual, multigrid error) pairs -------
+// Right-hand side of the learned-preconditioner workload on the device: the
+// divergence of u = sum_i a_i exp(-|x - c_i|^2 / (2 s_i^2)), evaluated at
+// level-0 cell centres: b = sum_i -(a_i . (x - c_i)) / s_i^2 g_i(x).
+// blobs: [n_blobs][7] = (cx, cy, cz, s, ax, ay, az).
+__global__ void pk_blob_rhs(LevelArgs L, const int32_t* __restrict__ coords, const float* __restrict__ blobs, int n_blobs,
+                            float* __restrict__ bout) {
+    const int bs = 1 << L.lg, m = bs - 1;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L.cells; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i >> (3 * L.lg);
+        const int v = (int)(i & ((1 << (3 * L.lg)) - 1));
+        const double px = coords[3 * k] * bs + (v & m) + 0.5, py = coords[3 * k + 1] * bs + ((v >> L.lg) & m) + 0.5,
+                     pz = coords[3 * k + 2] * bs + (v >> (2 * L.lg)) + 0.5;
+        double acc = 0.0;
+        for (int j = 0; j < n_blobs; ++j) {
+            const float* B = blobs + 7 * j;
+            const double dx = px - B[0], dy = py - B[1], dz = pz - B[2], s2 = (double)B[3] * B[3];
+            const double g = exp(-(dx * dx + dy * dy + dz * dz) / (2.0 * s2));
+            acc += -(B[4] * dx + B[5] * dy + B[6] * dz) / s2 * g;
+        }
+        bout[i] = (float)acc;
+    }
+}
+
+// e = xs - x (FP64 in, f32 out)
+__global__ void pk_sub64(int64_t n, const double* __restrict__ xs, const double* __restrict__ x, float* __restrict__ e) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        e[i] = (float)(xs[i] - x[i]);
+}
+
+// Fills b with the smooth-divergence right-hand side of random seed `seed`.
+static void blob_rhs(msbg_poisson* P, uint64_t seed, int n_blobs, float* b, DevBuf& blob_buf) {
+    PLevelDev& F = P->lv[0];
+    std::mt19937_64 rng(seed);
+    std::uniform_int_distribution<int64_t> pick_block(0, F.n() - 1);
+    std::uniform_real_distribution<double> u01(0.0, 1.0);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    std::vector<float> blobs((size_t)n_blobs * 7);
+    for (int j = 0; j < n_blobs; ++j) {
+        const uint64_t bid = F.bids[pick_block(rng)];
+        const double bx = (double)(bid % F.nx), by = (double)((bid / F.nx) % F.ny), bz = (double)(bid / (F.nx * F.ny));
+        blobs[7 * j + 0] = (float)((bx + u01(rng)) * F.bs);
+        blobs[7 * j + 1] = (float)((by + u01(rng)) * F.bs);
+        blobs[7 * j + 2] = (float)((bz + u01(rng)) * F.bs);
+        blobs[7 * j + 3] = (float)(4.0 + 12.0 * u01(rng));
+        for (int a = 0; a < 3; ++a) blobs[7 * j + 4 + a] = (float)nd(rng);
+    }
+    blob_buf.reserve(blobs.size() * 4);
+    CUDA_CHECK(cudaMemcpyAsync(blob_buf.p, blobs.data(), blobs.size() * 4, cudaMemcpyHostToDevice, P->ctx->stream));
+    begin_launch(P->ctx);
+    pk_blob_rhs<<<grid_for(F.cells()), 256, 0, P->ctx->stream>>>(level_args(F), F.coords.as<int32_t>(),
+                                                                  blob_buf.as<float>(), n_blobs, b);
+    after_launch(P->ctx, "pk_blob_rhs");
+    sync(P->ctx);  // the host blob table dies at scope end
+}
+
+// Training of the learned preconditioner on pairs the solver generates: for
+// each right-hand side, x* from MG-preconditioned CG to 1e-7, then plain
+// multigrid from zero; after V-cycle k the pair is (residual r_k, error
+// x* - x_k), or with target 1 the pair the hybrid preconditioner needs
+// (s_k = r_k - A V r_k, x* - x_k - V r_k).  Pairs go to a pool of `pool`
+// slots on the device; after each right-hand side, `steps_per_rhs` Adam
+// steps train on pool slots drawn at random.  out_scale is set from the
+// first right-hand side's pairs (mean rms(error) / rms(residual)).
+struct TrainStats {
+    int64_t steps = 0, pairs = 0;
+};
+
+static TrainStats train(msbg_poisson* P, int n_rhs, int mg_iters, int steps_per_rhs, int pool, float lr, int target,
+                        uint64_t seed, double* loss_hist, int64_t hist_cap) {
+    MSBG_REQUIRE(P->net, "learned preconditioner not set");
+    PLevelDev& F = P->lv[0];
+    const int64_t n = F.cells();
+    msbg_ctx* ctx = P->ctx;
+    DevBuf bbuf, xs, xk, blobs, pairs;
+    bbuf.reserve(n * 4);
+    xs.reserve(n * 8);
+    xk.reserve(n * 8);
+    pairs.reserve((size_t)pool * 2 * n * 4);
+    float* b = bbuf.as<float>();
+    float* r = (float*)P->work.p;  // solve() scratch, free between solves
+    float* z = r + n;
+    float* t = z + n;
+    std::mt19937_64 rng(seed ^ 0x5eedULL);
+    int64_t filled = 0, next = 0;
+    TrainStats st;
+    double scale_sum = 0.0;
+    int scale_cnt = 0;
+    for (int i = 0; i < n_rhs; ++i) {
+        blob_rhs(P, seed * 1000003ULL + (uint64_t)i, 32, b, blobs);
+        // reference solution
+        float* xf = (float*)P->work.p + 6 * n;  // uv slot as the f32 solution
+        CUDA_CHECK(cudaMemsetAsync(xf, 0, n * 4, ctx->stream));
+        solve(P, 1, xf, b, 1e-7, 500, nullptr, nullptr);
+        double* x64 = (double*)((float*)P->work.p + 4 * n);
+        CUDA_CHECK(cudaMemcpyAsync(xs.p, x64, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_CHECK(cudaMemsetAsync(xk.p, 0, n * 8, ctx->stream));
+        for (int k = 0; k < mg_iters; ++k) {
+            launch_residual64(P, xk.as<double>(), b, r);
+            float* pr = pairs.as<float>() + (size_t)next * 2 * n;
+            float* pe = pr + n;
+            begin_launch(ctx);
+            pk_sub64<<<grid_for(n), 256, 0, ctx->stream>>>(n, xs.as<double>(), xk.as<double>(), pe);
+            after_launch(ctx, "pk_sub64");
+            vcycle(P, 0, z, r, true);  // z = V r
+            if (target == 0) {
+                CUDA_CHECK(cudaMemcpyAsync(pr, r, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+            } else {
+                launch_residual(P, 0, z, r, pr);  // s = r - A V r
+                axpby(P, n, -1.0, z, 1.0, pe);    // e - V r
+            }
+            if (i == 0) {
+                const double a = dot(P, pe, pe, n), c = dot(P, pr, pr, n);
+                if (c > 0.0 && a > 0.0) {
+                    scale_sum += std::sqrt(a / c);
+                    scale_cnt++;
+                }
+            }
+            add64(P, n, 1.0, z, xk.as<double>());
+            next = (next + 1) % pool;
+            filled = std::min<int64_t>(filled + 1, pool);
+            st.pairs++;
+        }
+        if (i == 0 && scale_cnt) {
+            (void)t;
+            MSBG_REQUIRE(std::isfinite(scale_sum / scale_cnt), "non-finite output scale");
+            msbg_unet_set_output_scale(P->net, (float)(scale_sum / scale_cnt));
+        }
+        std::uniform_int_distribution<int64_t> pick(0, std::max<int64_t>(filled - 1, 0));
+        for (int s = 0; s < steps_per_rhs && filled > 0; ++s) {
+            const int64_t j = pick(rng);
+            const float* pr = pairs.as<float>() + (size_t)j * 2 * n;
+            const double l = unet_train_step(P->net, pr, pr + n, lr, true);
+            if (loss_hist && st.steps < hist_cap) loss_hist[st.steps] = l;
+            st.steps++;
+        }
+    }
+    sync(ctx);
+    return st;
+}
+
+// Mean relative L2 error over fresh pairs (seed `seed`) of: the network
+// alone N(r) against e, one V-cycle V r against e, and the hybrid V r +
+// N(r - A V r) against e.
+static void evaluate(msbg_poisson* P, int n_rhs, int mg_iters, uint64_t seed, double out[3]) {
+    PLevelDev& F = P->lv[0];
+    const int64_t n = F.cells();
+    msbg_ctx* ctx = P->ctx;
+    DevBuf bbuf, xs, xk, blobs, ebuf, tmp;
+    bbuf.reserve(n * 4);
+    xs.reserve(n * 8);
+    xk.reserve(n * 8);
+    ebuf.reserve(n * 4);
+    tmp.reserve(n * 4 * 3);
+    float* b = bbuf.as<float>();
+    float* e = ebuf.as<float>();
+    float* zn = tmp.as<float>();
+    float* zv = zn + n;
+    float* sres = zv + n;
+    double acc[3] = {0, 0, 0};
+    int cnt = 0;
+    for (int i = 0; i < n_rhs; ++i) {
+        blob_rhs(P, seed * 1000003ULL + (uint64_t)i, 32, b, blobs);
+        float* xf = (float*)P->work.p + 6 * n;
+        CUDA_CHECK(cudaMemsetAsync(xf, 0, n * 4, ctx->stream));
+        solve(P, 1, xf, b, 1e-7, 500, nullptr, nullptr);
+        CUDA_CHECK(cudaMemcpyAsync(xs.p, (double*)((float*)P->work.p + 4 * n), n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_CHECK(cudaMemsetAsync(xk.p, 0, n * 8, ctx->stream));
+        float* r = (float*)P->work.p;
+        for (int k = 0; k < mg_iters; ++k) {
+            launch_residual64(P, xk.as<double>(), b, r);
+            begin_launch(ctx);
+            pk_sub64<<<grid_for(n), 256, 0, ctx->stream>>>(n, xs.as<double>(), xk.as<double>(), e);
+            after_launch(ctx, "pk_sub64");
+            const double en = std::sqrt(dot(P, e, e, n));
+            vcycle(P, 0, zv, r, true);
+            unet_apply(P->net, r, zn);
+            axpby(P, n, -1.0, e, 1.0, zn);  // N r - e
+            acc[0] += std::sqrt(dot(P, zn, zn, n)) / en;
+            launch_residual(P, 0, zv, r, sres);
+            unet_apply(P->net, sres, zn);
+            axpby(P, n, 1.0, zv, 1.0, zn);   // V r + N(s)
+            axpby(P, n, -1.0, e, 1.0, zn);
+            acc[2] += std::sqrt(dot(P, zn, zn, n)) / en;
+            axpby(P, n, -1.0, e, 1.0, zv);   // V r - e
+            acc[1] += std::sqrt(dot(P, zv, zv, n)) / en;
+            // advance the plain multigrid iterate
+            vcycle(P, 0, zv, r, true);
+            add64(P, n, 1.0, zv, xk.as<double>());
+            ++cnt;
+        }
+    }
+    for (int j = 0; j < 3; ++j) out[j] = cnt ? acc[j] / cnt : 0.0;
 }
 
 }  // namespace msbg
@@ -662,7 +980,7 @@ int msbg_poisson_dot_device(msbg_poisson* P, const float* d_a, const float* d_b,
 int msbg_poisson_solve_device(msbg_poisson* P, int method, float* d_x, const float* d_b, double tol, int max_iter,
                               int* iters_out, double* rel_res_out, double* history) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(P && d_x && d_b && (method == 0 || method == 1) && max_iter >= 0 && tol > 0.0, "bad argument");
+    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     int it = solve(P, method, d_x, d_b, tol, max_iter, rel_res_out, history);
     if (iters_out) *iters_out = it;
@@ -672,7 +990,7 @@ int msbg_poisson_solve_device(msbg_poisson* P, int method, float* d_x, const flo
 int msbg_poisson_solve(msbg_poisson* P, int method, float* x, const float* b, double tol, int max_iter, int* iters_out,
                        double* rel_res_out, double* history) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(P && x && b && (method == 0 || method == 1) && max_iter >= 0 && tol > 0.0, "bad argument");
+    MSBG_REQUIRE(P && x && b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     const int64_t n = P->lv[0].cells();
     DevBuf io;
@@ -685,6 +1003,66 @@ int msbg_poisson_solve(msbg_poisson* P, int method, float* x, const float* b, do
     CUDA_CHECK(cudaMemcpyAsync(x, dx, n * 4, cudaMemcpyDeviceToHost, P->ctx->stream));
     sync(P->ctx);
     if (iters_out) *iters_out = it;
+    MSBG_API_END
+}
+
+int msbg_poisson_solve_f64_device(msbg_poisson* P, int method, double* d_x, const float* d_b, double tol, int max_iter,
+                                  int* iters_out, double* rel_res_out, double* history) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
+    set_device(P->ctx);
+    int it = solve(P, method, nullptr, d_b, tol, max_iter, rel_res_out, history, d_x);
+    if (iters_out) *iters_out = it;
+    MSBG_API_END
+}
+
+int msbg_poisson_set_preconditioner(msbg_poisson* P, msbg_unet* net) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P, "null argument");
+    if (net) {
+        MSBG_REQUIRE(P->lv[0].bs == 16 && unet_blocks(net) == P->lv[0].n() && unet_ctx(net) == P->ctx,
+                     "the network must be built on the solve's level-0 blocks (16^3) and context");
+    }
+    P->net = net;
+    MSBG_API_END
+}
+
+int msbg_poisson_solve_stats(const msbg_poisson* P, int* out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && out, "null argument");
+    out[0] = P->n_vcycle;
+    out[1] = P->n_net;
+    out[2] = P->fell_back;
+    out[3] = P->fallback_iter;
+    MSBG_API_END
+}
+
+int msbg_poisson_rhs_device(msbg_poisson* P, uint64_t seed, int n_blobs, float* d_b) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && d_b && n_blobs > 0 && n_blobs <= 4096, "bad argument");
+    set_device(P->ctx);
+    DevBuf blobs;
+    blob_rhs(P, seed, n_blobs, d_b, blobs);
+    MSBG_API_END
+}
+
+int msbg_poisson_train_preconditioner(msbg_poisson* P, int n_rhs, int mg_iters, int steps_per_rhs, int pool, float lr,
+                                      int target, uint64_t seed, double* loss_hist, int64_t hist_cap, int64_t* steps_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && n_rhs >= 0 && mg_iters > 0 && steps_per_rhs >= 0 && pool > 0 && lr >= 0.0f &&
+                     (target == 0 || target == 1),
+                 "bad argument");
+    set_device(P->ctx);
+    const TrainStats st = train(P, n_rhs, mg_iters, steps_per_rhs, pool, lr, target, seed, loss_hist, hist_cap);
+    if (steps_out) *steps_out = st.steps;
+    MSBG_API_END
+}
+
+int msbg_poisson_eval_preconditioner(msbg_poisson* P, int n_rhs, int mg_iters, uint64_t seed, double* out3) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && out3 && n_rhs > 0 && mg_iters > 0 && P->net, "bad argument");
+    set_device(P->ctx);
+    evaluate(P, n_rhs, mg_iters, seed, out3);
     MSBG_API_END
 }
 

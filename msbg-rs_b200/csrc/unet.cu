@@ -39,6 +39,7 @@ struct msbg_unet {
     bool weights_dirty = true;
     // activation pointers (into act)
     uint16_t *x0, *a0, *p1, *a1, *p2, *a2, *a3, *c2, *u1, *a4, *c1, *u0;
+    uint16_t* x0c;  // compact 1-channel input (bf16 [n0]) read by the direct first layer
     float* y;
     uint16_t *dyb, *du0m, *dc1, *da4m, *du1m, *dc2, *da3m, *da2m, *da1m, *da0m;
     float *dp2, *dp1;
@@ -68,14 +69,86 @@ __device__ __forceinline__ uint4 pack8(const float* f) {
     return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// x0[c] = (bf16(r[c] * s), 0, ..., 0): the 1-channel input padded to 16.
+// x0c[c] = bf16(r[c] * s); with x0 also the same value padded to 16
+// channels (the weight gradient of the first layer reads that form).
 __global__ void un_input_kernel(int64_t n, const float* __restrict__ r, const double* __restrict__ s_in,
-                                uint16_t* __restrict__ x0) {
+                                uint16_t* __restrict__ x0c, uint16_t* __restrict__ x0) {
     const float s = (float)(1.0 / *s_in);
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
-        uint4* o = reinterpret_cast<uint4*>(x0 + c * 16);
-        o[0] = make_uint4((uint32_t)tobf(r[c] * s), 0u, 0u, 0u);
-        o[1] = make_uint4(0u, 0u, 0u, 0u);
+        const uint16_t h = tobf(r[c] * s);
+        x0c[c] = h;
+        if (x0) {
+            uint4* o = reinterpret_cast<uint4*>(x0 + c * 16);
+            o[0] = make_uint4((uint32_t)h, 0u, 0u, 0u);
+            o[1] = make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+}
+
+// Neighbour cell of level-0 cell `cell` (16^3 blocks) shifted by tap t, or -1.
+__device__ __forceinline__ int64_t l0_tap(const int32_t* __restrict__ nbr27, int64_t nb, int64_t cell, int t) {
+    const int64_t k = cell >> 12;
+    const int v = (int)(cell & 4095);
+    const int gx = (v & 15) + t % 3 - 1, gy = ((v >> 4) & 15) + (t / 3) % 3 - 1, gz = (v >> 8) + t / 9 - 1;
+    const int ox = gx < 0 ? 0 : (gx > 15 ? 2 : 1), oy = gy < 0 ? 0 : (gy > 15 ? 2 : 1), oz = gz < 0 ? 0 : (gz > 15 ? 2 : 1);
+    const int code = ox + 3 * oy + 9 * oz;
+    const int32_t kk = code == 13 ? (int32_t)k : nbr27[k * 27 + code];
+    if (kk < 0 || kk >= nb) return -1;
+    return ((int64_t)kk << 12) + ((gx & 15) | ((gy & 15) << 4) | ((gz & 15) << 8));
+}
+
+// First layer on the CUDA cores: a0[c][o] = relu(b[o] + sum_t w[t][o][0] x[c + d(t)]),
+// 1 -> 16 channels (weights bf16 [27][16][16], input channel 0 only).
+__global__ void __launch_bounds__(128) un_conv_in1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
+                                                          const uint16_t* __restrict__ x0c, const uint16_t* __restrict__ w,
+                                                          const float* __restrict__ bias, uint16_t* __restrict__ a0) {
+    __shared__ float ws[27][16];
+    __shared__ float bs[16];
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16) * 16]);
+    if (threadIdx.x < 16) bs[threadIdx.x] = bias[threadIdx.x];
+    __syncthreads();
+    const int64_t n = nb << 12;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        float acc[16];
+#pragma unroll
+        for (int o = 0; o < 16; ++o) acc[o] = 0.0f;
+        for (int t = 0; t < 27; ++t) {
+            const int64_t src = l0_tap(nbr27, nb, c, t);
+            const float xv = src >= 0 ? bf(__ldg(x0c + src)) : 0.0f;
+#pragma unroll
+            for (int o = 0; o < 16; ++o) acc[o] = fmaf(ws[t][o], xv, acc[o]);
+        }
+#pragma unroll
+        for (int o = 0; o < 16; ++o) acc[o] = fmaxf(acc[o] + bs[o], 0.0f);
+        uint4* out = reinterpret_cast<uint4*>(a0 + c * 16);
+        out[0] = pack8(acc);
+        out[1] = pack8(acc + 8);
+    }
+}
+
+// Last layer on the CUDA cores: y[c] = b[0] + sum_t sum_i w[t][0][i] u[c + d(t)][i],
+// 16 -> 1 channel, f32 output.
+__global__ void __launch_bounds__(128) un_conv_out1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
+                                                           const uint16_t* __restrict__ u0, const uint16_t* __restrict__ w,
+                                                           const float* __restrict__ bias, float* __restrict__ y) {
+    __shared__ float ws[27][16];
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16)]);
+    __syncthreads();
+    const float b0 = bias[0];
+    const int64_t n = nb << 12;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (int t = 0; t < 27; ++t) {
+            const int64_t src = l0_tap(nbr27, nb, c, t);
+            if (src < 0) continue;
+            const uint4* row = reinterpret_cast<const uint4*>(u0 + src * 16);
+            float v[16];
+            unpack8(__ldg(row), v);
+            unpack8(__ldg(row + 1), v + 8);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc = fmaf(ws[t][i], v[i], acc);
+        }
+        y[c] = acc + b0;
     }
 }
 
@@ -348,7 +421,13 @@ static void skip_pool_mask(msbg_unet* U, int lf, int C, const uint16_t* gskip, c
 // Forward from the padded input x0; y (f32 [n0]) = network output.
 static void forward(msbg_unet* U) {
     if (U->weights_dirty) cast_weights(U);
-    conv_fwd(U, L0A, U->x0, U->a0);
+    {
+        const ULayer& L = U->layers[L0A];
+        begin_launch(U->ctx);
+        un_conv_in1_kernel<<<grid1(U->n[0], 128), 128, 0, U->ctx->stream>>>(
+            U->nbr.as<int32_t>(), U->nb, U->x0c, U->wb.as<uint16_t>() + L.wb_off, U->params.as<float>() + L.b_off, U->a0);
+        after_launch(U->ctx, "un_conv_in1_kernel");
+    }
     pool(U, 1, 16, U->a0, 0.125f, U->p1);
     conv_fwd(U, L1A, U->p1, U->a1);
     pool(U, 2, 32, U->a1, 0.125f, U->p2);
@@ -359,7 +438,13 @@ static void forward(msbg_unet* U) {
     conv_fwd(U, L1C, U->u1, U->a4);
     conv_fwd(U, L1D, U->a4, U->c1);
     up_add_relu(U, 0, 16, U->c1, U->a0, U->u0);
-    conv_fwd(U, L0C, U->u0, U->y, true, 1);
+    {
+        const ULayer& L = U->layers[L0C];
+        begin_launch(U->ctx);
+        un_conv_out1_kernel<<<grid1(U->n[0], 128), 128, 0, U->ctx->stream>>>(
+            U->nbr.as<int32_t>(), U->nb, U->u0, U->wb.as<uint16_t>() + L.wb_off, U->params.as<float>() + L.b_off, U->y);
+        after_launch(U->ctx, "un_conv_out1_kernel");
+    }
 }
 
 // Backward from dyb; fills every parameter gradient.
@@ -385,9 +470,9 @@ static void backward(msbg_unet* U) {
     conv_wgrad(U, L0A, U->x0, U->da0m);
 }
 
-static void input(msbg_unet* U, const float* r, const double* s_in) {
+static void input(msbg_unet* U, const float* r, const double* s_in, bool training) {
     begin_launch(U->ctx);
-    un_input_kernel<<<grid1(U->n[0]), 256, 0, U->ctx->stream>>>(U->n[0], r, s_in, U->x0);
+    un_input_kernel<<<grid1(U->n[0]), 256, 0, U->ctx->stream>>>(U->n[0], r, s_in, U->x0c, training ? U->x0 : nullptr);
     after_launch(U->ctx, "un_input_kernel");
 }
 
@@ -400,7 +485,7 @@ __global__ void un_output_kernel(int64_t n, const float* __restrict__ y, const d
 
 void unet_apply(msbg_unet* U, const float* r, float* z) {
     const double* s_in = rms_device(U, r);
-    input(U, r, s_in);
+    input(U, r, s_in, false);
     forward(U);
     begin_launch(U->ctx);
     un_output_kernel<<<grid1(U->n[0]), 256, 0, U->ctx->stream>>>(U->n[0], U->y, s_in, U->out_scale, z);
@@ -410,7 +495,7 @@ void unet_apply(msbg_unet* U, const float* r, float* z) {
 static double loss_and_grads(msbg_unet* U, const float* r, const float* e) {
     msbg_ctx* ctx = U->ctx;
     const double* s_in = rms_device(U, r);
-    input(U, r, s_in);
+    input(U, r, s_in, true);
     forward(U);
     double* part = red_part(U);
     double* sums = red_out(U) + 100;  // clear of the rms (8, 9) and bias sums (16 .. 79)
@@ -537,12 +622,14 @@ static void build(msbg_unet* U, uint64_t sx, uint64_t sy, uint64_t sz, const uin
                           {&U->dyb, n0 * 16}, {&U->du0m, n0 * 16}, {&U->dc1, n1 * 16},  {&U->da4m, n1 * 32},
                           {&U->du1m, n1 * 32}, {&U->dc2, n2 * 32}, {&U->da3m, n2 * 64}, {&U->da2m, n2 * 64},
                           {&U->da1m, n1 * 32}, {&U->da0m, n0 * 16}};
-    size_t bytes = 0;
+    size_t bytes = (((size_t)n0 * 2 + 255) & ~size_t(255));  // x0c
     for (const Slot& s : slots) bytes += ((size_t)s.elems * 2 + 255) & ~size_t(255);
     const size_t f32_bytes = (((size_t)n0 * 4 + 255) & ~size_t(255)) + (((size_t)n2 * 32 * 4 + 255) & ~size_t(255)) +
                              (((size_t)n1 * 16 * 4 + 255) & ~size_t(255));
     U->act.reserve(bytes + f32_bytes + 256);
     char* base = (char*)U->act.p;
+    U->x0c = reinterpret_cast<uint16_t*>(base);
+    base += ((size_t)n0 * 2 + 255) & ~size_t(255);
     for (const Slot& s : slots) {
         *s.ptr = reinterpret_cast<uint16_t*>(base);
         base += ((size_t)s.elems * 2 + 255) & ~size_t(255);
@@ -659,7 +746,7 @@ int msbg_unet_forward_raw_device(msbg_unet* U, const float* d_r, float* d_y) {
     MSBG_REQUIRE(U && d_r && d_y, "null argument");
     set_device(U->ctx);
     const double* s_in = rms_device(U, d_r);
-    input(U, d_r, s_in);
+    input(U, d_r, s_in, false);
     forward(U);
     CUDA_CHECK(cudaMemcpyAsync(d_y, U->y, U->n[0] * 4, cudaMemcpyDeviceToDevice, U->ctx->stream));
     sync(U->ctx);

@@ -14,7 +14,7 @@ import numpy as np
 from ._lib import call, ptr
 from .grid import Context
 
-MG, PCG = 0, 1
+MG, PCG, LEARNED, HYBRID, LEARNED_MG = 0, 1, 2, 3, 4
 
 
 class Poisson:
@@ -57,11 +57,15 @@ class Poisson:
         return out.value
 
     def solve_device(self, d_x, d_b, method=PCG, tol=1e-6, max_iter=100):
+        """Device solve; d_x f32 or float64 (the FP64 solution is kept as is)."""
         it = C.c_int()
         rel = C.c_double()
         hist = np.zeros(max(max_iter, 1), np.float64)
-        call("msbg_poisson_solve_device", self.handle, int(method), ptr(d_x), ptr(d_b), float(tol), int(max_iter),
-             C.byref(it), C.byref(rel), ptr(hist))
+        fn = "msbg_poisson_solve_f64_device" if str(getattr(d_x, "dtype", "")) == "torch.float64" else \
+            "msbg_poisson_solve_device"
+        call(fn, self.handle, int(method), ptr(d_x), ptr(d_b), float(tol), int(max_iter), C.byref(it), C.byref(rel),
+             ptr(hist))
+        self.last_history = hist[: it.value]
         return it.value, rel.value, hist[: it.value]
 
     def solve(self, b: np.ndarray, x0=None, method=PCG, tol=1e-6, max_iter=100):
@@ -74,6 +78,34 @@ class Poisson:
         call("msbg_poisson_solve", self.handle, int(method), ptr(x), ptr(bb), float(tol), int(max_iter), C.byref(it),
              C.byref(rel), ptr(hist))
         return x, it.value, rel.value, hist[: it.value]
+
+    # ---- learned preconditioner ------------------------------------------------
+    def set_preconditioner(self, net) -> None:
+        """Network for methods LEARNED (2) and HYBRID (3); None clears it."""
+        self._net = net
+        call("msbg_poisson_set_preconditioner", self.handle, net.handle if net is not None else None)
+
+    def solve_stats(self) -> dict:
+        """Preconditioner applications of the last solve and its fallback:
+        reason 0 none, 1 stall, 2 p.Ap <= 0, 3 r.z <= 0."""
+        out = np.zeros(4, np.int32)
+        call("msbg_poisson_solve_stats", self.handle, ptr(out))
+        return {"vcycles": int(out[0]), "network": int(out[1]), "fallback": int(out[2]), "fallback_iter": int(out[3])}
+
+    def rhs(self, d_b, seed: int, n_blobs: int = 32) -> None:
+        call("msbg_poisson_rhs_device", self.handle, int(seed), int(n_blobs), ptr(d_b))
+
+    def train_preconditioner(self, n_rhs=16, mg_iters=20, steps_per_rhs=20, pool=64, lr=1e-3, target=1, seed=1):
+        hist = np.zeros(max(1, n_rhs * steps_per_rhs), np.float64)
+        steps = C.c_int64()
+        call("msbg_poisson_train_preconditioner", self.handle, int(n_rhs), int(mg_iters), int(steps_per_rhs), int(pool),
+             float(lr), int(target), int(seed), ptr(hist), len(hist), C.byref(steps))
+        return hist[: steps.value]
+
+    def eval_preconditioner(self, n_rhs=2, mg_iters=10, seed=99) -> dict:
+        out = np.zeros(3, np.float64)
+        call("msbg_poisson_eval_preconditioner", self.handle, int(n_rhs), int(mg_iters), int(seed), ptr(out))
+        return {"network": out[0], "vcycle": out[1], "vcycle_plus_network": out[2]}
 
     def close(self):
         if self.handle:
