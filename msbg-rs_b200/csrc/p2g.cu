@@ -11,10 +11,11 @@
 //     27-bit mask; the active set is the sorted union over particle blocks.
 //  3. Splat: one CTA per (particle block, face direction) accumulates into a
 //     (bsx + 2M)^3 staging window in shared memory (M = ceil(r_p)), in FP64.
-//     Cells are visited in (2M+1)^3 colour phases: cells of one phase are
-//     2M+1 apart, so their face windows are disjoint and each warp owns its
-//     cell's faces -- no atomics, a fixed summation order.  A warp handles a
-//     cell: lanes take the cell's (2M+1)^3 candidate faces, loop over the
+//     Cells are visited by 2x2x2 tiles in (M+1)^3 colour phases: cells of
+//     two tiles of one phase are 2M+1 apart, so their face windows are
+//     disjoint and each warp owns its tile's faces -- no atomics, a fixed
+//     summation order.  A warp handles a tile's cells in turn: lanes take a
+//     cell's (2M+1)^2 candidate face columns, loop over the
 //     cell's particles, and evaluate the reference's per-face weight
 //     w = max(1 - d^2/r_p^2, 0)^3 with its exact f32 operation order and its
 //     exact clamped footprint (p2g.rs:263-330).
@@ -172,9 +173,10 @@ __device__ __forceinline__ int fp_field(uint64_t f, int ax, int face, int hi) {
 
 // Splat kernel: one CTA per (particle block, direction DIR).  The block's
 // (bsx + 2M)^3 staging window of face sums lives in shared memory in FP64.
-// Cells are visited in (2M+1)^3 colour phases (cells of a phase are 2M+1
-// apart, so their candidate face windows are disjoint) with a barrier between
-// phases; inside a phase one warp handles one cell.  The lanes of the warp
+// Cells are visited by 2x2x2 tiles in (M+1)^3 colour phases (cells of two
+// tiles of a phase are 2M+1 apart, so their candidate face windows are
+// disjoint) with a barrier between phases; inside a phase one warp handles
+// one tile, its 8 cells in a fixed order.  The lanes of the warp
 // take the (2M+1)^2 positions of the cell's face window across the two axes
 // other than the face axis, and each lane keeps the 2M+1 faces along the face
 // axis in FP64 registers.  For every particle of the cell (sorted order) a
@@ -203,17 +205,27 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
     const float* __restrict__ pv = a.pv[DIR];
     const float inv_r2 = a.inv_r2;
     __syncthreads();
-    for (int ph = 0; ph < WIN * WIN * WIN; ++ph) {
-        const int ox = ph % WIN, oy = (ph / WIN) % WIN, oz = ph / (WIN * WIN);
-        const int ncx = ox < BSX ? (BSX - ox + WIN - 1) / WIN : 0;
-        const int ncy = oy < BSX ? (BSX - oy + WIN - 1) / WIN : 0;
-        const int ncz = oz < BSX ? (BSX - oz + WIN - 1) / WIN : 0;
-        const int total = ncx * ncy * ncz;
-        for (int c = warp; c < total; c += nwarp) {
+    // Tiles of 2x2x2 cells coloured by tile coordinate mod K: cells of two
+    // tiles of one colour are at least 2K - 1 = 2M + 1 apart, so their face
+    // windows are disjoint; a warp takes a whole tile (8 cells in a fixed
+    // order) between barriers.
+    constexpr int T = BSX / 2, K = M + 1;
+    for (int ph = 0; ph < K * K * K; ++ph) {
+        const int ox = ph % K, oy = (ph / K) % K, oz = ph / (K * K);
+        const int ntx = ox < T ? (T - ox + K - 1) / K : 0;
+        const int nty = oy < T ? (T - oy + K - 1) / K : 0;
+        const int ntz = oz < T ? (T - oz + K - 1) / K : 0;
+        const int total = ntx * nty * ntz;
+        for (int tile = warp; tile < total; tile += nwarp) {
+          for (int sub = 0; sub < 8; ++sub) {
+            // cells of a tile have overlapping face windows: order this
+            // cell's shared-memory updates after the previous cell's across
+            // the warp's lanes
+            __syncwarp();
             int cell[3];
-            cell[0] = ox + WIN * (c % ncx);
-            cell[1] = oy + WIN * ((c / ncx) % ncy);
-            cell[2] = oz + WIN * (c / (ncx * ncy));
+            cell[0] = 2 * (ox + K * (tile % ntx)) + (sub & 1);
+            cell[1] = 2 * (oy + K * ((tile / ntx) % nty)) + ((sub >> 1) & 1);
+            cell[2] = 2 * (oz + K * (tile / (ntx * nty))) + (sub >> 2);
             const uint32_t lm = (uint32_t)morton3(cell[0], cell[1], cell[2]);
             const int b = cb[lm], e = ce[lm];
             if (b >= e) continue;
@@ -227,15 +239,31 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                 double am[WIN], av[WIN];
 #pragma unroll
                 for (int s = 0; s < WIN; ++s) am[s] = av[s] = 0.0;
-                for (int p = b; p < e; ++p) {
-                    const uint64_t f = a.fp[p];
+                // the cell's particles, 32 at a time: one coalesced load per
+                // lane, then broadcast to the lanes by shuffles
+                for (int p0 = b; p0 < e; p0 += 32) {
+                  const int cnt = min(32, e - p0);
+                  uint64_t f_l = 0;
+                  float m_l = 0.0f, mv_l = 0.0f, x_l = 0.0f, y_l = 0.0f, z_l = 0.0f;
+                  if (lane < cnt) {
+                      const int pl = p0 + lane;
+                      f_l = a.fp[pl];
+                      m_l = a.pm[pl];
+                      mv_l = m_l * pv[pl];
+                      x_l = a.px[pl] - 0.5f;
+                      y_l = a.py[pl] - 0.5f;
+                      z_l = a.pz[pl] - 0.5f;
+                  }
+                  for (int j = 0; j < cnt; ++j) {
+                    const uint64_t f = __shfl_sync(0xffffffffu, f_l, j);
+                    const float m_p = __shfl_sync(0xffffffffu, m_l, j);
+                    const float scale_mom = __shfl_sync(0xffffffffu, mv_l, j);
+                    const float pc[3] = {__shfl_sync(0xffffffffu, x_l, j), __shfl_sync(0xffffffffu, y_l, j),
+                                         __shfl_sync(0xffffffffu, z_l, j)};
                     if (!on || su < fp_field(f, U, 0, 0) || su > fp_field(f, U, 0, 1) || sv < fp_field(f, V, 0, 0) ||
                         sv > fp_field(f, V, 0, 1))
                         continue;
                     const int sf1 = fp_field(f, F, 1, 0), sf2 = fp_field(f, F, 1, 1);
-                    const float m_p = a.pm[p];
-                    const float scale_mom = m_p * pv[p];
-                    const float pc[3] = {a.px[p] - 0.5f, a.py[p] - 0.5f, a.pz[p] - 0.5f};
                     const float du = gu - pc[U], dv = gv - pc[V];
 #pragma unroll
                     for (int s = 0; s < WIN; ++s) {
@@ -257,6 +285,7 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                         am[s] += (double)(w * m_p);
                         av[s] += (double)(w * scale_mom);
                     }
+                  }
                 }
                 if (on) {
 #pragma unroll
@@ -273,6 +302,7 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                     }
                 }
             }
+          }
         }
         __syncthreads();
     }
@@ -343,8 +373,10 @@ static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
         CUDA_CHECK(cudaFuncSetAttribute(p2g_cells_kernel<BSX, M, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
+    constexpr int T = BSX / 2, K = M + 1, TW = (T + K - 1) / K;
+    constexpr int WARPS = TW * TW * TW < 32 ? TW * TW * TW : 32;
     begin_launch(ctx);
-    p2g_cells_kernel<BSX, M, DIR><<<(unsigned)npb, 1024, smem, ctx->stream>>>(a);
+    p2g_cells_kernel<BSX, M, DIR><<<(unsigned)npb, 32 * WARPS, smem, ctx->stream>>>(a);
     after_launch(ctx, "p2g_cells_kernel");
 }
 
