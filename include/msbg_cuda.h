@@ -364,6 +364,38 @@ int msbg_unet_forward_raw_device(msbg_unet* net, const float* d_r, float* d_y);
 int msbg_unet_train_step_device(msbg_unet* net, const float* d_r, const float* d_e, float lr, int update,
                                 double* loss_out);
 
+/* ---- batched Poisson solves ------------------------------------------------
+ * No counterpart in the reference.  Many independent problems (each a domain
+ * dims[3p..3p+2], block size bsx[p] in {4..32}, active block ids active[p]
+ * [n_active[p]]) are stacked in one hierarchy per block size (problems never
+ * touch at any level).  Problem p's level-0 cells are a contiguous range of
+ * its group's vectors (msbg_batch_problem), blocks in ascending id order.
+ * msbg_batch_buffers gives the group's device right-hand side (f32) and
+ * solution (FP64).  tune != 0 autotunes the launch shapes of the Jacobi and
+ * residual kernels per level (msbg_batch_tuning: per level the chosen shape
+ * indices (Jacobi, residual) and the level's cells).  msbg_batch_solve runs
+ * MG-preconditioned CG with per-problem scalars on the device; one cycle of
+ * iters_per_cycle iterations over all problems plus the FP64 residual
+ * replacement is a single CUDA graph launch; it stops when every problem
+ * reaches relative residual tol (true residual of the FP64 solution) or
+ * after max_cycles.  iters_out and rel_out are per problem.
+ * msbg_poisson_autotune tunes a single solve's hierarchy the same way. */
+typedef struct msbg_batch msbg_batch;
+int msbg_batch_create(msbg_ctx* ctx, int n_problems, const int* bsx, const uint64_t* dims, const uint64_t* const* active,
+                      const size_t* n_active, int tune, msbg_batch** out);
+int msbg_batch_destroy(msbg_batch* batch);
+int msbg_batch_groups(const msbg_batch* batch, int* n_groups);
+int msbg_batch_problem(const msbg_batch* batch, int p, int* group, uint64_t* cell_offset, uint64_t* n_cells);
+int msbg_batch_buffers(msbg_batch* batch, int group, float** d_b, double** d_x, uint64_t* n_cells, int* bsx);
+/* Host copies of one problem's right-hand side (f32, in) and solution (FP64, out). */
+int msbg_batch_set_rhs(msbg_batch* batch, int p, const float* b);
+int msbg_batch_get_solution(msbg_batch* batch, int p, double* x);
+int msbg_batch_tuning(const msbg_batch* batch, int group, int* cfg_out, uint64_t* cells_out, size_t cap,
+                      size_t* n_levels);
+int msbg_batch_solve(msbg_batch* batch, double tol, int iters_per_cycle, int max_cycles, int zero_x, int* iters_out,
+                     double* rel_out, int* cycles_out);
+int msbg_poisson_autotune(msbg_poisson* p, int* cfg_out, size_t cap, size_t* n_levels);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@ from .fluid import (MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend_device, p
 from .multires import downsample_channel_avg
 from .poisson import HYBRID, LEARNED, LEARNED_MG, MG, PCG, Poisson
 from .learned import UNet
+from .batch import Batch
 
 MsbgError = _lib.MsbgError
 CLAMP, NEUMANN, DIRICHLET = _lib.MSBG_CLAMP, _lib.MSBG_NEUMANN, _lib.MSBG_DIRICHLET
@@ -29,5 +30,5 @@ __all__ = [
     "BucketPlan", "bucket_indices", "morton3", "morton3_host", "morton_sort", "sort_block_list_morton",
     "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
     "particles_to_grid_device", "particles_to_grid_sorted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
-    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "UNet",
+    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "UNet", "Batch",
 ]

@@ -118,6 +118,16 @@ SIGNATURES = {
     "msbg_poisson_solve_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_solve": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_set_preconditioner": [_P, _P],
+    "msbg_poisson_autotune": [_P, _P, _SZ, _SZP],
+    "msbg_batch_create": [_P, _I, _P, _P, _P, _P, _I, C.POINTER(_P)],
+    "msbg_batch_destroy": [_P],
+    "msbg_batch_groups": [_P, C.POINTER(_I)],
+    "msbg_batch_problem": [_P, _I, C.POINTER(_I), _U64P, _U64P],
+    "msbg_batch_buffers": [_P, _I, C.POINTER(_P), C.POINTER(_P), _U64P, C.POINTER(_I)],
+    "msbg_batch_set_rhs": [_P, _I, _P],
+    "msbg_batch_get_solution": [_P, _I, _P],
+    "msbg_batch_tuning": [_P, _I, _P, _P, _SZ, _SZP],
+    "msbg_batch_solve": [_P, C.c_double, _I, _I, _I, _P, _P, C.POINTER(_I)],
     "msbg_poisson_solve_f64_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_solve_stats": [_P, _P],
     "msbg_poisson_rhs_device": [_P, _U64, _I, _P],

@@ -40,6 +40,7 @@ struct PLevelDev {
     DevBuf coords;   // int32 [n][3] block coordinates
     DevBuf parent;   // int32 [n] parent slot at level l+1 (the last level: unused)
     DevBuf x, b, r, t;  // f32 [cells]
+    int cfg_jac = 0, cfg_res = 0;  // launch shapes of the level's Jacobi and residual kernels (autotuned)
     int64_t n() const { return (int64_t)bids.size(); }
     int64_t cells() const { return n() * bs * bs * bs; }
 };
@@ -66,6 +67,14 @@ struct msbg_poisson {
     // PCG statistics of the last solve: preconditioner applications of each
     // kind and whether the learned preconditioner fell back to multigrid
     int n_net = 0, n_vcycle = 0, fell_back = 0, fallback_iter = -1;
+    // Batched solves: independent problems stacked in one hierarchy (see
+    // batch_build); each owns a contiguous range of level-0 blocks.
+    int np = 0;
+    std::vector<int64_t> prob_blocks;  // [np + 1] level-0 block offsets
+    msbg::DevBuf d_prob_blocks;        // int64 [np + 1]
+    msbg::DevBuf d_blk_prob;           // int32 [level-0 blocks] problem of each block
+    msbg::DevBuf bpart;                // f64 [level-0 blocks] per-block dot partials
+    msbg::DevBuf scal;                 // f64 [np][16] per-problem scalars
 };
 
 namespace msbg {
@@ -269,6 +278,19 @@ __global__ void pk_axpby(int64_t n, float a, const float* __restrict__ x, float 
 // ---- host side -----------------------------------------------------------------
 static unsigned grid_for(int64_t n) { return (unsigned)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 16); }
 
+// Launch shapes the autotuner chooses from for the cell-parallel level kernels
+// (grid-stride loops): threads per CTA and the grid cap in CTAs per SM.
+struct LaunchShape {
+    int threads, ctas_per_sm;
+};
+constexpr LaunchShape kShapes[] = {{256, 16}, {128, 16}, {512, 4}, {256, 4}, {128, 32}, {1024, 2}, {64, 32}, {256, 8}};
+constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+
+static dim3 shape_grid(int cfg, int64_t n) {
+    const LaunchShape& S = kShapes[cfg];
+    return dim3((unsigned)std::min<int64_t>(std::max<int64_t>((n + S.threads - 1) / S.threads, 1), 148LL * S.ctas_per_sm));
+}
+
 static LevelArgs level_args(const PLevelDev& L) {
     return LevelArgs{L.nbr.as<int32_t>(), L.lg, L.cells(), L.scale};
 }
@@ -278,7 +300,8 @@ static void upload(msbg_ctx* ctx, DevBuf& d, const void* h, size_t bytes) {
     if (bytes) CUDA_CHECK(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
 }
 
-static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, const uint64_t* active, size_t n_active) {
+static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, const uint64_t* active, size_t n_active,
+                  int max_grid_halvings = 1 << 30) {
     msbg_ctx* ctx = P->ctx;
     const uint64_t nx = (sx + bsx - 1) / bsx, ny = (sy + bsx - 1) / bsx, nz = (sz + bsx - 1) / bsx;
     std::vector<uint64_t> a(active, active + n_active);
@@ -292,13 +315,16 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
         PLevelDev& L = P->lv.back();
         L.bs = bsx; L.lg = ilog2i(bsx); L.nx = nx; L.ny = ny; L.nz = nz; L.scale = 1.0f; L.bids = a;
     }
+    int halvings = 0;
     while (P->lv.back().cells() > kPoissonDirect) {
         const PLevelDev& F = P->lv.back();
+        if (F.bs < 4 && halvings >= max_grid_halvings) break;
         PLevelDev C;
         C.scale = F.scale * 0.5f;
         if (F.bs >= 4) {
             C.bs = F.bs / 2; C.nx = F.nx; C.ny = F.ny; C.nz = F.nz; C.bids = F.bids;
         } else {
+            ++halvings;
             C.bs = F.bs; C.nx = (F.nx + 1) / 2; C.ny = (F.ny + 1) / 2; C.nz = (F.nz + 1) / 2;
             for (uint64_t b : F.bids) {
                 uint64_t bx = b % F.nx, by = (b / F.nx) % F.ny, bz = b / (F.nx * F.ny);
@@ -362,6 +388,7 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
     // dense FP64 inverse of the coarsest operator
     const PLevelDev& C = P->lv.back();
     const int64_t n = C.cells();
+    MSBG_REQUIRE(n <= 4 * kPoissonDirect, "coarsest level too large for the dense solve (too many batched problems)");
     P->nc = n;
     std::unordered_map<uint64_t, int32_t> slot;
     for (int64_t k = 0; k < C.n(); ++k) slot[C.bids[k]] = (int32_t)k;
@@ -429,7 +456,7 @@ static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
 static void launch_residual(msbg_poisson* P, int l, const float* x, const float* b, float* r) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
-    pk_residual<<<grid_for(L.cells()), 256, 0, P->ctx->stream>>>(level_args(L), x, b, r);
+    pk_residual<<<shape_grid(L.cfg_res, L.cells()), kShapes[L.cfg_res].threads, 0, P->ctx->stream>>>(level_args(L), x, b, r);
     after_launch(P->ctx, "pk_residual");
 }
 
@@ -442,7 +469,8 @@ static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps,
         const float* src = (s % 2 == 0) ? x : t;
         float* dst = (s % 2 == 0) ? t : x;
         begin_launch(P->ctx);
-        pk_jacobi<<<grid_for(L.cells()), 256, 0, P->ctx->stream>>>(level_args(L), (s == 0 && x_zero) ? nullptr : src, b, dst, omega);
+        pk_jacobi<<<shape_grid(L.cfg_jac, L.cells()), kShapes[L.cfg_jac].threads, 0, P->ctx->stream>>>(
+            level_args(L), (s == 0 && x_zero) ? nullptr : src, b, dst, omega);
         after_launch(P->ctx, "pk_jacobi");
     }
     if (sweeps % 2 == 1) CUDA_CHECK(cudaMemcpyAsync(x, t, L.cells() * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
@@ -886,6 +914,278 @@ static void evaluate(msbg_poisson* P, int n_rhs, int mg_iters, uint64_t seed, do
     for (int j = 0; j < 3; ++j) out[j] = cnt ? acc[j] / cnt : 0.0;
 }
 
+// ---- batched solves ------------------------------------------------------------
+// Many independent problems share one hierarchy: problem p's blocks are
+// placed at block z offset Z_p of a common virtual domain, with gaps of
+// 2^(L+1) blocks (L = the block-grid halvings the hierarchy may make), so no
+// two problems touch at any level and every operator is block-diagonal over
+// the problems.  Blocks sort by z first, so each problem owns a contiguous
+// range of every level's blocks.  CG runs with per-problem scalars kept on
+// the device (no host round trip inside an iteration), which lets a whole
+// cycle of iterations be captured into one CUDA graph.
+enum { S_RZ = 0, S_PQ, S_RZN, S_RR, S_BB, S_ALPHA, S_BETA, S_ACTIVE, S_ITER, S_WIDTH = 16 };
+
+// per-block FP64 partial of a . b (one CTA per block, fixed tree order)
+__global__ void __launch_bounds__(256) bk_block_dot(int64_t nblocks, int cells, const float* __restrict__ a,
+                                                    const float* __restrict__ b, double* __restrict__ part) {
+    __shared__ double sm[256];
+    for (int64_t k = blockIdx.x; k < nblocks; k += gridDim.x) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < cells; i += 256) s += (double)a[k * cells + i] * (double)b[k * cells + i];
+        sm[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = 128; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[k] = sm[0];
+        __syncthreads();
+    }
+}
+
+// scal[p][slot] = sum of the partials of problem p's blocks (one warp per problem)
+__global__ void bk_seg_sum(int np, const int64_t* __restrict__ pb, const double* __restrict__ part, double* __restrict__ scal,
+                           int slot) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += warps) {
+        double s = 0.0;
+        for (int64_t k = pb[p] + lane; k < pb[p + 1]; k += 32) s += part[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) scal[(int64_t)p * S_WIDTH + slot] = s;
+    }
+}
+
+// op 0: alpha = rz / pq; op 1: beta = rz_new / rz, rz = rz_new, one more
+// iteration counted; op 2: active = (r.r > tol^2 b.b).  Problems that are not
+// active get alpha = beta = 0 and stay where they are.
+__global__ void bk_scalars(int np, double* __restrict__ scal, int op, double tol2) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+        double* S = scal + (int64_t)p * S_WIDTH;
+        const bool on = S[S_ACTIVE] > 0.0;
+        if (op == 0) {
+            S[S_ALPHA] = (on && S[S_PQ] > 0.0) ? S[S_RZ] / S[S_PQ] : 0.0;
+        } else if (op == 1) {
+            S[S_BETA] = (on && S[S_RZ] > 0.0) ? S[S_RZN] / S[S_RZ] : 0.0;
+            S[S_RZ] = S[S_RZN];
+            if (on) S[S_ITER] += 1.0;
+        } else {
+            S[S_ACTIVE] = S[S_RR] > tol2 * S[S_BB] ? 1.0 : 0.0;
+        }
+    }
+}
+
+// y += sign * s_p x  (s_p = scal[problem of the cell's block][slot])
+__global__ void bk_axpy(int64_t n, int lg3, const int32_t* __restrict__ blk_prob, const double* __restrict__ scal, int slot,
+                        float sign, const float* __restrict__ x, float* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += (float)(sign * scal[(int64_t)blk_prob[i >> lg3] * S_WIDTH + slot]) * x[i];
+}
+
+// p = z + beta_p p
+__global__ void bk_xpay(int64_t n, int lg3, const int32_t* __restrict__ blk_prob, const double* __restrict__ scal,
+                        const float* __restrict__ z, float* __restrict__ p) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + (float)scal[(int64_t)blk_prob[i >> lg3] * S_WIDTH + S_BETA] * p[i];
+}
+
+// x64 += alpha_p p
+__global__ void bk_add64(int64_t n, int lg3, const int32_t* __restrict__ blk_prob, const double* __restrict__ scal,
+                         const float* __restrict__ p, double* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += scal[(int64_t)blk_prob[i >> lg3] * S_WIDTH + S_ALPHA] * (double)p[i];
+}
+
+static void seg_dot(msbg_poisson* P, const float* a, const float* b, int slot) {
+    const PLevelDev& F = P->lv[0];
+    const int cells = F.bs * F.bs * F.bs;
+    begin_launch(P->ctx);
+    bk_block_dot<<<(unsigned)std::min<int64_t>(F.n(), 148 * 8), 256, 0, P->ctx->stream>>>(F.n(), cells, a, b,
+                                                                                         P->bpart.as<double>());
+    after_launch(P->ctx, "bk_block_dot");
+    begin_launch(P->ctx);
+    bk_seg_sum<<<(unsigned)((P->np * 32 + 255) / 256), 256, 0, P->ctx->stream>>>(
+        P->np, P->d_prob_blocks.as<int64_t>(), P->bpart.as<double>(), P->scal.as<double>(), slot);
+    after_launch(P->ctx, "bk_seg_sum");
+}
+
+static void scalars(msbg_poisson* P, int op, double tol) {
+    begin_launch(P->ctx);
+    bk_scalars<<<(unsigned)((P->np + 127) / 128), 128, 0, P->ctx->stream>>>(P->np, P->scal.as<double>(), op, tol * tol);
+    after_launch(P->ctx, "bk_scalars");
+}
+
+// Start of a batched solve (not captured): r = b - A x, b.b, r.r, active flags.
+static void batch_start(msbg_poisson* P, double* x64, const float* b, double tol) {
+    const int64_t n = P->lv[0].cells();
+    float* r = (float*)P->work.p;
+    CUDA_CHECK(cudaMemsetAsync(P->scal.p, 0, (size_t)P->np * S_WIDTH * 8, P->ctx->stream));
+    launch_residual64(P, x64, b, r);
+    seg_dot(P, b, b, S_BB);
+    seg_dot(P, r, r, S_RR);
+    scalars(P, 2, tol);
+    (void)n;
+}
+
+// One cycle (capturable): restart CG from the current true residual r, K
+// iterations of MG-preconditioned CG with per-problem scalars, then the true
+// residual of the FP64 solution replaces r (FP64 residual-based iterative
+// refinement) and the active flags are updated.
+static void batch_cycle(msbg_poisson* P, double* x64, const float* b, int K, double tol) {
+    const PLevelDev& F = P->lv[0];
+    const int64_t n = F.cells();
+    const int lg3 = 3 * F.lg;
+    float* r = (float*)P->work.p;
+    float* z = r + n;
+    float* p = z + n;
+    float* q = p + n;
+    const int32_t* bp = P->d_blk_prob.as<int32_t>();
+    double* sc = P->scal.as<double>();
+    msbg_ctx* ctx = P->ctx;
+    vcycle(P, 0, z, r, true);
+    CUDA_CHECK(cudaMemcpyAsync(p, z, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    seg_dot(P, r, z, S_RZ);
+    for (int k = 0; k < K; ++k) {
+        launch_matvec(P, 0, p, q);
+        seg_dot(P, p, q, S_PQ);
+        scalars(P, 0, tol);
+        begin_launch(ctx);
+        bk_add64<<<grid_for(n), 256, 0, ctx->stream>>>(n, lg3, bp, sc, p, x64);
+        after_launch(ctx, "bk_add64");
+        begin_launch(ctx);
+        bk_axpy<<<grid_for(n), 256, 0, ctx->stream>>>(n, lg3, bp, sc, S_ALPHA, -1.0f, q, r);
+        after_launch(ctx, "bk_axpy");
+        vcycle(P, 0, z, r, true);
+        seg_dot(P, r, z, S_RZN);
+        scalars(P, 1, tol);
+        begin_launch(ctx);
+        bk_xpay<<<grid_for(n), 256, 0, ctx->stream>>>(n, lg3, bp, sc, z, p);
+        after_launch(ctx, "bk_xpay");
+    }
+    launch_residual64(P, x64, b, r);
+    seg_dot(P, r, r, S_RR);
+    scalars(P, 2, tol);
+}
+
+// Autotuner: for every level but the coarsest, time each launch shape of the
+// Jacobi and residual kernels on the level's own buffers (CUDA events, three
+// launches after one warm-up) and keep the fastest.
+static void autotune(msbg_poisson* P) {
+    msbg_ctx* ctx = P->ctx;
+    MSBG_REQUIRE(!ctx->timing, "autotuning needs per-kernel timing off");
+    cudaEvent_t e0, e1;
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    for (size_t l = 0; l + 1 < P->lv.size(); ++l) {
+        PLevelDev& L = P->lv[l];
+        const int64_t cells = L.cells();
+        CUDA_CHECK(cudaMemsetAsync(L.x.p, 0, cells * 4, ctx->stream));
+        CUDA_CHECK(cudaMemsetAsync(L.b.p, 0, cells * 4, ctx->stream));
+        for (int kind = 0; kind < 2; ++kind) {
+            float best = 1e30f;
+            int best_cfg = 0;
+            for (int c = 0; c < kNumShapes; ++c) {
+                auto run = [&]() {
+                    if (kind == 0)
+                        pk_jacobi<<<shape_grid(c, cells), kShapes[c].threads, 0, ctx->stream>>>(
+                            level_args(L), L.x.as<float>(), L.b.as<float>(), L.t.as<float>(), P->omega);
+                    else
+                        pk_residual<<<shape_grid(c, cells), kShapes[c].threads, 0, ctx->stream>>>(
+                            level_args(L), L.x.as<float>(), L.b.as<float>(), L.r.as<float>());
+                };
+                run();
+                CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+                for (int rep = 0; rep < 3; ++rep) run();
+                CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+                CUDA_CHECK(cudaEventSynchronize(e1));
+                CUDA_CHECK(cudaGetLastError());
+                float ms = 0.0f;
+                CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                ctx->launches += 4;
+                if (ms < best) {
+                    best = ms;
+                    best_cfg = c;
+                }
+            }
+            if (kind == 0) L.cfg_jac = best_cfg;
+            else L.cfg_res = best_cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+}  // namespace msbg
+
+// A batch: problems grouped by block size, each group one stacked hierarchy.
+struct msbg_batch {
+    msbg_ctx* ctx = nullptr;
+    std::vector<msbg_poisson*> groups;
+    std::vector<int> prob_group, prob_index;  // per problem: group and index inside it
+    std::vector<msbg::DevBuf> b, x;           // per group: f32 right-hand sides, FP64 solutions
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_k = 0, graph_kernels = 0;
+    double graph_tol = 0.0;
+    ~msbg_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (msbg_poisson* P : groups) delete P;
+    }
+};
+
+namespace msbg {
+
+static void batch_group_build(msbg_poisson* P, int bsx, const std::vector<int>& probs, const uint64_t* dims,
+                              const uint64_t* const* active, const size_t* n_active) {
+    int64_t NX = 1, NY = 1, nzmax = 1;
+    for (int p : probs) {
+        NX = std::max<int64_t>(NX, (int64_t)((dims[3 * p] + bsx - 1) / bsx));
+        NY = std::max<int64_t>(NY, (int64_t)((dims[3 * p + 1] + bsx - 1) / bsx));
+        nzmax = std::max<int64_t>(nzmax, (int64_t)((dims[3 * p + 2] + bsx - 1) / bsx));
+    }
+    const int L = ilog2i((uint64_t)std::max(NX, std::max(NY, nzmax))) + 1;  // halvings that shrink any problem to one block
+    const int64_t G = int64_t(1) << (L + 1);
+    std::vector<uint64_t> all;
+    std::vector<int64_t> zoff(probs.size());
+    int64_t Z = 0;
+    for (size_t i = 0; i < probs.size(); ++i) {
+        const int p = probs[i];
+        const uint64_t nx = (dims[3 * p] + bsx - 1) / bsx, ny = (dims[3 * p + 1] + bsx - 1) / bsx,
+                       nz = (dims[3 * p + 2] + bsx - 1) / bsx;
+        MSBG_REQUIRE(n_active[p] > 0, "a batched problem has no active blocks");
+        zoff[i] = Z;
+        for (size_t j = 0; j < n_active[p]; ++j) {
+            const uint64_t b = active[p][j];
+            MSBG_REQUIRE(b < nx * ny * nz, "active block id out of range");
+            const uint64_t bx = b % nx, by = (b / nx) % ny, bz = b / (nx * ny);
+            all.push_back(bx + by * (uint64_t)NX + (bz + (uint64_t)Z) * (uint64_t)(NX * NY));
+        }
+        const int64_t align = int64_t(1) << L;
+        Z = ((Z + (int64_t)nz + align - 1) / align) * align + G;
+    }
+    build(P, (uint64_t)NX * bsx, (uint64_t)NY * bsx, (uint64_t)Z * bsx, bsx, all.data(), all.size(), L);
+    // problem ranges of the level-0 blocks (sorted by z, so contiguous)
+    const PLevelDev& F = P->lv[0];
+    P->np = (int)probs.size();
+    P->prob_blocks.assign(P->np + 1, 0);
+    std::vector<int32_t> blk_prob(F.n());
+    size_t k = 0;
+    for (int i = 0; i < P->np; ++i) {
+        P->prob_blocks[i] = (int64_t)k;
+        const int64_t z_hi = (i + 1 < P->np) ? zoff[i + 1] : INT64_MAX;
+        while (k < F.bids.size() && (int64_t)(F.bids[k] / (uint64_t)(NX * NY)) < z_hi) blk_prob[k++] = i;
+    }
+    P->prob_blocks[P->np] = (int64_t)k;
+    MSBG_REQUIRE(k == F.bids.size(), "batched problem layout is inconsistent");
+    upload(P->ctx, P->d_prob_blocks, P->prob_blocks.data(), P->prob_blocks.size() * 8);
+    upload(P->ctx, P->d_blk_prob, blk_prob.data(), blk_prob.size() * 4);
+    P->bpart.reserve((size_t)F.n() * 8 + 64);
+    P->scal.reserve((size_t)P->np * S_WIDTH * 8 + 64);
+    sync(P->ctx);
+}
+
 }  // namespace msbg
 
 using namespace msbg;
@@ -1063,6 +1363,220 @@ int msbg_poisson_eval_preconditioner(msbg_poisson* P, int n_rhs, int mg_iters, u
     MSBG_REQUIRE(P && out3 && n_rhs > 0 && mg_iters > 0 && P->net, "bad argument");
     set_device(P->ctx);
     evaluate(P, n_rhs, mg_iters, seed, out3);
+    MSBG_API_END
+}
+
+int msbg_poisson_autotune(msbg_poisson* P, int* cfg_out, size_t cap, size_t* n_levels) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P, "null argument");
+    set_device(P->ctx);
+    autotune(P);
+    if (n_levels) *n_levels = P->lv.size();
+    for (size_t l = 0; l < P->lv.size() && cfg_out && 2 * l + 1 < cap; ++l) {
+        cfg_out[2 * l] = P->lv[l].cfg_jac;
+        cfg_out[2 * l + 1] = P->lv[l].cfg_res;
+    }
+    MSBG_API_END
+}
+
+int msbg_batch_create(msbg_ctx* ctx, int n_problems, const int* bsx, const uint64_t* dims, const uint64_t* const* active,
+                      const size_t* n_active, int tune, msbg_batch** out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx && out && n_problems > 0 && bsx && dims && active && n_active, "null argument");
+    MSBG_REQUIRE(n_problems <= 256, "at most 256 problems per batch");
+    set_device(ctx);
+    auto* B = new msbg_batch;
+    B->ctx = ctx;
+    try {
+        B->prob_group.assign(n_problems, -1);
+        B->prob_index.assign(n_problems, -1);
+        std::vector<int> sizes;
+        for (int p = 0; p < n_problems; ++p) {
+            MSBG_REQUIRE(is_pow2((uint64_t)bsx[p]) && bsx[p] >= 4 && bsx[p] <= 32, "batched block sizes are powers of two in [4, 32]");
+            int g = -1;
+            for (size_t i = 0; i < sizes.size(); ++i)
+                if (sizes[i] == bsx[p]) g = (int)i;
+            if (g < 0) {
+                g = (int)sizes.size();
+                sizes.push_back(bsx[p]);
+            }
+            B->prob_group[p] = g;
+        }
+        for (size_t g = 0; g < sizes.size(); ++g) {
+            std::vector<int> probs;
+            for (int p = 0; p < n_problems; ++p)
+                if (B->prob_group[p] == (int)g) {
+                    B->prob_index[p] = (int)probs.size();
+                    probs.push_back(p);
+                }
+            auto* P = new msbg_poisson;
+            P->ctx = ctx;
+            B->groups.push_back(P);
+            batch_group_build(P, sizes[g], probs, dims, active, n_active);
+            if (tune) autotune(P);
+            const int64_t n = P->lv[0].cells();
+            B->b.emplace_back();
+            B->x.emplace_back();
+            B->b.back().reserve((size_t)n * 4 + 256);
+            B->x.back().reserve((size_t)n * 8 + 256);
+            CUDA_CHECK(cudaMemsetAsync(B->b.back().p, 0, (size_t)n * 4, ctx->stream));
+            CUDA_CHECK(cudaMemsetAsync(B->x.back().p, 0, (size_t)n * 8, ctx->stream));
+        }
+        sync(ctx);
+    } catch (...) {
+        delete B;
+        throw;
+    }
+    *out = B;
+    MSBG_API_END
+}
+
+int msbg_batch_destroy(msbg_batch* B) {
+    MSBG_API_BEGIN
+    if (!B) return MSBG_OK;
+    cudaSetDevice(B->ctx->device);
+    cudaStreamSynchronize(B->ctx->stream);
+    delete B;
+    MSBG_API_END
+}
+
+int msbg_batch_problem(const msbg_batch* B, int p, int* group, uint64_t* cell_offset, uint64_t* n_cells) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && p >= 0 && p < (int)B->prob_group.size(), "bad argument");
+    const int g = B->prob_group[p], i = B->prob_index[p];
+    const msbg_poisson* P = B->groups[g];
+    const int64_t cb = (int64_t)P->lv[0].bs * P->lv[0].bs * P->lv[0].bs;
+    if (group) *group = g;
+    if (cell_offset) *cell_offset = (uint64_t)(P->prob_blocks[i] * cb);
+    if (n_cells) *n_cells = (uint64_t)((P->prob_blocks[i + 1] - P->prob_blocks[i]) * cb);
+    MSBG_API_END
+}
+
+int msbg_batch_buffers(msbg_batch* B, int g, float** d_b, double** d_x, uint64_t* n_cells, int* bsx) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && g >= 0 && g < (int)B->groups.size(), "bad argument");
+    if (d_b) *d_b = B->b[g].as<float>();
+    if (d_x) *d_x = B->x[g].as<double>();
+    if (n_cells) *n_cells = (uint64_t)B->groups[g]->lv[0].cells();
+    if (bsx) *bsx = B->groups[g]->lv[0].bs;
+    MSBG_API_END
+}
+
+int msbg_batch_set_rhs(msbg_batch* B, int p, const float* b) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && b && p >= 0 && p < (int)B->prob_group.size(), "bad argument");
+    set_device(B->ctx);
+    const int g = B->prob_group[p], i = B->prob_index[p];
+    const msbg_poisson* P = B->groups[g];
+    const int64_t cb = (int64_t)P->lv[0].bs * P->lv[0].bs * P->lv[0].bs;
+    const int64_t off = P->prob_blocks[i] * cb, cnt = (P->prob_blocks[i + 1] - P->prob_blocks[i]) * cb;
+    CUDA_CHECK(cudaMemcpyAsync(B->b[g].as<float>() + off, b, (size_t)cnt * 4, cudaMemcpyHostToDevice, B->ctx->stream));
+    sync(B->ctx);
+    MSBG_API_END
+}
+
+int msbg_batch_get_solution(msbg_batch* B, int p, double* x) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && x && p >= 0 && p < (int)B->prob_group.size(), "bad argument");
+    set_device(B->ctx);
+    const int g = B->prob_group[p], i = B->prob_index[p];
+    const msbg_poisson* P = B->groups[g];
+    const int64_t cb = (int64_t)P->lv[0].bs * P->lv[0].bs * P->lv[0].bs;
+    const int64_t off = P->prob_blocks[i] * cb, cnt = (P->prob_blocks[i + 1] - P->prob_blocks[i]) * cb;
+    CUDA_CHECK(cudaMemcpyAsync(x, B->x[g].as<double>() + off, (size_t)cnt * 8, cudaMemcpyDeviceToHost, B->ctx->stream));
+    sync(B->ctx);
+    MSBG_API_END
+}
+
+int msbg_batch_groups(const msbg_batch* B, int* n_groups) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && n_groups, "null argument");
+    *n_groups = (int)B->groups.size();
+    MSBG_API_END
+}
+
+int msbg_batch_tuning(const msbg_batch* B, int g, int* cfg_out, uint64_t* cells_out, size_t cap, size_t* n_levels) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && g >= 0 && g < (int)B->groups.size() && n_levels, "bad argument");
+    const msbg_poisson* P = B->groups[g];
+    *n_levels = P->lv.size();
+    for (size_t l = 0; l < P->lv.size() && l < cap; ++l) {
+        if (cfg_out) {
+            cfg_out[2 * l] = P->lv[l].cfg_jac;
+            cfg_out[2 * l + 1] = P->lv[l].cfg_res;
+        }
+        if (cells_out) cells_out[l] = (uint64_t)P->lv[l].cells();
+    }
+    MSBG_API_END
+}
+
+// Solves every problem of the batch to relative residual `tol` (true
+// residual of the FP64 solution) from the current solutions (zero_x: from
+// zero).  Each cycle -- iters_per_cycle CG iterations for all problems and
+// the FP64 residual replacement -- is one CUDA graph launch.
+int msbg_batch_solve(msbg_batch* B, double tol, int iters_per_cycle, int max_cycles, int zero_x, int* iters_out,
+                     double* rel_out, int* cycles_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(B && tol > 0.0 && iters_per_cycle > 0 && max_cycles >= 0, "bad argument");
+    msbg_ctx* ctx = B->ctx;
+    MSBG_REQUIRE(!ctx->timing, "per-kernel timing must be off for the captured batch solve");
+    set_device(ctx);
+    for (size_t g = 0; g < B->groups.size(); ++g) {
+        msbg_poisson* P = B->groups[g];
+        if (zero_x) CUDA_CHECK(cudaMemsetAsync(B->x[g].p, 0, (size_t)P->lv[0].cells() * 8, ctx->stream));
+        batch_start(P, B->x[g].as<double>(), B->b[g].as<float>(), tol);
+    }
+    if (!B->exec || B->graph_k != iters_per_cycle || B->graph_tol != tol) {
+        if (B->exec) cudaGraphExecDestroy(B->exec);
+        if (B->graph) cudaGraphDestroy(B->graph);
+        B->exec = nullptr;
+        B->graph = nullptr;
+        const uint64_t l0 = ctx->launches;
+        CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (size_t g = 0; g < B->groups.size(); ++g)
+                batch_cycle(B->groups[g], B->x[g].as<double>(), B->b[g].as<float>(), iters_per_cycle, tol);
+        } catch (...) {
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(ctx->stream, &tmp);
+            if (tmp) cudaGraphDestroy(tmp);
+            ctx->launches = l0;
+            throw;
+        }
+        CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &B->graph));
+        CUDA_CHECK(cudaGraphInstantiate(&B->exec, B->graph, 0));
+        B->graph_k = iters_per_cycle;
+        B->graph_tol = tol;
+        B->graph_kernels = (int)(ctx->launches - l0);
+        ctx->launches = l0;
+    }
+    std::vector<std::vector<double>> sc(B->groups.size());
+    auto read_scalars = [&]() {
+        bool any = false;
+        for (size_t g = 0; g < B->groups.size(); ++g) {
+            const msbg_poisson* P = B->groups[g];
+            sc[g].resize((size_t)P->np * S_WIDTH);
+            CUDA_CHECK(cudaMemcpyAsync(sc[g].data(), P->scal.p, sc[g].size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        sync(ctx);
+        for (size_t g = 0; g < B->groups.size(); ++g)
+            for (int i = 0; i < B->groups[g]->np; ++i) any |= sc[g][(size_t)i * S_WIDTH + S_ACTIVE] > 0.0;
+        return any;
+    };
+    bool any = read_scalars();
+    int cycles = 0;
+    while (any && cycles < max_cycles) {
+        CUDA_CHECK(cudaGraphLaunch(B->exec, ctx->stream));
+        ctx->launches += (uint64_t)B->graph_kernels;
+        ++cycles;
+        any = read_scalars();
+    }
+    for (size_t p = 0; p < B->prob_group.size(); ++p) {
+        const double* S = sc[B->prob_group[p]].data() + (size_t)B->prob_index[p] * S_WIDTH;
+        if (iters_out) iters_out[p] = (int)S[S_ITER];
+        if (rel_out) rel_out[p] = S[S_BB] > 0.0 ? std::sqrt(S[S_RR] / S[S_BB]) : 0.0;
+    }
+    if (cycles_out) *cycles_out = cycles;
     MSBG_API_END
 }
 

@@ -144,3 +144,32 @@ def smooth_divergence_rhs(size: int, bsx: int, active: np.ndarray, seed: int = 4
             acc += -(d @ amp[i]) / sig[i] ** 2 * np.exp(-r2 / (2.0 * sig[i] ** 2))
         out[s:s + chunk] = acc
     return out.astype(np.float32).reshape(len(bids), bsx ** 3)
+
+
+def batched_problems(n: int = 64, seed: int = 3, edges=(32, 64, 128, 256), block_sizes=(8, 16),
+                     fraction=(0.05, 0.6)):
+    """The batched-solve configuration: n problems, each a cube of edge drawn
+    from `edges`, blocks of 8^3 or 16^3, an active fraction uniform in
+    `fraction` made of the blocks closest to a random sphere surface (a shell
+    of that volume fraction), right-hand side uniform in [-1, 1] with its
+    mean removed.  Returns [(dims, bsx, active, rhs)], rhs [n_active][bsx^3]
+    f32 in ascending block-id order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        edge = int(rng.choice(edges))
+        bsx = int(rng.choice(block_sizes))
+        nb = edge // bsx
+        f = rng.uniform(*fraction)
+        b = np.arange(nb)
+        bz, by, bx = np.meshgrid(b, b, b, indexing="ij")
+        centre = (np.stack([bx, by, bz], -1).reshape(-1, 3) + 0.5) * bsx
+        c = rng.uniform(0.3, 0.7, 3) * edge
+        r = rng.uniform(0.2, 0.45) * edge
+        d = np.abs(np.linalg.norm(centre - c, axis=1) - r)
+        k = max(1, int(np.ceil(f * nb ** 3)))
+        active = np.sort(np.argsort(d, kind="stable")[:k]).astype(np.uint64)
+        rhs = rng.uniform(-1.0, 1.0, (k, bsx ** 3))
+        rhs -= rhs.mean()
+        out.append(((edge, edge, edge), bsx, active, rhs.astype(np.float32)))
+    return out
