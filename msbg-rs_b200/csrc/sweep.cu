@@ -17,6 +17,7 @@
 // where the reference calls mul_add.  Results are bit-identical to the CPU
 // restatement in oracle/.
 #include <algorithm>
+#include <type_traits>
 
 #include "sweep.cuh"
 
@@ -84,6 +85,7 @@ __device__ __forceinline__ float stencil_bilaplacian(const float* h, int i, int 
 
 struct SweepArgs {
     void* payload;              // fine payload (grid dtype)
+    float* xface;               // [slots][2][bsx^2] stored x-planes of every block ([z][y]), or null
     const float* coarse;        // coarse payload (f32) for multiresolution halos
     const int32_t* nbr;         // [n][27]
     const int32_t* bxyz;        // [n][4]: block coords + flags (bit h-1: interior for halo h)
@@ -131,13 +133,167 @@ template <int ST> __device__ __forceinline__ bool xhalo_needed(int dx, int dy, i
     return (dy == 0 && dz == 0) || (dx == 1 && dy + dz == 1 && (dy == 1 || dz == 1));
 }
 
+// The stencil over one staged block: thread (x, y) walks its z-column, reads
+// the staged values from shared memory, writes the result in place (and the
+// block's new x-planes to the side buffer).
+template <class E, int BSX, int ST>
+__device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+    constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
+    constexpr int HSX = BSX + 2 * HALO;
+    constexpr int RS = Stage<BSX>::RS;
+    constexpr int PL = HSX * RS;
+    constexpr int X0 = 4 - HALO;
+    constexpr int N = BSX * BSX * BSX;
+    typename E::T* payload = (typename E::T*)a.payload;
+    if (tid < BSX * BSX) {
+        const int x = tid % BSX, y = tid / BSX;
+        typename E::T* out = payload + (size_t)slot * N + x + y * BSX;
+        // this block's new x-planes go to the side buffer as well
+        float* xo = (a.xface && (x == 0 || x == BSX - 1))
+                        ? a.xface + ((size_t)slot * 2 + (x == 0 ? 0 : 1)) * (BSX * BSX) + y
+                        : nullptr;
+        const int i0 = (HALO * HSX + (y + HALO)) * RS + X0 + x + HALO;  // z = 0
+        const float dt = a.dt;
+        const int clamp01 = a.clamp01;
+        if (ST == MSBG_LAPLACIAN) {
+            // taps along z slide through registers: 5 shared loads per output
+            float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
+#pragma unroll 4
+            for (int z = 0; z < BSX; ++z) {
+                const int i = i0 + z * PL;
+                const float lx = h[i - 1], rx = h[i + 1], dyu = h[i - RS], dyd = h[i + RS];
+                float nbs = lx + rx;
+                nbs = nbs + dyu;
+                nbs = nbs + dyd;
+                nbs = nbs + zb;
+                nbs = nbs + zf;
+                const float lap = fmaf(c, -6.0f, nbs);
+                const float fx = (rx - lx) * 0.5f, fy = (dyd - dyu) * 0.5f, fz = (zf - zb) * 0.5f;
+                const float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
+                const float nv = fmaf(dt * lap, g, c);
+                const typename E::T sv = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                out[z * BSX * BSX] = sv;
+                if (xo) xo[z * BSX] = E::load(sv);
+                zb = c;
+                c = zf;
+                if (z + 1 < BSX) zf = h[i + 2 * PL];
+            }
+        } else if (ST == MSBG_MEAN_CURVATURE) {
+            // plane z-1: cross (c, x-, x+, y-, y+); plane z: 3x3; plane z+1: cross
+            float pc = h[i0 - PL], pxm = h[i0 - PL - 1], pxp = h[i0 - PL + 1], pym = h[i0 - PL - RS], pyp = h[i0 - PL + RS];
+            float c = h[i0], cxm = h[i0 - 1], cxp = h[i0 + 1], cym = h[i0 - RS], cyp = h[i0 + RS];
+            float nc = h[i0 + PL], nxm = h[i0 + PL - 1], nxp = h[i0 + PL + 1], nym = h[i0 + PL - RS], nyp = h[i0 + PL + RS];
+#pragma unroll 2
+            for (int z = 0; z < BSX; ++z) {
+                const int i = i0 + z * PL;
+                const float xpyp = h[i + 1 + RS], xpym = h[i + 1 - RS], xmyp = h[i - 1 + RS], xmym = h[i - 1 - RS];
+                // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
+                const float f0 = c, f1 = cxm, f2 = cxp, f3 = cym, f4 = cyp, f5 = pc, f6 = nc;
+                const float fx = (f2 - f1) * 0.5f, fy = (f4 - f3) * 0.5f, fz = (f6 - f5) * 0.5f;
+                const float fxx = (f1 + f2) - 2.0f * f0, fyy = (f3 + f4) - 2.0f * f0, fzz = (f5 + f6) - 2.0f * f0;
+                const float d1 = xpyp, d2 = xpym, d3 = xmyp, d4 = xmym;
+                const float d5 = nxp, d6 = pxp, d7 = nxm, d8 = pxm;
+                const float d9 = nyp, d10 = pyp, d11 = nym, d12 = pym;
+                const float fyx = (((d1 - d2) - d3) + d4) * 0.25f;
+                const float fzx = (((d5 - d6) - d7) + d8) * 0.25f;
+                const float fzy = (((d9 - d10) - d11) + d12) * 0.25f;
+                const float cross = (fx * (fy * fyx) + fx * (fz * fzx)) + fy * (fz * fzy);
+                const float hnum = fmaf(fy * fy + fz * fz, fxx, fmaf(fx * fx + fz * fz, fyy, fmaf(fx * fx + fy * fy, fzz, -2.0f * cross)));
+                const float grad = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+                const float hc = grad > 1e-7f ? hnum / grad : 0.0f;
+                const float d = clampf(dt * hc, -0.1f, 0.1f);
+                const float nv = f0 + d;
+                const typename E::T sv = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                out[z * BSX * BSX] = sv;
+                if (xo) xo[z * BSX] = E::load(sv);
+                pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
+                c = nc; cxm = nxm; cxp = nxp; cym = nym; cyp = nyp;
+                if (z + 1 < BSX) {
+                    const int j = i + 2 * PL;
+                    nc = h[j]; nxm = h[j - 1]; nxp = h[j + 1]; nym = h[j - RS]; nyp = h[j + RS];
+                }
+            }
+        } else {
+#pragma unroll 4
+            for (int z = 0; z < BSX; ++z) {
+                const int i = i0 + z * PL;
+                const typename E::T sv = E::store(stencil_bilaplacian(h, i, RS, PL, dt, clamp01));
+                out[z * BSX * BSX] = sv;
+                if (xo) xo[z * BSX] = E::load(sv);
+            }
+        }
+    }
+}
+
+// General staging (blocks at the domain edge): resolve every staged
+// coordinate with the Neumann rule (solver.rs:205-209).  ok/dd/ll are shared
+// scratch arrays [3][HSX].
+template <class E, int BSX, int ST>
+__device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const int32_t* nb, int pi, int8_t* ok, int8_t* dd,
+                              int8_t* ll) {
+    constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
+    constexpr int HSX = BSX + 2 * HALO;
+    constexpr int RS = Stage<BSX>::RS;
+    constexpr int X0 = 4 - HALO;
+    constexpr int LG = Lg<BSX>::v;
+    constexpr int N = BSX * BSX * BSX;
+    const typename E::T* payload = (const typename E::T*)a.payload;
+    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+    // General path (blocks at the domain edge): resolve every staged
+    // coordinate with the Neumann rule (solver.rs:205-209).
+    for (int i = tid; i < 3 * HSX; i += nthr) {
+        int ax = i / HSX, hh = i % HSX;
+        int32_t smax = ax == 0 ? a.sx : ax == 1 ? a.sy : a.sz;
+        int32_t b0 = a.bxyz[(size_t)pi * 4 + ax];
+        int32_t g = b0 * BSX + hh - HALO, r;
+        bool o = resolve_axis(g, smax - 1, MSBG_NEUMANN, &r);
+        ok[ax * HSX + hh] = o;
+        dd[ax * HSX + hh] = (int8_t)((r >> LG) - b0 + 1);
+        ll[ax * HSX + hh] = (int8_t)(r & (BSX - 1));
+    }
+    __syncthreads();
+    for (int r = warp; r < HSX * HSX; r += nwarp) {
+        const int hz = r / HSX, hy = r % HSX;
+        const bool midy = hy >= HALO && hy < HALO + BSX, midz = hz >= HALO && hz < HALO + BSX;
+        for (int hx = lane; hx < HSX; hx += 32) {
+            const bool midx = hx >= HALO && hx < HALO + BSX;
+            const int nout = (!midx) + (!midy) + (!midz);
+            bool need;
+            if (ST == MSBG_LAPLACIAN) {
+                need = nout <= 1;
+            } else if (ST == MSBG_MEAN_CURVATURE) {
+                need = nout <= 2;
+            } else {
+                const bool d1x = hx == HALO - 1 || hx == HALO + BSX, d1y = hy == HALO - 1 || hy == HALO + BSX,
+                           d1z = hz == HALO - 1 || hz == HALO + BSX;
+                need = nout <= 1 || (nout == 2 && (midx || d1x) && (midy || d1y) && (midz || d1z));
+            }
+            if (!need) continue;
+            float v = a.empty;
+            if (ok[hx] && ok[HSX + hy] && ok[2 * HSX + hz]) {
+                const int c = nb[dd[hx] + 3 * dd[HSX + hy] + 9 * dd[2 * HSX + hz]];
+                const int lx = ll[hx], ly = ll[HSX + hy], lz = ll[2 * HSX + hz];
+                if (c >= 0) {
+                    v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
+                } else if (c == kCodeFull) {
+                    v = a.full;
+                } else if (c <= kCodeCoarse0) {
+                    constexpr int CLG = LG - 1;
+                    const int cs = kCodeCoarse0 - c;
+                    v = a.coarse[(size_t)cs * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
+                }
+            }
+            h[(hz * HSX + hy) * RS + X0 + hx] = v;
+        }
+    }
+}
+
 template <class E, int BSX, int ST>
 __global__ void __launch_bounds__(BSX * BSX < 32 ? 32 : BSX * BSX)
 sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
     constexpr int HSX = BSX + 2 * HALO;
     constexpr int RS = Stage<BSX>::RS;
-    constexpr int PL = HSX * RS;
     constexpr int X0 = 4 - HALO;  // column of halo x = 0
     constexpr int LG = Lg<BSX>::v;
     constexpr int N = BSX * BSX * BSX;
@@ -148,7 +304,7 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     __shared__ int32_t flags;
     __shared__ int8_t ok[3][HSX], dd[3][HSX], ll[3][HSX];
     typename E::T* payload = (typename E::T*)a.payload;
-    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+    const int tid = threadIdx.x, nthr = blockDim.x;
 
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const int pi = order[t];
@@ -284,7 +440,11 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
                     }
                 }
                 if (dx[k] >= 0) {
-                    if (c >= 0) {
+                    if (c >= 0 && a.xface && (lx == 0 || lx == BSX - 1)) {
+                        // x-plane cells from the side buffer: 16 contiguous
+                        // floats per (z) row instead of one sector per cell
+                        vx[k] = a.xface[((size_t)c * 2 + (lx == 0 ? 0 : 1)) * (BSX * BSX) + lz * BSX + ly];
+                    } else if (c >= 0) {
                         vx[k] = E::load(payload[(size_t)c * N + lx + (ly << LG) + (lz << (2 * LG))]);
                     } else if (c <= kCodeCoarse0) {
                         constexpr int CLG = LG > 0 ? LG - 1 : 0;
@@ -298,124 +458,211 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
             for (int k = 0; k < KX; ++k)
                 if (dx[k] >= 0) h[dx[k]] = vx[k];
         } else {
-            // General path (blocks at the domain edge): resolve every staged
-            // coordinate with the Neumann rule (solver.rs:205-209).
-            for (int i = tid; i < 3 * HSX; i += nthr) {
-                int ax = i / HSX, hh = i % HSX;
-                int32_t smax = ax == 0 ? a.sx : ax == 1 ? a.sy : a.sz;
-                int32_t b0 = a.bxyz[(size_t)pi * 4 + ax];
-                int32_t g = b0 * BSX + hh - HALO, r;
-                bool o = resolve_axis(g, smax - 1, MSBG_NEUMANN, &r);
-                ok[ax][hh] = o;
-                dd[ax][hh] = (int8_t)((r >> LG) - b0 + 1);
-                ll[ax][hh] = (int8_t)(r & (BSX - 1));
-            }
-            __syncthreads();
-            for (int r = warp; r < HSX * HSX; r += nwarp) {
-                const int hz = r / HSX, hy = r % HSX;
-                const bool midy = hy >= HALO && hy < HALO + BSX, midz = hz >= HALO && hz < HALO + BSX;
-                for (int hx = lane; hx < HSX; hx += 32) {
-                    const bool midx = hx >= HALO && hx < HALO + BSX;
-                    const int nout = (!midx) + (!midy) + (!midz);
-                    bool need;
-                    if (ST == MSBG_LAPLACIAN) {
-                        need = nout <= 1;
-                    } else if (ST == MSBG_MEAN_CURVATURE) {
-                        need = nout <= 2;
-                    } else {
-                        const bool d1x = hx == HALO - 1 || hx == HALO + BSX, d1y = hy == HALO - 1 || hy == HALO + BSX,
-                                   d1z = hz == HALO - 1 || hz == HALO + BSX;
-                        need = nout <= 1 || (nout == 2 && (midx || d1x) && (midy || d1y) && (midz || d1z));
-                    }
-                    if (!need) continue;
-                    float v = a.empty;
-                    if (ok[0][hx] && ok[1][hy] && ok[2][hz]) {
-                        const int c = nb[dd[0][hx] + 3 * dd[1][hy] + 9 * dd[2][hz]];
-                        const int lx = ll[0][hx], ly = ll[1][hy], lz = ll[2][hz];
-                        if (c >= 0) {
-                            v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
-                        } else if (c == kCodeFull) {
-                            v = a.full;
-                        } else if (c <= kCodeCoarse0) {
-                            constexpr int CLG = LG - 1;
-                            const int cs = kCodeCoarse0 - c;
-                            v = a.coarse[(size_t)cs * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
-                        }
-                    }
-                    h[(hz * HSX + hy) * RS + X0 + hx] = v;
-                }
-            }
+            stage_general<E, BSX, ST>(a, h, nb, pi, &ok[0][0], &dd[0][0], &ll[0][0]);
         }
         __syncthreads();
-        if (tid < BSX * BSX) {
-            const int x = tid % BSX, y = tid / BSX;
-            const int slot = nb[13];
-            typename E::T* out = payload + (size_t)slot * N + x + y * BSX;
-            const int i0 = (HALO * HSX + (y + HALO)) * RS + X0 + x + HALO;  // z = 0
-            const float dt = a.dt;
-            const int clamp01 = a.clamp01;
-            if (ST == MSBG_LAPLACIAN) {
-                // taps along z slide through registers: 5 shared loads per output
-                float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
-#pragma unroll 4
-                for (int z = 0; z < BSX; ++z) {
-                    const int i = i0 + z * PL;
-                    const float lx = h[i - 1], rx = h[i + 1], dyu = h[i - RS], dyd = h[i + RS];
-                    float nbs = lx + rx;
-                    nbs = nbs + dyu;
-                    nbs = nbs + dyd;
-                    nbs = nbs + zb;
-                    nbs = nbs + zf;
-                    const float lap = fmaf(c, -6.0f, nbs);
-                    const float fx = (rx - lx) * 0.5f, fy = (dyd - dyu) * 0.5f, fz = (zf - zb) * 0.5f;
-                    const float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
-                    const float nv = fmaf(dt * lap, g, c);
-                    out[z * BSX * BSX] = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
-                    zb = c;
-                    c = zf;
-                    if (z + 1 < BSX) zf = h[i + 2 * PL];
-                }
-            } else if (ST == MSBG_MEAN_CURVATURE) {
-                // plane z-1: cross (c, x-, x+, y-, y+); plane z: 3x3; plane z+1: cross
-                float pc = h[i0 - PL], pxm = h[i0 - PL - 1], pxp = h[i0 - PL + 1], pym = h[i0 - PL - RS], pyp = h[i0 - PL + RS];
-                float c = h[i0], cxm = h[i0 - 1], cxp = h[i0 + 1], cym = h[i0 - RS], cyp = h[i0 + RS];
-                float nc = h[i0 + PL], nxm = h[i0 + PL - 1], nxp = h[i0 + PL + 1], nym = h[i0 + PL - RS], nyp = h[i0 + PL + RS];
-#pragma unroll 2
-                for (int z = 0; z < BSX; ++z) {
-                    const int i = i0 + z * PL;
-                    const float xpyp = h[i + 1 + RS], xpym = h[i + 1 - RS], xmyp = h[i - 1 + RS], xmym = h[i - 1 - RS];
-                    // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
-                    const float f0 = c, f1 = cxm, f2 = cxp, f3 = cym, f4 = cyp, f5 = pc, f6 = nc;
-                    const float fx = (f2 - f1) * 0.5f, fy = (f4 - f3) * 0.5f, fz = (f6 - f5) * 0.5f;
-                    const float fxx = (f1 + f2) - 2.0f * f0, fyy = (f3 + f4) - 2.0f * f0, fzz = (f5 + f6) - 2.0f * f0;
-                    const float d1 = xpyp, d2 = xpym, d3 = xmyp, d4 = xmym;
-                    const float d5 = nxp, d6 = pxp, d7 = nxm, d8 = pxm;
-                    const float d9 = nyp, d10 = pyp, d11 = nym, d12 = pym;
-                    const float fyx = (((d1 - d2) - d3) + d4) * 0.25f;
-                    const float fzx = (((d5 - d6) - d7) + d8) * 0.25f;
-                    const float fzy = (((d9 - d10) - d11) + d12) * 0.25f;
-                    const float cross = (fx * (fy * fyx) + fx * (fz * fzx)) + fy * (fz * fzy);
-                    const float hnum = fmaf(fy * fy + fz * fz, fxx, fmaf(fx * fx + fz * fz, fyy, fmaf(fx * fx + fy * fy, fzz, -2.0f * cross)));
-                    const float grad = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
-                    const float hc = grad > 1e-7f ? hnum / grad : 0.0f;
-                    const float d = clampf(dt * hc, -0.1f, 0.1f);
-                    const float nv = f0 + d;
-                    out[z * BSX * BSX] = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
-                    pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
-                    c = nc; cxm = nxm; cxp = nxp; cym = nym; cyp = nyp;
-                    if (z + 1 < BSX) {
-                        const int j = i + 2 * PL;
-                        nc = h[j]; nxm = h[j - 1]; nxp = h[j + 1]; nym = h[j - RS]; nyp = h[j + RS];
-                    }
-                }
+        sweep_compute<E, BSX, ST>(a, h, nb[13], tid);
+    }
+}
+
+// ---- pipelined f32 sweep ------------------------------------------------------
+// Persistent CTAs, two staging buffers: while a CTA computes one block, the
+// cp.async copies of the next block it owns (interior blocks: centre, face
+// rows, x-planes from the side buffer) are in flight into the other buffer,
+// so staging latency overlaps the stencil instead of preceding it.  Blocks at
+// the domain edge are staged synchronously by stage_general.  f32 grids only
+// (cp.async copies bytes; the other storage types need dequantising).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int K> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory"); }
+
+// Issues the staging of an interior block (flag bit HALO-1 set) into h.
+template <int BSX, int ST>
+__device__ __forceinline__ void issue_interior_f32(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
+    constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
+    constexpr int HSX = BSX + 2 * HALO;
+    constexpr int RS = Stage<BSX>::RS;
+    constexpr int X0 = 4 - HALO;
+    constexpr int LG = Lg<BSX>::v;
+    constexpr int N = BSX * BSX * BSX;
+    constexpr int QR = BSX / 4;
+    constexpr int NT = BSX * BSX < 32 ? 32 : BSX * BSX;
+    const float* payload = (const float*)a.payload;
+    const int tid = threadIdx.x;
+    const int c13 = nb[13];
+    for (int it = tid; it < N / 4; it += NT) {
+        const int q = it % QR, r = it / QR, y = r % BSX, z = r / BSX;
+        cp_async16(h + ((z + HALO) * HSX + y + HALO) * RS + 4 + 4 * q, payload + (size_t)c13 * N + 4 * it);
+    }
+    constexpr int NFACE = 4 * HALO * BSX * QR;
+    constexpr int NEDGE = ST == MSBG_LAPLACIAN ? 0 : 4 * QR;
+    for (int it = tid; it < NFACE + NEDGE; it += NT) {
+        int c, dst, lyq, lzq, srcoff;
+        if (it < NFACE) {
+            const int q = it % QR, rr = it / QR;
+            const int row = rr % BSX, pd = rr / BSX;
+            const int axis = pd / (2 * HALO), sd = pd % (2 * HALO);
+            const int side = sd < HALO ? -1 : 1, d = sd < HALO ? sd + 1 : sd - HALO + 1;
+            const int l = side < 0 ? BSX - d : d - 1;
+            const int hh = side < 0 ? HALO - d : HALO + BSX - 1 + d;
+            if (axis == 0) {
+                c = nb[13 + 3 * side];
+                srcoff = (l << LG) + (row << (2 * LG)) + 4 * q;
+                dst = ((row + HALO) * HSX + hh) * RS + 4 + 4 * q;
+                lyq = l;
+                lzq = row;
             } else {
-#pragma unroll 4
-                for (int z = 0; z < BSX; ++z) {
-                    const int i = i0 + z * PL;
-                    out[z * BSX * BSX] = E::store(stencil_bilaplacian(h, i, RS, PL, dt, clamp01));
-                }
+                c = nb[13 + 9 * side];
+                srcoff = (row << LG) + (l << (2 * LG)) + 4 * q;
+                dst = (hh * HSX + row + HALO) * RS + 4 + 4 * q;
+                lyq = row;
+                lzq = l;
+            }
+        } else {
+            const int e = it - NFACE, q = e % QR, corner = e / QR;
+            const int sy = (corner & 1) ? 1 : -1, sz = (corner & 2) ? 1 : -1;
+            lyq = sy < 0 ? BSX - 1 : 0;
+            lzq = sz < 0 ? BSX - 1 : 0;
+            const int hy = sy < 0 ? HALO - 1 : HALO + BSX, hz = sz < 0 ? HALO - 1 : HALO + BSX;
+            c = nb[13 + 3 * sy + 9 * sz];
+            dst = (hz * HSX + hy) * RS + 4 + 4 * q;
+            srcoff = (lyq << LG) + (lzq << (2 * LG)) + 4 * q;
+        }
+        if (c >= 0) {
+            cp_async16(h + dst, payload + (size_t)c * N + srcoff);
+        } else if (c <= kCodeCoarse0) {
+            constexpr int CLG = LG > 0 ? LG - 1 : 0;
+            const int lx = srcoff & (BSX - 1);
+            const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((lyq >> 1) << CLG) + ((lzq >> 1) << (2 * CLG));
+            *reinterpret_cast<float4*>(h + dst) = make_float4(cp[lx >> 1], cp[(lx + 1) >> 1], cp[(lx + 2) >> 1], cp[(lx + 3) >> 1]);
+        } else {
+            const float f = c == kCodeFull ? a.full : a.empty;
+            *reinterpret_cast<float4*>(h + dst) = make_float4(f, f, f, f);
+        }
+    }
+    constexpr int NXF = 2 * HALO * BSX * BSX;
+    constexpr int NXE = ST == MSBG_LAPLACIAN ? 0 : 8 * BSX;
+    for (int it = tid; it < NXF + NXE; it += NT) {
+        int c, lx, ly, lz, dst;
+        if (it < NXF) {
+            const int y = it % BSX, z = (it / BSX) % BSX, sd = it / (BSX * BSX);
+            const int side = sd < HALO ? -1 : 1, d = sd < HALO ? sd + 1 : sd - HALO + 1;
+            lx = side < 0 ? BSX - d : d - 1;
+            ly = y;
+            lz = z;
+            const int hx = side < 0 ? HALO - d : HALO + BSX - 1 + d;
+            c = nb[13 + side];
+            dst = ((z + HALO) * HSX + y + HALO) * RS + X0 + hx;
+        } else {
+            const int e = it - NXF, j = e % BSX, kind = e / BSX;
+            const int sx = (kind & 1) ? 1 : -1, so = (kind & 2) ? 1 : -1;
+            lx = sx < 0 ? BSX - 1 : 0;
+            const int hx = sx < 0 ? HALO - 1 : HALO + BSX;
+            const int ho = so < 0 ? HALO - 1 : HALO + BSX, lo = so < 0 ? BSX - 1 : 0;
+            if (kind < 4) {
+                ly = j;
+                lz = lo;
+                c = nb[13 + sx + 9 * so];
+                dst = (ho * HSX + j + HALO) * RS + X0 + hx;
+            } else {
+                ly = lo;
+                lz = j;
+                c = nb[13 + sx + 3 * so];
+                dst = ((j + HALO) * HSX + ho) * RS + X0 + hx;
             }
         }
+        if (c >= 0 && a.xface && (lx == 0 || lx == BSX - 1)) {
+            cp_async4(h + dst, a.xface + ((size_t)c * 2 + (lx == 0 ? 0 : 1)) * (BSX * BSX) + lz * BSX + ly);
+        } else if (c >= 0) {
+            cp_async4(h + dst, payload + (size_t)c * N + lx + (ly << LG) + (lz << (2 * LG)));
+        } else if (c <= kCodeCoarse0) {
+            constexpr int CLG = LG > 0 ? LG - 1 : 0;
+            h[dst] = a.coarse[(size_t)(kCodeCoarse0 - c) * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
+        } else {
+            h[dst] = c == kCodeFull ? a.full : a.empty;
+        }
+    }
+}
+
+template <int BSX, int ST>
+__global__ void __launch_bounds__(BSX * BSX < 32 ? 32 : BSX * BSX)
+sweep_pipe_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
+    constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
+    constexpr int HSX = BSX + 2 * HALO;
+    constexpr int BUF = HSX * HSX * Stage<BSX>::RS;  // floats per staging buffer
+    extern __shared__ float4 h4[];
+    float* hb = reinterpret_cast<float*>(h4);
+    __shared__ int32_t nbs[2][27];
+    __shared__ int32_t flg[2], pis[2];
+    __shared__ int8_t ok[3][HSX], dd[3][HSX], ll[3][HSX];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    int t = blockIdx.x;
+    if (t >= n) return;
+    auto meta = [&](int tt, int b) {
+        const int pi = order[tt];
+        if (tid < 27) nbs[b][tid] = a.nbr[(size_t)pi * 27 + tid];
+        if (tid == nthr - 1) {
+            flg[b] = a.bxyz[(size_t)pi * 4 + 3];
+            pis[b] = pi;
+        }
+    };
+    meta(t, 0);
+    __syncthreads();
+    if ((flg[0] >> (HALO - 1)) & 1) issue_interior_f32<BSX, ST>(a, hb, nbs[0]);
+    cp_async_commit();
+    for (int j = 0; t < n; t += gridDim.x, ++j) {
+        const int b = j & 1, bn = b ^ 1;
+        const int tn = t + gridDim.x;
+        if (tn < n) meta(tn, bn);
+        __syncthreads();  // nbs[bn] visible; every thread is done with buffer bn (the previous block)
+        if (tn < n && ((flg[bn] >> (HALO - 1)) & 1)) issue_interior_f32<BSX, ST>(a, hb + bn * BUF, nbs[bn]);
+        cp_async_commit();
+        if ((flg[b] >> (HALO - 1)) & 1) cp_async_wait<1>();  // this block's copies have landed
+        else stage_general<ElemF32, BSX, ST>(a, hb + b * BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
+        __syncthreads();
+        sweep_compute<ElemF32, BSX, ST>(a, hb + b * BUF, nbs[b][13], tid);
+    }
+    cp_async_wait<0>();
+}
+
+// Copies the x-planes (x = 0 and x = bsx-1) of the listed slots into the side
+// buffer: [slot][plane][z][y].
+template <class E, int BSX>
+__global__ void xface_init_kernel(const typename E::T* __restrict__ payload, const int32_t* __restrict__ slots, size_t n,
+                                  float* __restrict__ xface) {
+    constexpr int LG = Lg<BSX>::v, N = BSX * BSX * BSX, P = BSX * BSX;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n * 2 * P; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = e / (2 * P);
+        const int r = (int)(e % (2 * P)), side = r / P, zy = r % P, z = zy / BSX, y = zy % BSX;
+        const int32_t slot = slots[k];
+        const int x = side ? BSX - 1 : 0;
+        xface[((size_t)slot * 2 + side) * P + zy] = E::load(payload[(size_t)slot * N + x + (y << LG) + (z << (2 * LG))]);
+    }
+}
+
+template <class E, int BSX>
+static void launch_xface_init(msbg_ctx* ctx, const void* payload, const int32_t* slots, size_t n, float* xface) {
+    if (!n) return;
+    begin_launch(ctx);
+    xface_init_kernel<E, BSX><<<(unsigned)std::min<size_t>((n * 2 * BSX * BSX + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
+        (const typename E::T*)payload, slots, n, xface);
+    after_launch(ctx, "xface_init_kernel");
+}
+
+template <class E>
+static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_t* slots, size_t n, float* xface) {
+    switch (bsx) {
+        case 4: launch_xface_init<E, 4>(ctx, payload, slots, n, xface); break;
+        case 8: launch_xface_init<E, 8>(ctx, payload, slots, n, xface); break;
+        case 16: launch_xface_init<E, 16>(ctx, payload, slots, n, xface); break;
+        default: launch_xface_init<E, 32>(ctx, payload, slots, n, xface); break;
     }
 }
 
@@ -427,9 +674,33 @@ static void launch_phase(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order
     static bool attr_set = false;  // per instantiation
     if (!attr_set) {
         CUDA_CHECK(cudaFuncSetAttribute(sweep_phase_kernel<E, BSX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // all of the SM's unified L1/shared storage as shared memory: more
+        // CTAs (and their staging loads) resident per SM
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_phase_kernel<E, BSX, ST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
         attr_set = true;
     }
     const int threads = BSX * BSX < 32 ? 32 : BSX * BSX;
+    // the double-buffered kernel for f32 and one-cell halos (two 25-tap
+    // buffers would leave too few CTAs per SM)
+    if (std::is_same<E, ElemF32>::value && BSX >= 8 && ST != MSBG_BILAPLACIAN) {
+        static bool pattr = false;
+        if (!pattr) {
+            CUDA_CHECK(cudaFuncSetAttribute(sweep_pipe_kernel<BSX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
+            CUDA_CHECK(cudaFuncSetAttribute(sweep_pipe_kernel<BSX, ST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            (int)cudaSharedmemCarveoutMaxShared));
+            pattr = true;
+        }
+        int per_sm = 0;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_pipe_kernel<BSX, ST>, threads, 2 * smem));
+        int sms = 0;
+        CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        const int grid = std::max(1, std::min(n, std::max(per_sm, 1) * sms));
+        begin_launch(ctx);
+        sweep_pipe_kernel<BSX, ST><<<(unsigned)grid, threads, 2 * smem, ctx->stream>>>(a, order, n);
+        after_launch(ctx, "sweep_phase_kernel");
+        return;
+    }
     begin_launch(ctx);
     sweep_phase_kernel<E, BSX, ST><<<(unsigned)n, threads, smem, ctx->stream>>>(a, order, n);
     after_launch(ctx, "sweep_phase_kernel");
@@ -531,6 +802,21 @@ static SweepPlan* get_plan(msbg_grid* g, msbg_grid* coarse, const uint8_t* level
     }
     plan->color_off[8] = pi;
     plan->n = (size_t)pi;
+    // slots read through x-planes: x-side neighbours (faces and edges) that are value blocks
+    {
+        std::vector<int32_t> xs;
+        for (size_t k = 0; k < nbr.size(); k += 27)
+            for (int j = 0; j < 27; ++j)
+                if (j % 3 != 1 && nbr[k + j] >= 0) xs.push_back(nbr[k + j]);
+        std::sort(xs.begin(), xs.end());
+        xs.erase(std::unique(xs.begin(), xs.end()), xs.end());
+        plan->n_xslots = xs.size();
+        if (!xs.empty()) {
+            plan->xslots.reserve(xs.size() * 4);
+            CUDA_CHECK(cudaMemcpyAsync(plan->xslots.p, xs.data(), xs.size() * 4, cudaMemcpyHostToDevice, g->ctx->stream));
+            sync(g->ctx);
+        }
+    }
     if (pi) {
         plan->nbr.reserve(nbr.size() * 4);
         plan->bxyz.reserve(bxyz.size() * 4);
@@ -569,6 +855,19 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
     a.full = coarse ? 0.0f : quantize_roundtrip(g->dtype, g->full_value);
     a.dt = dt;
     a.clamp01 = clamp01 ? 1 : 0;
+    // x-plane side buffer: sized for every slot, refreshed from the payload at
+    // the start of each call (the payload may have changed in between)
+    {
+        const size_t slots = g->n_slots();
+        if (plan->xface_slots < slots) {
+            plan->xface.reserve(slots * 2 * g->bsx * g->bsx * sizeof(float));
+            plan->xface_slots = slots;
+        }
+        a.xface = plan->xface.as<float>();
+        if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+        else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+        else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+    }
     const int32_t* order = plan->order.as<int32_t>();
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 8; ++c) {

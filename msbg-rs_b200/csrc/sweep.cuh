@@ -18,6 +18,12 @@ struct SweepPlan {
     DevBuf nbr;    // int32 [n][27]
     DevBuf bxyz;   // int32 [n][3]
     DevBuf order;  // int32 [n] plan indices grouped by colour
+    // Slots whose x-faces the sweep reads (x-neighbours of active blocks, as
+    // faces or edges), for the x-face side buffer (see sweep.cu).
+    DevBuf xslots;  // int32 [n_xslots]
+    size_t n_xslots = 0;
+    DevBuf xface;   // f32 [n_slots][2][bsx^2]: x = 0 and x = bsx-1 planes, [z][y]
+    size_t xface_slots = 0;
 };
 
 }  // namespace msbg
