@@ -173,3 +173,100 @@ def batched_problems(n: int = 64, seed: int = 3, edges=(32, 64, 128, 256), block
         rhs -= rhs.mean()
         out.append(((edge, edge, edge), bsx, active, rhs.astype(np.float32)))
     return out
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 3, base: float = 64.0, amplitude: float = 10.0) -> np.ndarray:
+    """Value noise at points p [n][3]: random values on lattices of spacing
+    base / 2^o (o < octaves), trilinearly interpolated, amplitudes halving per
+    octave, scaled so the octaves together span +-amplitude."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros(len(p), np.float64)
+    norm = sum(0.5 ** o for o in range(octaves))
+    for o in range(octaves):
+        h = base / 2 ** o
+        q = p / h
+        i0 = np.floor(q).astype(np.int64)
+        f = q - i0
+        m = int(np.max(i0)) + 2
+        lat = rng.uniform(-1.0, 1.0, (m + 1, m + 1, m + 1))
+        acc = np.zeros(len(p))
+        for dz in (0, 1):
+            for dy in (0, 1):
+                for dx in (0, 1):
+                    w = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * (f[:, 2] if dz else 1 - f[:, 2])
+                    acc += w * lat[np.clip(i0[:, 0] + dx, 0, m), np.clip(i0[:, 1] + dy, 0, m), np.clip(i0[:, 2] + dz, 0, m)]
+        out += acc * (0.5 ** o)
+    return out * (amplitude / norm)
+
+
+@dataclass
+class PhaseField:
+    """The full phase-field FLIP step: size^3 domain of 16^3 blocks, a sphere
+    of radius 0.3 size perturbed by 3-octave value noise of amplitude 10
+    cells; 4 levels by the distance of a block centre to the surface (< 16
+    cells: level 0, < 48: 1, < 112: 2, else 3); 8 particles per cell within
+    12 cells of the surface (a band of width 24), velocities N(0, 1), mass 1;
+    the phase field 0.5 (1 - tanh(phi / 2)) on the level-0 blocks."""
+
+    size: int
+    levels: np.ndarray      # [n_blocks] u8
+    fine_blocks: np.ndarray
+    phase: np.ndarray       # [n_fine][4096] f32
+    pos: np.ndarray
+    vel: np.ndarray
+    mass: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return len(self.mass)
+
+
+def phase_field(size: int = 512, seed: int = 5, ppc: int = 8, band: float = 12.0) -> PhaseField:
+    bsx = 16
+    nb = size // bsx
+    c = size / 2.0
+    r0 = 0.3 * size
+
+    def phi(p):
+        d = p - c
+        rr = np.linalg.norm(d, axis=1)
+        return rr - (r0 + value_noise(p, seed))
+
+    b = np.arange(nb)
+    bz, by, bx = np.meshgrid(b, b, b, indexing="ij")
+    centre = (np.stack([bx, by, bz], -1).reshape(-1, 3) + 0.5) * bsx
+    dist = np.abs(phi(centre))
+    lv = np.full(nb ** 3, 3, np.uint8)
+    lv[dist < 112] = 2
+    lv[dist < 48] = 1
+    lv[dist < 16] = 0
+    fine = np.nonzero(lv == 0)[0].astype(np.uint64)
+    cells = np.arange(bsx ** 3)
+    lx, ly, lz = cells % bsx, (cells // bsx) % bsx, cells // (bsx * bsx)
+    fb = fine.astype(np.int64)
+    cx = ((fb % nb)[:, None] * bsx + lx[None, :]).reshape(-1)
+    cy = (((fb // nb) % nb)[:, None] * bsx + ly[None, :]).reshape(-1)
+    cz = ((fb // (nb * nb))[:, None] * bsx + lz[None, :]).reshape(-1)
+    cc = np.stack([cx, cy, cz], -1).astype(np.float64) + 0.5
+    ph = np.empty(len(cc))
+    chunk = 1 << 21
+    for s in range(0, len(cc), chunk):
+        ph[s:s + chunk] = phi(cc[s:s + chunk])
+    phase = (0.5 * (1.0 - np.tanh(ph / 2.0))).astype(np.float32).reshape(len(fine), bsx ** 3)
+    inband = np.abs(ph) < band
+    origin = np.repeat(cc[inband] - 0.5, ppc, axis=0).astype(np.float32)
+    rng = np.random.default_rng(seed + 1)
+    pos = origin + rng.random(origin.shape, dtype=np.float32)
+    pos = np.minimum(pos, np.nextafter(origin + 1, origin, dtype=np.float32))
+    vel = rng.standard_normal(origin.shape, dtype=np.float32)
+    mass = np.ones(len(pos), np.float32)
+    order = rng.permutation(len(pos))
+    return PhaseField(size, lv, fine, phase, pos[order], vel[order], mass[order])
+
+
+def bf16_bits(a: np.ndarray) -> np.ndarray:
+    """f32 -> bf16 bit patterns, round to nearest even (the device store rule)."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    nan = (u & 0x7FFFFFFF) > 0x7F800000
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return np.where(nan, ((u >> 16) | 0x40).astype(np.uint16), r)
