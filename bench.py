@@ -514,9 +514,9 @@ def _finish(dist):
 
 
 # DRAM bytes per launch of the 7-tap sweep phase on the 2048^3 shell (7,007
-# blocks per colour), mean of two ncu-captured launches
-# (profiles/sweep_phase_kernel_shell2048.txt): 263.76 MB read + 79.98 MB written.
-SWEEP_TRAFFIC_2048 = 263.76e6 + 79.98e6
+# blocks per colour), mean of two ncu-captured launches of the pipelined kernel
+# (profiles/sweep_phase_kernel_shell2048.txt): 160.21 MB read + 76.05 MB written.
+SWEEP_TRAFFIC_2048 = 160.21e6 + 76.05e6
 
 SMOOTHER_STENCILS = {0: "7-tap laplacian", 1: "19-tap mean curvature", 2: "25-tap bilaplacian"}
 
