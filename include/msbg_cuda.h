@@ -309,7 +309,8 @@ int msbg_poisson_rhs_device(msbg_poisson* p, uint64_t seed, int n_blobs, float* 
  * (seeds seed*1000003 + i), the MG-PCG solution x* to 1e-7, then plain
  * V-cycles from zero giving (residual r_k, error x* - x_k) after each cycle
  * (target 0), or (r_k - A V r_k, x* - x_k - V r_k) (target 1, for method 3).
- * Pairs fill a device pool of `pool` slots; after each right-hand side,
+ * target | 2 takes the pairs along MG-preconditioned CG iterates instead of
+ * plain V-cycles.  Pairs fill a device pool of `pool` slots; after each right-hand side,
  * steps_per_rhs Adam steps (learning rate lr) on random pool slots.  The
  * network's output scale is set from the first right-hand side's pairs.
  * loss_hist (may be NULL) receives up to hist_cap per-step losses. */

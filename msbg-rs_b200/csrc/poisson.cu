@@ -788,7 +788,7 @@ struct TrainStats {
 };
 
 static TrainStats train(msbg_poisson* P, int n_rhs, int mg_iters, int steps_per_rhs, int pool, float lr, int target,
-                        uint64_t seed, double* loss_hist, int64_t hist_cap) {
+                        uint64_t seed, double* loss_hist, int64_t hist_cap, int source = 0) {
     MSBG_REQUIRE(P->net, "learned preconditioner not set");
     PLevelDev& F = P->lv[0];
     const int64_t n = F.cells();
@@ -816,8 +816,19 @@ static TrainStats train(msbg_poisson* P, int n_rhs, int mg_iters, int steps_per_
         double* x64 = (double*)((float*)P->work.p + 4 * n);
         CUDA_CHECK(cudaMemcpyAsync(xs.p, x64, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
         CUDA_CHECK(cudaMemsetAsync(xk.p, 0, n * 8, ctx->stream));
-        for (int k = 0; k < mg_iters; ++k) {
+        // source 1: the iterates of MG-preconditioned CG (residuals as CG sees
+        // them; r is updated recursively, p and q live in the pool's scratch)
+        float* pv = t;
+        float* qv = t + n;
+        double rz = 0.0;
+        if (source == 1) {
             launch_residual64(P, xk.as<double>(), b, r);
+            vcycle(P, 0, z, r, true);
+            CUDA_CHECK(cudaMemcpyAsync(pv, z, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+            rz = dot(P, r, z, n);
+        }
+        for (int k = 0; k < mg_iters; ++k) {
+            if (source == 0) launch_residual64(P, xk.as<double>(), b, r);
             float* pr = pairs.as<float>() + (size_t)next * 2 * n;
             float* pe = pr + n;
             begin_launch(ctx);
@@ -837,7 +848,21 @@ static TrainStats train(msbg_poisson* P, int n_rhs, int mg_iters, int steps_per_
                     scale_cnt++;
                 }
             }
-            add64(P, n, 1.0, z, xk.as<double>());
+            if (source == 0) {
+                add64(P, n, 1.0, z, xk.as<double>());
+            } else {
+                launch_matvec(P, 0, pv, qv);
+                const double pq = dot(P, pv, qv, n);
+                if (pq > 0.0 && rz > 0.0) {
+                    const double alpha = rz / pq;
+                    add64(P, n, alpha, pv, xk.as<double>());
+                    axpby(P, n, -alpha, qv, 1.0, r);
+                    vcycle(P, 0, z, r, true);
+                    const double rz2 = dot(P, r, z, n);
+                    axpby(P, n, 1.0, z, rz2 / rz, pv);
+                    rz = rz2;
+                }
+            }
             next = (next + 1) % pool;
             filled = std::min<int64_t>(filled + 1, pool);
             st.pairs++;
@@ -1350,10 +1375,13 @@ int msbg_poisson_train_preconditioner(msbg_poisson* P, int n_rhs, int mg_iters, 
                                       int target, uint64_t seed, double* loss_hist, int64_t hist_cap, int64_t* steps_out) {
     MSBG_API_BEGIN
     MSBG_REQUIRE(P && n_rhs >= 0 && mg_iters > 0 && steps_per_rhs >= 0 && pool > 0 && lr >= 0.0f &&
-                     (target == 0 || target == 1),
+                     (target & 1) == target % 2 && target >= 0 && target <= 3,
                  "bad argument");
     set_device(P->ctx);
-    const TrainStats st = train(P, n_rhs, mg_iters, steps_per_rhs, pool, lr, target, seed, loss_hist, hist_cap);
+    // target bit 0: pair kind (0 residual/error, 1 post-V-cycle); bit 1: the
+    // iterates of MG-preconditioned CG instead of plain V-cycles
+    const TrainStats st = train(P, n_rhs, mg_iters, steps_per_rhs, pool, lr, target & 1, seed, loss_hist, hist_cap,
+                                target >> 1);
     if (steps_out) *steps_out = st.steps;
     MSBG_API_END
 }
