@@ -72,3 +72,25 @@ def test_second_solve_reuses_graph(problems, solved):
         B.set_rhs(p, rng.uniform(-1, 1, b.size).astype(np.float32))
     its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=8, max_cycles=40)
     assert np.all(rel <= 1e-8) and cyc > 0
+
+
+def test_single_problem_and_single_block(msbg, ctx, oracle):
+    """A batch of one problem, and a problem of one block next to a larger one."""
+    rng = np.random.default_rng(21)
+    probs = [((32, 32, 32), 8, np.array([13], np.uint64)), ((64, 64, 64), 16, np.array([0, 1, 2, 5, 6], np.uint64))]
+    for subset in ([probs[0]], probs):
+        B = msbg.Batch(ctx, subset, tune=False)
+        rhs = []
+        for p, (dims, bs, act) in enumerate(subset):
+            b = rng.uniform(-1, 1, len(act) * bs ** 3).astype(np.float32)
+            rhs.append(b)
+            B.set_rhs(p, b)
+        its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=4, max_cycles=50)
+        assert np.all(rel <= 1e-8)
+        for p, (dims, bs, act) in enumerate(subset):
+            n = dims[0] // bs
+            x = B.solution(p)
+            ax = oracle.poisson_matvec(act.astype(np.int64), n, n, n, bs, x)
+            bb = rhs[p].astype(np.float64)
+            assert np.linalg.norm(bb - ax) / np.linalg.norm(bb) <= 2e-8
+        B.close()

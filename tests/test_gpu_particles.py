@@ -130,6 +130,8 @@ def check_p2g(msbg, ctx, oracle, pos, vel, mass, s, bsx, r_p):
 @pytest.mark.parametrize("n,s,bsx,r_p,seed", [
     (1, 32, 16, 2.0, 1), (500, 32, 16, 2.0, 2), (20000, 64, 16, 2.0, 3), (20000, 64, 16, 1.5, 4),
     (8000, 48, 8, 2.0, 5), (5000, 64, 16, 3.0, 6),
+    # r_p <= 1 (8 tile phases) and r_p 3 on 8^3 blocks (64 phases, one warp per CTA)
+    (3000, 32, 16, 1.0, 7), (4000, 32, 8, 3.0, 8),
 ])
 def test_p2g_matches_oracle(msbg, ctx, oracle, n, s, bsx, r_p, seed):
     pos, vel, mass = make_particles(n, s, seed)

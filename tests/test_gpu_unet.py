@@ -89,3 +89,23 @@ def test_training_reduces_loss_and_keeps_padding(msbg, ctx):
         w = p[o:ob].reshape(27, co, ci)
         assert not np.any(w[:, cor:, :]) and not np.any(w[:, :, cir:])
         assert not np.any(p[ob + cor:ob + co])
+
+
+@pytest.mark.parametrize("n_axis,n_active", [(1, 1), (2, 3)])
+def test_tiny_networks_match_oracle(msbg, ctx, n_axis, n_active):
+    """One and three blocks: every level's last tensor-core tile is partial
+    (a single 16^3 block has 64 level-2 cells, half a 128-cell tile)."""
+    import torch
+    unet, net, act, nbr, rng = setup(msbg, ctx, seed=11 + n_active, n_axis=n_axis, n_active=n_active)
+    net.set_output_scale(0.5)
+    r = rng.standard_normal(net.n).astype(np.float32)
+    e = rng.standard_normal(net.n).astype(np.float32)
+    d_r, d_e = torch.from_numpy(r).cuda(), torch.from_numpy(e).cuda()
+    y = torch.empty(net.n, device="cuda")
+    net.forward_raw(d_r, y)
+    o = unet.UNet(nbr, net.params(), out_scale=0.5)
+    assert rel(y.cpu().numpy(), o.forward(r)) < 1e-2
+    net.train_step(d_r, d_e, lr=0.0, update=False)
+    g = net.grads()
+    _, go = o.grads(r, e)
+    assert rel(g, go) < 5e-2
