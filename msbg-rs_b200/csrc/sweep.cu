@@ -228,7 +228,9 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
 // General staging (blocks at the domain edge): resolve every staged
 // coordinate with the Neumann rule (solver.rs:205-209).  ok/dd/ll are shared
 // scratch arrays [3][HSX].
-template <class E, int BSX, int ST>
+template <int BSX> struct Compact;
+
+template <class E, int BSX, int ST, bool COMPACT = false>
 __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const int32_t* nb, int pi, int8_t* ok, int8_t* dd,
                               int8_t* ll) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
@@ -283,7 +285,8 @@ __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const i
                     v = a.coarse[(size_t)cs * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((lz >> 1) << (2 * CLG)))];
                 }
             }
-            h[(hz * HSX + hy) * RS + X0 + hx] = v;
+            if (COMPACT) h[Compact<BSX>::index(hx, hy, hz)] = v;
+            else h[(hz * HSX + hy) * RS + X0 + hx] = v;
         }
     }
 }
@@ -632,6 +635,270 @@ sweep_pipe_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     cp_async_wait<0>();
 }
 
+// ---- compact staging layout (one-cell halos) -------------------------------
+// Rows of BSX floats for the block and its y/z halo, [hz][hy][x] with hy, hz in
+// 0..BSX+1 (halo coordinates) and x in 0..BSX-1; the x = -1 and x = BSX halo
+// columns apart, [hz][4 + hy - 1] at a row pitch of XP floats, so that the
+// BSX y-values of one z sit 16-byte aligned.  Two buffers of this size let
+// 4 CTAs share an SM (the padded layout allows 3).
+template <int BSX> struct Compact {
+    static constexpr int H = BSX + 2;
+    static constexpr int MAIN = H * H * BSX;  // floats
+    static constexpr int XP = ((BSX + 2 + 3 + 3) / 4) * 4;  // x-halo row pitch: columns 3 .. BSX+4
+    static constexpr int XS = H * XP;
+    static constexpr int BUF = MAIN + 2 * XS;
+    __device__ __forceinline__ static int index(int hx, int hy, int hz) {
+        if (hx == 0) return MAIN + hz * XP + 3 + hy;
+        if (hx == BSX + 1) return MAIN + XS + hz * XP + 3 + hy;
+        return (hz * H + hy) * BSX + hx - 1;
+    }
+};
+
+// Issues the staging of an interior block (one-cell halo) in the compact layout.
+template <int BSX, int ST>
+__device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
+    using CL = Compact<BSX>;
+    constexpr int H = CL::H;
+    constexpr int LG = Lg<BSX>::v;
+    constexpr int N = BSX * BSX * BSX;
+    constexpr int QR = BSX / 4;
+    constexpr int NT = BSX * BSX;
+    const float* payload = (const float*)a.payload;
+    const int tid = threadIdx.x;
+    const int c13 = nb[13];
+    // centre rows
+#pragma unroll
+    for (int k = 0; k < N / 4 / NT; ++k) {
+        const int it = tid + k * NT;
+        const int q = it % QR, r = it / QR, y = r & (BSX - 1), z = r >> LG;
+        cp_async16(h + ((z + 1) * H + y + 1) * BSX + 4 * q, payload + (size_t)c13 * N + 4 * it);
+    }
+    // y and z face rows (and the four x-edge rows of the 19-tap stencil)
+    constexpr int NFACE = 4 * BSX * QR;
+    constexpr int NEDGE = ST == MSBG_LAPLACIAN ? 0 : 4 * QR;
+    for (int it = tid; it < NFACE + NEDGE; it += NT) {
+        int c, dst, srcoff, ly, lz;
+        if (it < NFACE) {
+            const int q = it % QR, rr = it / QR, row = rr % BSX, pd = rr / BSX;  // pd: y-, y+, z-, z+
+            const int side = (pd & 1) ? 1 : -1, l = side < 0 ? BSX - 1 : 0, hh = side < 0 ? 0 : H - 1;
+            if (pd < 2) {
+                c = nb[13 + 3 * side];
+                ly = l;
+                lz = row;
+                dst = ((row + 1) * H + hh) * BSX + 4 * q;
+            } else {
+                c = nb[13 + 9 * side];
+                ly = row;
+                lz = l;
+                dst = (hh * H + row + 1) * BSX + 4 * q;
+            }
+            srcoff = (ly << LG) + (lz << (2 * LG)) + 4 * q;
+        } else {
+            const int e = it - NFACE, q = e % QR, corner = e / QR;
+            const int sy = (corner & 1) ? 1 : -1, sz = (corner & 2) ? 1 : -1;
+            ly = sy < 0 ? BSX - 1 : 0;
+            lz = sz < 0 ? BSX - 1 : 0;
+            c = nb[13 + 3 * sy + 9 * sz];
+            dst = ((sz < 0 ? 0 : H - 1) * H + (sy < 0 ? 0 : H - 1)) * BSX + 4 * q;
+            srcoff = (ly << LG) + (lz << (2 * LG)) + 4 * q;
+        }
+        if (c >= 0) {
+            cp_async16(h + dst, payload + (size_t)c * N + srcoff);
+        } else if (c <= kCodeCoarse0) {
+            constexpr int CLG = LG - 1;
+            const int lx = srcoff & (BSX - 1);
+            const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((ly >> 1) << CLG) + ((lz >> 1) << (2 * CLG));
+            *reinterpret_cast<float4*>(h + dst) = make_float4(cp[lx >> 1], cp[(lx + 1) >> 1], cp[(lx + 2) >> 1], cp[(lx + 3) >> 1]);
+        } else {
+            const float f = c == kCodeFull ? a.full : a.empty;
+            *reinterpret_cast<float4*>(h + dst) = make_float4(f, f, f, f);
+        }
+    }
+    // x-halo planes: BSX rows of BSX y-values per side, 16-byte copies from the
+    // side buffer (x = BSX-1 plane of the -x neighbour, x = 0 plane of the +x one)
+    constexpr int NXR = 2 * BSX * QR;
+    for (int it = tid; it < NXR; it += NT) {
+        const int q = it % QR, z = (it / QR) % BSX, side = it / (QR * BSX);  // side 0: x = -1, 1: x = BSX
+        const int c = nb[13 + (side ? 1 : -1)];
+        float* d = h + CL::MAIN + side * CL::XS + (z + 1) * CL::XP + 4 + 4 * q;
+        if (c >= 0) {
+            cp_async16(d, a.xface + ((size_t)c * 2 + (side ? 0 : 1)) * (BSX * BSX) + z * BSX + 4 * q);
+        } else if (c <= kCodeCoarse0) {
+            constexpr int CLG = LG - 1;
+            const int lx = side ? 0 : BSX - 1;
+            const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((lx >> 1) | ((z >> 1) << (2 * CLG)));
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = cp[((4 * q + j) >> 1) << CLG];
+            *reinterpret_cast<float4*>(d) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+            const float f = c == kCodeFull ? a.full : a.empty;
+            *reinterpret_cast<float4*>(d) = make_float4(f, f, f, f);
+        }
+    }
+    if (ST != MSBG_LAPLACIAN) {
+        // x-halo edges: along y at z = -1 / BSX (rows of the diagonal
+        // neighbours' x-planes) and along z at y = -1 / BSX (strided)
+        for (int it = tid; it < 4 * QR + 4 * BSX; it += NT) {
+            if (it < 4 * QR) {
+                const int q = it % QR, kind = it / QR;  // kind: x side (bit 0), z side (bit 1)
+                const int sx = (kind & 1) ? 1 : -1, sz = (kind & 2) ? 1 : -1;
+                const int c = nb[13 + sx + 9 * sz];
+                const int lz = sz < 0 ? BSX - 1 : 0, hz = sz < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
+                float* d = h + CL::MAIN + side * CL::XS + hz * CL::XP + 4 + 4 * q;
+                if (c >= 0) {
+                    cp_async16(d, a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + lz * BSX + 4 * q);
+                } else if (c <= kCodeCoarse0) {
+                    constexpr int CLG = LG - 1;
+                    const int lx = sx < 0 ? BSX - 1 : 0;
+                    const float* cp = a.coarse + (size_t)(kCodeCoarse0 - c) * (N / 8) + ((lx >> 1) | ((lz >> 1) << (2 * CLG)));
+                    float v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) v[j] = cp[((4 * q + j) >> 1) << CLG];
+                    *reinterpret_cast<float4*>(d) = make_float4(v[0], v[1], v[2], v[3]);
+                } else {
+                    const float f = c == kCodeFull ? a.full : a.empty;
+                    *reinterpret_cast<float4*>(d) = make_float4(f, f, f, f);
+                }
+            } else {
+                const int e = it - 4 * QR, j = e % BSX, kind = e / BSX;  // x side (bit 0), y side (bit 1)
+                const int sx = (kind & 1) ? 1 : -1, sy = (kind & 2) ? 1 : -1;
+                const int c = nb[13 + sx + 3 * sy];
+                const int ly = sy < 0 ? BSX - 1 : 0, hy = sy < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
+                float* d = h + CL::MAIN + side * CL::XS + (j + 1) * CL::XP + 3 + hy;
+                if (c >= 0) {
+                    cp_async4(d, a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly);
+                } else if (c <= kCodeCoarse0) {
+                    constexpr int CLG = LG - 1;
+                    const int lx = sx < 0 ? BSX - 1 : 0;
+                    *d = a.coarse[(size_t)(kCodeCoarse0 - c) * (N / 8) + ((lx >> 1) | ((ly >> 1) << CLG) | ((j >> 1) << (2 * CLG)))];
+                } else {
+                    *d = c == kCodeFull ? a.full : a.empty;
+                }
+            }
+        }
+    }
+}
+
+// The stencil over a block staged in the compact layout (thread (x, y) walks
+// its z-column).  x-1 and x+1 come through per-thread accessors: from the
+// block rows, or from the x-halo columns for x = 0 and x = BSX-1.
+template <int BSX, int ST, bool CLAMP>
+__device__ __forceinline__ void compute_compact(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+    using CL = Compact<BSX>;
+    constexpr int H = CL::H;
+    constexpr int RS = BSX, PL = H * BSX;
+    constexpr int N = BSX * BSX * BSX;
+    float* payload = (float*)a.payload;
+    const int x = tid % BSX, y = tid / BSX;
+    float* out = payload + (size_t)slot * N + x + y * BSX;
+    float* xo = (x == 0 || x == BSX - 1) ? a.xface + ((size_t)slot * 2 + (x == 0 ? 0 : 1)) * (BSX * BSX) + y : nullptr;
+    const int i0 = (1 * H + (y + 1)) * BSX + x;  // z = 0
+    // left / right neighbour accessors: value at (x -+ 1, y + dy, z + dz) = p[(z + dz) * sz + dy * sy]
+    const float* lp = x > 0 ? h + i0 - 1 : h + CL::MAIN + 1 * CL::XP + 3 + (y + 1);
+    const float* rp = x < BSX - 1 ? h + i0 + 1 : h + CL::MAIN + CL::XS + 1 * CL::XP + 3 + (y + 1);
+    const int lsz = x > 0 ? PL : CL::XP, lsy = x > 0 ? RS : 1;
+    const int rsz = x < BSX - 1 ? PL : CL::XP, rsy = x < BSX - 1 ? RS : 1;
+    const float dt = a.dt;
+    if (ST == MSBG_LAPLACIAN) {
+        float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
+#pragma unroll 4
+        for (int z = 0; z < BSX; ++z) {
+            const int i = i0 + z * PL;
+            const float lx = lp[z * lsz], rx = rp[z * rsz], dyu = h[i - RS], dyd = h[i + RS];
+            float nbs = lx + rx;
+            nbs = nbs + dyu;
+            nbs = nbs + dyd;
+            nbs = nbs + zb;
+            nbs = nbs + zf;
+            const float lap = fmaf(c, -6.0f, nbs);
+            const float fx = (rx - lx) * 0.5f, fy = (dyd - dyu) * 0.5f, fz = (zf - zb) * 0.5f;
+            const float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
+            float nv = fmaf(dt * lap, g, c);
+            if (CLAMP) nv = clampf(nv, 0.0f, 1.0f);
+            out[z * BSX * BSX] = nv;
+            if (xo) xo[z * BSX] = nv;
+            zb = c;
+            c = zf;
+            if (z + 1 < BSX) zf = h[i + 2 * PL];
+        }
+    } else {
+        // plane z-1: cross (c, x-, x+, y-, y+); plane z: 3x3; plane z+1: cross
+        float pc = h[i0 - PL], pxm = lp[-lsz], pxp = rp[-rsz], pym = h[i0 - PL - RS], pyp = h[i0 - PL + RS];
+        float c = h[i0], cxm = lp[0], cxp = rp[0], cym = h[i0 - RS], cyp = h[i0 + RS];
+        float nc = h[i0 + PL], nxm = lp[lsz], nxp = rp[rsz], nym = h[i0 + PL - RS], nyp = h[i0 + PL + RS];
+#pragma unroll 2
+        for (int z = 0; z < BSX; ++z) {
+            const int i = i0 + z * PL;
+            const float xpyp = rp[z * rsz + rsy], xpym = rp[z * rsz - rsy], xmyp = lp[z * lsz + lsy], xmym = lp[z * lsz - lsy];
+            // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
+            const float f0 = c, f1 = cxm, f2 = cxp, f3 = cym, f4 = cyp, f5 = pc, f6 = nc;
+            const float fx = (f2 - f1) * 0.5f, fy = (f4 - f3) * 0.5f, fz = (f6 - f5) * 0.5f;
+            const float fxx = (f1 + f2) - 2.0f * f0, fyy = (f3 + f4) - 2.0f * f0, fzz = (f5 + f6) - 2.0f * f0;
+            const float d1 = xpyp, d2 = xpym, d3 = xmyp, d4 = xmym;
+            const float d5 = nxp, d6 = pxp, d7 = nxm, d8 = pxm;
+            const float d9 = nyp, d10 = pyp, d11 = nym, d12 = pym;
+            const float fyx = (((d1 - d2) - d3) + d4) * 0.25f;
+            const float fzx = (((d5 - d6) - d7) + d8) * 0.25f;
+            const float fzy = (((d9 - d10) - d11) + d12) * 0.25f;
+            const float cross = (fx * (fy * fyx) + fx * (fz * fzx)) + fy * (fz * fzy);
+            const float hnum = fmaf(fy * fy + fz * fz, fxx, fmaf(fx * fx + fz * fz, fyy, fmaf(fx * fx + fy * fy, fzz, -2.0f * cross)));
+            const float grad = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+            const float hc = grad > 1e-7f ? hnum / grad : 0.0f;
+            const float d = clampf(dt * hc, -0.1f, 0.1f);
+            float nv = f0 + d;
+            if (CLAMP) nv = clampf(nv, 0.0f, 1.0f);
+            out[z * BSX * BSX] = nv;
+            if (xo) xo[z * BSX] = nv;
+            pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
+            c = nc; cxm = nxm; cxp = nxp; cym = nym; cyp = nyp;
+            if (z + 1 < BSX) {
+                const int j = i + 2 * PL;
+                nc = h[j]; nxm = lp[(z + 2) * lsz]; nxp = rp[(z + 2) * rsz]; nym = h[j - RS]; nyp = h[j + RS];
+            }
+        }
+    }
+}
+
+template <int BSX, int ST, bool CLAMP>
+__global__ void __launch_bounds__(BSX * BSX, BSX == 16 ? 4 : 1)
+sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
+    using CL = Compact<BSX>;
+    extern __shared__ float4 h4[];
+    float* hb = reinterpret_cast<float*>(h4);
+    __shared__ int32_t nbs[2][27];
+    __shared__ int32_t flg[2], pis[2];
+    __shared__ int8_t ok[3][BSX + 2], dd[3][BSX + 2], ll[3][BSX + 2];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    int t = blockIdx.x;
+    if (t >= n) return;
+    auto meta = [&](int tt, int b) {
+        const int pi = order[tt];
+        if (tid < 27) nbs[b][tid] = a.nbr[(size_t)pi * 27 + tid];
+        if (tid == nthr - 1) {
+            flg[b] = a.bxyz[(size_t)pi * 4 + 3];
+            pis[b] = pi;
+        }
+    };
+    meta(t, 0);
+    __syncthreads();
+    if (flg[0] & 1) issue_compact<BSX, ST>(a, hb, nbs[0]);
+    cp_async_commit();
+    for (int j = 0; t < n; t += gridDim.x, ++j) {
+        const int b = j & 1, bn = b ^ 1;
+        const int tn = t + gridDim.x;
+        if (tn < n) meta(tn, bn);
+        __syncthreads();  // nbs[bn] visible; every thread is done with buffer bn (the previous block)
+        if (tn < n && (flg[bn] & 1)) issue_compact<BSX, ST>(a, hb + bn * CL::BUF, nbs[bn]);
+        cp_async_commit();
+        if (flg[b] & 1) cp_async_wait<1>();  // this block's copies have landed
+        else stage_general<ElemF32, BSX, ST, true>(a, hb + b * CL::BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
+        __syncthreads();
+        compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+    }
+    cp_async_wait<0>();
+}
+
 // Copies the x-planes (x = 0 and x = bsx-1) of the listed slots into the side
 // buffer: [slot][plane][z][y].
 template <class E, int BSX>
@@ -666,6 +933,27 @@ static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_
     }
 }
 
+template <int BSX, int ST, bool CLAMP>
+static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
+    const size_t smem = 2 * sizeof(float) * Compact<BSX>::BUF;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+        attr = true;
+    }
+    const int threads = BSX * BSX;
+    int per_sm = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_compact_kernel<BSX, ST, CLAMP>, threads, smem));
+    int sms = 0;
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const int grid = std::max(1, std::min(n, std::max(per_sm, 1) * sms));
+    begin_launch(ctx);
+    sweep_compact_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
+    after_launch(ctx, "sweep_phase_kernel");
+}
+
 template <class E, int BSX, int ST>
 static void launch_phase(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
@@ -681,8 +969,13 @@ static void launch_phase(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order
         attr_set = true;
     }
     const int threads = BSX * BSX < 32 ? 32 : BSX * BSX;
-    // the double-buffered kernel for f32 and one-cell halos (two 25-tap
-    // buffers would leave too few CTAs per SM)
+    // f32 with one-cell halos: the double-buffered kernel in the compact
+    // layout (two 25-tap buffers would leave too few CTAs per SM)
+    if (std::is_same<E, ElemF32>::value && BSX >= 8 && ST != MSBG_BILAPLACIAN && a.xface) {
+        if (a.clamp01) launch_compact<BSX, ST, true>(ctx, a, order, n);
+        else launch_compact<BSX, ST, false>(ctx, a, order, n);
+        return;
+    }
     if (std::is_same<E, ElemF32>::value && BSX >= 8 && ST != MSBG_BILAPLACIAN) {
         static bool pattr = false;
         if (!pattr) {
