@@ -370,7 +370,7 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
     y, z, velocity component, mass, packed footprint; one launch per
     direction); 24 B written per face-cell of the active blocks for the
     combine; 12 B read + 12 B written per particle for G2P; 24 B per element
-    per radix pass (3 passes per sort)."""
+    per onesweep radix pass (3 passes per sort)."""
     if kernel == "sweep_phase_kernel":
         return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
@@ -379,7 +379,7 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
         return 24.0 * n_active * 4096 * launches
     if kernel == "g2p_kernel":
         return 24.0 * n * launches
-    if kernel == "rs_scatter_kernel":
+    if kernel == "os_pass_kernel":
         return 24.0 * n * launches
     if kernel == "permute_kernel":
         return 28.0 * n * launches

@@ -126,6 +126,13 @@ struct ScratchLayout {
 // stream first, so kernels still in flight never see their scratch freed.
 char* scratch(msbg_ctx* ctx, const ScratchLayout& L);
 
+// The device status word collects bits from bounded waits that gave up: 1 =
+// an mbarrier wait in a tensor-core kernel, 2 = a radix-sort look-back.
+// raise_device_status(ctx, word) clears the word and throws when it is
+// non-zero; check_device_status reads it (synchronising) and does the same.
+void raise_device_status(msbg_ctx* ctx, int word);
+void check_device_status(msbg_ctx* ctx);
+
 inline int ilog2i(uint64_t v) { int l = 0; while ((uint64_t(1) << l) < v) ++l; return l; }
 inline bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
 inline unsigned div_up(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }

@@ -324,16 +324,6 @@ void conv3_wgrad(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uin
     MSBG_THROW(MSBG_ERR_ARG, "conv3: channel counts must be 16, 32 or 64");
 }
 
-void check_device_status(msbg_ctx* ctx) {
-    int h = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&h, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
-    if (h) {
-        CUDA_CHECK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->stream));
-        MSBG_THROW(MSBG_ERR_TIMEOUT, "a bounded wait inside a tensor-core kernel gave up");
-    }
-}
-
 }  // namespace msbg
 
 using namespace msbg;

@@ -48,6 +48,5 @@ void conv3_wgrad(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uin
 
 // Device status word check after a synchronisation: throws MSBG_ERR_TIMEOUT
 // when a bounded wait inside a kernel gave up.
-void check_device_status(msbg_ctx* ctx);
 
 }  // namespace msbg

@@ -9,6 +9,22 @@ namespace msbg {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+void raise_device_status(msbg_ctx* ctx, int word) {
+    if (!word) return;
+    CUDA_CHECK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->stream));
+    std::string what;
+    if (word & 1) what += "an mbarrier wait inside a tensor-core kernel";
+    if (word & 2) what += std::string(what.empty() ? "" : " and ") + "a radix-sort look-back";
+    MSBG_THROW(MSBG_ERR_TIMEOUT, what + " waited more than a second and gave up");
+}
+
+void check_device_status(msbg_ctx* ctx) {
+    int h = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&h, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    raise_device_status(ctx, h);
+}
+
 char* scratch(msbg_ctx* ctx, const ScratchLayout& L) {
     if (L.size > ctx->scratch.bytes) {
         // Grow preserving contents: a multi-phase pipeline extends its layout

@@ -467,9 +467,11 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
                                                             (int64_t)u->nz, px, py, pz, pm, v0, v1, v2, fmask, fpk, bad);
     after_launch(ctx, "p2g_gather_kernel");
     const size_t npb = sorted_segments(ctx, skeys, n, (uint64_t)(3 * lg), pb_key, pb_starts, ScratchLayout::at<char>(base, o_tmp));
-    int hbad = 0;
+    int hbad = 0, hstatus = 0;
     CUDA_CHECK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);
+    raise_device_status(ctx, hstatus);
     MSBG_REQUIRE(!hbad, "a particle lies outside the domain");
 
     // ---- phase 2: active set ------------------------------------------------
@@ -504,7 +506,9 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     size_t nuniq = sorted_segments(ctx, csort, npb * 27, 0, act, ast, ScratchLayout::at<char>(base, o_ctmp));
     std::vector<uint64_t> active(nuniq);
     CUDA_CHECK(cudaMemcpyAsync(active.data(), act, nuniq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);
+    raise_device_status(ctx, hstatus);
     if (!active.empty() && active.back() == u->n_blocks) active.pop_back();  // the "none" sentinel
     const size_t na = active.size();
     std::vector<int32_t> slots(na);

@@ -1,22 +1,23 @@
-// sort.cu -- stable LSD radix sort (8-bit digits, reduce-then-scan), device
-// scans, per-particle Morton keys (multires/sort.rs:5-22), bucket_indices
+// sort.cu -- stable onesweep LSD radix sort (8-bit digits), device scans,
+// per-particle Morton keys (multires/sort.rs:5-22), bucket_indices
 // (particles/sort.rs:174-269) and sort_block_list_morton (multires/sort.rs:35-57).
 //
-// Each pass: (1) per-tile digit histograms, (2) a digit-major exclusive scan of
-// those histograms, (3) a scatter in which every tile ranks its keys stably
-// (warp __match_any_sync + a running per-digit prefix across the tile's rounds)
-// and writes them to digit base + tile prefix + rank.  Stable, so sorting
-// (key, index) pairs reproduces a stable CPU sort exactly.
+// The sort reads the keys once to histogram every digit at the same time
+// (os_hist_kernel), then runs one kernel per digit (os_pass_kernel).  In a
+// pass, each CTA takes the next tile id from a counter (so every lower tile
+// belongs to a CTA that is already running), ranks its tile's keys stably in
+// shared memory, publishes the tile's per-digit counts, and finds the counts
+// of all lower tiles by decoupled look-back over a status array of 64-bit
+// words (flag and count in one word, so a reader never sees one without the
+// other).  The keys then leave shared memory in digit order, so each digit's
+// run is written contiguously.  Stable, so sorting (key, index) pairs
+// reproduces a stable CPU sort exactly.
 #include <algorithm>
 #include <mutex>
 
 #include "sort.cuh"
 
 namespace msbg {
-
-constexpr int RS_THREADS = 256;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -53,21 +54,6 @@ __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
     return warp_ex + x - v;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) rs_hist_kernel(const uint64_t* keys, size_t n, int shift, uint32_t* counts,
-                                                              unsigned n_tiles) {
-    __shared__ uint32_t c[256];
-    c[threadIdx.x] = 0;
-    __syncthreads();
-    const size_t base = (size_t)blockIdx.x * RS_TILE;
-#pragma unroll
-    for (int j = 0; j < RS_ITEMS; ++j) {
-        size_t i = base + (size_t)j * RS_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&c[(keys[i] >> shift) & 255], 1u);
-    }
-    __syncthreads();
-    counts[(size_t)threadIdx.x * n_tiles + blockIdx.x] = c[threadIdx.x];
-}
-
 // One CTA per row: exclusive scan of the row in place, row total to totals.
 __global__ void __launch_bounds__(1024) scan_rows_kernel(uint32_t* data, size_t row_len, uint32_t* totals) {
     uint32_t* row = data + (size_t)blockIdx.x * row_len;
@@ -82,46 +68,224 @@ __global__ void __launch_bounds__(1024) scan_rows_kernel(uint32_t* data, size_t 
     if (threadIdx.x == 0 && totals) totals[blockIdx.x] = carry;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                                                 uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, size_t n,
-                                                                 int shift, const uint32_t* __restrict__ counts,
-                                                                 const uint32_t* __restrict__ totals, unsigned n_tiles) {
-    __shared__ uint32_t base_d[256];
-    __shared__ uint32_t wcnt[RS_THREADS / 32][256];
-    __shared__ uint32_t run[256];
-    const int tid = threadIdx.x, warp = tid >> 5;
-    uint32_t tot;
-    uint32_t ex = block_exclusive_scan(totals[tid], &tot);
-    base_d[tid] = ex + counts[(size_t)tid * n_tiles + blockIdx.x];
-    run[tid] = 0;
-    const size_t base = (size_t)blockIdx.x * RS_TILE;
-    for (int j = 0; j < RS_ITEMS; ++j) {
-        const size_t i = base + (size_t)j * RS_THREADS + tid;
-        const bool valid = i < n;
-        const uint64_t key = valid ? kin[i] : 0;
-        const uint32_t d = valid ? (uint32_t)((key >> shift) & 255) : 256u;
+constexpr int OS_THREADS = 256;
+constexpr int OS_ITEMS = 8;  // even, and 32 * OS_ITEMS < 65536
+constexpr int OS_TILE = OS_THREADS * OS_ITEMS;
+constexpr int OS_WARPS = OS_THREADS / 32;
+constexpr int OS_MAX_PASSES = 8;
+constexpr int OH_ITEMS = 8;
+constexpr int OS_LOOKBACK = 8;  // predecessor tiles read per look-back round
+constexpr uint64_t OS_AGGREGATE = 1ull << 32;  // word holds this tile's own count
+constexpr uint64_t OS_INCLUSIVE = 2ull << 32;  // word holds the count of tiles 0..k
+constexpr size_t OS_PASS_SMEM = (size_t)OS_TILE * (8 + 4);
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t os_globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Histogram of every digit of every key, and zeroing of the first pass's
+// status array.  Each thread takes OH_ITEMS consecutive keys and adds runs of
+// equal digits with one shared atomic (keys that are nearly sorted already,
+// such as particles sorted in the previous step, share their high digits).
+__global__ void __launch_bounds__(256) os_hist_kernel(const uint64_t* __restrict__ keys, size_t n, int passes,
+                                                      uint32_t* __restrict__ hist, uint64_t* __restrict__ zero,
+                                                      size_t n_zero) {
+    __shared__ uint32_t h[OS_MAX_PASSES * 256];
+    for (int q = threadIdx.x; q < OS_MAX_PASSES * 256; q += blockDim.x) h[q] = 0;
+    __syncthreads();
+    const size_t chunk = (size_t)blockDim.x * OH_ITEMS;
+    for (size_t b = blockIdx.x * chunk; b < n; b += (size_t)gridDim.x * chunk) {
+        const size_t i0 = b + (size_t)threadIdx.x * OH_ITEMS;
+        const int cnt = i0 >= n ? 0 : (n - i0 < (size_t)OH_ITEMS ? (int)(n - i0) : OH_ITEMS);
+        uint64_t k[OH_ITEMS];
 #pragma unroll
-        for (int w = 0; w < RS_THREADS / 32; ++w) wcnt[w][tid] = 0;
-        __syncthreads();
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t lt = __popc(peers & lanemask_lt());
-        if (valid && lt == 0) wcnt[warp][d] = __popc(peers);
-        __syncthreads();
-        uint32_t acc = run[tid];
+        for (int j = 0; j < OH_ITEMS; ++j) k[j] = j < cnt ? keys[i0 + j] : 0;
+        if (!cnt) continue;
+        for (int p = 0; p < passes; ++p) {
+            const int sh = 8 * p;
+            uint32_t cur = (uint32_t)(k[0] >> sh) & 255u, run = 0;
 #pragma unroll
-        for (int w = 0; w < RS_THREADS / 32; ++w) {
-            uint32_t t = wcnt[w][tid];
-            wcnt[w][tid] = acc;
-            acc += t;
+            for (int j = 0; j < OH_ITEMS; ++j) {
+                if (j < cnt) {
+                    const uint32_t d = (uint32_t)(k[j] >> sh) & 255u;
+                    if (d != cur) {
+                        atomicAdd(&h[p * 256 + cur], run);
+                        cur = d;
+                        run = 0;
+                    }
+                    ++run;
+                }
+            }
+            atomicAdd(&h[p * 256 + cur], run);
         }
-        run[tid] = acc;
-        __syncthreads();
-        if (valid) {
-            const uint32_t pos = base_d[d] + wcnt[warp][d] + lt;
-            kout[pos] = key;
-            vout[pos] = vin ? vin[i] : (uint32_t)i;
+    }
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_zero; i += (size_t)gridDim.x * blockDim.x)
+        zero[i] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < passes * 256; q += blockDim.x)
+        if (h[q]) atomicAdd(&hist[q], h[q]);
+}
+
+// One digit pass.  Tile t holds keys [t*OS_TILE, (t+1)*OS_TILE); warp w of the
+// CTA ranks the tile's w-th run of 32*OS_ITEMS keys, item j of lane l being
+// key w*32*OS_ITEMS + j*32 + l, so (warp, item, lane) order is index order and
+// the local sort is stable.  `status` holds tiles*256 words for this pass
+// (zeroed before the launch); `status_next` (the next pass's array, or null)
+// is zeroed here, tile by tile.  A look-back that waits more than a second
+// sets bit 2 of *err and carries on with what it has (the result is then wrong and
+// the host reports the error), so no CTA can spin forever.
+__global__ void __launch_bounds__(OS_THREADS, 4)
+    os_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+                   uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist,
+                   uint64_t* status, uint64_t* __restrict__ status_next, uint32_t* tile_counter, int* err) {
+    extern __shared__ __align__(16) unsigned char os_smem[];
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(os_smem);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(os_smem + (size_t)OS_TILE * 8);
+    __shared__ uint32_t s_wc[OS_WARPS][256];    // per-warp digit counts, then offsets
+    __shared__ uint32_t s_match[OS_WARPS][256];  // per-warp lane masks of one round
+    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    const uint32_t hist_d = hist[tid];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        s_wc[w][lane + 32 * q] = 0;
+        s_match[w][lane + 32 * q] = 0;
+    }
+    __syncthreads();
+    const size_t tile = s_tile;
+    const size_t tile_base = tile * OS_TILE;
+    const size_t wbase = tile_base + (size_t)w * 32 * OS_ITEMS;
+    const uint32_t lt = lanemask_lt();
+
+    // keys of this warp still inside the array (0 for warps past the end)
+    const int rem = wbase >= n ? 0 : (n - wbase >= (size_t)(32 * OS_ITEMS) ? 32 * OS_ITEMS : (int)(n - wbase));
+    uint64_t key[OS_ITEMS];
+#pragma unroll
+    for (int j = 0; j < OS_ITEMS; ++j) key[j] = j * 32 + lane < rem ? kin[wbase + lane + j * 32] : 0;
+    // warp-level stable ranking, one round per item: every lane ORs its bit
+    // into its digit's mask, so the mask read back holds the lanes with the
+    // same digit; the lowest of them adds the group's size to the warp's
+    // count and clears the mask for the next round
+    uint32_t rank[OS_ITEMS / 2];  // two 16-bit ranks per word (a warp ranks at most 32*OS_ITEMS keys)
+    uint32_t* wc = s_wc[w];
+    uint32_t* wm = s_match[w];
+#pragma unroll
+    for (int j = 0; j < OS_ITEMS; ++j) {
+        const bool valid = j * 32 + lane < rem;
+        const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
+        if (valid) atomicOr(&wm[d], 1u << lane);
+        __syncwarp();
+        const uint32_t peers = valid ? wm[d] : 0u;
+        const uint32_t lower = __popc(peers & lt);
+        const uint32_t c = valid ? wc[d] : 0u;
+        __syncwarp();
+        if (valid && lower == 0) {
+            wc[d] = c + __popc(peers);
+            wm[d] = 0;
         }
-        __syncthreads();
+        __syncwarp();
+        if (j & 1) rank[j >> 1] |= (c + lower) << 16;
+        else rank[j >> 1] = c + lower;
+    }
+    __syncthreads();
+
+    // thread tid owns digit tid: tile count, publish, then each warp's
+    // offset of the digit inside the tile's local sort
+    uint32_t count = 0;
+#pragma unroll
+    for (int q = 0; q < OS_WARPS; ++q) count += s_wc[q][tid];
+    uint64_t* my_status = status + tile * 256 + tid;
+    st_relaxed_u64(my_status, (tile == 0 ? OS_INCLUSIVE : OS_AGGREGATE) | count);
+    if (status_next) status_next[tile * 256 + tid] = 0;
+    uint32_t total;
+    const uint32_t local = block_exclusive_scan(count, &total);
+    const uint32_t global = block_exclusive_scan(hist_d, &total);
+    {
+        uint32_t run = local;
+#pragma unroll
+        for (int q = 0; q < OS_WARPS; ++q) {
+            const uint32_t c = s_wc[q][tid];
+            s_wc[q][tid] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+
+    // local sort into shared memory
+#pragma unroll
+    for (int j = 0; j < OS_ITEMS; ++j) {
+        if (j * 32 + lane < rem) {
+            const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
+            const uint32_t pos = wc[d] + ((rank[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+            s_keys[pos] = key[j];
+            s_vals[pos] = vin ? vin[wbase + lane + j * 32] : (uint32_t)(wbase + lane + j * 32);
+        }
+    }
+
+    // decoupled look-back for digit tid, OS_LOOKBACK predecessors per round:
+    // add aggregates until an inclusive count; stop at a tile that has not
+    // published yet and read again from there
+    uint32_t before = 0;
+    if (tile > 0) {
+        size_t k = tile - 1;  // highest tile not yet added
+        uint64_t t0 = 0;
+        uint32_t spins = 0;
+        while (true) {
+            uint64_t sv[OS_LOOKBACK];
+#pragma unroll
+            for (int q = 0; q < OS_LOOKBACK; ++q)
+                sv[q] = k >= (size_t)q ? ld_relaxed_u64(status + (k - q) * 256 + tid) : OS_INCLUSIVE;
+            int used = 0;
+            bool done = false;
+#pragma unroll
+            for (int q = 0; q < OS_LOOKBACK; ++q) {
+                if (used == q && !done) {
+                    const uint64_t flag = sv[q] & (3ull << 32);
+                    if (flag != 0) {
+                        before += (uint32_t)sv[q];
+                        done = flag == OS_INCLUSIVE;
+                        ++used;
+                    }
+                }
+            }
+            if (done) break;
+            k -= used;
+            if (used < OS_LOOKBACK && (++spins & 15u) == 0) {
+                const uint64_t now = os_globaltimer();
+                if (!t0) t0 = now;
+                else if (now - t0 > 1000000000ull) {
+                    atomicOr(err, 2);
+                    break;
+                }
+            }
+        }
+        st_relaxed_u64(my_status, OS_INCLUSIVE | (before + count));
+    }
+    s_base[tid] = global + before - local;
+    __syncthreads();
+
+    const int in_tile = n - tile_base < (size_t)OS_TILE ? (int)(n - tile_base) : OS_TILE;
+    for (int i = tid; i < in_tile; i += OS_THREADS) {
+        const uint64_t k = s_keys[i];
+        const uint32_t dst = s_base[(uint32_t)(k >> shift) & 255u] + (uint32_t)i;  // modulo 2^32, as s_base is
+        if (dst < n) {  // always true unless a look-back gave up
+            kout[dst] = k;
+            vout[dst] = s_vals[i];
+        }
     }
 }
 
@@ -132,33 +296,46 @@ __global__ void iota_copy_kernel(const uint64_t* kin, const uint32_t* vin, uint6
     }
 }
 
-static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+static constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-size_t radix_sort_scratch_bytes(size_t n) {
-    size_t tiles = (n + RS_TILE - 1) / RS_TILE;
-    return align256(n * 8) + align256(n * 4) + align256(256 * std::max<size_t>(tiles, 1) * 4) + align256(256 * 4);
+// Scratch of the onesweep sort: ping-pong keys and values, the digit
+// histograms with one tile counter per pass, and two status arrays (pass p
+// uses array p % 2 and clears the other for pass p + 1).
+static constexpr size_t onesweep_scratch_bytes(size_t n) {
+    return align256(n * 8) + align256(n * 4) + align256(OS_MAX_PASSES * 256 * 4 + OS_MAX_PASSES * 4) +
+           2 * align256(((n + OS_TILE - 1) / OS_TILE) * 256 * 8);
 }
+
+size_t radix_sort_scratch_bytes(size_t n) { return onesweep_scratch_bytes(n); }
 
 void radix_sort_pairs(msbg_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
                       uint32_t* vals_out, size_t n, int end_bit, void* tmp) {
     if (!n) return;
     MSBG_REQUIRE(n < (1ULL << 32), "radix sort supports < 2^32 items");
+    MSBG_REQUIRE(end_bit >= 0 && end_bit <= 64, "radix sort end_bit out of range");
     const int passes = (end_bit + 7) / 8;
-    const unsigned tiles = (unsigned)((n + RS_TILE - 1) / RS_TILE);
     if (passes == 0) {
         begin_launch(ctx);
         iota_copy_kernel<<<std::min<size_t>(div_up(n, 256), 4096), 256, 0, ctx->stream>>>(keys_in, vals_in, keys_out, vals_out, n);
         after_launch(ctx, "iota_copy_kernel");
         return;
     }
+    const size_t tiles = (n + OS_TILE - 1) / OS_TILE;
     char* t = (char*)tmp;
     uint64_t* kt = (uint64_t*)t;
     t += align256(n * 8);
     uint32_t* vt = (uint32_t*)t;
     t += align256(n * 4);
-    uint32_t* counts = (uint32_t*)t;
-    t += align256(256 * (size_t)tiles * 4);
-    uint32_t* totals = (uint32_t*)t;
+    uint32_t* hist = (uint32_t*)t;
+    uint32_t* counters = hist + OS_MAX_PASSES * 256;
+    t += align256(OS_MAX_PASSES * 256 * 4 + OS_MAX_PASSES * 4);
+    uint64_t* status[2] = {(uint64_t*)t, (uint64_t*)(t + align256(tiles * 256 * 8))};
+    CUDA_CHECK(cudaMemsetAsync(hist, 0, OS_MAX_PASSES * 256 * 4 + OS_MAX_PASSES * 4, ctx->stream));
+    begin_launch(ctx);
+    os_hist_kernel<<<(unsigned)std::min<size_t>(div_up(n, 256 * OH_ITEMS), 148 * 8), 256, 0, ctx->stream>>>(
+        keys_in, n, passes, hist, status[0], tiles * 256);
+    after_launch(ctx, "os_hist_kernel");
+    CUDA_CHECK(cudaFuncSetAttribute(os_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OS_PASS_SMEM));
     const uint64_t* ki = keys_in;
     const uint32_t* vi = vals_in;
     for (int p = 0; p < passes; ++p) {
@@ -166,14 +343,10 @@ void radix_sort_pairs(msbg_ctx* ctx, const uint64_t* keys_in, const uint32_t* va
         uint64_t* ko = to_out ? keys_out : kt;
         uint32_t* vo = to_out ? vals_out : vt;
         begin_launch(ctx);
-        rs_hist_kernel<<<tiles, RS_THREADS, 0, ctx->stream>>>(ki, n, 8 * p, counts, tiles);
-        after_launch(ctx, "rs_hist_kernel");
-        begin_launch(ctx);
-        scan_rows_kernel<<<256, 1024, 0, ctx->stream>>>(counts, tiles, totals);
-        after_launch(ctx, "scan_rows_kernel");
-        begin_launch(ctx);
-        rs_scatter_kernel<<<tiles, RS_THREADS, 0, ctx->stream>>>(ki, vi, ko, vo, n, 8 * p, counts, totals, tiles);
-        after_launch(ctx, "rs_scatter_kernel");
+        os_pass_kernel<<<(unsigned)tiles, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(
+            ki, vi, ko, vo, n, 8 * p, hist + p * 256, status[p & 1], p + 1 < passes ? status[(p + 1) & 1] : nullptr,
+            counters + p, ctx->status.as<int>());
+        after_launch(ctx, "os_pass_kernel");
         ki = ko;
         vi = vo;
     }
@@ -401,8 +574,7 @@ size_t bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n, ui
 constexpr size_t kNoAllocMaxParticles = size_t(1) << 18;
 constexpr size_t a256c(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr size_t kNoAllocKeysBytes = a256c(kNoAllocMaxParticles * 8);
-constexpr size_t kNoAllocSortBytes = a256c(kNoAllocMaxParticles * 8) + a256c(kNoAllocMaxParticles * 4) +
-                                     a256c(256 * ((kNoAllocMaxParticles + RS_TILE - 1) / RS_TILE) * 4) + a256c(256 * 4);
+constexpr size_t kNoAllocSortBytes = onesweep_scratch_bytes(kNoAllocMaxParticles);
 constexpr size_t kNoAllocScratchBytes = kNoAllocKeysBytes + kNoAllocSortBytes + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -482,7 +654,7 @@ int msbg_sort_block_list_morton(msbg_ctx* ctx, uint64_t* blocks, size_t n, uint6
     gather_u64_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(db, dp, dk, n);
     after_launch(ctx, "gather_u64_kernel");
     CUDA_CHECK(cudaMemcpyAsync(blocks, dk, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    check_device_status(ctx);
     MSBG_API_END
 }
 
@@ -491,6 +663,7 @@ int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_
     MSBG_REQUIRE(ctx && ((d_pos && d_keys_out && d_perm_out) || !n), "null argument");
     set_device(ctx);
     morton_sort_device(ctx, d_pos, n, d_keys_out, d_perm_out);
+    check_device_status(ctx);
     MSBG_API_END
 }
 
@@ -524,6 +697,7 @@ int msbg_morton_sort_noalloc_device(msbg_ctx* ctx, const float* d_pos, size_t n,
     morton_keys(ctx, d_pos, n, keys);
     const int bits = key_bits(ctx, keys, n, bits_word);
     radix_sort_pairs(ctx, keys, nullptr, d_keys_out, d_perm_out, n, bits, sort_tmp);
+    check_device_status(ctx);
     MSBG_API_END
 }
 
@@ -541,7 +715,7 @@ int msbg_morton_sort(msbg_ctx* ctx, const float* pos, size_t n, uint64_t* keys_o
     morton_sort_device(ctx, dpos, n, dk, dp);
     CUDA_CHECK(cudaMemcpyAsync(keys_out, dk, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_CHECK(cudaMemcpyAsync(perm_out, dp, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    check_device_status(ctx);
     MSBG_API_END
 }
 
@@ -564,6 +738,7 @@ int msbg_bucket_indices_device(msbg_ctx* ctx, const uint64_t* d_bids, size_t n, 
     MSBG_REQUIRE(ctx && d_starts && n_blocks_out && ((d_bids && d_particle_blocks && d_perm) || !n), "null argument");
     set_device(ctx);
     *n_blocks_out = bucket_indices_device(ctx, d_bids, n, d_particle_blocks, d_starts, d_perm);
+    check_device_status(ctx);
     MSBG_API_END
 }
 
@@ -589,7 +764,7 @@ int msbg_bucket_indices(msbg_ctx* ctx, const uint64_t* bids, size_t n, uint64_t*
     CUDA_CHECK(cudaMemcpyAsync(particle_blocks, dblk, nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_CHECK(cudaMemcpyAsync(starts, dst, (nb + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_CHECK(cudaMemcpyAsync(perm, dp, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    check_device_status(ctx);
     *n_blocks_out = nb;
     MSBG_API_END
 }
