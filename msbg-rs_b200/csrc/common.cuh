@@ -126,8 +126,16 @@ struct ScratchLayout {
 // stream first, so kernels still in flight never see their scratch freed.
 char* scratch(msbg_ctx* ctx, const ScratchLayout& L);
 
+// Nanoseconds of the GPU's global timer (bounded waits measure with it).
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // The device status word collects bits from bounded waits that gave up: 1 =
-// an mbarrier wait in a tensor-core kernel, 2 = a radix-sort look-back.
+// an mbarrier wait in a tensor-core kernel, 2 = a radix-sort look-back, 4 = a
+// P2G tile-order wait.
 // raise_device_status(ctx, word) clears the word and throws when it is
 // non-zero; check_device_status reads it (synchronising) and does the same.
 void raise_device_status(msbg_ctx* ctx, int word);

@@ -38,8 +38,9 @@ struct SplatArgs {
     const int32_t* cell_begin;               // [npb][bsx^3] by local Morton code
     const int32_t* cell_end;
     const uint64_t* pb_key;                  // block Morton key per particle block
-    const uint64_t* fp;                      // packed clipped footprints per particle
+    const uint64_t* lane_mask[3];            // per direction: clipped footprint as lane and face bits
     double* partial;                         // [npb][3][2][W^3]
+    int* status;                             // device status word (bit 4: a tile wait gave up)
     float r_p, inv_r2;
 };
 
@@ -119,16 +120,21 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
 
 // Payload gather into cell-sorted SoA (perm == null: already sorted), each
 // particle's block-footprint mask (particles/mod.rs:207-212 footprint_axis
-// with r_scan = (r_p + 1) / bsx, relative to its own block) and its clipped
-// face footprints in staging coordinates of its block (p2g.rs:263-270): per
-// axis, for the cell-centred offset (0.5) and the face offset (1.0), lo and hi
-// as 5-bit fields of a u64 (bits ((axis*2 + face)*2 + hi)*5).
+// with r_scan = (r_p + 1) / bsx, relative to its own block) and, per face
+// direction, its clipped face footprint (p2g.rs:263-270) relative to its own
+// cell as the splat kernel's lane and face bits: for direction DIR with face
+// axis F and lane axes U, V (U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2),
+// bit du + (2M+1) dv (du, dv in [0, 2M]) is set when the cell-centred
+// footprint (offset 0.5) holds the lane's row, at cell offsets du - M and
+// dv - M along U and V, and bit 56 + s (s in [0, 2M]) when the face
+// footprint (offset 1.0) along F holds cell offset s - 1 - M.
 __global__ void p2g_gather_kernel(const float* pos, const float* vel, const float* mass, const uint32_t* perm, size_t n,
                                   int lg, int M, float r_p, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz,
                                   float* px, float* py, float* pz, float* pm, float* v0, float* v1, float* v2,
-                                  uint32_t* fmask, uint64_t* fp, int* bad) {
+                                  uint32_t* fmask, uint64_t* lane_mask, int* bad) {
     const float bsx = (float)(1 << lg);
     const int32_t B = 1 << lg;
+    const int WIN = 2 * M + 1;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const size_t s = perm ? perm[i] : i;
         const float x = pos[3 * s], y = pos[3 * s + 1], z = pos[3 * s + 2];
@@ -138,10 +144,11 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
         const float p[3] = {x, y, z};
         const int64_t nn[3] = {nx, ny, nz};
         uint32_t lo[3], hi[3];
-        uint64_t f = 0;
+        int32_t a1[3][2], a2[3][2], cell[3];
         bool out = false;
         for (int ax = 0; ax < 3; ++ax) {
-            const int64_t cb = p[ax] > 0.0f ? (int64_t)p[ax] >> lg : 0;  // the particle's block (p as usize >> lg)
+            const int64_t c = p[ax] > 0.0f ? (int64_t)p[ax] : 0;  // the particle's cell (p as usize)
+            const int64_t cb = c >> lg;                              // and block
             if (cb >= nn[ax]) out = true;
             const float b = p[ax] / bsx;
             const int64_t l = max((int64_t)(int32_t)truncf(b - r_scan_bsx), (int64_t)0);
@@ -149,15 +156,31 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             lo[ax] = (uint32_t)(min(max(l - cb, (int64_t)-1), (int64_t)1) + 1);
             hi[ax] = (uint32_t)(min(max(h - cb, (int64_t)-1), (int64_t)1) + 1);
             const int32_t b0 = (int32_t)cb * B;
+            cell[ax] = (int32_t)(c - (int64_t)b0);
             for (int face = 0; face < 2; ++face) {
+                // staging coordinates (global - (b0 - M)) of the clipped footprint
                 const float of = face ? 1.0f : 0.5f;
-                const int32_t a1 = min(max((int32_t)ceilf((p[ax] - r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
-                const int32_t a2 = min(max((int32_t)floorf((p[ax] + r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
-                f |= (uint64_t)(a1 & 31) << (((ax * 2 + face) * 2) * 5);
-                f |= (uint64_t)(a2 & 31) << (((ax * 2 + face) * 2 + 1) * 5);
+                a1[ax][face] = min(max((int32_t)ceilf((p[ax] - r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
+                a2[ax][face] = min(max((int32_t)floorf((p[ax] + r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
             }
         }
-        fp[i] = f;
+        for (int dir = 0; dir < 3; ++dir) {
+            const int F = dir, U = dir == 0 ? 1 : 0, V = dir == 2 ? 1 : 2;
+            uint64_t m = 0;
+            for (int dv = 0; dv < WIN; ++dv) {
+                const int sv = cell[V] + dv;  // staging coordinate of the lane row: cell + M + (dv - M)
+                if (sv < a1[V][0] || sv > a2[V][0]) continue;
+                for (int du = 0; du < WIN; ++du) {
+                    const int su = cell[U] + du;
+                    if (su >= a1[U][0] && su <= a2[U][0]) m |= 1ull << (du + WIN * dv);
+                }
+            }
+            for (int f = 0; f < WIN; ++f) {
+                const int sf = cell[F] + f - 1;  // staging coordinate of face offset f - 1 - M
+                if (sf >= a1[F][1] && sf <= a2[F][1]) m |= 1ull << (56 + f);
+            }
+            lane_mask[(size_t)dir * n + i] = m;
+        }
         if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
         uint32_t m = 0;
         for (uint32_t dz = lo[2]; dz <= hi[2]; ++dz)
@@ -167,23 +190,56 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
     }
 }
 
-__device__ __forceinline__ int fp_field(uint64_t f, int ax, int face, int hi) {
-    return (int)((f >> (((ax * 2 + face) * 2 + hi) * 5)) & 31);
+// Pairs of f32 in one 64-bit register, and the paired IEEE single-precision
+// operations of sm_100 (each half rounded to nearest, exactly as the scalar
+// operation).  A paired product that feeds a paired sum directly can be
+// fused into one paired multiply-add by the code generator even with .rn
+// (measured on B200), so callers keep such products scalar.
+__device__ __forceinline__ uint64_t f2_pack(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
 }
 
 // Splat kernel: one CTA per (particle block, direction DIR).  The block's
 // (bsx + 2M)^3 staging window of face sums lives in shared memory in FP64.
-// Cells are visited by 2x2x2 tiles in (M+1)^3 colour phases (cells of two
-// tiles of a phase are 2M+1 apart, so their candidate face windows are
-// disjoint) with a barrier between phases; inside a phase one warp handles
-// one tile, its 8 cells in a fixed order.  The lanes of the warp
-// take the (2M+1)^2 positions of the cell's face window across the two axes
-// other than the face axis, and each lane keeps the 2M+1 faces along the face
-// axis in FP64 registers.  For every particle of the cell (sorted order) a
-// lane evaluates the reference's f32 term for each of its faces that lies in
-// the particle's clipped footprint (p2g.rs:263-330, operation by operation),
-// then adds its register sums to the staging window: a fixed summation order,
-// no atomics.
+// Cells are grouped in 2x2x2 tiles; a warp takes a whole tile (its 8 cells in
+// a fixed order).  The face windows of two tiles overlap only when the tiles
+// are at most M apart along every axis, so tiles coloured by tile coordinate
+// mod (M+1) never overlap within a colour.  Warps take tiles from a shared
+// counter in colour-major order, and before adding into the window a warp
+// waits until every overlapping tile of a lower colour is done (per-tile
+// flags in shared memory).  Every face therefore receives its cells'
+// contributions in colour order, then cell order: a fixed summation order
+// with no atomics and no CTA-wide barrier between colours.
+//
+// Inside a cell, the lanes of the warp take the (2M+1)^2 positions of the
+// cell's face window across the two axes other than the face axis, and each
+// lane keeps the 2M+1 faces along the face axis in FP64 registers.  For every
+// particle of the cell (sorted order) a lane evaluates the reference's f32
+// term for each of its faces inside the particle's clipped footprint
+// (p2g.rs:263-330, operation by operation; the footprint arrives as the
+// particle's lane and face bits), then adds its register sums to the window.
+// A tile wait that runs past a second sets bit 4 of the status word and goes
+// on (the result is then wrong and the host reports the error).
 template <int BSX, int M, int DIR>
 __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
     constexpr int W = BSX + 2 * M;
@@ -191,10 +247,32 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
     constexpr int WIN = 2 * M + 1;
     constexpr int NUV = WIN * WIN;       // lane positions
     constexpr int Q = (NUV + 31) / 32;   // lane rounds
-    extern __shared__ double st[];       // [2][W^3]: mass, momentum
+    constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
+    constexpr int NNB = WIN * WIN * WIN;  // tile offsets in [-M, M]^3
+    constexpr int NP = (WIN + 1) / 2;    // face pairs
+    static_assert(WIN <= 7 && NUV <= 56, "lane and face bits must fit one u64");
+    extern __shared__ double st[];       // [2][W^3]: mass, momentum; then per-warp particle slots
+    __shared__ uint32_t s_done[NT];
+    __shared__ uint16_t s_order[NT];     // tiles in colour-major order
+    __shared__ uint32_t s_next;
     const int k_pb = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
+    float4* wslot = reinterpret_cast<float4*>(st + 2 * WW) + (size_t)(tid >> 5) * 64;  // [64] float4 per warp
     for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
+    for (int t = tid; t < NT; t += blockDim.x) {
+        s_done[t] = 0;
+        const int tx = t % T, ty = (t / T) % T, tz = t / (T * T);
+        const int cx = tx % K, cy = ty % K, cz = tz % K;
+        const int ci = cx + K * (cy + K * cz);
+        int base = 0;
+        for (int c = 0; c < ci; ++c) {
+            const int ox = c % K, oy = (c / K) % K, oz = c / (K * K);
+            base += ((T - ox + K - 1) / K) * ((T - oy + K - 1) / K) * ((T - oz + K - 1) / K);
+        }
+        const int ntx = (T - cx + K - 1) / K, nty = (T - cy + K - 1) / K;
+        s_order[base + (tx / K) + ntx * ((ty / K) + nty * (tz / K))] = (uint16_t)t;
+    }
+    if (tid == 0) s_next = 0;
     const uint64_t key = a.pb_key[k_pb];
     const int32_t b0[3] = {(int32_t)compact3(key) * BSX, (int32_t)compact3(key >> 1) * BSX,
                            (int32_t)compact3(key >> 2) * BSX};
@@ -203,87 +281,139 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
     const int32_t* cb = a.cell_begin + (size_t)k_pb * BSX * BSX * BSX;
     const int32_t* ce = a.cell_end + (size_t)k_pb * BSX * BSX * BSX;
     const float* __restrict__ pv = a.pv[DIR];
+    const uint64_t* __restrict__ lmask = a.lane_mask[DIR];
     const float inv_r2 = a.inv_r2;
     __syncthreads();
-    // Tiles of 2x2x2 cells coloured by tile coordinate mod K: cells of two
-    // tiles of one colour are at least 2K - 1 = 2M + 1 apart, so their face
-    // windows are disjoint; a warp takes a whole tile (8 cells in a fixed
-    // order) between barriers.
-    constexpr int T = BSX / 2, K = M + 1;
-    for (int ph = 0; ph < K * K * K; ++ph) {
-        const int ox = ph % K, oy = (ph / K) % K, oz = ph / (K * K);
-        const int ntx = ox < T ? (T - ox + K - 1) / K : 0;
-        const int nty = oy < T ? (T - oy + K - 1) / K : 0;
-        const int ntz = oz < T ? (T - oz + K - 1) / K : 0;
-        const int total = ntx * nty * ntz;
-        for (int tile = warp; tile < total; tile += nwarp) {
-          for (int sub = 0; sub < 8; ++sub) {
+    while (true) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(&s_next, 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= (uint32_t)NT) break;
+        const int t = s_order[q];
+        const int tc[3] = {t % T, (t / T) % T, t / (T * T)};
+        const int ci = tc[0] % K + K * (tc[1] % K + K * (tc[2] % K));
+        // the tile's cell ranges, one cell per lane, fetched before the wait
+        int cbeg = 0, cend = 0;
+        if (lane < 8) {
+            const uint32_t lm = (uint32_t)morton3(2 * tc[0] + (lane & 1), 2 * tc[1] + ((lane >> 1) & 1), 2 * tc[2] + (lane >> 2));
+            cbeg = cb[lm];
+            cend = ce[lm];
+        }
+        // wait for the overlapping tiles of lower colours
+        {
+            uint64_t t0 = 0;
+            uint32_t spins = 0;
+            while (true) {
+                bool ready = true;
+                for (int o = lane; o < NNB; o += 32) {
+                    const int nx = tc[0] + o % WIN - M, ny = tc[1] + (o / WIN) % WIN - M, nz = tc[2] + o / (WIN * WIN) - M;
+                    if (nx < 0 || ny < 0 || nz < 0 || nx >= T || ny >= T || nz >= T) continue;
+                    if (nx % K + K * (ny % K + K * (nz % K)) >= ci) continue;
+                    if (!*(volatile uint32_t*)&s_done[nx + T * (ny + T * nz)]) ready = false;
+                }
+                if (__all_sync(0xffffffffu, ready)) break;
+                __nanosleep(64);
+                if ((++spins & 63u) == 0) {
+                    const uint64_t now = globaltimer_ns();
+                    if (!t0) t0 = now;
+                    else if (now - t0 > 1000000000ull) {
+                        if (lane == 0) atomicOr(a.status, 4);
+                        break;
+                    }
+                }
+            }
+            __threadfence_block();
+        }
+        for (int sub = 0; sub < 8; ++sub) {
             // cells of a tile have overlapping face windows: order this
             // cell's shared-memory updates after the previous cell's across
             // the warp's lanes
             __syncwarp();
-            int cell[3];
-            cell[0] = 2 * (ox + K * (tile % ntx)) + (sub & 1);
-            cell[1] = 2 * (oy + K * ((tile / ntx) % nty)) + ((sub >> 1) & 1);
-            cell[2] = 2 * (oz + K * (tile / (ntx * nty))) + (sub >> 2);
-            const uint32_t lm = (uint32_t)morton3(cell[0], cell[1], cell[2]);
-            const int b = cb[lm], e = ce[lm];
+            const int b = __shfl_sync(0xffffffffu, cbeg, sub), e = __shfl_sync(0xffffffffu, cend, sub);
             if (b >= e) continue;
+            int cell[3];
+            cell[0] = 2 * tc[0] + (sub & 1);
+            cell[1] = 2 * tc[1] + ((sub >> 1) & 1);
+            cell[2] = 2 * tc[2] + (sub >> 2);
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int uv = lane + 32 * q;
+            for (int qq = 0; qq < Q; ++qq) {
+                const int uv = lane + 32 * qq;
                 const bool on = uv < NUV;
                 // staging coordinates of this lane's row: U, V offsets in [-M, M]
-                const int su = cell[U] + M + (uv % WIN) - M, sv = cell[V] + M + (uv / WIN) - M;
+                const int su = cell[U] + (uv % WIN), sv = cell[V] + (uv / WIN);
                 const float gu = (float)(b0[U] - M + su), gv = (float)(b0[V] - M + sv);
+                // face positions along F, in pairs: staging cell[F] + s - 1
+                uint64_t gf2[NP];
+#pragma unroll
+                for (int h = 0; h < NP; ++h) {
+                    const int s0 = 2 * h, s1 = 2 * h + 1 < WIN ? 2 * h + 1 : 2 * h;
+                    gf2[h] = f2_pack((float)(b0[F] - M + cell[F] + s0 - 1), (float)(b0[F] - M + cell[F] + s1 - 1));
+                }
                 double am[WIN], av[WIN];
 #pragma unroll
                 for (int s = 0; s < WIN; ++s) am[s] = av[s] = 0.0;
                 // the cell's particles, 32 at a time: one coalesced load per
-                // lane, then broadcast to the lanes by shuffles
+                // lane into the warp's staging slots, then broadcast reads
                 for (int p0 = b; p0 < e; p0 += 32) {
                   const int cnt = min(32, e - p0);
-                  uint64_t f_l = 0;
-                  float m_l = 0.0f, mv_l = 0.0f, x_l = 0.0f, y_l = 0.0f, z_l = 0.0f;
+                  __syncwarp();
                   if (lane < cnt) {
                       const int pl = p0 + lane;
-                      f_l = a.fp[pl];
-                      m_l = a.pm[pl];
-                      mv_l = m_l * pv[pl];
-                      x_l = a.px[pl] - 0.5f;
-                      y_l = a.py[pl] - 0.5f;
-                      z_l = a.pz[pl] - 0.5f;
+                      const uint64_t f = lmask[pl];
+                      const float m = a.pm[pl];
+                      const float pc[3] = {a.px[pl] - 0.5f, a.py[pl] - 0.5f, a.pz[pl] - 0.5f};
+                      wslot[lane] = make_float4(pc[U], pc[V], pc[F], m);
+                      wslot[32 + lane] = make_float4(m * pv[pl], __uint_as_float((uint32_t)f),
+                                                     __uint_as_float((uint32_t)(f >> 32)), 0.0f);
                   }
+                  __syncwarp();
                   for (int j = 0; j < cnt; ++j) {
-                    const uint64_t f = __shfl_sync(0xffffffffu, f_l, j);
-                    const float m_p = __shfl_sync(0xffffffffu, m_l, j);
-                    const float scale_mom = __shfl_sync(0xffffffffu, mv_l, j);
-                    const float pc[3] = {__shfl_sync(0xffffffffu, x_l, j), __shfl_sync(0xffffffffu, y_l, j),
-                                         __shfl_sync(0xffffffffu, z_l, j)};
-                    if (!on || su < fp_field(f, U, 0, 0) || su > fp_field(f, U, 0, 1) || sv < fp_field(f, V, 0, 0) ||
-                        sv > fp_field(f, V, 0, 1))
-                        continue;
-                    const int sf1 = fp_field(f, F, 1, 0), sf2 = fp_field(f, F, 1, 1);
-                    const float du = gu - pc[U], dv = gv - pc[V];
+                    const float4 P = wslot[j];        // U, V, F coordinates (minus 0.5), mass
+                    const float4 R = wslot[32 + j];   // momentum, lane bits (low, high)
+                    const uint32_t f_lo = __float_as_uint(R.y), f_hi = __float_as_uint(R.z);
+                    if (!on || !(((qq == 0 ? f_lo : f_hi) >> lane) & 1u)) continue;
+                    const float m_p = P.w, scale_mom = R.x;
+                    const uint32_t fbits = f_hi >> 24;  // bit s: face s inside the footprint
+                    const float du = gu - P.x, dv = gv - P.y;
+                    const uint64_t pf2 = f2_pack(P.z, P.z);
+                    // p2g.rs:287-325: dz2 = dz*dz; dyz = dz2 + dy*dy; dist_sq = dx*dx + dyz,
+                    // with (dx, dy, dz) = (df, du, dv), (du, df, dv) or (du, dv, df)
+                    float hoist0 = 0.0f, hoist1 = 0.0f;
+                    if (DIR == 0) hoist0 = dv * dv + du * du;  // dyz
+                    else if (DIR == 1) { hoist0 = dv * dv; hoist1 = du * du; }  // dz2, dx*dx
+                    else { hoist0 = dv * dv; hoist1 = du * du; }                // dy*dy, dx*dx
+                    const uint64_t h02 = f2_pack(hoist0, hoist0), h12 = f2_pack(hoist1, hoist1);
 #pragma unroll
-                    for (int s = 0; s < WIN; ++s) {
-                        // face-axis offset in [-M-1, M-1] -> staging cell[F] + s - 1
-                        const int sf = cell[F] + s - 1;
-                        if (sf < sf1 || sf > sf2) continue;
-                        const float df = (float)(b0[F] - M + sf) - pc[F];
-                        // p2g.rs:287-325: dz2 = dz*dz; dyz = dz2 + dy*dy; dist_sq = dx*dx + dyz
-                        float dx, dy, dz;
-                        if (DIR == 0) { dx = df; dy = du; dz = dv; }
-                        else if (DIR == 1) { dx = du; dy = df; dz = dv; }
-                        else { dx = du; dy = dv; dz = df; }
-                        const float dz2 = dz * dz;
-                        const float dyz = dz2 + dy * dy;
-                        const float dist_sq = dx * dx + dyz;
-                        const float df2 = (dist_sq + df) + 0.25f;
-                        float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
-                        w = (w * w) * w;
-                        am[s] += (double)(w * m_p);
-                        av[s] += (double)(w * scale_mom);
+                    for (int h = 0; h < NP; ++h) {
+                        const uint64_t df = f2_sub(gf2[h], pf2);
+                        // products that feed a sum stay scalar: a paired
+                        // product feeding a paired sum may be contracted
+                        float d0, d1;
+                        f2_unpack(df, d0, d1);
+                        const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
+                        uint64_t dist;
+                        if (DIR == 0) dist = f2_add(sq, h02);                 // dx*dx + dyz
+                        else if (DIR == 1) dist = f2_add(h12, f2_add(h02, sq));  // dx*dx + (dz2 + dy*dy)
+                        else dist = f2_add(h12, f2_add(sq, h02));             // dx*dx + (dz2 + dy*dy)
+                        const uint64_t df2 = f2_add(f2_add(dist, df), f2_pack(0.25f, 0.25f));
+                        float e0, e1;
+                        f2_unpack(df2, e0, e1);
+                        const uint64_t t = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
+                        float w0, w1;
+                        f2_unpack(t, w0, w1);
+                        w0 = ((fbits >> (2 * h)) & 1u) ? fmaxf(w0, 0.0f) : 0.0f;
+                        w1 = ((fbits >> (2 * h + 1)) & 1u) ? fmaxf(w1, 0.0f) : 0.0f;
+                        uint64_t w = f2_pack(w0, w1);
+                        w = f2_mul(f2_mul(w, w), w);
+                        float tm0, tm1, tv0, tv1;
+                        f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
+                        f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
+                        am[2 * h] += (double)tm0;
+                        av[2 * h] += (double)tv0;
+                        if (2 * h + 1 < WIN) {
+                            am[2 * h + 1] += (double)tm1;
+                            av[2 * h + 1] += (double)tv1;
+                        }
                     }
                   }
                 }
@@ -302,10 +432,12 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                     }
                 }
             }
-          }
         }
-        __syncthreads();
+        __syncwarp();
+        __threadfence_block();
+        if (lane == 0) *(volatile uint32_t*)&s_done[t] = 1u;
     }
+    __syncthreads();
     double* out = a.partial + ((size_t)k_pb * 3 + DIR) * 2 * WW;
     for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
 }
@@ -367,14 +499,14 @@ static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<
 template <int BSX, int M, int DIR>
 static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     constexpr int W = BSX + 2 * M;
-    const size_t smem = 2 * sizeof(double) * W * W * W;
+    constexpr int T = BSX / 2, NT = T * T * T;
+    constexpr int WARPS = NT < 32 ? NT : 32;
+    const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 64 * sizeof(float4);
     static bool attr = false;
     if (!attr) {
         CUDA_CHECK(cudaFuncSetAttribute(p2g_cells_kernel<BSX, M, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    constexpr int T = BSX / 2, K = M + 1, TW = (T + K - 1) / K;
-    constexpr int WARPS = TW * TW * TW < 32 ? TW * TW * TW : 32;
     begin_launch(ctx);
     p2g_cells_kernel<BSX, M, DIR><<<(unsigned)npb, 32 * WARPS, smem, ctx->stream>>>(a);
     after_launch(ctx, "p2g_cells_kernel");
@@ -436,7 +568,7 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     // ---- phase 1: sort, gather, particle blocks -------------------------------
     ScratchLayout L1;
     const size_t o_keys = L1.add<uint64_t>(n), o_skeys = L1.add<uint64_t>(n), o_perm = L1.add<uint32_t>(n),
-                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_fp = L1.add<uint64_t>(n),
+                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_fp = L1.add<uint64_t>(3 * n),
                  o_pbk = L1.add<uint64_t>(n + 1),
                  o_pbs = L1.add<uint64_t>(n + 2), o_tmp = L1.add<char>(std::max(radix_sort_scratch_bytes(n), segment_scratch_bytes(n))),
                  o_bad = L1.add<int>(4);
@@ -546,7 +678,8 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     s.cell_begin = cell_begin;
     s.cell_end = cell_end;
     s.pb_key = pb_key;
-    s.fp = fpk;
+    for (int d = 0; d < 3; ++d) s.lane_mask[d] = fpk + (size_t)d * n;
+    s.status = ctx->status.as<int>();
     s.partial = partial;
     s.r_p = r_p;
     s.inv_r2 = 1.0f / (r_p * r_p);
@@ -563,7 +696,9 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     c.nx = (int64_t)u->nx;
     c.ny = (int64_t)u->ny;
     if (na) dispatch(ctx, bsx, M, nullptr, 0, &c, na);
+    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);  // `slots` (host) and the scratch layout end here
+    raise_device_status(ctx, hstatus);
     if (n_active_out) *n_active_out = na;
     (void)a256;
 }

@@ -89,12 +89,6 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ uint64_t os_globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // Histogram of every digit of every key, and zeroing of the first pass's
 // status array.  Each thread takes OH_ITEMS consecutive keys and adds runs of
 // equal digits with one shared atomic (keys that are nearly sorted already,
@@ -265,7 +259,7 @@ __global__ void __launch_bounds__(OS_THREADS, 4)
             if (done) break;
             k -= used;
             if (used < OS_LOOKBACK && (++spins & 15u) == 0) {
-                const uint64_t now = os_globaltimer();
+                const uint64_t now = globaltimer_ns();
                 if (!t0) t0 = now;
                 else if (now - t0 > 1000000000ull) {
                     atomicOr(err, 2);
