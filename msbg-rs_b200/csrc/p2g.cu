@@ -164,21 +164,23 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
                 a2[ax][face] = min(max((int32_t)floorf((p[ax] + r_p) - of), b0 - M), b0 + B + M - 1) - (b0 - M);
             }
         }
+        // per axis, the offsets k in [0, 2M] whose staging coordinate
+        // cell + k (cell-centred, face 0) or cell + k - 1 (faces, face 1)
+        // lies in the clipped footprint: a contiguous run of bits
+        uint32_t run[3][2];
+        for (int ax = 0; ax < 3; ++ax)
+            for (int face = 0; face < 2; ++face) {
+                const int lo = max(a1[ax][face] - cell[ax] + face, 0), hi = min(a2[ax][face] - cell[ax] + face, WIN - 1);
+                run[ax][face] = lo > hi ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
+            }
         for (int dir = 0; dir < 3; ++dir) {
             const int F = dir, U = dir == 0 ? 1 : 0, V = dir == 2 ? 1 : 2;
-            uint64_t m = 0;
-            for (int dv = 0; dv < WIN; ++dv) {
-                const int sv = cell[V] + dv;  // staging coordinate of the lane row: cell + M + (dv - M)
-                if (sv < a1[V][0] || sv > a2[V][0]) continue;
-                for (int du = 0; du < WIN; ++du) {
-                    const int su = cell[U] + du;
-                    if (su >= a1[U][0] && su <= a2[U][0]) m |= 1ull << (du + WIN * dv);
-                }
-            }
-            for (int f = 0; f < WIN; ++f) {
-                const int sf = cell[F] + f - 1;  // staging coordinate of face offset f - 1 - M
-                if (sf >= a1[F][1] && sf <= a2[F][1]) m |= 1ull << (56 + f);
-            }
+            // lane bit du + WIN dv for du in run U, dv in run V: the U run
+            // repeated at the V run's rows (one product, no carries)
+            uint64_t rows = 0;
+            for (int dv = 0; dv < WIN; ++dv)
+                if ((run[V][0] >> dv) & 1u) rows |= 1ull << (WIN * dv);
+            const uint64_t m = (uint64_t)run[U][0] * rows | ((uint64_t)run[F][1] << 56);
             lane_mask[(size_t)dir * n + i] = m;
         }
         if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
@@ -371,9 +373,12 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                     const float4 P = wslot[j];        // U, V, F coordinates (minus 0.5), mass
                     const float4 R = wslot[32 + j];   // momentum, lane bits (low, high)
                     const uint32_t f_lo = __float_as_uint(R.y), f_hi = __float_as_uint(R.z);
-                    if (!on || !(((qq == 0 ? f_lo : f_hi) >> lane) & 1u)) continue;
+                    // bit s: face s inside the footprint, none when the lane's
+                    // row is outside it (no branch: the warp stays converged,
+                    // and a zero weight adds +0 to a sum that starts at +0)
+                    const uint32_t lanebit = on ? (((qq == 0 ? f_lo : f_hi) >> lane) & 1u) : 0u;
+                    const uint32_t fbits = (f_hi >> 24) & (0u - lanebit);
                     const float m_p = P.w, scale_mom = R.x;
-                    const uint32_t fbits = f_hi >> 24;  // bit s: face s inside the footprint
                     const float du = gu - P.x, dv = gv - P.y;
                     const uint64_t pf2 = f2_pack(P.z, P.z);
                     // p2g.rs:287-325: dz2 = dz*dz; dyz = dz2 + dy*dy; dist_sq = dx*dx + dyz,
