@@ -192,6 +192,11 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
     }
 }
 
+// Warps of a splat CTA.  Tiles wait for their overlapping predecessors, so
+// more warps mostly wait longer; 20 (one CTA per SM, up to 96 registers a
+// thread) measured fastest on B200 among 16, 20, 24 and 32.
+constexpr int kSplatWarps = 20;
+
 // Pairs of f32 in one 64-bit register, and the paired IEEE single-precision
 // operations of sm_100 (each half rounded to nearest, exactly as the scalar
 // operation).  A paired product that feeds a paired sum directly can be
@@ -243,7 +248,7 @@ __device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
 // A tile wait that runs past a second sets bit 4 of the status word and goes
 // on (the result is then wrong and the host reports the error).
 template <int BSX, int M, int DIR>
-__global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
+__global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArgs a) {
     constexpr int W = BSX + 2 * M;
     constexpr int WW = W * W * W;
     constexpr int WIN = 2 * M + 1;
@@ -251,8 +256,10 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
     constexpr int Q = (NUV + 31) / 32;   // lane rounds
     constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
     constexpr int NNB = WIN * WIN * WIN;  // tile offsets in [-M, M]^3
+    constexpr int NR = (NNB + 31) / 32;   // of them per lane
     constexpr int NP = (WIN + 1) / 2;    // face pairs
     static_assert(WIN <= 7 && NUV <= 56, "lane and face bits must fit one u64");
+    static_assert(NT < 0xffff, "tile indices must fit 16 bits");
     extern __shared__ double st[];       // [2][W^3]: mass, momentum; then per-warp particle slots
     __shared__ uint32_t s_done[NT];
     __shared__ uint16_t s_order[NT];     // tiles in colour-major order
@@ -301,20 +308,38 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
             cbeg = cb[lm];
             cend = ce[lm];
         }
-        // wait for the overlapping tiles of lower colours
-        {
+        // the overlapping tiles of lower colours: each lane takes up to NR of
+        // them; the warp waits for them before its first shared-memory add
+        // of this tile (so the tile's first cell is computed meanwhile),
+        // drops each as it is seen done, and sleeps between rounds
+        uint32_t nbi[(NR + 1) / 2];  // tile indices, two 16-bit fields per word, 0xffff = none
+#pragma unroll
+        for (int k = 0; k < (NR + 1) / 2; ++k) nbi[k] = 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            const int o = lane + 32 * k;
+            const int nx = tc[0] + o % WIN - M, ny = tc[1] + (o / WIN) % WIN - M, nz = tc[2] + o / (WIN * WIN) - M;
+            const bool dep = o < NNB && nx >= 0 && ny >= 0 && nz >= 0 && nx < T && ny < T && nz < T &&
+                             nx % K + K * (ny % K + K * (nz % K)) < ci;
+            if (dep) nbi[k >> 1] &= ~(0xffffu << (16 * (k & 1))) | ((uint32_t)(nx + T * (ny + T * nz)) << (16 * (k & 1)));
+        }
+        bool deps_pending = true;
+        auto wait_deps = [&]() {
             uint64_t t0 = 0;
-            uint32_t spins = 0;
+            uint32_t spins = 0, sleep_ns = 32;
             while (true) {
                 bool ready = true;
-                for (int o = lane; o < NNB; o += 32) {
-                    const int nx = tc[0] + o % WIN - M, ny = tc[1] + (o / WIN) % WIN - M, nz = tc[2] + o / (WIN * WIN) - M;
-                    if (nx < 0 || ny < 0 || nz < 0 || nx >= T || ny >= T || nz >= T) continue;
-                    if (nx % K + K * (ny % K + K * (nz % K)) >= ci) continue;
-                    if (!*(volatile uint32_t*)&s_done[nx + T * (ny + T * nz)]) ready = false;
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const uint32_t idx = (nbi[k >> 1] >> (16 * (k & 1))) & 0xffffu;
+                    if (idx != 0xffffu) {
+                        if (*(volatile uint32_t*)&s_done[idx]) nbi[k >> 1] |= 0xffffu << (16 * (k & 1));
+                        else ready = false;
+                    }
                 }
                 if (__all_sync(0xffffffffu, ready)) break;
-                __nanosleep(64);
+                __nanosleep(sleep_ns);
+                sleep_ns = sleep_ns < 512 ? 2 * sleep_ns : 512;
                 if ((++spins & 63u) == 0) {
                     const uint64_t now = globaltimer_ns();
                     if (!t0) t0 = now;
@@ -325,7 +350,8 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                 }
             }
             __threadfence_block();
-        }
+            deps_pending = false;
+        };
         for (int sub = 0; sub < 8; ++sub) {
             // cells of a tile have overlapping face windows: order this
             // cell's shared-memory updates after the previous cell's across
@@ -422,6 +448,7 @@ __global__ void __launch_bounds__(1024, 1) p2g_cells_kernel(SplatArgs a) {
                     }
                   }
                 }
+                if (deps_pending) wait_deps();
                 if (on) {
 #pragma unroll
                     for (int s = 0; s < WIN; ++s) {
@@ -505,7 +532,7 @@ template <int BSX, int M, int DIR>
 static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     constexpr int W = BSX + 2 * M;
     constexpr int T = BSX / 2, NT = T * T * T;
-    constexpr int WARPS = NT < 32 ? NT : 32;
+    constexpr int WARPS = NT < kSplatWarps ? NT : kSplatWarps;
     const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 64 * sizeof(float4);
     static bool attr = false;
     if (!attr) {
