@@ -122,17 +122,73 @@ __global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, i
     }
 }
 
-// MacSampler::sample::<Linear> (fluid/g2p.rs:26-32): component a is a
-// cell-centred sample of velocity[a] at p - 1/2 e_a.
-__global__ void g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz, const float* __restrict__ pos, size_t n, int bc,
-                           float* __restrict__ out) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
-        const float cx = px - 0.5f, cy = py - 0.5f, cz = pz - 0.5f;
-        out[3 * i + 0] = sample_linear_dev(gx, (px - 0.5f) - 0.5f, cy, cz, bc);
-        out[3 * i + 1] = sample_linear_dev(gy, cx, (py - 0.5f) - 0.5f, cz, bc);
-        out[3 * i + 2] = sample_linear_dev(gz, cx, cy, (pz - 0.5f) - 0.5f, bc);
+// One component's sample when its 2x2x2 corners lie inside the domain
+// (gather_map's interior case, no boundary condition applies): the code of
+// the block of corner (0, 0, 0) and, for corners in the next block along an
+// axis, that block's code (looked up only where the corners cross).
+struct InteriorCorners {
+    int32_t code[8];
+    int32_t vid[8];
+    float x, y, z;
+    bool ok;
+};
+
+__device__ __forceinline__ InteriorCorners interior_corners(const SampleGrid& g, float x, float y, float z) {
+    InteriorCorners f;
+    f.x = x; f.y = y; f.z = z;
+    const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
+    const int32_t ix0 = (int32_t)floorf(x), iy0 = (int32_t)floorf(y), iz0 = (int32_t)floorf(z);
+    f.ok = ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + 1 < g.sx && iy0 + 1 < g.sy && iz0 + 1 < g.sz;
+    const int32_t jx0 = f.ok ? ix0 : 0, jy0 = f.ok ? iy0 : 0, jz0 = f.ok ? iz0 : 0;
+    const uint64_t sy = (uint64_t)g.nx, sz = (uint64_t)g.nx * g.ny;
+    const uint64_t bid0 = (uint64_t)(jx0 >> lg) + (uint64_t)(jy0 >> lg) * sy + (uint64_t)(jz0 >> lg) * sz;
+    const int32_t c0 = f.ok ? block_code(g, bid0) : kCodeEmpty;
+    const bool crx = (jx0 & mask) == mask, cry = (jy0 & mask) == mask, crz = (jz0 & mask) == mask;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int i = s & 1, j = (s >> 1) & 1, k = s >> 2;
+        const bool other = (i && crx) || (j && cry) || (k && crz);
+        const uint64_t bid = bid0 + (uint64_t)(i && crx) + (j && cry ? sy : 0) + (k && crz ? sz : 0);
+        f.code[s] = f.ok && other ? block_code(g, bid) : c0;
+        f.vid[s] = ((jx0 + i) & mask) | (((jy0 + j) & mask) << lg) | (((jz0 + k) & mask) << (2 * lg));
     }
+    return f;
+}
+
+// The eight corners of an interior sample, loaded together, then the same
+// three-level lerp as sample_linear_dev.
+__device__ __forceinline__ float interior_sample(const SampleGrid& g, const InteriorCorners& f) {
+    float c[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+        c[s] = f.code[s] >= 0 ? __ldg(g.payload + ((size_t)f.code[s] << (3 * g.lg)) + f.vid[s])
+                              : (f.code[s] == kCodeFull ? g.full : g.empty);
+    const float fx = floorf(f.x), fy = floorf(f.y), fz = floorf(f.z);
+    const float u = f.x - fx, v = f.y - fy, w = f.z - fz;
+    const float c00 = lerpf(c[0], c[1], u), c10 = lerpf(c[2], c[3], u), c01 = lerpf(c[4], c[5], u),
+                c11 = lerpf(c[6], c[7], u);
+    const float c0 = lerpf(c00, c10, v), c1 = lerpf(c01, c11, v);
+    return lerpf(c0, c1, w);
+}
+
+// MacSampler::sample::<Linear> (fluid/g2p.rs:26-32): component a is a
+// cell-centred sample of velocity[a] at p - 1/2 e_a.  One thread per
+// particle; the block lookups, then the 24 corner loads, are issued
+// together; only samples whose corners leave the domain take the general
+// gather (boundary conditions).
+__global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz,
+                                                  const float* __restrict__ pos, size_t n, int bc, float* __restrict__ out) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    const float cx = px - 0.5f, cy = py - 0.5f, cz = pz - 0.5f;
+    const float x0 = (px - 0.5f) - 0.5f, y1 = (py - 0.5f) - 0.5f, z2 = (pz - 0.5f) - 0.5f;
+    const InteriorCorners f0 = interior_corners(gx, x0, cy, cz);
+    const InteriorCorners f1 = interior_corners(gy, cx, y1, cz);
+    const InteriorCorners f2 = interior_corners(gz, cx, cy, z2);
+    out[3 * i + 0] = f0.ok ? interior_sample(gx, f0) : sample_linear_dev(gx, x0, cy, cz, bc);
+    out[3 * i + 1] = f1.ok ? interior_sample(gy, f1) : sample_linear_dev(gy, cx, y1, cz, bc);
+    out[3 * i + 2] = f2.ok ? interior_sample(gz, f2) : sample_linear_dev(gz, cx, cy, z2, bc);
 }
 
 // g2p_blend (fluid/g2p.rs:42-45), component-wise.
@@ -231,7 +287,7 @@ void g2p_device(msbg_mac* m, const float* d_pos, size_t n, int bc, float* d_out)
     if (!n) return;
     SampleGrid gx = sample_grid(m->ch[0]), gy = sample_grid(m->ch[1]), gz = sample_grid(m->ch[2]);
     begin_launch(m->ctx);
-    g2p_kernel<<<grid_for(n), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, d_out);
+    g2p_kernel<<<(unsigned)div_up(n, 256), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, d_out);
     after_launch(m->ctx, "g2p_kernel");
 }
 

@@ -511,10 +511,25 @@ __global__ void gather_u64_kernel(const uint64_t* src, const uint32_t* perm, uin
 }
 
 // dst[i] = src[perm[i]] for items of `width` floats.
-__global__ void permute_kernel(const uint32_t* perm, size_t n, int width, const float* src, float* dst) {
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n * width; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t i = t / width, c = t % width;
-        dst[t] = src[(size_t)perm[i] * width + c];
+// dst[i] = src[perm[i]] for rows of `width` floats: one thread per row (one
+// index load, the row's floats gathered together); W > 0 fixes the width at
+// compile time, W = 0 reads it from `width`.
+template <int W>
+__global__ void permute_kernel(const uint32_t* __restrict__ perm, size_t n, int width, const float* __restrict__ src,
+                               float* __restrict__ dst) {
+    const int w = W > 0 ? W : width;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float* s = src + (size_t)__ldg(perm + i) * w;
+        float* d = dst + i * w;
+        if (W > 0) {
+            float v[W > 0 ? W : 1];
+#pragma unroll
+            for (int c = 0; c < W; ++c) v[c] = __ldg(s + c);
+#pragma unroll
+            for (int c = 0; c < W; ++c) d[c] = v[c];
+        } else {
+            for (int c = 0; c < w; ++c) d[c] = __ldg(s + c);
+        }
     }
 }
 
@@ -721,7 +736,10 @@ int msbg_permute_device(msbg_ctx* ctx, const uint32_t* d_perm, size_t n, int wid
     if (!n) return MSBG_OK;
     set_device(ctx);
     begin_launch(ctx);
-    permute_kernel<<<grid_for(n * width), 256, 0, ctx->stream>>>(d_perm, n, width, d_src, d_dst);
+    const unsigned g = (unsigned)std::max<size_t>(div_up(n, 256), 1);
+    if (width == 1) permute_kernel<1><<<g, 256, 0, ctx->stream>>>(d_perm, n, width, d_src, d_dst);
+    else if (width == 3) permute_kernel<3><<<g, 256, 0, ctx->stream>>>(d_perm, n, width, d_src, d_dst);
+    else permute_kernel<0><<<g, 256, 0, ctx->stream>>>(d_perm, n, width, d_src, d_dst);
     after_launch(ctx, "permute_kernel");
     MSBG_API_END
 }
