@@ -720,11 +720,16 @@ def run_poisson(args, world, rank, local):
     ctx.synchronize()
     t_train = time.perf_counter() - t_train
     ev = P.eval_preconditioner(n_rhs=2, mg_iters=10, seed=99)
-    methods = {"plain_mg": msbg.MG, "mg_pcg": msbg.PCG, "learned_pcg": msbg.LEARNED, "hybrid_pcg": msbg.HYBRID,
-               "learned_mg": msbg.LEARNED_MG}
-    head = "hybrid_pcg"
+    # (method, network lead applications for LEARNED_LEAD)
+    methods = {"plain_mg": (msbg.MG, 0), "mg_pcg": (msbg.PCG, 0), "learned_pcg": (msbg.LEARNED, 0),
+               "hybrid_pcg": (msbg.HYBRID, 0), "learned_mg": (msbg.LEARNED_MG, 0),
+               "lead1_pcg": (msbg.LEARNED_LEAD, 1), "lead2_pcg": (msbg.LEARNED_LEAD, 2),
+               "lead3_pcg": (msbg.LEARNED_LEAD, 3), "lead1_nopost_pcg": (msbg.LEARNED_LEAD, -1)}
+    head = "lead1_pcg"
 
-    def one(method):
+    def one(spec):
+        method, lead = spec
+        P.set_network_lead(lead)
         x.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -764,7 +769,8 @@ def run_poisson(args, world, rank, local):
                             "history": [float("%.3g" % v) for v in P.last_history[:12]]}
     # end to end through the C ABI with host arrays
     t = time.perf_counter()
-    _, it_h, rel_h, _ = P.solve(bh.reshape(-1), method=methods[head], tol=1e-6, max_iter=400)
+    P.set_network_lead(methods[head][1])
+    _, it_h, rel_h, _ = P.solve(bh.reshape(-1), method=methods[head][0], tol=1e-6, max_iter=400)
     learned = {"pairs": args.train_rhs * args.train_iters, "adam_steps": int(len(hist)), "train_s": t_train,
                "loss_first": float(np.mean(hist[:20])) if len(hist) else None,
                "loss_last": float(np.mean(hist[-20:])) if len(hist) else None,

@@ -292,6 +292,12 @@ int msbg_poisson_solve(msbg_poisson* p, int method, float* x, const float* b, do
  * V-cycle applications, network applications, the fallback reason (0 none,
  * 1 stall, 2 p.Ap <= 0, 3 r.z <= 0) and the iteration it happened at. */
 int msbg_poisson_set_preconditioner(msbg_poisson* p, msbg_unet* net);
+/* Method 5: flexible CG whose first |k| preconditioner applications are
+ * method 3's (V-cycle, network, V-cycle; without the last V-cycle for k < 0),
+ * after which CG restarts from the current iterate with the V-cycle
+ * preconditioner; k = 0 makes method 5 plain MG-preconditioned CG.
+ * Default 1. */
+int msbg_poisson_set_network_lead(msbg_poisson* p, int k);
 /* msbg_poisson_solve_device with the solution in FP64 (d_x: initial guess in,
  * solution out).  The f32 entry points round the FP64 solution on return; on
  * smooth right-hand sides that rounding alone can leave a relative residual

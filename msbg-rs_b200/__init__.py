@@ -18,7 +18,7 @@ from .particles import BucketPlan, bucket_indices, morton3, morton3_host, morton
 from .fluid import (MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend_device, particles_to_grid, particles_to_grid_device,
                     particles_to_grid_sorted_device)
 from .multires import downsample_channel_avg
-from .poisson import HYBRID, LEARNED, LEARNED_MG, MG, PCG, Poisson
+from .poisson import HYBRID, LEARNED, LEARNED_LEAD, LEARNED_MG, MG, PCG, Poisson
 from .learned import UNet
 from .batch import Batch
 
@@ -30,5 +30,5 @@ __all__ = [
     "BucketPlan", "bucket_indices", "morton3", "morton3_host", "morton_sort", "sort_block_list_morton",
     "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
     "particles_to_grid_device", "particles_to_grid_sorted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
-    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "UNet", "Batch",
+    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch",
 ]

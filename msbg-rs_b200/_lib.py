@@ -118,6 +118,7 @@ SIGNATURES = {
     "msbg_poisson_solve_device": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_solve": [_P, _I, _P, _P, C.c_double, _I, C.POINTER(_I), C.POINTER(C.c_double), _P],
     "msbg_poisson_set_preconditioner": [_P, _P],
+    "msbg_poisson_set_network_lead": [_P, _I],
     "msbg_poisson_autotune": [_P, _P, _SZ, _SZP],
     "msbg_batch_create": [_P, _I, _P, _P, _P, _P, _I, C.POINTER(_P)],
     "msbg_batch_destroy": [_P],

@@ -67,6 +67,8 @@ struct msbg_poisson {
     // PCG statistics of the last solve: preconditioner applications of each
     // kind and whether the learned preconditioner fell back to multigrid
     int n_net = 0, n_vcycle = 0, fell_back = 0, fallback_iter = -1;
+    int net_lead = 1;       // method 5: preconditioner applications that use the network
+    int net_lead_post = 1;  // method 5: those applications end with the post-smoothing V-cycle
     // Batched solves: independent problems stacked in one hierarchy (see
     // batch_build); each owns a contiguous range of level-0 blocks.
     int np = 0;
@@ -550,19 +552,22 @@ static void post_smooth(msbg_poisson* P, float* z, const float* r, float* s, flo
 
 // z = V r, then the network's correction of the remaining error,
 // z += N(r - A z), then post_smooth (V-cycle, network, V-cycle).
-static void learned_cycle(msbg_poisson* P, float* z, const float* r, float* s, float* u) {
+static void learned_cycle(msbg_poisson* P, float* z, const float* r, float* s, float* u, bool post = true) {
     const int64_t n = P->lv[0].cells();
     vcycle(P, 0, z, r, true);
     launch_residual(P, 0, z, r, s);
     unet_apply(P->net, s, u);
     axpby(P, n, 1.0, u, 1.0, z);
-    post_smooth(P, z, r, s, u);
+    if (post) post_smooth(P, z, r, s, u);
 }
 
 // method 0: V-cycles (x += V(b - A x)); 1: MG-preconditioned CG; 2: flexible
 // CG preconditioned by the learned network; 3: flexible CG preconditioned by
 // a V-cycle plus the network's correction of the V-cycle's remaining error,
-// z = V r + N(r - A V r).  Methods 2 and 3 fall back to the V-cycle
+// z = V r + N(r - A V r); 5: method 3's preconditioner for the first
+// net_lead applications (where the network removes most error per cost),
+// then CG restarted from the current iterate with V-cycles.  Methods 2, 3
+// and 5 fall back to the V-cycle
 // preconditioner (and restart) when the residual stalls (three iterations in
 // a row without a 5 % decrease) or a search direction loses positivity.  The
 // solution accumulates in FP64 and convergence is judged on the true
@@ -585,6 +590,7 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
     P->n_net = P->n_vcycle = P->fell_back = 0;
     P->fallback_iter = -1;
     if (method >= 2) MSBG_REQUIRE(P->net != nullptr, "learned preconditioner not set (msbg_poisson_set_preconditioner)");
+    if (method == 5 && P->net_lead <= 0) method = 1;
     const double bn = std::sqrt(dot(P, b, b, n));
     if (bn == 0.0) {
         if (x64_ext) CUDA_CHECK(cudaMemsetAsync(x64_ext, 0, n * 8, P->ctx->stream));
@@ -630,7 +636,8 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
         }
     } else {
         int pc = method == 1 ? PC_MG : (method == 2 ? PC_NET : PC_HYBRID);
-        const bool flexible = method >= 2;
+        bool flexible = method >= 2;
+        const int lead = method == 5 ? P->net_lead : -1;
         auto precondition = [&](const float* rr, float* zz) {
             if (pc == PC_MG) {
                 vcycle(P, 0, zz, rr, true);
@@ -641,8 +648,9 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                 P->n_net++;
                 P->n_vcycle++;
             } else {
-                learned_cycle(P, zz, rr, sv, uv);
-                P->n_vcycle += 2;
+                const bool post = !(lead > 0 && P->net_lead_post == 0);
+                learned_cycle(P, zz, rr, sv, uv, post);
+                P->n_vcycle += post ? 2 : 1;
                 P->n_net++;
             }
         };
@@ -696,6 +704,15 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
             // over a window: less than a halving in the last 4 iterations
             if (flexible && pc != PC_MG && since >= 4 && rn > 0.5 * rn_hist[rn_hist.size() - 5]) {
                 fall_back(1);
+                continue;
+            }
+            if (lead > 0 && pc == PC_HYBRID && P->n_net >= lead) {
+                // method 5: the lead is over; CG restarts from the current
+                // iterate with the fixed V-cycle preconditioner
+                pc = PC_MG;
+                flexible = false;
+                restart();
+                since = 0;
                 continue;
             }
             precondition(r, z);
@@ -1305,7 +1322,7 @@ int msbg_poisson_dot_device(msbg_poisson* P, const float* d_a, const float* d_b,
 int msbg_poisson_solve_device(msbg_poisson* P, int method, float* d_x, const float* d_b, double tol, int max_iter,
                               int* iters_out, double* rel_res_out, double* history) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
+    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 5 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     int it = solve(P, method, d_x, d_b, tol, max_iter, rel_res_out, history);
     if (iters_out) *iters_out = it;
@@ -1315,7 +1332,7 @@ int msbg_poisson_solve_device(msbg_poisson* P, int method, float* d_x, const flo
 int msbg_poisson_solve(msbg_poisson* P, int method, float* x, const float* b, double tol, int max_iter, int* iters_out,
                        double* rel_res_out, double* history) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(P && x && b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
+    MSBG_REQUIRE(P && x && b && method >= 0 && method <= 5 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     const int64_t n = P->lv[0].cells();
     DevBuf io;
@@ -1334,7 +1351,7 @@ int msbg_poisson_solve(msbg_poisson* P, int method, float* x, const float* b, do
 int msbg_poisson_solve_f64_device(msbg_poisson* P, int method, double* d_x, const float* d_b, double tol, int max_iter,
                                   int* iters_out, double* rel_res_out, double* history) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 4 && max_iter >= 0 && tol > 0.0, "bad argument");
+    MSBG_REQUIRE(P && d_x && d_b && method >= 0 && method <= 5 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     int it = solve(P, method, nullptr, d_b, tol, max_iter, rel_res_out, history, d_x);
     if (iters_out) *iters_out = it;
@@ -1349,6 +1366,14 @@ int msbg_poisson_set_preconditioner(msbg_poisson* P, msbg_unet* net) {
                      "the network must be built on the solve's level-0 blocks (16^3) and context");
     }
     P->net = net;
+    MSBG_API_END
+}
+
+int msbg_poisson_set_network_lead(msbg_poisson* P, int k) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P, "null argument");
+    P->net_lead = k >= 0 ? k : -k;
+    P->net_lead_post = k >= 0 ? 1 : 0;
     MSBG_API_END
 }
 

@@ -85,11 +85,13 @@ __global__ void un_input_kernel(int64_t n, const float* __restrict__ r, const do
     }
 }
 
-// Neighbour cell of level-0 cell `cell` (16^3 blocks) shifted by tap t, or -1.
-__device__ __forceinline__ int64_t l0_tap(const int32_t* __restrict__ nbr27, int64_t nb, int64_t cell, int t) {
-    const int64_t k = cell >> 12;
-    const int v = (int)(cell & 4095);
-    const int gx = (v & 15) + t % 3 - 1, gy = ((v >> 4) & 15) + (t / 3) % 3 - 1, gz = (v >> 8) + t / 9 - 1;
+// Level-0 halo staging: CTA (block k, octant o) covers the 8^3 cells of
+// octant o of block k; halo cell h in [0, 10^3) sits at in-block coordinate
+// octant origin - 1 + (h % 10, h / 10 % 10, h / 100), in the neighbouring
+// block across a face (nbr27) where it leaves the block; -1 where that block
+// is not in the set.
+__device__ __forceinline__ int64_t l0_halo_cell(const int32_t* __restrict__ nbr27, int64_t nb, int64_t k, int o, int h) {
+    const int gx = (o & 1) * 8 - 1 + h % 10, gy = ((o >> 1) & 1) * 8 - 1 + (h / 10) % 10, gz = (o >> 2) * 8 - 1 + h / 100;
     const int ox = gx < 0 ? 0 : (gx > 15 ? 2 : 1), oy = gy < 0 ? 0 : (gy > 15 ? 2 : 1), oz = gz < 0 ? 0 : (gz > 15 ? 2 : 1);
     const int code = ox + 3 * oy + 9 * oz;
     const int32_t kk = code == 13 ? (int32_t)k : nbr27[k * 27 + code];
@@ -98,57 +100,77 @@ __device__ __forceinline__ int64_t l0_tap(const int32_t* __restrict__ nbr27, int
 }
 
 // First layer on the CUDA cores: a0[c][o] = relu(b[o] + sum_t w[t][o][0] x[c + d(t)]),
-// 1 -> 16 channels (weights bf16 [27][16][16], input channel 0 only).
-__global__ void __launch_bounds__(128) un_conv_in1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
+// 1 -> 16 channels (weights bf16 [27][16][16], input channel 0 only).  One CTA
+// per (block, octant): the octant's 10^3 input halo in shared memory, one
+// thread per cell, taps in order t = 0..26 (fmaf).
+__global__ void __launch_bounds__(256) un_conv_in1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
                                                           const uint16_t* __restrict__ x0c, const uint16_t* __restrict__ w,
                                                           const float* __restrict__ bias, uint16_t* __restrict__ a0) {
     __shared__ float ws[27][16];
     __shared__ float bs[16];
+    __shared__ float xs[1000];
+    const int64_t k = blockIdx.x >> 3;
+    const int o = blockIdx.x & 7;
     for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16) * 16]);
     if (threadIdx.x < 16) bs[threadIdx.x] = bias[threadIdx.x];
+    for (int h = threadIdx.x; h < 1000; h += blockDim.x) {
+        const int64_t src = l0_halo_cell(nbr27, nb, k, o, h);
+        xs[h] = src >= 0 ? bf(__ldg(x0c + src)) : 0.0f;
+    }
     __syncthreads();
-    const int64_t n = nb << 12;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = threadIdx.x; c < 512; c += blockDim.x) {
+        const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
         float acc[16];
 #pragma unroll
-        for (int o = 0; o < 16; ++o) acc[o] = 0.0f;
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0f;
+#pragma unroll 3
         for (int t = 0; t < 27; ++t) {
-            const int64_t src = l0_tap(nbr27, nb, c, t);
-            const float xv = src >= 0 ? bf(__ldg(x0c + src)) : 0.0f;
+            const float xv = xs[((z + t / 9) * 10 + (y + (t / 3) % 3)) * 10 + (x + t % 3)];
 #pragma unroll
-            for (int o = 0; o < 16; ++o) acc[o] = fmaf(ws[t][o], xv, acc[o]);
+            for (int q = 0; q < 16; ++q) acc[q] = fmaf(ws[t][q], xv, acc[q]);
         }
 #pragma unroll
-        for (int o = 0; o < 16; ++o) acc[o] = fmaxf(acc[o] + bs[o], 0.0f);
-        uint4* out = reinterpret_cast<uint4*>(a0 + c * 16);
+        for (int q = 0; q < 16; ++q) acc[q] = fmaxf(acc[q] + bs[q], 0.0f);
+        const int64_t cell = (k << 12) + (((o & 1) * 8 + x) | ((((o >> 1) & 1) * 8 + y) << 4) | (((o >> 2) * 8 + z) << 8));
+        uint4* out = reinterpret_cast<uint4*>(a0 + cell * 16);
         out[0] = pack8(acc);
         out[1] = pack8(acc + 8);
     }
 }
 
 // Last layer on the CUDA cores: y[c] = b[0] + sum_t sum_i w[t][0][i] u[c + d(t)][i],
-// 16 -> 1 channel, f32 output.
-__global__ void __launch_bounds__(128) un_conv_out1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
+// 16 -> 1 channel, f32 output.  One CTA per (block, octant): the octant's
+// 10^3 halo of 16-channel rows in shared memory as two planes of 8 channels
+// (16-byte rows, conflict-free), one thread per cell.
+__global__ void __launch_bounds__(256) un_conv_out1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
                                                            const uint16_t* __restrict__ u0, const uint16_t* __restrict__ w,
                                                            const float* __restrict__ bias, float* __restrict__ y) {
     __shared__ float ws[27][16];
+    __shared__ uint4 us[2][1000];
+    const int64_t k = blockIdx.x >> 3;
+    const int o = blockIdx.x & 7;
     for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16)]);
+    for (int e = threadIdx.x; e < 2000; e += blockDim.x) {
+        const int h = e >> 1, half = e & 1;
+        const int64_t src = l0_halo_cell(nbr27, nb, k, o, h);
+        us[half][h] = src >= 0 ? __ldg(reinterpret_cast<const uint4*>(u0 + src * 16) + half) : make_uint4(0u, 0u, 0u, 0u);
+    }
     __syncthreads();
     const float b0 = bias[0];
-    const int64_t n = nb << 12;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = threadIdx.x; c < 512; c += blockDim.x) {
+        const int x = c & 7, yy = (c >> 3) & 7, z = c >> 6;
         float acc = 0.0f;
+#pragma unroll 3
         for (int t = 0; t < 27; ++t) {
-            const int64_t src = l0_tap(nbr27, nb, c, t);
-            if (src < 0) continue;
-            const uint4* row = reinterpret_cast<const uint4*>(u0 + src * 16);
+            const int h = ((z + t / 9) * 10 + (yy + (t / 3) % 3)) * 10 + (x + t % 3);
             float v[16];
-            unpack8(__ldg(row), v);
-            unpack8(__ldg(row + 1), v + 8);
+            unpack8(us[0][h], v);
+            unpack8(us[1][h], v + 8);
 #pragma unroll
             for (int i = 0; i < 16; ++i) acc = fmaf(ws[t][i], v[i], acc);
         }
-        y[c] = acc + b0;
+        const int64_t cell = (k << 12) + (((o & 1) * 8 + x) | ((((o >> 1) & 1) * 8 + yy) << 4) | (((o >> 2) * 8 + z) << 8));
+        y[cell] = acc + b0;
     }
 }
 
@@ -424,7 +446,7 @@ static void forward(msbg_unet* U) {
     {
         const ULayer& L = U->layers[L0A];
         begin_launch(U->ctx);
-        un_conv_in1_kernel<<<grid1(U->n[0], 128), 128, 0, U->ctx->stream>>>(
+        un_conv_in1_kernel<<<(unsigned)(U->nb * 8), 256, 0, U->ctx->stream>>>(
             U->nbr.as<int32_t>(), U->nb, U->x0c, U->wb.as<uint16_t>() + L.wb_off, U->params.as<float>() + L.b_off, U->a0);
         after_launch(U->ctx, "un_conv_in1_kernel");
     }
@@ -441,7 +463,7 @@ static void forward(msbg_unet* U) {
     {
         const ULayer& L = U->layers[L0C];
         begin_launch(U->ctx);
-        un_conv_out1_kernel<<<grid1(U->n[0], 128), 128, 0, U->ctx->stream>>>(
+        un_conv_out1_kernel<<<(unsigned)(U->nb * 8), 256, 0, U->ctx->stream>>>(
             U->nbr.as<int32_t>(), U->nb, U->u0, U->wb.as<uint16_t>() + L.wb_off, U->params.as<float>() + L.b_off, U->y);
         after_launch(U->ctx, "un_conv_out1_kernel");
     }

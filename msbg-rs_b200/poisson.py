@@ -14,7 +14,7 @@ import numpy as np
 from ._lib import call, ptr
 from .grid import Context
 
-MG, PCG, LEARNED, HYBRID, LEARNED_MG = 0, 1, 2, 3, 4
+MG, PCG, LEARNED, HYBRID, LEARNED_MG, LEARNED_LEAD = 0, 1, 2, 3, 4, 5
 
 
 class Poisson:
@@ -84,6 +84,12 @@ class Poisson:
         """Network for methods LEARNED (2) and HYBRID (3); None clears it."""
         self._net = net
         call("msbg_poisson_set_preconditioner", self.handle, net.handle if net is not None else None)
+
+    def set_network_lead(self, k: int) -> None:
+        """Method LEARNED_LEAD (5): the first |k| preconditioner applications
+        are HYBRID's (V-cycle, network, V-cycle; no last V-cycle for k < 0),
+        then CG restarts with plain V-cycles."""
+        call("msbg_poisson_set_network_lead", self.handle, int(k))
 
     def solve_stats(self) -> dict:
         """Preconditioner applications of the last solve and its fallback:

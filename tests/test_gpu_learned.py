@@ -48,10 +48,11 @@ def test_network_correction_beats_vcycle_alone(trained):
     assert ev["vcycle_plus_network"] < 0.9 * ev["vcycle"], ev
 
 
-@pytest.mark.parametrize("method", ["HYBRID", "LEARNED", "LEARNED_MG"])
+@pytest.mark.parametrize("method", ["HYBRID", "LEARNED", "LEARNED_MG", "LEARNED_LEAD"])
 def test_learned_solves_reach_tolerance(msbg, oracle, trained, method):
     import torch
     act, P, net, hist = trained
+    P.set_network_lead(2)
     b = torch.empty(P.n, device="cuda")
     P.rhs(b, seed=12345)
     x = torch.zeros(P.n, device="cuda", dtype=torch.float64)
@@ -88,3 +89,26 @@ def test_preconditioner_must_match_blocks(msbg, ctx):
         b = torch.ones(P.n, device="cuda")
         x = torch.zeros(P.n, device="cuda")
         P.solve_device(x, b, method=msbg.LEARNED)
+
+
+def test_network_lead_counts_and_restart(msbg, oracle, trained):
+    """LEARNED_LEAD applies the network exactly k times, then finishes with
+    V-cycles; k = 0 is plain MG-preconditioned CG (same iterations)."""
+    import torch
+    act, P, net, hist = trained
+    b = torch.empty(P.n, device="cuda")
+    P.rhs(b, seed=2024)
+    x = torch.zeros(P.n, device="cuda", dtype=torch.float64)
+    for k in (1, 3, -1):
+        x.zero_()
+        P.set_network_lead(k)
+        it, rel, h = P.solve_device(x, b, method=msbg.LEARNED_LEAD, tol=1e-6, max_iter=200)
+        st = P.solve_stats()
+        assert rel <= 1e-6 and st["network"] == abs(k), (k, st)
+        assert true_rel(oracle, act, x.cpu().numpy(), b.cpu().numpy().astype(np.float64)) <= 2e-6
+    x.zero_()
+    P.set_network_lead(0)
+    it0, rel0, _ = P.solve_device(x, b, method=msbg.LEARNED_LEAD, tol=1e-6, max_iter=200)
+    x.zero_()
+    it1, rel1, _ = P.solve_device(x, b, method=msbg.PCG, tol=1e-6, max_iter=200)
+    assert it0 == it1 and P.solve_stats()["network"] == 0
