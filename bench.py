@@ -327,7 +327,17 @@ def run_ours(args, world, rank, local):
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": traffic, "algorithmic_bytes_per_launch": per_launch, "launches": dom[1][0],
                 "avg_launch_us": round(dom[1][1] / dom[1][0] * 1e3, 2)}
-    sweep_k = kernels.get("sweep_phase_kernel")
+        ipu = INST_PER_UNIT.get(dom[0])
+        if ipu is not None:
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+            ach = ipu * n * dom[1][0] / (dom[1][1] * 1e-3) / 1e9
+            pk = 4.0 * sms * mhz * 1e6 / 1e9
+            roof["issue"] = {"inst_per_particle_per_launch": round(ipu, 1), "achieved_ginst_s": round(ach, 1),
+                             "peak_ginst_s": round(pk, 1), "frac": round(ach / pk, 4),
+                             "source": "warp instructions per particle from ncu at 128^3; peak = 4 per SM per clock "
+                                       "at the sampled SM clock"}
+    sweep_k = sweep_kernel_time(kernels)
     smoother = None
     if sweep_k:
         cells = n_fine * 4096 * SWEEPS * prof_steps
@@ -371,7 +381,7 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
     direction); 24 B written per face-cell of the active blocks for the
     combine; 12 B read + 12 B written per particle for G2P; 24 B per element
     per onesweep radix pass (3 passes per sort)."""
-    if kernel == "sweep_phase_kernel":
+    if kernel in SWEEP_KERNELS:
         return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
         return 28.0 * n * launches
@@ -388,10 +398,30 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
 
 # DRAM bytes (read + write) per launch measured by ncu on a smaller case of
 # the same kernel, per unit of work: p2g_cells_kernel at 128^3 (5,767,168
-# particles, one direction per launch) read 168.23 MB and wrote 4.79 MB
+# particles, one direction per launch) read 167.33 MB and wrote 4.32 MB
 # (profiles/p2g_cells_kernel_flip128.txt); traffic grows with the particle
 # count, so it is scaled by particles.
-TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (168.23e6 + 4.79e6) / 5767168}
+TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.33e6 + 4.32e6) / 5767168}
+
+# Warp instructions per unit of work from the same capture (688,348,057 per
+# launch at 128^3): the splat is bound by instruction issue, not by DRAM, so
+# its second roofline is issue slots (4 warp instructions per SM per clock).
+INST_PER_UNIT = {"p2g_cells_kernel": 688348057 / 5767168}
+
+
+# The smoother's sweep kernels (one of them runs, by element type and halo).
+SWEEP_KERNELS = ("sweep_compact_kernel", "sweep_pipe_kernel", "sweep_phase_kernel")
+
+
+def sweep_kernel_time(kern):
+    """(launches, ms) summed over the sweep kernels in a timing report, or None."""
+    hits = [kern[k] for k in SWEEP_KERNELS if k in kern]
+    return (sum(h[0] for h in hits), sum(h[1] for h in hits)) if hits else None
+
+
+def sweep_kernel_name(kern):
+    hits = [k for k in SWEEP_KERNELS if k in kern]
+    return "+".join(hits) if hits else "sweep_compact_kernel"
 
 
 def measured_traffic(kernel, n):
@@ -578,10 +608,10 @@ def run_smoother(args, world, rank, local):
     ms = _max_over_ranks(dist, ms, dev)
     cells = nb * 4096 * SWEEPS
     peak, peak_kind = load_peaks()
-    sk = kern.get("sweep_phase_kernel", (0, float("nan")))
+    sk = sweep_kernel_time(kern) or (0, float("nan"))
     k_ms = sk[1] / args.steps
     achieved = 8.0 * cells / (k_ms * 1e-3) / 1e9
-    roof = {"kernel": "sweep_phase_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+    roof = {"kernel": sweep_kernel_name(kern), "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": SWEEP_TRAFFIC_2048 if size == 2048 and stencil == 0 else None,
             "algorithmic_bytes_per_launch": 8.0 * cells / max(sk[0] / args.steps, 1),
@@ -592,7 +622,7 @@ def run_smoother(args, world, rank, local):
         if st == stencil:
             continue
         o_ms, o_k = timed(st, 2, 1)
-        ok = o_k.get("sweep_phase_kernel", (1, float("nan")))
+        ok = sweep_kernel_time(o_k) or (1, float("nan"))
         others[SMOOTHER_STENCILS[st]] = {"ms_per_10_sweeps": o_ms, "cell_updates_per_s": cells / (o_ms * 1e-3),
                                          "kernel_gbs_algorithmic": 8.0 * cells / (ok[1] / 2 * 1e-3) / 1e9}
     # weighted-Jacobi relaxation of the Poisson operator on the same blocks

@@ -655,14 +655,14 @@ template <int BSX> struct Compact {
 };
 
 // Issues the staging of an interior block (one-cell halo) in the compact layout.
-template <int BSX, int ST>
+template <int BSX, int ST, int NT = BSX * BSX>
 __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
     using CL = Compact<BSX>;
     constexpr int H = CL::H;
     constexpr int LG = Lg<BSX>::v;
     constexpr int N = BSX * BSX * BSX;
     constexpr int QR = BSX / 4;
-    constexpr int NT = BSX * BSX;
+    static_assert((N / 4) % NT == 0, "centre rows must split evenly over the threads");
     const float* payload = (const float*)a.payload;
     const int tid = threadIdx.x;
     const int c13 = nb[13];
@@ -860,8 +860,104 @@ __device__ __forceinline__ void compute_compact(const SweepArgs& a, const float*
     }
 }
 
+// Pairs of f32 in one 64-bit register and the paired IEEE single-precision
+// operations of sm_100 (each half rounded as the scalar operation).  The
+// stencil below feeds no paired product directly into a paired sum (the
+// code generator may fuse such a pair even with .rn); its products go to
+// explicit fused multiply-adds, as in the scalar form.
+__device__ __forceinline__ uint64_t sw_pack(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void sw_unpack(uint64_t v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t sw_add(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t sw_sub(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t sw_mul(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t sw_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ uint64_t sw_ld2(const float* p) { return *reinterpret_cast<const uint64_t*>(p); }
+
+// The 7-tap stencil over a block staged in the compact layout, two
+// x-columns per thread: thread (xp, y) walks columns x = 2 xp and x + 1 along
+// z with paired arithmetic, the same operations in the same order per cell
+// as compute_compact.  The pair's outer neighbours come from the block rows
+// or, at x = 0 and x + 1 = BSX - 1, from the x-halo columns.
+template <int BSX, bool CLAMP>
+__device__ __forceinline__ void compute_compact_pair(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+    using CL = Compact<BSX>;
+    constexpr int H = CL::H;
+    constexpr int RS = BSX, PL = H * BSX;
+    constexpr int N = BSX * BSX * BSX;
+    float* payload = (float*)a.payload;
+    const int xp = tid % (BSX / 2), y = tid / (BSX / 2), x = 2 * xp;
+    float* out = payload + (size_t)slot * N + x + y * BSX;
+    float* xo0 = x == 0 ? a.xface + ((size_t)slot * 2 + 0) * (BSX * BSX) + y : nullptr;
+    float* xo1 = x + 1 == BSX - 1 ? a.xface + ((size_t)slot * 2 + 1) * (BSX * BSX) + y : nullptr;
+    const int i0 = (1 * H + (y + 1)) * BSX + x;  // z = 0, column x
+    const float* lp = x > 0 ? h + i0 - 1 : h + CL::MAIN + 1 * CL::XP + 3 + (y + 1);
+    const float* rp = x + 2 < BSX ? h + i0 + 2 : h + CL::MAIN + CL::XS + 1 * CL::XP + 3 + (y + 1);
+    const int lsz = x > 0 ? PL : CL::XP, rsz = x + 2 < BSX ? PL : CL::XP;
+    const uint64_t m6 = sw_pack(-6.0f, -6.0f), half = sw_pack(0.5f, 0.5f), dt2 = sw_pack(a.dt, a.dt);
+    uint64_t zb = sw_ld2(h + i0 - PL), c = sw_ld2(h + i0), zf = sw_ld2(h + i0 + PL);
+#pragma unroll 4
+    for (int z = 0; z < BSX; ++z) {
+        const int i = i0 + z * PL;
+        float c0, c1;
+        sw_unpack(c, c0, c1);
+        const uint64_t lx = sw_pack(lp[z * lsz], c0), rx = sw_pack(c1, rp[z * rsz]);
+        const uint64_t dyu = sw_ld2(h + i - RS), dyd = sw_ld2(h + i + RS);
+        uint64_t nbs = sw_add(lx, rx);
+        nbs = sw_add(nbs, dyu);
+        nbs = sw_add(nbs, dyd);
+        nbs = sw_add(nbs, zb);
+        nbs = sw_add(nbs, zf);
+        const uint64_t lap = sw_fma(c, m6, nbs);
+        const uint64_t fx = sw_mul(sw_sub(rx, lx), half), fy = sw_mul(sw_sub(dyd, dyu), half), fz = sw_mul(sw_sub(zf, zb), half);
+        float s0, s1;
+        sw_unpack(sw_fma(fx, fx, sw_fma(fy, fy, sw_mul(fz, fz))), s0, s1);
+        const uint64_t g = sw_pack(sqrtf(s0), sqrtf(s1));
+        float n0, n1;
+        sw_unpack(sw_fma(sw_mul(dt2, lap), g, c), n0, n1);
+        if (CLAMP) {
+            n0 = clampf(n0, 0.0f, 1.0f);
+            n1 = clampf(n1, 0.0f, 1.0f);
+        }
+        *reinterpret_cast<float2*>(out + z * BSX * BSX) = make_float2(n0, n1);
+        if (xo0) xo0[z * BSX] = n0;
+        if (xo1) xo1[z * BSX] = n1;
+        zb = c;
+        c = zf;
+        if (z + 1 < BSX) zf = sw_ld2(h + i + 2 * PL);
+    }
+}
+
+// Threads of a compact-sweep CTA: the 7-tap stencil takes two columns per
+// thread, the 19-tap one a column.
+template <int BSX, int ST> struct CompactThreads {
+    static constexpr bool pair = ST == MSBG_LAPLACIAN && BSX >= 8;
+    static constexpr int v = pair ? BSX * BSX / 2 : BSX * BSX;
+};
+
 template <int BSX, int ST, bool CLAMP>
-__global__ void __launch_bounds__(BSX * BSX, BSX == 16 ? 4 : 1)
+__global__ void __launch_bounds__(CompactThreads<BSX, ST>::v, BSX == 16 ? 4 : 1)
 sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     using CL = Compact<BSX>;
     extern __shared__ float4 h4[];
@@ -882,19 +978,21 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     };
     meta(t, 0);
     __syncthreads();
-    if (flg[0] & 1) issue_compact<BSX, ST>(a, hb, nbs[0]);
+    constexpr int NT = CompactThreads<BSX, ST>::v;
+    if (flg[0] & 1) issue_compact<BSX, ST, NT>(a, hb, nbs[0]);
     cp_async_commit();
     for (int j = 0; t < n; t += gridDim.x, ++j) {
         const int b = j & 1, bn = b ^ 1;
         const int tn = t + gridDim.x;
         if (tn < n) meta(tn, bn);
         __syncthreads();  // nbs[bn] visible; every thread is done with buffer bn (the previous block)
-        if (tn < n && (flg[bn] & 1)) issue_compact<BSX, ST>(a, hb + bn * CL::BUF, nbs[bn]);
+        if (tn < n && (flg[bn] & 1)) issue_compact<BSX, ST, NT>(a, hb + bn * CL::BUF, nbs[bn]);
         cp_async_commit();
         if (flg[b] & 1) cp_async_wait<1>();  // this block's copies have landed
         else stage_general<ElemF32, BSX, ST, true>(a, hb + b * CL::BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
         __syncthreads();
-        compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
     }
     cp_async_wait<0>();
 }
@@ -943,7 +1041,7 @@ static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* ord
                                         (int)cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
-    const int threads = BSX * BSX;
+    const int threads = CompactThreads<BSX, ST>::v;
     int per_sm = 0;
     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_compact_kernel<BSX, ST, CLAMP>, threads, smem));
     int sms = 0;
@@ -951,7 +1049,7 @@ static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* ord
     const int grid = std::max(1, std::min(n, std::max(per_sm, 1) * sms));
     begin_launch(ctx);
     sweep_compact_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
-    after_launch(ctx, "sweep_phase_kernel");
+    after_launch(ctx, "sweep_compact_kernel");
 }
 
 template <class E, int BSX, int ST>
@@ -991,7 +1089,7 @@ static void launch_phase(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order
         const int grid = std::max(1, std::min(n, std::max(per_sm, 1) * sms));
         begin_launch(ctx);
         sweep_pipe_kernel<BSX, ST><<<(unsigned)grid, threads, 2 * smem, ctx->stream>>>(a, order, n);
-        after_launch(ctx, "sweep_phase_kernel");
+        after_launch(ctx, "sweep_pipe_kernel");
         return;
     }
     begin_launch(ctx);
