@@ -962,37 +962,65 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     using CL = Compact<BSX>;
     extern __shared__ float4 h4[];
     float* hb = reinterpret_cast<float*>(h4);
-    __shared__ int32_t nbs[2][27];
-    __shared__ int32_t flg[2], pis[2];
+    // block metadata in a ring of three slots: the neighbour codes and flags
+    // of block t + 2 g are loaded into registers while block t is computed
+    // and written to the ring after it, so their latency is hidden
+    __shared__ int32_t nbs[3][27];
+    __shared__ int32_t flg[3], pis[3];
     __shared__ int8_t ok[3][BSX + 2], dd[3][BSX + 2], ll[3][BSX + 2];
     const int tid = threadIdx.x, nthr = blockDim.x;
+    const int g = gridDim.x;
     int t = blockIdx.x;
     if (t >= n) return;
-    auto meta = [&](int tt, int b) {
-        const int pi = order[tt];
-        if (tid < 27) nbs[b][tid] = a.nbr[(size_t)pi * 27 + tid];
+    const bool meta_thread = tid < 27 || tid == nthr - 1;
+    auto load_meta = [&](int pi, int32_t& nbv, int32_t& flv) {
+        if (tid < 27) nbv = a.nbr[(size_t)pi * 27 + tid];
+        if (tid == nthr - 1) flv = a.bxyz[(size_t)pi * 4 + 3];
+    };
+    auto put_meta = [&](int sl, int pi, int32_t nbv, int32_t flv) {
+        if (tid < 27) nbs[sl][tid] = nbv;
         if (tid == nthr - 1) {
-            flg[b] = a.bxyz[(size_t)pi * 4 + 3];
-            pis[b] = pi;
+            flg[sl] = flv;
+            pis[sl] = pi;
         }
     };
-    meta(t, 0);
+    int pi2 = 0;
+    if (meta_thread) {
+        int32_t nbv = 0, flv = 0;
+        const int pi0 = order[t];
+        load_meta(pi0, nbv, flv);
+        put_meta(0, pi0, nbv, flv);
+        if (t + g < n) {
+            const int pi1 = order[t + g];
+            load_meta(pi1, nbv, flv);
+            put_meta(1, pi1, nbv, flv);
+        }
+        if (t + 2 * g < n) pi2 = order[t + 2 * g];
+    }
     __syncthreads();
     constexpr int NT = CompactThreads<BSX, ST>::v;
     if (flg[0] & 1) issue_compact<BSX, ST, NT>(a, hb, nbs[0]);
     cp_async_commit();
-    for (int j = 0; t < n; t += gridDim.x, ++j) {
+    for (int j = 0; t < n; t += g, ++j) {
+        const int sl = j % 3, sn = (j + 1) % 3, s2 = (j + 2) % 3;
         const int b = j & 1, bn = b ^ 1;
-        const int tn = t + gridDim.x;
-        if (tn < n) meta(tn, bn);
-        __syncthreads();  // nbs[bn] visible; every thread is done with buffer bn (the previous block)
-        if (tn < n && (flg[bn] & 1)) issue_compact<BSX, ST, NT>(a, hb + bn * CL::BUF, nbs[bn]);
+        const int tn = t + g, t2 = t + 2 * g, t3 = t + 3 * g;
+        int32_t nb2 = 0, fl2 = 0;
+        int pi3 = 0;
+        if (meta_thread) {
+            if (t2 < n) load_meta(pi2, nb2, fl2);
+            if (t3 < n) pi3 = order[t3];
+        }
+        __syncthreads();  // slot sn visible; every thread is done with buffer bn (the previous block)
+        if (tn < n && (flg[sn] & 1)) issue_compact<BSX, ST, NT>(a, hb + bn * CL::BUF, nbs[sn]);
         cp_async_commit();
-        if (flg[b] & 1) cp_async_wait<1>();  // this block's copies have landed
-        else stage_general<ElemF32, BSX, ST, true>(a, hb + b * CL::BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
+        if (flg[sl] & 1) cp_async_wait<1>();  // this block's copies have landed
+        else stage_general<ElemF32, BSX, ST, true>(a, hb + b * CL::BUF, nbs[sl], pis[sl], &ok[0][0], &dd[0][0], &ll[0][0]);
         __syncthreads();
-        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
-        else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
+        else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
+        if (meta_thread && t2 < n) put_meta(s2, pi2, nb2, fl2);
+        pi2 = pi3;
     }
     cp_async_wait<0>();
 }
