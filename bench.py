@@ -544,9 +544,9 @@ def _finish(dist):
 
 
 # DRAM bytes per launch of the 7-tap sweep phase on the 2048^3 shell (7,007
-# blocks per colour), mean of two ncu-captured launches of the pipelined kernel
-# (profiles/sweep_phase_kernel_shell2048.txt): 160.21 MB read + 76.05 MB written.
-SWEEP_TRAFFIC_2048 = 160.21e6 + 76.05e6
+# blocks per colour), mean of two ncu-captured launches of the compact kernel
+# (profiles/sweep_compact_kernel_shell2048.txt): 160.23 MB read + 74.49 MB written.
+SWEEP_TRAFFIC_2048 = 160.23e6 + 74.49e6
 
 SMOOTHER_STENCILS = {0: "7-tap laplacian", 1: "19-tap mean curvature", 2: "25-tap bilaplacian"}
 
