@@ -257,7 +257,10 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
     constexpr int NNB = WIN * WIN * WIN;  // tile offsets in [-M, M]^3
     constexpr int NR = (NNB + 31) / 32;   // of them per lane
-    constexpr int NP = (WIN + 1) / 2;    // face pairs
+    // Faces s = 1 .. WIN-1 in pairs; face 0 (offset -M-1) is inside a
+    // particle's footprint only when the particle sits exactly on a face
+    // plane, so it is evaluated alone, and only for such particles.
+    constexpr int NP = (WIN - 1) / 2;    // face pairs (2h+1, 2h+2)
     static_assert(WIN <= 7 && NUV <= 56, "lane and face bits must fit one u64");
     static_assert(NT < 0xffff, "tile indices must fit 16 bits");
     extern __shared__ double st[];       // [2][W^3]: mass, momentum; then per-warp particle slots
@@ -373,10 +376,9 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                 // face positions along F, in pairs: staging cell[F] + s - 1
                 uint64_t gf2[NP];
 #pragma unroll
-                for (int h = 0; h < NP; ++h) {
-                    const int s0 = 2 * h, s1 = 2 * h + 1 < WIN ? 2 * h + 1 : 2 * h;
-                    gf2[h] = f2_pack((float)(b0[F] - M + cell[F] + s0 - 1), (float)(b0[F] - M + cell[F] + s1 - 1));
-                }
+                for (int h = 0; h < NP; ++h)
+                    gf2[h] = f2_pack((float)(b0[F] - M + cell[F] + 2 * h), (float)(b0[F] - M + cell[F] + 2 * h + 1));
+                const float gf0 = (float)(b0[F] - M + cell[F] - 1);
                 double am[WIN], av[WIN];
 #pragma unroll
                 for (int s = 0; s < WIN; ++s) am[s] = av[s] = 0.0;
@@ -432,19 +434,31 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                         const uint64_t t = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
                         float w0, w1;
                         f2_unpack(t, w0, w1);
-                        w0 = ((fbits >> (2 * h)) & 1u) ? fmaxf(w0, 0.0f) : 0.0f;
-                        w1 = ((fbits >> (2 * h + 1)) & 1u) ? fmaxf(w1, 0.0f) : 0.0f;
+                        w0 = ((fbits >> (2 * h + 1)) & 1u) ? fmaxf(w0, 0.0f) : 0.0f;
+                        w1 = ((fbits >> (2 * h + 2)) & 1u) ? fmaxf(w1, 0.0f) : 0.0f;
                         uint64_t w = f2_pack(w0, w1);
                         w = f2_mul(f2_mul(w, w), w);
                         float tm0, tm1, tv0, tv1;
                         f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
                         f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
-                        am[2 * h] += (double)tm0;
-                        av[2 * h] += (double)tv0;
-                        if (2 * h + 1 < WIN) {
-                            am[2 * h + 1] += (double)tm1;
-                            av[2 * h + 1] += (double)tv1;
-                        }
+                        am[2 * h + 1] += (double)tm0;
+                        av[2 * h + 1] += (double)tv0;
+                        am[2 * h + 2] += (double)tm1;
+                        av[2 * h + 2] += (double)tv1;
+                    }
+                    if ((f_hi >> 24) & 1u) {  // face 0: the same for every lane of the warp
+                        const float df = gf0 - P.z;
+                        const float sq = df * df;
+                        float dist;
+                        if (DIR == 0) dist = sq + hoist0;
+                        else if (DIR == 1) dist = hoist1 + (hoist0 + sq);
+                        else dist = hoist1 + (sq + hoist0);
+                        const float df2 = (dist + df) + 0.25f;
+                        float w = 1.0f - df2 * inv_r2;
+                        w = (fbits & 1u) ? fmaxf(w, 0.0f) : 0.0f;
+                        w = (w * w) * w;
+                        am[0] += (double)(w * m_p);
+                        av[0] += (double)(w * scale_mom);
                     }
                   }
                 }
