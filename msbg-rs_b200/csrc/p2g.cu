@@ -63,32 +63,32 @@ __global__ void __launch_bounds__(256) p2g_combine_kernel(CombineArgs a) {
     constexpr int N = BSX * BSX * BSX;
     constexpr int LG = P2GLg<BSX>::v;
     __shared__ int32_t rank[27];
-    __shared__ int8_t order[27];
     const int j = blockIdx.x, dir = blockIdx.y;
     const uint64_t bid = a.active[j];
     const int64_t bx = (int64_t)(bid % a.nx), by = (int64_t)((bid / a.nx) % a.ny), bz = (int64_t)(bid / (a.nx * a.ny));
     if (threadIdx.x < 27) rank[threadIdx.x] = a.nbr_rank[(size_t)j * 27 + threadIdx.x];
-    if (threadIdx.x == 0) {
-        // Contributions are added in the colour order of the contributing
-        // particle block (the reference commits colour by colour).
-        int t = 0;
-        for (int c = 0; c < 8; ++c)
-            for (int d = 0; d < 27; ++d) {
-                const int64_t X = bx + d % 3 - 1, Y = by + (d / 3) % 3 - 1, Z = bz + d / 9 - 1;
-                if ((int)((X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2)) == c) order[t++] = (int8_t)d;
-            }
-    }
     __syncthreads();
+    const int px = (int)(bx & 1), py = (int)(by & 1), pz = (int)(bz & 1);
     const int32_t slot = a.slots[j];
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         const int lx = i & (BSX - 1), ly = (i >> LG) & (BSX - 1), lz = i >> (2 * LG);
+        // Contributions are added in the colour order of the contributing
+        // particle block (the reference commits colour by colour).  A face
+        // lies in the window of the block itself and, along each axis, of at
+        // most one neighbour (-1 within M of the low side, +1 within M of
+        // the high side; 2M <= bsx), and the two differ in parity, so each
+        // colour names at most one contributing block.
+        const int ex = lx < M ? -1 : (lx >= BSX - M ? 1 : 0);
+        const int ey = ly < M ? -1 : (ly >= BSX - M ? 1 : 0);
+        const int ez = lz < M ? -1 : (lz >= BSX - M ? 1 : 0);
         double sm = 0.0, sv = 0.0;
-        for (int t = 0; t < 27; ++t) {
-            const int d = order[t];
-            const int r = rank[d];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int ox = (c & 1) == px ? 0 : ex, oy = ((c >> 1) & 1) == py ? 0 : ey, oz = ((c >> 2) & 1) == pz ? 0 : ez;
+            if (((c & 1) != px && !ex) || (((c >> 1) & 1) != py && !ey) || (((c >> 2) & 1) != pz && !ez)) continue;
+            const int r = rank[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
             if (r < 0) continue;
-            const int sx = lx - BSX * (d % 3 - 1) + M, sy = ly - BSX * ((d / 3) % 3 - 1) + M, sz = lz - BSX * (d / 9 - 1) + M;
-            if (sx < 0 || sy < 0 || sz < 0 || sx >= W || sy >= W || sz >= W) continue;
+            const int sx = lx - BSX * ox + M, sy = ly - BSX * oy + M, sz = lz - BSX * oz + M;
             const double* p = a.partial + ((size_t)r * 3 + dir) * 2 * WW + (sz * W + sy) * W + sx;
             sm += p[0];
             sv += p[WW];
