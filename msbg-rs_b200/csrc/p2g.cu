@@ -192,6 +192,12 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
     }
 }
 
+// Particles a splat warp stages at once (two float4 each): a whole typical
+// tile where the FP64 window leaves room in shared memory, 32 otherwise.
+template <int BSX, int M> struct SplatCap {
+    static constexpr int v = 2 * 8 * (BSX + 2 * M) * (BSX + 2 * M) * (BSX + 2 * M) <= 131072 ? 128 : 32;
+};
+
 // Warps of a splat CTA.  Tiles wait for their overlapping predecessors, so
 // more warps mostly wait longer; 20 (one CTA per SM, up to 96 registers a
 // thread) measured fastest on B200 among 16, 20, 24 and 32.
@@ -256,6 +262,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     constexpr int Q = (NUV + 31) / 32;   // lane rounds
     constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
     constexpr int NNB = WIN * WIN * WIN;  // tile offsets in [-M, M]^3
+    constexpr int CAP = SplatCap<BSX, M>::v;
     constexpr int NR = (NNB + 31) / 32;   // of them per lane
     // Faces s = 1 .. WIN-1 in pairs; face 0 (offset -M-1) is inside a
     // particle's footprint only when the particle sits exactly on a face
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     __shared__ uint32_t s_next;
     const int k_pb = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31;
-    float4* wslot = reinterpret_cast<float4*>(st + 2 * WW) + (size_t)(tid >> 5) * 64;  // [64] float4 per warp
+    float4* wslot = reinterpret_cast<float4*>(st + 2 * WW) + (size_t)(tid >> 5) * 2 * SplatCap<BSX, M>::v;
     for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
     for (int t = tid; t < NT; t += blockDim.x) {
         s_done[t] = 0;
@@ -355,6 +362,8 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
             __threadfence_block();
             deps_pending = false;
         };
+        const int e_tile = (int)__reduce_max_sync(0xffffffffu, lane < 8 ? (uint32_t)cend : 0u);
+        int st_lo = 0, st_hi = 0;  // the particles held by the warp's staging slots
         for (int sub = 0; sub < 8; ++sub) {
             // cells of a tile have overlapping face windows: order this
             // cell's shared-memory updates after the previous cell's across
@@ -382,24 +391,34 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                 double am[WIN], av[WIN];
 #pragma unroll
                 for (int s = 0; s < WIN; ++s) am[s] = av[s] = 0.0;
-                // the cell's particles, 32 at a time: one coalesced load per
-                // lane into the warp's staging slots, then broadcast reads
-                for (int p0 = b; p0 < e; p0 += 32) {
-                  const int cnt = min(32, e - p0);
-                  __syncwarp();
-                  if (lane < cnt) {
-                      const int pl = p0 + lane;
-                      const uint64_t f = lmask[pl];
-                      const float m = a.pm[pl];
-                      const float pc[3] = {a.px[pl] - 0.5f, a.py[pl] - 0.5f, a.pz[pl] - 0.5f};
-                      wslot[lane] = make_float4(pc[U], pc[V], pc[F], m);
-                      wslot[32 + lane] = make_float4(m * pv[pl], __uint_as_float((uint32_t)f),
-                                                     __uint_as_float((uint32_t)(f >> 32)), 0.0f);
+                // the cell's particles from the warp's staging slots, which
+                // hold up to CAP consecutive particles of the tile (the 8 cells
+                // of a tile are one contiguous range of the sorted order):
+                // staged with coalesced loads, CAP / 32 per lane, then read by
+                // broadcast
+                for (int p0 = b; p0 < e;) {
+                  if (p0 < st_lo || p0 >= st_hi) {
+                      __syncwarp();
+                      st_lo = p0;
+                      st_hi = min(p0 + CAP, e_tile);
+#pragma unroll
+                      for (int k = 0; k < CAP / 32; ++k) {
+                          const int pl = st_lo + lane + 32 * k;
+                          if (pl < st_hi) {
+                              const uint64_t f = lmask[pl];
+                              const float m = a.pm[pl];
+                              const float pc[3] = {a.px[pl] - 0.5f, a.py[pl] - 0.5f, a.pz[pl] - 0.5f};
+                              wslot[pl - st_lo] = make_float4(pc[U], pc[V], pc[F], m);
+                              wslot[CAP + pl - st_lo] = make_float4(m * pv[pl], __uint_as_float((uint32_t)f),
+                                                                    __uint_as_float((uint32_t)(f >> 32)), 0.0f);
+                          }
+                      }
+                      __syncwarp();
                   }
-                  __syncwarp();
-                  for (int j = 0; j < cnt; ++j) {
-                    const float4 P = wslot[j];        // U, V, F coordinates (minus 0.5), mass
-                    const float4 R = wslot[32 + j];   // momentum, lane bits (low, high)
+                  const int pend = min(e, st_hi);
+                  for (int j = p0; j < pend; ++j) {
+                    const float4 P = wslot[j - st_lo];        // U, V, F coordinates (minus 0.5), mass
+                    const float4 R = wslot[CAP + j - st_lo];  // momentum, lane bits (low, high)
                     const uint32_t f_lo = __float_as_uint(R.y), f_hi = __float_as_uint(R.z);
                     // bit s: face s inside the footprint, none when the lane's
                     // row is outside it (no branch: the warp stays converged,
@@ -461,6 +480,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                         av[0] += (double)(w * scale_mom);
                     }
                   }
+                  p0 = pend;
                 }
                 if (deps_pending) wait_deps();
                 if (on) {
@@ -547,7 +567,7 @@ static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     constexpr int W = BSX + 2 * M;
     constexpr int T = BSX / 2, NT = T * T * T;
     constexpr int WARPS = NT < kSplatWarps ? NT : kSplatWarps;
-    const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 64 * sizeof(float4);
+    const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 2 * SplatCap<BSX, M>::v * sizeof(float4);
     static bool attr = false;
     if (!attr) {
         CUDA_CHECK(cudaFuncSetAttribute(p2g_cells_kernel<BSX, M, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
