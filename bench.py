@@ -440,15 +440,15 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
 
 # DRAM bytes (read + write) per launch measured by ncu on a smaller case of
 # the same kernel, per unit of work: p2g_cells_kernel at 128^3 (5,767,168
-# particles, one direction per launch) read 167.33 MB and wrote 4.32 MB
+# particles, one direction per launch) read 167.28 MB and wrote 3.96 MB
 # (profiles/p2g_cells_kernel_flip128.txt); traffic grows with the particle
 # count, so it is scaled by particles.
-TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.33e6 + 4.32e6) / 5767168}
+TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.28e6 + 3.96e6) / 5767168}
 
-# Warp instructions per unit of work from the same capture (688,348,057 per
+# Warp instructions per unit of work from the same capture (575,950,823 per
 # launch at 128^3): the splat is bound by instruction issue, not by DRAM, so
 # its second roofline is issue slots (4 warp instructions per SM per clock).
-INST_PER_UNIT = {"p2g_cells_kernel": 688348057 / 5767168}
+INST_PER_UNIT = {"p2g_cells_kernel": 575950823 / 5767168}
 
 
 # The smoother's sweep kernels (one of them runs, by element type and halo).
