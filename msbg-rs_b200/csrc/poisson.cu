@@ -174,6 +174,64 @@ __global__ void pk_jacobi(LevelArgs L, const float* __restrict__ x, const float*
     }
 }
 
+// The 7-point kernels on 16^3 blocks, one CTA per block: thread (x, y) walks
+// its z-column with the planes below and above in registers (the next one
+// prefetched), the current plane and its x/y halo from the face neighbours
+// in shared memory.  Each value of x is read once (plus the block's halo
+// faces), coalesced.  The neighbour sum adds x-1, x+1, y-1, y+1, z-1, z+1 in
+// that order, zeros outside the active blocks, as nb_sum.
+// OP 0: weighted Jacobi xn = w (b + s nb) / (6 s) + (1 - w) x (x null: the
+// first sweep from zero); 1: residual r = b - s (6 x - nb); 2: y = s (6 x - nb).
+template <int OP>
+__global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __restrict__ x, const float* __restrict__ b,
+                                                  float* __restrict__ out, float omega) {
+    __shared__ float pl[18][18];
+    __shared__ int32_t nb[6];
+    const int64_t k = blockIdx.x;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int col = tx + (ty << 4);
+    const int64_t base = k << 12;
+    const float inv_d = 1.0f / (6.0f * L.scale);
+    if (OP == 0 && !x) {
+        for (int z = 0; z < 16; ++z) out[base + col + (z << 8)] = omega * b[base + col + (z << 8)] * inv_d;
+        return;
+    }
+    if (threadIdx.x < 6) nb[threadIdx.x] = L.nbr[k * 6 + threadIdx.x];
+    __syncthreads();
+    const int32_t nxm = nb[0], nxp = nb[1], nym = nb[2], nyp = nb[3], nzm = nb[4], nzp = nb[5];
+    const float* xb = x + base;
+    auto plane = [&](int z) -> float {  // this column's value at plane z in [-1, 16]
+        if (z < 0) return nzm >= 0 ? x[((int64_t)nzm << 12) + col + (15 << 8)] : 0.0f;
+        if (z > 15) return nzp >= 0 ? x[((int64_t)nzp << 12) + col] : 0.0f;
+        return xb[col + (z << 8)];
+    };
+    float down = plane(-1), cur = plane(0), up = plane(1);
+    for (int z = 0; z < 16; ++z) {
+        const float upn = z + 2 <= 16 ? plane(z + 2) : 0.0f;
+        const float bz = OP == 2 ? 0.0f : b[base + col + (z << 8)];
+        pl[ty + 1][tx + 1] = cur;
+        if (tx == 0) pl[ty + 1][0] = nxm >= 0 ? x[((int64_t)nxm << 12) + 15 + (ty << 4) + (z << 8)] : 0.0f;
+        if (tx == 15) pl[ty + 1][17] = nxp >= 0 ? x[((int64_t)nxp << 12) + (ty << 4) + (z << 8)] : 0.0f;
+        if (ty == 0) pl[0][tx + 1] = nym >= 0 ? x[((int64_t)nym << 12) + tx + (15 << 4) + (z << 8)] : 0.0f;
+        if (ty == 15) pl[17][tx + 1] = nyp >= 0 ? x[((int64_t)nyp << 12) + tx + (z << 8)] : 0.0f;
+        __syncthreads();
+        float sn = pl[ty + 1][tx];
+        sn += pl[ty + 1][tx + 2];
+        sn += pl[ty][tx + 1];
+        sn += pl[ty + 2][tx + 1];
+        sn += down;
+        sn += up;
+        const int64_t i = base + col + (z << 8);
+        if (OP == 0) out[i] = omega * (bz + L.scale * sn) * inv_d + (1.0f - omega) * cur;
+        else if (OP == 1) out[i] = bz - L.scale * (6.0f * cur - sn);
+        else out[i] = L.scale * (6.0f * cur - sn);
+        __syncthreads();
+        down = cur;
+        cur = up;
+        up = upn;
+    }
+}
+
 // Restriction: coarse cell = 1/8 of the sum of its (up to 8) active children.
 // Children are visited in z-major order of their offset.
 struct TransferArgs {
@@ -451,6 +509,11 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
 static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
+    if (L.lg == 4) {
+        pk_block16<2><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), x, nullptr, y, 0.0f);
+        after_launch(P->ctx, "pk_block16_matvec");
+        return;
+    }
     pk_matvec<<<grid_for(L.cells()), 256, 0, P->ctx->stream>>>(level_args(L), x, y);
     after_launch(P->ctx, "pk_matvec");
 }
@@ -458,6 +521,11 @@ static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
 static void launch_residual(msbg_poisson* P, int l, const float* x, const float* b, float* r) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
+    if (L.lg == 4) {
+        pk_block16<1><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), x, b, r, 0.0f);
+        after_launch(P->ctx, "pk_block16_residual");
+        return;
+    }
     pk_residual<<<shape_grid(L.cfg_res, L.cells()), kShapes[L.cfg_res].threads, 0, P->ctx->stream>>>(level_args(L), x, b, r);
     after_launch(P->ctx, "pk_residual");
 }
@@ -471,6 +539,12 @@ static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps,
         const float* src = (s % 2 == 0) ? x : t;
         float* dst = (s % 2 == 0) ? t : x;
         begin_launch(P->ctx);
+        if (L.lg == 4) {
+            pk_block16<0><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), (s == 0 && x_zero) ? nullptr : src, b,
+                                                                        dst, omega);
+            after_launch(P->ctx, "pk_block16_jacobi");
+            continue;
+        }
         pk_jacobi<<<shape_grid(L.cfg_jac, L.cells()), kShapes[L.cfg_jac].threads, 0, P->ctx->stream>>>(
             level_args(L), (s == 0 && x_zero) ? nullptr : src, b, dst, omega);
         after_launch(P->ctx, "pk_jacobi");
