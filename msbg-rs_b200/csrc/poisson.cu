@@ -77,6 +77,19 @@ struct msbg_poisson {
     msbg::DevBuf d_blk_prob;           // int32 [level-0 blocks] problem of each block
     msbg::DevBuf bpart;                // f64 [level-0 blocks] per-block dot partials
     msbg::DevBuf scal;                 // f64 [np][16] per-problem scalars
+    // Captured V-cycles of the single-problem solve, one per (x, b) pair: a
+    // V-cycle is some 40 small launches, which one graph launch replaces.
+    struct VGraph {
+        float* x;
+        const float* b;
+        cudaGraphExec_t exec;
+        int kernels;
+    };
+    std::vector<VGraph> vgraphs;
+    ~msbg_poisson() {
+        for (auto& g : vgraphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
 };
 
 namespace msbg {
@@ -174,26 +187,29 @@ __global__ void pk_jacobi(LevelArgs L, const float* __restrict__ x, const float*
     }
 }
 
-// The 7-point kernels on 16^3 blocks, one CTA per block: thread (x, y) walks
-// its z-column with the planes below and above in registers (the next one
-// prefetched), the current plane and its x/y halo from the face neighbours
-// in shared memory.  Each value of x is read once (plus the block's halo
+// The 7-point kernels on 16^3 blocks, one CTA per slab of kB16Slab z-planes
+// of a block: thread (x, y) walks its z-column with the planes below and
+// above in registers (the next one prefetched), the current plane and its x/y
+// halo from the face neighbours in shared memory.  Each value of x is read once (plus the block's halo
 // faces), coalesced.  The neighbour sum adds x-1, x+1, y-1, y+1, z-1, z+1 in
 // that order, zeros outside the active blocks, as nb_sum.
 // OP 0: weighted Jacobi xn = w (b + s nb) / (6 s) + (1 - w) x (x null: the
 // first sweep from zero); 1: residual r = b - s (6 x - nb); 2: y = s (6 x - nb).
+constexpr int kB16Slab = 4;  // z-planes per CTA (shorter dependent chains, more CTAs)
+
 template <int OP>
 __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __restrict__ x, const float* __restrict__ b,
                                                   float* __restrict__ out, float omega) {
     __shared__ float pl[18][18];
     __shared__ int32_t nb[6];
-    const int64_t k = blockIdx.x;
+    const int64_t k = blockIdx.x / (16 / kB16Slab);
+    const int z0 = (int)(blockIdx.x % (16 / kB16Slab)) * kB16Slab;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int col = tx + (ty << 4);
     const int64_t base = k << 12;
     const float inv_d = 1.0f / (6.0f * L.scale);
     if (OP == 0 && !x) {
-        for (int z = 0; z < 16; ++z) out[base + col + (z << 8)] = omega * b[base + col + (z << 8)] * inv_d;
+        for (int z = z0; z < z0 + kB16Slab; ++z) out[base + col + (z << 8)] = omega * b[base + col + (z << 8)] * inv_d;
         return;
     }
     if (threadIdx.x < 6) nb[threadIdx.x] = L.nbr[k * 6 + threadIdx.x];
@@ -205,8 +221,8 @@ __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __re
         if (z > 15) return nzp >= 0 ? x[((int64_t)nzp << 12) + col] : 0.0f;
         return xb[col + (z << 8)];
     };
-    float down = plane(-1), cur = plane(0), up = plane(1);
-    for (int z = 0; z < 16; ++z) {
+    float down = plane(z0 - 1), cur = plane(z0), up = plane(z0 + 1);
+    for (int z = z0; z < z0 + kB16Slab; ++z) {
         const float upn = z + 2 <= 16 ? plane(z + 2) : 0.0f;
         const float bz = OP == 2 ? 0.0f : b[base + col + (z << 8)];
         pl[ty + 1][tx + 1] = cur;
@@ -510,7 +526,7 @@ static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
     if (L.lg == 4) {
-        pk_block16<2><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), x, nullptr, y, 0.0f);
+        pk_block16<2><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), x, nullptr, y, 0.0f);
         after_launch(P->ctx, "pk_block16_matvec");
         return;
     }
@@ -522,7 +538,7 @@ static void launch_residual(msbg_poisson* P, int l, const float* x, const float*
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
     if (L.lg == 4) {
-        pk_block16<1><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), x, b, r, 0.0f);
+        pk_block16<1><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), x, b, r, 0.0f);
         after_launch(P->ctx, "pk_block16_residual");
         return;
     }
@@ -540,7 +556,7 @@ static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps,
         float* dst = (s % 2 == 0) ? t : x;
         begin_launch(P->ctx);
         if (L.lg == 4) {
-            pk_block16<0><<<(unsigned)L.n(), 256, 0, P->ctx->stream>>>(level_args(L), (s == 0 && x_zero) ? nullptr : src, b,
+            pk_block16<0><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), (s == 0 && x_zero) ? nullptr : src, b,
                                                                         dst, omega);
             after_launch(P->ctx, "pk_block16_jacobi");
             continue;
@@ -610,6 +626,43 @@ static void add64(msbg_poisson* P, int64_t n, double a, const float* d, double* 
     after_launch(P->ctx, "pk_add64");
 }
 
+// A V-cycle from level 0 with x = 0 on entry, launched as a captured graph
+// (captured on the first use of each (x, b) pair).  With per-kernel timing
+// on, the launches go to the stream one by one so that each is timed.
+static void vcycle_top(msbg_poisson* P, float* x, const float* b) {
+    msbg_ctx* ctx = P->ctx;
+    if (ctx->timing) {
+        vcycle(P, 0, x, b, true);
+        return;
+    }
+    msbg_poisson::VGraph* g = nullptr;
+    for (auto& v : P->vgraphs)
+        if (v.x == x && v.b == b) g = &v;
+    if (!g) {
+        const uint64_t l0 = ctx->launches;
+        cudaGraph_t graph = nullptr;
+        CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            vcycle(P, 0, x, b, true);
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            ctx->launches = l0;
+            throw;
+        }
+        CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &graph));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) MSBG_THROW(MSBG_ERR_CUDA, std::string("V-cycle graph: ") + cudaGetErrorString(e));
+        P->vgraphs.push_back({x, b, exec, (int)(ctx->launches - l0)});
+        ctx->launches = l0;
+        g = &P->vgraphs.back();
+    }
+    CUDA_CHECK(cudaGraphLaunch(g->exec, ctx->stream));
+    ctx->launches += (uint64_t)g->kernels;
+}
+
 // Preconditioners of the CG solve.
 enum { PC_MG = 0, PC_NET = 1, PC_HYBRID = 2 };
 
@@ -620,7 +673,7 @@ enum { PC_MG = 0, PC_NET = 1, PC_HYBRID = 2 };
 static void post_smooth(msbg_poisson* P, float* z, const float* r, float* s, float* u) {
     const int64_t n = P->lv[0].cells();
     launch_residual(P, 0, z, r, s);
-    vcycle(P, 0, u, s, true);
+    vcycle_top(P, u, s);
     axpby(P, n, 1.0, u, 1.0, z);
 }
 
@@ -628,7 +681,7 @@ static void post_smooth(msbg_poisson* P, float* z, const float* r, float* s, flo
 // z += N(r - A z), then post_smooth (V-cycle, network, V-cycle).
 static void learned_cycle(msbg_poisson* P, float* z, const float* r, float* s, float* u, bool post = true) {
     const int64_t n = P->lv[0].cells();
-    vcycle(P, 0, z, r, true);
+    vcycle_top(P, z, r);
     launch_residual(P, 0, z, r, s);
     unet_apply(P->net, s, u);
     axpby(P, n, 1.0, u, 1.0, z);
@@ -692,7 +745,7 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                 P->n_net++;
                 P->n_vcycle++;
             } else {
-                vcycle(P, 0, z, r, true);
+                vcycle_top(P, z, r);
             }
             P->n_vcycle++;
             add64(P, n, 1.0, z, x64);
@@ -714,7 +767,7 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
         const int lead = method == 5 ? P->net_lead : -1;
         auto precondition = [&](const float* rr, float* zz) {
             if (pc == PC_MG) {
-                vcycle(P, 0, zz, rr, true);
+                vcycle_top(P, zz, rr);
                 P->n_vcycle++;
             } else if (pc == PC_NET) {
                 unet_apply(P->net, rr, zz);
