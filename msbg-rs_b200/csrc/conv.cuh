@@ -46,7 +46,4 @@ void conv3_forward(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const u
 void conv3_wgrad(msbg_ctx* ctx, const ConvLevel& L, int cin, int cout, const uint16_t* x, const uint16_t* dy, float* dw,
                  bool acc);
 
-// Device status word check after a synchronisation: throws MSBG_ERR_TIMEOUT
-// when a bounded wait inside a kernel gave up.
-
 }  // namespace msbg
