@@ -11,10 +11,16 @@
 // Convolution:  y[c][o] = b[o] + sum_t sum_i w[t][o][i] x[c + d(t)][i],
 //   t = (dx+1) + 3 (dy+1) + 9 (dz+1), weights bf16 [27][Cout][Cin].
 // Forward and the data gradient (the same convolution with the taps
-// mirrored and Cin/Cout swapped) run as conv3_fwd_kernel: one CTA computes
-// a tile of 128 output cells x Cout in TMEM; per tap its threads gather the
-// shifted input rows into a K-major operand and the weights into a K-major
-// operand in shared memory (three stages), one thread issues Cin/16 MMAs and
+// mirrored and Cin/Cout swapped) run on 8^3 blocks with Cin, Cout <= 32 as
+// conv3_b8_kernel: persistent CTAs copy each block's 10^3 input halo into
+// shared memory once (double-buffered) and the weights of all taps once;
+// every tap's operand for one z-plane of the block is a strided view of the
+// halo, so the MMAs (M = 64 cells of a plane) need no per-tap staging, and
+// eight warps issue the eight planes' MMAs side by side.  Other shapes run as
+// conv3_fwd_kernel: one CTA computes a tile of 128 output cells x Cout in
+// TMEM; per tap its threads gather the shifted input rows (cp.async,
+// several taps in flight) into a K-major operand and the weights into a
+// K-major operand in shared memory, one thread issues Cin/16 MMAs and
 // commits them to the stage's mbarrier.  The weight gradient
 //   dw[t][o][i] = sum_c x[c + d(t)][i] dy[c][o]
 // runs as conv3_wgrad_kernel: M = the (tap, Cin) pairs in tiles of 128,

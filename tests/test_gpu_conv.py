@@ -19,6 +19,10 @@ CASES = [
     (8, 2, 0.55, 64, 64),
     (7, 2, 0.5, 64, 32),
     (4, 4, 0.7, 16, 16),
+    (4, 3, 0.6, 32, 64),
+    (4, 3, 0.6, 64, 16),
+    (4, 3, 0.7, 16, 64),
+    (4, 3, 0.6, 64, 32),
 ]
 
 
