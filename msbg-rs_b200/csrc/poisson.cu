@@ -351,6 +351,62 @@ __global__ void pk_axpby(int64_t n, float a, const float* __restrict__ x, float 
         y[i] = a * x[i] + b * y[i];
 }
 
+// CG scalars kept on the device between kernels (one host read per iteration):
+// sc[SC_RZ] = r.z, sc[SC_PQ] = p.Ap, sc[SC_ALPHA], sc[SC_RR] = r.r,
+// sc[SC_RZ2] = the new r.z, sc[SC_ZR] = z.r_old (flexible CG), sc[SC_BETA],
+// sc[SC_BAD] != 0 when p.Ap <= 0 or r.z is not finite (the updates below are
+// then skipped and the host restarts or stops).
+enum { SC_RZ, SC_PQ, SC_ALPHA, SC_RR, SC_RZ2, SC_ZR, SC_BETA, SC_BAD, SC_COUNT };
+
+// Stage 2 of p.Ap (the same tree as pk_dot_final), then alpha = r.z / p.Ap.
+__global__ void __launch_bounds__(DOT_THREADS) pk_dot_final_alpha(const double* __restrict__ partial, int np,
+                                                                   double* __restrict__ sc) {
+    __shared__ double sm[DOT_THREADS];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += DOT_THREADS) s += partial[i];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = DOT_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double pq = sm[0], rz = sc[SC_RZ];
+        const bool bad = !(pq > 0.0) || !isfinite(rz);
+        sc[SC_PQ] = pq;
+        sc[SC_BAD] = bad ? 1.0 : 0.0;
+        sc[SC_ALPHA] = bad ? 0.0 : rz / pq;
+    }
+}
+
+// x += alpha p (FP64) and r = (-alpha) q + r (f32) as fused multiply-adds,
+// skipped on breakdown.
+__global__ void pk_cg_update(int64_t n, const double* __restrict__ sc, const float* __restrict__ p,
+                             const float* __restrict__ q, double* __restrict__ x, float* __restrict__ r) {
+    if (sc[SC_BAD] != 0.0) return;
+    const double a = sc[SC_ALPHA];
+    const float na = (float)-a;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = fma(a, (double)p[i], x[i]);
+        r[i] = fmaf(na, q[i], r[i]);
+    }
+}
+
+// beta = r.z_new / r.z (or (r.z_new - z.r_old) / r.z for flexible CG); r.z = r.z_new.
+__global__ void pk_cg_beta(double* __restrict__ sc, int flexible) {
+    const double rz2 = sc[SC_RZ2];
+    sc[SC_BETA] = flexible ? (rz2 - sc[SC_ZR]) / sc[SC_RZ] : rz2 / sc[SC_RZ];
+    sc[SC_RZ] = rz2;
+}
+
+// p = z + beta p (f32; beta from the device; the product rounded, then the sum)
+__global__ void pk_cg_direction(int64_t n, const double* __restrict__ sc, const float* __restrict__ z,
+                                float* __restrict__ p) {
+    const float b = (float)sc[SC_BETA];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = __fadd_rn(z[i], __fmul_rn(b, p[i]));
+}
+
 // ---- host side -----------------------------------------------------------------
 static unsigned grid_for(int64_t n) { return (unsigned)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 16); }
 
@@ -607,6 +663,34 @@ static double dot(msbg_poisson* P, const float* a, const float* b, int64_t n) {
     return h;
 }
 
+// The CG scalar block (SC_COUNT doubles after the dot partials and result).
+static double* cg_scalars(msbg_poisson* P) {
+    return (double*)((char*)P->work.p + P->work.bytes - (DOT_BLOCKS + 16) * 8) + DOT_BLOCKS + 2;
+}
+
+// a.b into sc[slot] on the device (no host read); SC_PQ also sets alpha.
+static void dot_dev(msbg_poisson* P, const float* a, const float* b, int64_t n, int slot) {
+    double* part = (double*)((char*)P->work.p + P->work.bytes - (DOT_BLOCKS + 16) * 8);
+    double* sc = cg_scalars(P);
+    begin_launch(P->ctx);
+    pk_dot_partial<<<DOT_BLOCKS, DOT_THREADS, 0, P->ctx->stream>>>(a, b, n, part);
+    after_launch(P->ctx, "pk_dot_partial");
+    begin_launch(P->ctx);
+    if (slot == SC_PQ) {
+        pk_dot_final_alpha<<<1, DOT_THREADS, 0, P->ctx->stream>>>(part, DOT_BLOCKS, sc);
+        after_launch(P->ctx, "pk_dot_final_alpha");
+    } else {
+        pk_dot_final<<<1, DOT_THREADS, 0, P->ctx->stream>>>(part, DOT_BLOCKS, sc + slot);
+        after_launch(P->ctx, "pk_dot_final");
+    }
+}
+
+// Host copy of the CG scalar block (waits for the stream).
+static void read_scalars(msbg_poisson* P, double* h) {
+    CUDA_CHECK(cudaMemcpyAsync(h, cg_scalars(P), SC_COUNT * 8, cudaMemcpyDeviceToHost, P->ctx->stream));
+    sync(P->ctx);
+}
+
 static void axpby(msbg_poisson* P, int64_t n, double a, const float* x, double b, float* y) {
     begin_launch(P->ctx);
     pk_axpby<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, (float)a, x, (float)b, y);
@@ -782,10 +866,14 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
             }
         };
         double rz = 0.0;
+        double* sc = cg_scalars(P);
+        double hs[SC_COUNT];
         auto restart = [&]() {
             precondition(r, z);
             CUDA_CHECK(cudaMemcpyAsync(p, z, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
-            rz = dot(P, r, z, n);
+            dot_dev(P, r, z, n, SC_RZ);
+            read_scalars(P, hs);
+            rz = hs[SC_RZ];
         };
         int since = 0;  // iterations since the last (re)start
         std::vector<double> rn_hist;
@@ -800,20 +888,24 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
         restart();
         if (flexible && !(rz > 0.0)) fall_back(3);
         while (rn > tol * bn && it < max_iter) {
+            // q = A p, alpha = r.z / p.Ap, x += alpha p, r -= alpha q and r.r
+            // run back to back on the device; the host reads the scalars once
             launch_matvec(P, 0, p, q);
-            const double pq = dot(P, p, q, n);
-            if (!(pq > 0.0) || !std::isfinite(rz)) {
+            dot_dev(P, p, q, n, SC_PQ);
+            if (flexible) CUDA_CHECK(cudaMemcpyAsync(r_old, r, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
+            begin_launch(P->ctx);
+            pk_cg_update<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, p, q, x64, r);
+            after_launch(P->ctx, "pk_cg_update");
+            dot_dev(P, r, r, n, SC_RR);
+            read_scalars(P, hs);
+            if (hs[SC_BAD] != 0.0) {  // p.Ap <= 0: x and r were left as they were
                 if (flexible && pc != PC_MG) {
                     fall_back(2);
                     continue;
                 }
                 MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
             }
-            const double alpha = rz / pq;
-            add64(P, n, alpha, p, x64);
-            if (flexible) CUDA_CHECK(cudaMemcpyAsync(r_old, r, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
-            axpby(P, n, -alpha, q, 1.0, r);
-            rn = std::sqrt(dot(P, r, r, n));
+            rn = std::sqrt(hs[SC_RR]);
             ++it;
             if (rn <= tol * bn) {
                 launch_residual64(P, x64, b, r);
@@ -843,15 +935,21 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                 continue;
             }
             precondition(r, z);
-            const double rz2 = dot(P, r, z, n);
-            double beta = rz2 / rz;
-            if (flexible) beta = (rz2 - dot(P, z, r_old, n)) / rz;
-            if (flexible && pc != PC_MG && !(rz2 > 0.0)) {
-                fall_back(3);
-                continue;
+            dot_dev(P, r, z, n, SC_RZ2);
+            if (flexible) dot_dev(P, z, r_old, n, SC_ZR);
+            begin_launch(P->ctx);
+            pk_cg_beta<<<1, 1, 0, P->ctx->stream>>>(sc, flexible ? 1 : 0);
+            after_launch(P->ctx, "pk_cg_beta");
+            if (flexible && pc != PC_MG) {
+                read_scalars(P, hs);
+                if (!(hs[SC_RZ] > 0.0)) {  // the new r.z
+                    fall_back(3);
+                    continue;
+                }
             }
-            rz = rz2;
-            axpby(P, n, 1.0, z, beta, p);
+            begin_launch(P->ctx);
+            pk_cg_direction<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, z, p);
+            after_launch(P->ctx, "pk_cg_direction");
         }
     }
     if (!x64_ext) {

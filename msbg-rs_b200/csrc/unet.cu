@@ -101,55 +101,79 @@ __device__ __forceinline__ int64_t l0_halo_cell(const int32_t* __restrict__ nbr2
 
 // First layer on the CUDA cores: a0[c][o] = relu(b[o] + sum_t w[t][o][0] x[c + d(t)]),
 // 1 -> 16 channels (weights bf16 [27][16][16], input channel 0 only).  One CTA
-// per (block, octant): the octant's 10^3 input halo in shared memory, one
-// thread per cell, taps in order t = 0..26 (fmaf).
+// per (block, octant): the octant's 10^3 input halo in shared memory; each
+// thread computes cells (x, y, z) and (x, y, z + 4) of the octant, taps in
+// order t = 0..26 (fmaf), the tap loop unrolled so every halo offset is a
+// constant and each tap's 16 weights are read once for both cells.
 __global__ void __launch_bounds__(256) un_conv_in1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
                                                           const uint16_t* __restrict__ x0c, const uint16_t* __restrict__ w,
                                                           const float* __restrict__ bias, uint16_t* __restrict__ a0) {
-    __shared__ float ws[27][16];
+    __shared__ float4 ws[27][4];
     __shared__ float bs[16];
     __shared__ float xs[1000];
     const int64_t k = blockIdx.x >> 3;
     const int o = blockIdx.x & 7;
-    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16) * 16]);
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x)
+        reinterpret_cast<float*>(ws)[e] = bf(w[(e / 16) * 256 + (e % 16) * 16]);
     if (threadIdx.x < 16) bs[threadIdx.x] = bias[threadIdx.x];
     for (int h = threadIdx.x; h < 1000; h += blockDim.x) {
         const int64_t src = l0_halo_cell(nbr27, nb, k, o, h);
         xs[h] = src >= 0 ? bf(__ldg(x0c + src)) : 0.0f;
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < 512; c += blockDim.x) {
-        const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
-        float acc[16];
+    const int c = threadIdx.x;  // cells c and c + 256 of the octant
+    const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
+    const float* xp = xs + (z * 10 + y) * 10 + x;
+    float acc0[16], acc1[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = 0.0f;
-#pragma unroll 3
-        for (int t = 0; t < 27; ++t) {
-            const float xv = xs[((z + t / 9) * 10 + (y + (t / 3) % 3)) * 10 + (x + t % 3)];
+    for (int q = 0; q < 16; ++q) acc0[q] = acc1[q] = 0.0f;
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[q] = fmaf(ws[t][q], xv, acc[q]);
+    for (int t = 0; t < 27; ++t) {
+        const int off = ((t / 9) * 10 + (t / 3) % 3) * 10 + t % 3;
+        const float x0 = xp[off], x1 = xp[off + 400];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            const float4 wv = ws[t][qq];
+            acc0[4 * qq] = fmaf(wv.x, x0, acc0[4 * qq]);
+            acc0[4 * qq + 1] = fmaf(wv.y, x0, acc0[4 * qq + 1]);
+            acc0[4 * qq + 2] = fmaf(wv.z, x0, acc0[4 * qq + 2]);
+            acc0[4 * qq + 3] = fmaf(wv.w, x0, acc0[4 * qq + 3]);
+            acc1[4 * qq] = fmaf(wv.x, x1, acc1[4 * qq]);
+            acc1[4 * qq + 1] = fmaf(wv.y, x1, acc1[4 * qq + 1]);
+            acc1[4 * qq + 2] = fmaf(wv.z, x1, acc1[4 * qq + 2]);
+            acc1[4 * qq + 3] = fmaf(wv.w, x1, acc1[4 * qq + 3]);
         }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fmaxf(acc[q] + bs[q], 0.0f);
-        const int64_t cell = (k << 12) + (((o & 1) * 8 + x) | ((((o >> 1) & 1) * 8 + y) << 4) | (((o >> 2) * 8 + z) << 8));
-        uint4* out = reinterpret_cast<uint4*>(a0 + cell * 16);
-        out[0] = pack8(acc);
-        out[1] = pack8(acc + 8);
     }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        acc0[q] = fmaxf(acc0[q] + bs[q], 0.0f);
+        acc1[q] = fmaxf(acc1[q] + bs[q], 0.0f);
+    }
+    const int64_t gx = (o & 1) * 8 + x, gy = ((o >> 1) & 1) * 8 + y, gz = (o >> 2) * 8 + z;
+    const int64_t cell0 = (k << 12) + (gx | (gy << 4) | (gz << 8)), cell1 = cell0 + (4 << 8);
+    uint4* out0 = reinterpret_cast<uint4*>(a0 + cell0 * 16);
+    out0[0] = pack8(acc0);
+    out0[1] = pack8(acc0 + 8);
+    uint4* out1 = reinterpret_cast<uint4*>(a0 + cell1 * 16);
+    out1[0] = pack8(acc1);
+    out1[1] = pack8(acc1 + 8);
 }
 
 // Last layer on the CUDA cores: y[c] = b[0] + sum_t sum_i w[t][0][i] u[c + d(t)][i],
 // 16 -> 1 channel, f32 output.  One CTA per (block, octant): the octant's
 // 10^3 halo of 16-channel rows in shared memory as two planes of 8 channels
-// (16-byte rows, conflict-free), one thread per cell.
+// (16-byte rows, conflict-free); each thread computes cells (x, y, z) and
+// (x, y, z + 4), taps in order and channels in order within a tap (fmaf),
+// the tap loop unrolled so every halo offset is a constant.
 __global__ void __launch_bounds__(256) un_conv_out1_kernel(const int32_t* __restrict__ nbr27, int64_t nb,
                                                            const uint16_t* __restrict__ u0, const uint16_t* __restrict__ w,
                                                            const float* __restrict__ bias, float* __restrict__ y) {
-    __shared__ float ws[27][16];
+    __shared__ float4 ws[27][4];
     __shared__ uint4 us[2][1000];
     const int64_t k = blockIdx.x >> 3;
     const int o = blockIdx.x & 7;
-    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e / 16][e % 16] = bf(w[(e / 16) * 256 + (e % 16)]);
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x)
+        reinterpret_cast<float*>(ws)[e] = bf(w[(e / 16) * 256 + (e % 16)]);
     for (int e = threadIdx.x; e < 2000; e += blockDim.x) {
         const int h = e >> 1, half = e & 1;
         const int64_t src = l0_halo_cell(nbr27, nb, k, o, h);
@@ -157,21 +181,31 @@ __global__ void __launch_bounds__(256) un_conv_out1_kernel(const int32_t* __rest
     }
     __syncthreads();
     const float b0 = bias[0];
-    for (int c = threadIdx.x; c < 512; c += blockDim.x) {
-        const int x = c & 7, yy = (c >> 3) & 7, z = c >> 6;
-        float acc = 0.0f;
-#pragma unroll 3
-        for (int t = 0; t < 27; ++t) {
-            const int h = ((z + t / 9) * 10 + (yy + (t / 3) % 3)) * 10 + (x + t % 3);
-            float v[16];
-            unpack8(us[0][h], v);
-            unpack8(us[1][h], v + 8);
+    const int c = threadIdx.x;  // cells c and c + 256 of the octant
+    const int x = c & 7, yy = (c >> 3) & 7, z = c >> 6;
+    const int h0 = (z * 10 + yy) * 10 + x;
+    float acc0 = 0.0f, acc1 = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc = fmaf(ws[t][i], v[i], acc);
+    for (int t = 0; t < 27; ++t) {
+        const int h = h0 + ((t / 9) * 10 + (t / 3) % 3) * 10 + t % 3;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            float v0[8], v1[8];
+            unpack8(us[half][h], v0);
+            unpack8(us[half][h + 400], v1);
+            const float4 wa = ws[t][2 * half], wb = ws[t][2 * half + 1];
+            const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                acc0 = fmaf(wv[i], v0[i], acc0);
+                acc1 = fmaf(wv[i], v1[i], acc1);
+            }
         }
-        const int64_t cell = (k << 12) + (((o & 1) * 8 + x) | ((((o >> 1) & 1) * 8 + yy) << 4) | (((o >> 2) * 8 + z) << 8));
-        y[cell] = acc + b0;
     }
+    const int64_t gx = (o & 1) * 8 + x, gy = ((o >> 1) & 1) * 8 + yy, gz = (o >> 2) * 8 + z;
+    const int64_t cell0 = (k << 12) + (gx | (gy << 4) | (gz << 8));
+    y[cell0] = acc0 + b0;
+    y[cell0 + (4 << 8)] = acc1 + b0;
 }
 
 // Coarse cell i of level lgc (same block, cells twice the size) from its 8
