@@ -93,6 +93,13 @@ struct msbg_ctx {
     uint64_t launches = 0;
     msbg::DevBuf scratch;
     msbg::DevBuf status;  // int32 device status word
+    // Page-locked, device-mapped buffer for the library's own small device ->
+    // host reads (status words, counts, block lists): a kernel writes them
+    // there, so they never queue behind a caller's large transfer on a copy
+    // engine.
+    void* rb_host = nullptr;
+    void* rb_dev = nullptr;
+    size_t rb_cap = 0;
 
     // Per-kernel CUDA-event timing (off by default): every launch between
     // begin_launch and after_launch is bracketed by two events on the stream.
@@ -180,6 +187,34 @@ inline void after_launch(msbg_ctx* ctx, const char* what) {
 void resolve_timing(msbg_ctx* ctx);
 
 inline void sync(msbg_ctx* ctx) { CUDA_CHECK(cudaStreamSynchronize(ctx->stream)); }
+
+// Device -> host reads of a few bytes each through the context's mapped
+// read-back buffer (a kernel copies them there; no copy engine): add() enqueues
+// on the context stream, wait() synchronises the stream and copies the values
+// out.  Reads that do not fit in the buffer fall back to cudaMemcpyAsync.
+class SmallReads {
+  public:
+    explicit SmallReads(msbg_ctx* ctx) : ctx_(ctx) {}
+    void add(void* host_dst, const void* dev_src, size_t bytes);
+    void wait();
+
+  private:
+    struct Item {
+        void* dst;
+        size_t off, bytes;
+        bool staged;
+    };
+    msbg_ctx* ctx_;
+    size_t used_ = 0;
+    std::vector<Item> items_;
+};
+
+// One small read, waited for.
+inline void read_small(msbg_ctx* ctx, void* host_dst, const void* dev_src, size_t bytes) {
+    SmallReads r(ctx);
+    r.add(host_dst, dev_src, bytes);
+    r.wait();
+}
 
 inline void set_device(msbg_ctx* ctx) { CUDA_CHECK(cudaSetDevice(ctx->device)); }
 

@@ -1,5 +1,6 @@
 // grid.cu -- context, device sparse grid, block transfer and halo gather.
 #include <algorithm>
+#include <cstring>
 
 #include "grid.cuh"
 #include "sweep.cuh"
@@ -21,9 +22,42 @@ void raise_device_status(msbg_ctx* ctx, int word) {
 
 void check_device_status(msbg_ctx* ctx) {
     int h = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&h, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    read_small(ctx, &h, ctx->status.p, 4);
     raise_device_status(ctx, h);
+}
+
+__global__ void readback_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, size_t n) {
+    if ((((uintptr_t)src | (uintptr_t)dst | n) & 3) == 0) {
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n / 4; i += (size_t)gridDim.x * blockDim.x)
+            reinterpret_cast<uint32_t*>(dst)[i] = reinterpret_cast<const uint32_t*>(src)[i];
+    } else {
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+            dst[i] = src[i];
+    }
+}
+
+void SmallReads::add(void* host_dst, const void* dev_src, size_t bytes) {
+    if (!bytes) return;
+    const size_t off = (used_ + 15) & ~size_t(15);
+    if (ctx_->rb_dev && off + bytes <= ctx_->rb_cap) {
+        begin_launch(ctx_);
+        readback_kernel<<<(unsigned)std::min<size_t>(div_up(bytes, 1024), 64), 256, 0, ctx_->stream>>>(
+            (const uint8_t*)dev_src, (uint8_t*)ctx_->rb_dev + off, bytes);
+        after_launch(ctx_, "readback_kernel");
+        items_.push_back({host_dst, off, bytes, true});
+        used_ = off + bytes;
+    } else {
+        CUDA_CHECK(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, ctx_->stream));
+        items_.push_back({host_dst, 0, bytes, false});
+    }
+}
+
+void SmallReads::wait() {
+    sync(ctx_);
+    for (const Item& it : items_)
+        if (it.staged) std::memcpy(it.dst, (const char*)ctx_->rb_host + it.off, it.bytes);
+    items_.clear();
+    used_ = 0;
 }
 
 char* scratch(msbg_ctx* ctx, const ScratchLayout& L) {
@@ -442,6 +476,7 @@ const char* msbg_status_string(int s) {
 
 const char* msbg_last_error(void) { return g_last_error.c_str(); }
 
+
 int msbg_ctx_create(int device, msbg_ctx** out) {
     MSBG_API_BEGIN
     MSBG_REQUIRE(out, "null output");
@@ -455,8 +490,12 @@ int msbg_ctx_create(int device, msbg_ctx** out) {
         CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         c->status.reserve(64);
         CUDA_CHECK(cudaMemsetAsync(c->status.p, 0, 64, c->stream));
+        c->rb_cap = (size_t)1 << 20;
+        CUDA_CHECK(cudaHostAlloc(&c->rb_host, c->rb_cap, cudaHostAllocMapped));
+        CUDA_CHECK(cudaHostGetDevicePointer(&c->rb_dev, c->rb_host, 0));
         CUDA_CHECK(cudaStreamSynchronize(c->stream));
     } catch (...) {
+        if (c->rb_host) cudaFreeHost(c->rb_host);
         delete c;
         throw;
     }
@@ -474,6 +513,7 @@ int msbg_ctx_destroy(msbg_ctx* ctx) {
     if (ctx->open) cudaEventDestroy(ctx->open);
     ctx->scratch.release();
     ctx->status.release();
+    if (ctx->rb_host) cudaFreeHost(ctx->rb_host);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     MSBG_API_END

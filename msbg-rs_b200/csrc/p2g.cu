@@ -666,9 +666,12 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     after_launch(ctx, "p2g_gather_kernel");
     const size_t npb = sorted_segments(ctx, skeys, n, (uint64_t)(3 * lg), pb_key, pb_starts, ScratchLayout::at<char>(base, o_tmp));
     int hbad = 0, hstatus = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    {
+        SmallReads rd(ctx);
+        rd.add(&hbad, bad, 4);
+        rd.add(&hstatus, ctx->status.p, 4);
+        rd.wait();
+    }
     raise_device_status(ctx, hstatus);
     MSBG_REQUIRE(!hbad, "a particle lies outside the domain");
 
@@ -703,9 +706,12 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     radix_sort_pairs(ctx, cand, nullptr, csort, cperm, npb * 27, cbits, ScratchLayout::at<char>(base, o_ctmp));
     size_t nuniq = sorted_segments(ctx, csort, npb * 27, 0, act, ast, ScratchLayout::at<char>(base, o_ctmp));
     std::vector<uint64_t> active(nuniq);
-    CUDA_CHECK(cudaMemcpyAsync(active.data(), act, nuniq * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    {
+        SmallReads rd(ctx);
+        rd.add(active.data(), act, nuniq * 8);
+        rd.add(&hstatus, ctx->status.p, 4);
+        rd.wait();
+    }
     raise_device_status(ctx, hstatus);
     if (!active.empty() && active.back() == u->n_blocks) active.pop_back();  // the "none" sentinel
     const size_t na = active.size();
@@ -762,8 +768,7 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     c.nx = (int64_t)u->nx;
     c.ny = (int64_t)u->ny;
     if (na) dispatch(ctx, bsx, M, nullptr, 0, &c, na);
-    CUDA_CHECK(cudaMemcpyAsync(&hstatus, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);  // `slots` (host) and the scratch layout end here
+    read_small(ctx, &hstatus, ctx->status.p, 4);  // waits: `slots` (host) and the scratch layout end here
     raise_device_status(ctx, hstatus);
     if (n_active_out) *n_active_out = na;
     (void)a256;

@@ -420,8 +420,7 @@ int key_bits(msbg_ctx* ctx, const uint64_t* d_keys, size_t n, void* tmp8) {
     max_u64_kernel<<<std::min<size_t>(div_up(n, 256), 1184), 256, 0, ctx->stream>>>(d_keys, n, (unsigned long long*)tmp8);
     after_launch(ctx, "max_u64_kernel");
     uint64_t m = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&m, tmp8, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    read_small(ctx, &m, tmp8, 8);
     int b = 0;
     while (b < 64 && (m >> b)) ++b;
     return b;
@@ -469,8 +468,7 @@ size_t sorted_segments(msbg_ctx* ctx, const uint64_t* d_sorted, size_t n, uint64
     seg_write_kernel<<<g, 256, 0, ctx->stream>>>(d_sorted, n, shift, f, idx, d_uniq, d_starts, count);
     after_launch(ctx, "seg_write_kernel");
     uint32_t c = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&c, count, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    read_small(ctx, &c, count, 4);
     return c;
 }
 
