@@ -63,6 +63,7 @@ struct msbg_poisson {
     int nu1 = 2, nu2 = 2;
     float omega = 2.0f / 3.0f;
     msbg::DevBuf work;   // PCG vectors + dot partials
+    msbg::DevBuf io;     // device copies of host x and b (msbg_poisson_solve), kept between calls
     msbg_unet* net = nullptr;  // learned preconditioner (not owned)
     // PCG statistics of the last solve: preconditioner applications of each
     // kind and whether the learned preconditioner fell back to multigrid
@@ -658,8 +659,7 @@ static double dot(msbg_poisson* P, const float* a, const float* b, int64_t n) {
     pk_dot_final<<<1, DOT_THREADS, 0, P->ctx->stream>>>(part, DOT_BLOCKS, part + DOT_BLOCKS);
     after_launch(P->ctx, "pk_dot_final");
     double h = 0.0;
-    CUDA_CHECK(cudaMemcpyAsync(&h, part + DOT_BLOCKS, 8, cudaMemcpyDeviceToHost, P->ctx->stream));
-    sync(P->ctx);
+    read_small(P->ctx, &h, part + DOT_BLOCKS, 8);
     return h;
 }
 
@@ -686,10 +686,7 @@ static void dot_dev(msbg_poisson* P, const float* a, const float* b, int64_t n, 
 }
 
 // Host copy of the CG scalar block (waits for the stream).
-static void read_scalars(msbg_poisson* P, double* h) {
-    CUDA_CHECK(cudaMemcpyAsync(h, cg_scalars(P), SC_COUNT * 8, cudaMemcpyDeviceToHost, P->ctx->stream));
-    sync(P->ctx);
-}
+static void read_scalars(msbg_poisson* P, double* h) { read_small(P->ctx, h, cg_scalars(P), SC_COUNT * 8); }
 
 static void axpby(msbg_poisson* P, int64_t n, double a, const float* x, double b, float* y) {
     begin_launch(P->ctx);
@@ -1560,7 +1557,7 @@ int msbg_poisson_solve(msbg_poisson* P, int method, float* x, const float* b, do
     MSBG_REQUIRE(P && x && b && method >= 0 && method <= 5 && max_iter >= 0 && tol > 0.0, "bad argument");
     set_device(P->ctx);
     const int64_t n = P->lv[0].cells();
-    DevBuf io;
+    DevBuf& io = P->io;
     io.reserve((size_t)n * 8 + 512);
     float* dx = io.as<float>();
     float* db = dx + n;
@@ -1831,12 +1828,13 @@ int msbg_batch_solve(msbg_batch* B, double tol, int iters_per_cycle, int max_cyc
     std::vector<std::vector<double>> sc(B->groups.size());
     auto read_scalars = [&]() {
         bool any = false;
+        SmallReads rd(ctx);
         for (size_t g = 0; g < B->groups.size(); ++g) {
             const msbg_poisson* P = B->groups[g];
             sc[g].resize((size_t)P->np * S_WIDTH);
-            CUDA_CHECK(cudaMemcpyAsync(sc[g].data(), P->scal.p, sc[g].size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            rd.add(sc[g].data(), P->scal.p, sc[g].size() * 8);
         }
-        sync(ctx);
+        rd.wait();
         for (size_t g = 0; g < B->groups.size(); ++g)
             for (int i = 0; i < B->groups[g]->np; ++i) any |= sc[g][(size_t)i * S_WIDTH + S_ACTIVE] > 0.0;
         return any;

@@ -566,8 +566,7 @@ static double loss_and_grads(msbg_unet* U, const float* r, const float* e) {
     after_launch(ctx, "un_dy_kernel");
     backward(U);
     double h[2];
-    CUDA_CHECK(cudaMemcpyAsync(h, sums, 16, cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
+    read_small(ctx, h, sums, 16);
     check_device_status(ctx);
     return h[0] > 0.0 ? h[1] / h[0] : 0.0;
 }
