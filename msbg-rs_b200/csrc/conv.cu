@@ -195,8 +195,9 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvLevel L, const uint1
 // the halo: 8 groups (y) of 8 rows (x), the groups 160 bytes apart, so one
 // lane of warp z issues every MMA of plane z (M = the 64 cells of the plane,
 // N = Cout, K = Cin per tap) back to back with no per-tap staging.  Plane z
-// of a block accumulates in TMEM columns z * Cout .. of one of two accumulators, in the
-// M = 64 data-path layout (row m of the plane in lane (m % 16) + 32 (m / 16)).
+// of a block accumulates in TMEM columns z * Cout .. of one of two
+// accumulators, in the M = 64 data-path layout (row m of the plane in lane
+// (m % 16) + 32 (m / 16)).
 // While the tensor core works on block i, the threads copy the halo of block
 // i + 1 and write out block i - 1.
 constexpr int kB8Threads = 512;
@@ -220,9 +221,10 @@ struct B8Smem {
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kB8Threads) conv3_b8_kernel(ConvLevel L, const uint16_t* __restrict__ x,
-                                                       const uint16_t* __restrict__ w, const float* __restrict__ bias,
-                                                       int relu, const uint16_t* __restrict__ mask, int out_f32,
-                                                       int out_ch, void* __restrict__ y, int* __restrict__ status) {
+                                                              const uint16_t* __restrict__ w,
+                                                              const float* __restrict__ bias, int relu,
+                                                              const uint16_t* __restrict__ mask, int out_f32, int out_ch,
+                                                              void* __restrict__ y, int* __restrict__ status) {
     using S = B8Smem<CIN, COUT>;
     constexpr int KCH = S::KCH;
     constexpr uint32_t SBO_W = KCH * 128;
@@ -306,6 +308,7 @@ __global__ void __launch_bounds__(kB8Threads) conv3_b8_kernel(ConvLevel L, const
             const uint32_t d = tmem + (uint32_t)(buf * S::ACC_COLS + z * COUT);
 #pragma unroll 1
             for (int dz = 0; dz < 3; ++dz) {
+                // dz * 100: one halo plane (1600 bytes) in the 16-byte units of the address field
                 const uint64_t az = a0 + (uint64_t)(dz * 100), bz = b0 + (uint64_t)((dz * 9 * S::B_BYTES) >> 4);
 #pragma unroll
                 for (int r = 0; r < 9; ++r) {
