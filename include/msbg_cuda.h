@@ -173,12 +173,21 @@ int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_
  * into the library (about 5 MB, held by every device that loads the library
  * until exit), so n is limited to 262144 particles; larger n returns
  * MSBG_ERR_ARG.  The first call on a device looks up the array's device
- * address: make it before any stream capture.  Calls share the array, so
- * calls whose GPU work overlaps in time race; calls ordered on one stream do
- * not.  Returns MSBG_ERR_STATE while per-kernel timing is enabled (timing
- * creates CUDA events). */
+ * address: make it before any stream capture.  Each call blocks the host
+ * until its stream reaches the end of the sort: it reads the largest key (to
+ * choose the number of digit passes) and the bounded-wait status word back.
+ * Calls share the array, so calls whose GPU work overlaps in time race;
+ * calls ordered on one stream do not.  The device address is looked up once
+ * per device and kept, so a cudaDeviceReset while the library is loaded is
+ * not supported.  Returns MSBG_ERR_STATE while per-kernel timing is enabled
+ * (timing creates CUDA events). */
 int msbg_morton_sort_noalloc_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d_keys_out,
                                     uint32_t* d_perm_out);
+/* No counterpart in the reference (test hook).  Runs one radix-sort digit
+ * pass whose look-back waits for counts that are never published, with a
+ * time limit of limit_ns (1e5 to 1e9): returns MSBG_ERR_TIMEOUT with the
+ * context's status word cleared, so the context stays usable. */
+int msbg_test_sort_lookback_timeout(msbg_ctx* ctx, uint64_t limit_ns);
 /* Applies a sort permutation to per-particle data: dst[i] = src[perm[i]] for
  * items of `width` floats (the payload gather of bucket_particles,
  * fluid/mod.rs:71-91, and bucket_by_block, particles/sort.rs:274-285). */

@@ -75,6 +75,7 @@ SIGNATURES = {
     "msbg_morton_sort": [_P, _P, _SZ, _P, _P],
     "msbg_morton_sort_device": [_P, _P, _SZ, _P, _P],
     "msbg_morton_sort_noalloc_device": [_P, _P, _SZ, _P, _P],
+    "msbg_test_sort_lookback_timeout": [_P, _U64],
     "msbg_permute_device": [_P, _P, _SZ, _I, _P, _P],
     "msbg_bucket_indices": [_P, _P, _SZ, _P, _P, _P, _SZP],
     "msbg_bucket_indices_device": [_P, _P, _SZ, _P, _P, _P, _SZP],

@@ -17,7 +17,7 @@ void raise_device_status(msbg_ctx* ctx, int word) {
     if (word & 1) what += "an mbarrier wait inside a tensor-core kernel";
     if (word & 2) what += std::string(what.empty() ? "" : " and ") + "a radix-sort look-back";
     if (word & 4) what += std::string(what.empty() ? "" : " and ") + "a P2G tile-order wait";
-    MSBG_THROW(MSBG_ERR_TIMEOUT, what + " waited more than a second and gave up");
+    MSBG_THROW(MSBG_ERR_TIMEOUT, what + " waited past its time limit and gave up");
 }
 
 void check_device_status(msbg_ctx* ctx) {

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                 if ((++spins & 63u) == 0) {
                     const uint64_t now = globaltimer_ns();
                     if (!t0) t0 = now;
-                    else if (now - t0 > 1000000000ull) {
+                    else if (now - t0 > kWaitLimitNs) {
                         if (lane == 0) atomicOr(a.status, 4);
                         break;
                     }

@@ -137,13 +137,15 @@ __global__ void __launch_bounds__(256) os_hist_kernel(const uint64_t* __restrict
 // key w*32*OS_ITEMS + j*32 + l, so (warp, item, lane) order is index order and
 // the local sort is stable.  `status` holds tiles*256 words for this pass
 // (zeroed before the launch); `status_next` (the next pass's array, or null)
-// is zeroed here, tile by tile.  A look-back that waits more than a second
-// sets bit 2 of *err and carries on with what it has (the result is then wrong and
-// the host reports the error), so no CTA can spin forever.
+// is zeroed here, tile by tile.  A look-back that waits more than limit_ns
+// (one second in a sort) sets bit 2 of *err and carries on with what it has
+// (the result is then wrong and the host reports the error), so no CTA can
+// spin forever.
 __global__ void __launch_bounds__(OS_THREADS, 4)
     os_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
                    uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist,
-                   uint64_t* status, uint64_t* __restrict__ status_next, uint32_t* tile_counter, int* err) {
+                   uint64_t* status, uint64_t* __restrict__ status_next, uint32_t* tile_counter, int* err,
+                   uint64_t limit_ns) {
     extern __shared__ __align__(16) unsigned char os_smem[];
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(os_smem);
     uint32_t* s_vals = reinterpret_cast<uint32_t*>(os_smem + (size_t)OS_TILE * 8);
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(OS_THREADS, 4)
             if (used < OS_LOOKBACK && (++spins & 15u) == 0) {
                 const uint64_t now = globaltimer_ns();
                 if (!t0) t0 = now;
-                else if (now - t0 > 1000000000ull) {
+                else if (now - t0 > limit_ns) {
                     atomicOr(err, 2);
                     break;
                 }
@@ -339,7 +341,7 @@ void radix_sort_pairs(msbg_ctx* ctx, const uint64_t* keys_in, const uint32_t* va
         begin_launch(ctx);
         os_pass_kernel<<<(unsigned)tiles, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(
             ki, vi, ko, vo, n, 8 * p, hist + p * 256, status[p & 1], p + 1 < passes ? status[(p + 1) & 1] : nullptr,
-            counters + p, ctx->status.as<int>());
+            counters + p, ctx->status.as<int>(), kWaitLimitNs);
         after_launch(ctx, "os_pass_kernel");
         ki = ko;
         vi = vo;
@@ -678,7 +680,10 @@ int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_
 // allocating: the temporaries live in the library's fixed device scratch
 // array.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress), so make that first call before capturing the
-// stream into a CUDA graph.  All calls share the one array: calls whose GPU
+// stream into a CUDA graph; the address is kept for the life of the process,
+// so a cudaDeviceReset while the library is loaded is not supported.  Each
+// call blocks the host until the sort is done (it reads the largest key and
+// the status word back).  All calls share the one array: calls whose GPU
 // work overlaps in time (different streams or contexts on one device) race on
 // it; calls ordered on one stream do not.  Every scratch word is written
 // before it is read in a call (the key-bits word is cleared on the stream),
@@ -704,6 +709,40 @@ int msbg_morton_sort_noalloc_device(msbg_ctx* ctx, const float* d_pos, size_t n,
     morton_keys(ctx, d_pos, n, keys);
     const int bits = key_bits(ctx, keys, n, bits_word);
     radix_sort_pairs(ctx, keys, nullptr, d_keys_out, d_perm_out, n, bits, sort_tmp);
+    check_device_status(ctx);
+    MSBG_API_END
+}
+
+// Test hook for the bounded look-back wait: one digit pass of two tiles runs
+// with a single CTA that takes tile 1, so the tile-0 counts it waits for are
+// never published.  The wait gives up after limit_ns, sets the radix-sort bit
+// of the status word, and the call returns MSBG_ERR_TIMEOUT with the word
+// cleared, leaving the context usable.
+int msbg_test_sort_lookback_timeout(msbg_ctx* ctx, uint64_t limit_ns) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(ctx, "null argument");
+    MSBG_REQUIRE(limit_ns >= 100000ull && limit_ns <= kWaitLimitNs, "limit_ns must lie in [1e5, 1e9]");
+    set_device(ctx);
+    const size_t n = 2 * (size_t)OS_TILE;
+    ScratchLayout L;
+    const size_t ok = L.add<uint64_t>(n), ov = L.add<uint32_t>(n), oko = L.add<uint64_t>(n), ovo = L.add<uint32_t>(n),
+                 oh = L.add<uint32_t>(256), ost = L.add<uint64_t>(2 * 256), oc = L.add<uint32_t>(1);
+    char* base = scratch(ctx, L);
+    uint64_t* keys = ScratchLayout::at<uint64_t>(base, ok);
+    uint32_t* hist = ScratchLayout::at<uint32_t>(base, oh);
+    uint64_t* status = ScratchLayout::at<uint64_t>(base, ost);
+    uint32_t* counter = ScratchLayout::at<uint32_t>(base, oc);
+    CUDA_CHECK(cudaMemsetAsync(keys, 0, n * 8, ctx->stream));
+    CUDA_CHECK(cudaMemsetAsync(hist, 0, 256 * 4, ctx->stream));
+    CUDA_CHECK(cudaMemsetAsync(status, 0, 2 * 256 * 8, ctx->stream));
+    const uint32_t one = 1;  // the CTA's tile id: tile 0 never runs
+    CUDA_CHECK(cudaMemcpyAsync(counter, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_CHECK(cudaFuncSetAttribute(os_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OS_PASS_SMEM));
+    begin_launch(ctx);
+    os_pass_kernel<<<1, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(keys, nullptr, ScratchLayout::at<uint64_t>(base, oko),
+                                                                ScratchLayout::at<uint32_t>(base, ovo), n, 0, hist, status,
+                                                                nullptr, counter, ctx->status.as<int>(), limit_ns);
+    after_launch(ctx, "os_pass_kernel");
     check_device_status(ctx);
     MSBG_API_END
 }

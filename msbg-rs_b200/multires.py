@@ -1,6 +1,6 @@
-"""Multiresolution helpers on the device: downsample_channel_avg
-(multires/downsample.rs:13-59) and the per-block level assignment used by the
-multiresolution workloads."""
+"""Multiresolution helper on the device: downsample_channel_avg
+(multires/downsample.rs:13-59), the 2^3 box-average restriction of one level's
+blocks to the next coarser level."""
 from __future__ import annotations
 
 from ._lib import call

@@ -2,11 +2,11 @@
 
 The reference's differential tests hard-code golden values produced by the
 original C++ MSBG binaries.  This script reads them as text from a checkout of
-msbg-rs (default /root/reference) and writes them, with their file:line
-provenance, into reference_goldens.json, which the tests load.  Run it only
-where the reference checkout exists:
+msbg-rs (the first argument, else the MSBG_RS_DIR environment variable) and
+writes them, with their file:line provenance, into reference_goldens.json,
+which the tests load.  Run it only where the reference checkout exists:
 
-    python tests/golden/extract_goldens.py [path/to/msbg-rs]
+    python tests/golden/extract_goldens.py path/to/msbg-rs
 """
 from __future__ import annotations
 
@@ -91,4 +91,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MSBG_RS_DIR")
+    if not src:
+        sys.exit("usage: extract_goldens.py path/to/msbg-rs (or set MSBG_RS_DIR)")
+    main(src)

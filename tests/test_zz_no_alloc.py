@@ -47,6 +47,42 @@ def test_noalloc_morton_sort_matches_allocating_entry_point(msbg, ctx):
         assert torch.equal(p_fixed, p_alloc)
 
 
+def test_noalloc_morton_sort_allocates_nothing(msbg):
+    """On a fresh context the call leaves the context's scratch arena empty,
+    and once the library's kernels are loaded, further calls leave the
+    device's free memory unchanged."""
+    import torch
+
+    lib = msbg._lib.lib()
+    ptr = msbg._lib.ptr
+    fresh = msbg.Context(0)
+    try:
+        n = 50000
+        pos = np.random.default_rng(7).uniform(0.0, 100.0, (n, 3)).astype(np.float32)
+        dpos = torch.from_numpy(pos).cuda()
+        keys = torch.empty(n, dtype=torch.int64, device="cuda")
+        perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        used = C.c_uint64()
+
+        def run():
+            msbg._lib.check(lib.msbg_morton_sort_noalloc_device(fresh.handle, ptr(dpos), C.c_size_t(n), ptr(keys),
+                                                                ptr(perm)))
+
+        run()
+        msbg._lib.check(lib.msbg_ctx_scratch_bytes(fresh.handle, C.byref(used)))
+        assert used.value == 0
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        run()
+        run()
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free_before
+        msbg._lib.check(lib.msbg_ctx_scratch_bytes(fresh.handle, C.byref(used)))
+        assert used.value == 0
+    finally:
+        fresh.close()
+
+
 def test_noalloc_morton_sort_rejects_oversize(msbg, ctx):
     import torch
 
