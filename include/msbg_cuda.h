@@ -264,8 +264,10 @@ int msbg_downsample_avg(msbg_grid* dst, msbg_grid* src);
  * blocks in ascending block-id order, [n_active][bsx^3] f32 (the block
  * payload layout).  The multigrid hierarchy halves the block size down to 2,
  * then halves the block grid, down to <= 1024 cells solved by a dense FP64
- * inverse; level operators are the Galerkin products (0.5^l times the 7-point
- * stencil).  Dot products and norms are FP64. */
+ * inverse.  Level l rediscretises the 7-point stencil on cells of width 2^l
+ * (0.25^l times the stencil, with boundary-corrected diagonals and cell
+ * masks); prolongation is cell-centred trilinear and restriction its
+ * transpose / 8.  Dot products and norms are FP64. */
 int msbg_poisson_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int bsx, const uint64_t* active,
                         size_t n, msbg_poisson** out);
 int msbg_poisson_destroy(msbg_poisson* p);

@@ -926,17 +926,28 @@ void or_downsample_avg(const float* fine, int64_t n_blocks, int bsx, float* coar
 // FP64 Poisson oracle (no reference implementation: parity unpinned).
 //
 // Problem: the unknowns are the cells of the active blocks (block size bs on
-// an nx*ny*nz block grid); every other cell is zero (Dirichlet).  At level l
-//   (A_l x)_c = s_l * (6 x_c - sum of the x of its active face neighbours),
-//   s_l = 0.5^l,
-// the Galerkin operator R A P for piecewise-constant prolongation P and
-// averaging restriction R = P^T / 8 (docs/roadmap.md:618-627 states the
-// matvec `y = D x - sum nb` and relaxation `y = w (b + sum nb) D^-1 + (1-w) x`).
-// Hierarchy: level l+1 has cells of twice the size.  While bs_l >= 4 the
-// block grid is kept and the block size halves ("same grid" levels); from
-// bs_l == 2 on, the block grid halves and the block size stays 2 (a coarse
-// block is active when any of its 8 child blocks is).  Coarsening stops at
-// <= kPoissonDirect cells, which are solved directly (dense Cholesky, FP64).
+// an nx*ny*nz block grid); every other cell is zero (Dirichlet).  Level 0:
+//   (A_0 x)_c = 6 x_c - sum of the x of its active face neighbours
+// (docs/roadmap.md:618-627: matvec `y = D x - sum nb`, relaxation
+// `y = w (b + sum nb) D^-1 + (1-w) x`).  Level l+1 has cells twice as wide.
+// While bs_l >= 4 the block grid is kept and the block size halves ("same
+// grid" levels); from bs_l == 2 on, the block grid halves and the block size
+// stays 2.  A coarse cell is active when any of its 8 children is, so every
+// level covers the same cells as level 0 (while coarse cells are no wider
+// than a level-0 block).  At level l the operator is the 7-point stencil
+// rediscretised on cells of width 2^l, in the units of the level-0 equation:
+//   (A_l x)_c = s_l ((6 - g_l m_c) x_c - sum of active neighbours),
+//   s_l = 0.25^l,
+// where m_c counts the missing face neighbours of c and g_l places the zero
+// Dirichlet value where level 0 has it, half a level-0 cell outside the
+// boundary face: linear extrapolation from the cell centre, at distance
+// d = (1/2 + 2^(-l-1)) cells of level l from that point, gives the ghost
+// value g_l x_c with g_l = 1 - 1/d (g_0 = 0).  Prolongation P is cell-centred
+// trilinear (per axis 3/4 from the parent cell and 1/4 from its neighbour on
+// the child's side; inactive coarse cells count as zero) and restriction is
+// R = P^T / 8, so the V-cycle with nu1 = nu2 is a symmetric preconditioner.
+// Coarsening stops at <= kPoissonDirect cells, which are solved directly
+// (dense Cholesky, FP64; inactive cells have identity rows).
 // V-cycle: nu1 weighted-Jacobi sweeps, residual, restriction, recursion,
 // prolongation-correction, nu2 sweeps.
 // ===========================================================================
@@ -950,6 +961,8 @@ struct PLevel {
     std::vector<int64_t> nbr;   // [n][6] slot of the -x,+x,-y,+y,-z,+z neighbour block or -1
     std::vector<int64_t> parent;  // [n] slot of the parent block at level l+1
     double scale;
+    double ghost = 0.0;           // g_l
+    std::vector<uint8_t> mask;    // per cell: active (empty = all active)
     int64_t n() const { return (int64_t)bids.size(); }
     int64_t cells() const { return n() * bs * bs * bs; }
 };
@@ -993,6 +1006,29 @@ static inline double nbsum(const PLevel& L, const double* x, int64_t k, int cx, 
     return s;
 }
 
+// 1 when the cell at (cx,cy,cz) relative to block k (one coordinate may be -1
+// or bs) is an active cell
+static inline int present(const PLevel& L, int64_t k, int cx, int cy, int cz) {
+    int64_t kk = k;
+    if (cx < 0) { kk = L.nbr[k * 6 + 0]; cx += L.bs; }
+    else if (cx >= L.bs) { kk = L.nbr[k * 6 + 1]; cx -= L.bs; }
+    else if (cy < 0) { kk = L.nbr[k * 6 + 2]; cy += L.bs; }
+    else if (cy >= L.bs) { kk = L.nbr[k * 6 + 3]; cy -= L.bs; }
+    else if (cz < 0) { kk = L.nbr[k * 6 + 4]; cz += L.bs; }
+    else if (cz >= L.bs) { kk = L.nbr[k * 6 + 5]; cz -= L.bs; }
+    if (kk < 0) return 0;
+    if (L.mask.empty()) return 1;
+    const size_t N = (size_t)L.bs * L.bs * L.bs;
+    return L.mask[kk * N + ((size_t)cx | ((size_t)cy << L.lg) | ((size_t)cz << (2 * L.lg)))];
+}
+
+// 6 - g_l m_c (unscaled diagonal)
+static inline double diag_of(const PLevel& L, int64_t k, int cx, int cy, int cz) {
+    const int miss = 6 - present(L, k, cx - 1, cy, cz) - present(L, k, cx + 1, cy, cz) - present(L, k, cx, cy - 1, cz) -
+                     present(L, k, cx, cy + 1, cz) - present(L, k, cx, cy, cz - 1) - present(L, k, cx, cy, cz + 1);
+    return 6.0 - L.ghost * miss;
+}
+
 static void p_matvec(const PLevel& L, const double* x, double* y) {
     const size_t N = (size_t)L.bs * L.bs * L.bs;
 #pragma omp parallel for schedule(static)
@@ -1001,7 +1037,8 @@ static void p_matvec(const PLevel& L, const double* x, double* y) {
             for (int cy = 0; cy < L.bs; ++cy)
                 for (int cx = 0; cx < L.bs; ++cx) {
                     size_t i = k * N + ((size_t)cx | ((size_t)cy << L.lg) | ((size_t)cz << (2 * L.lg)));
-                    y[i] = L.scale * (6.0 * x[i] - nbsum(L, x, k, cx, cy, cz));
+                    if (!L.mask.empty() && !L.mask[i]) { y[i] = 0.0; continue; }
+                    y[i] = L.scale * (diag_of(L, k, cx, cy, cz) * x[i] - nbsum(L, x, k, cx, cy, cz));
                 }
 }
 
@@ -1015,8 +1052,9 @@ static void p_jacobi(const PLevel& L, double* x, const double* b, double omega, 
                 for (int cy = 0; cy < L.bs; ++cy)
                     for (int cx = 0; cx < L.bs; ++cx) {
                         size_t i = k * N + ((size_t)cx | ((size_t)cy << L.lg) | ((size_t)cz << (2 * L.lg)));
+                        if (!L.mask.empty() && !L.mask[i]) { tmp[i] = 0.0; continue; }
                         double sn = nbsum(L, x, k, cx, cy, cz);
-                        tmp[i] = omega * (b[i] + L.scale * sn) / (6.0 * L.scale) + (1.0 - omega) * x[i];
+                        tmp[i] = omega * (b[i] + L.scale * sn) / (diag_of(L, k, cx, cy, cz) * L.scale) + (1.0 - omega) * x[i];
                     }
         std::copy(tmp.begin(), tmp.end(), x);
     }
@@ -1052,7 +1090,7 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
     while ((int)H.lv.size() < max_levels && H.lv.back().cells() > kPoissonDirect) {
         const PLevel& F = H.lv.back();
         PLevel C;
-        C.scale = F.scale * 0.5;
+        C.scale = F.scale * 0.25;
         if (F.bs >= 4) {
             C.bs = F.bs / 2; C.nx = F.nx; C.ny = F.ny; C.nz = F.nz;
             C.bids = F.bids;
@@ -1066,6 +1104,8 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
             C.bids.erase(std::unique(C.bids.begin(), C.bids.end()), C.bids.end());
         }
         C.lg = ilog2(C.bs);
+        const double d = 0.5 + std::ldexp(1.0, -(int)H.lv.size() - 1);
+        C.ghost = 1.0 - 1.0 / d;
         H.lv.push_back(C);
     }
     for (auto& L : H.lv) {
@@ -1073,6 +1113,26 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
         std::vector<int64_t> sl((size_t)(L.nx * L.ny * L.nz), -1);
         for (int64_t k = 0; k < L.n(); ++k) sl[L.bids[k]] = k;
         H.slot.push_back(sl);
+    }
+    // cell masks: a coarse cell is active when any of its 8 children is
+    for (size_t l = 1; l < H.lv.size(); ++l) {
+        PLevel& C = H.lv[l];
+        const PLevel& F = H.lv[l - 1];
+        const size_t N = (size_t)C.bs * C.bs * C.bs;
+        C.mask.assign(N * C.n(), 0);
+        for (int64_t k = 0; k < C.n(); ++k) {
+            const int64_t b = C.bids[k], bx = b % C.nx, by = (b / C.nx) % C.ny, bz = b / (C.nx * C.ny);
+            for (size_t v = 0; v < N; ++v) {
+                const int cx = v & (C.bs - 1), cy = (v >> C.lg) & (C.bs - 1), cz = (int)(v >> (2 * C.lg));
+                const int64_t q[3] = {bx * C.bs + cx, by * C.bs + cy, bz * C.bs + cz};
+                uint8_t a = 0;
+                for (int c = 0; c < 8; ++c) {
+                    const int64_t fi = cell_index(F, H.slot[l - 1], 2 * q[0] + (c & 1), 2 * q[1] + ((c >> 1) & 1), 2 * q[2] + (c >> 2));
+                    if (fi >= 0 && (F.mask.empty() || F.mask[fi])) a = 1;
+                }
+                C.mask[k * N + v] = a;
+            }
+        }
     }
     const PLevel& C = H.lv.back();
     const int64_t n = C.cells();
@@ -1084,6 +1144,7 @@ static void build_hier(PHier& H, const int64_t* active, int64_t n_active, int64_
         e[j] = 1.0;
         p_matvec(C, e.data(), col.data());
         for (int64_t i = 0; i < n; ++i) A[(size_t)i * n + j] = col[i];
+        if (!C.mask.empty() && !C.mask[j]) A[(size_t)j * n + j] = 1.0;  // inactive cell: identity row
         e[j] = 0.0;
     }
     for (int64_t j = 0; j < n; ++j) {
@@ -1133,27 +1194,50 @@ static void vcycle(const PHier& H, int l, double* x, const double* b, int nu1, i
     p_jacobi(F, x, b, omega, nu1, tmp);
     p_matvec(F, x, r.data());
     for (size_t i = 0; i < tot; ++i) r[i] = b[i] - r[i];
-    // restriction: each fine cell adds 1/8 of its residual to its parent cell
+    // restriction R = P^T / 8: each fine cell adds w / 8 of its residual to
+    // each of the (up to 8) coarse cells its prolongation reads
     for (int64_t k = 0; k < F.n(); ++k) {
         int64_t bid = F.bids[k], bx = bid % F.nx, by = (bid / F.nx) % F.ny, bz = bid / (F.nx * F.ny);
         for (int cz = 0; cz < F.bs; ++cz)
             for (int cy = 0; cy < F.bs; ++cy)
                 for (int cx = 0; cx < F.bs; ++cx) {
-                    int64_t gx = bx * F.bs + cx, gy = by * F.bs + cy, gz = bz * F.bs + cz;
-                    int64_t ci = cell_index(C, H.slot[l + 1], gx >> 1, gy >> 1, gz >> 1);
-                    bc[ci] += r[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))];
+                    const int64_t g[3] = {bx * F.bs + cx, by * F.bs + cy, bz * F.bs + cz};
+                    const double rf = r[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))];
+                    for (int c = 0; c < 8; ++c) {
+                        int64_t q[3];
+                        double w = 1.0;
+                        for (int a = 0; a < 3; ++a) {
+                            const bool far = (c >> a) & 1;
+                            q[a] = (g[a] >> 1) + (far ? ((g[a] & 1) ? 1 : -1) : 0);
+                            w *= far ? 0.25 : 0.75;
+                        }
+                        if (q[0] < 0 || q[1] < 0 || q[2] < 0) continue;
+                        const int64_t ci = cell_index(C, H.slot[l + 1], q[0], q[1], q[2]);
+                        if (ci >= 0 && (C.mask.empty() || C.mask[ci])) bc[ci] += (w * 0.125) * rf;
+                    }
                 }
     }
-    for (size_t i = 0; i < totc; ++i) bc[i] /= 8.0;
     vcycle(H, l + 1, xc.data(), bc.data(), nu1, nu2, omega);
-    for (int64_t k = 0; k < F.n(); ++k) {  // prolongation: injection
+    for (int64_t k = 0; k < F.n(); ++k) {  // prolongation: trilinear
         int64_t bid = F.bids[k], bx = bid % F.nx, by = (bid / F.nx) % F.ny, bz = bid / (F.nx * F.ny);
         for (int cz = 0; cz < F.bs; ++cz)
             for (int cy = 0; cy < F.bs; ++cy)
                 for (int cx = 0; cx < F.bs; ++cx) {
-                    int64_t gx = bx * F.bs + cx, gy = by * F.bs + cy, gz = bz * F.bs + cz;
-                    int64_t ci = cell_index(C, H.slot[l + 1], gx >> 1, gy >> 1, gz >> 1);
-                    x[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))] += g_corr * xc[ci];
+                    const int64_t g[3] = {bx * F.bs + cx, by * F.bs + cy, bz * F.bs + cz};
+                    double v = 0.0;
+                    for (int c = 0; c < 8; ++c) {
+                        int64_t q[3];
+                        double w = 1.0;
+                        for (int a = 0; a < 3; ++a) {
+                            const bool far = (c >> a) & 1;
+                            q[a] = (g[a] >> 1) + (far ? ((g[a] & 1) ? 1 : -1) : 0);
+                            w *= far ? 0.25 : 0.75;
+                        }
+                        if (q[0] < 0 || q[1] < 0 || q[2] < 0) continue;
+                        const int64_t ci = cell_index(C, H.slot[l + 1], q[0], q[1], q[2]);
+                        if (ci >= 0 && (C.mask.empty() || C.mask[ci])) v += w * xc[ci];
+                    }
+                    x[k * N + ((size_t)cx | ((size_t)cy << F.lg) | ((size_t)cz << (2 * F.lg)))] += g_corr * v;
                 }
     }
     p_jacobi(F, x, b, omega, nu2, tmp);

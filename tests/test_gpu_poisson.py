@@ -92,8 +92,27 @@ def test_vcycle_is_a_contraction(msbg, ctx):
         P.vcycle(x, b)
         norms.append(P.residual(x, b, r))
     factors = [norms[i + 1] / norms[i] for i in range(5)]
-    # piecewise-constant prolongation: a modest, mesh-dependent contraction
-    assert max(factors) < 0.9, factors
+    # trilinear prolongation, rediscretised coarse operators with boundary-
+    # corrected diagonals: the FP64 oracle contracts by 0.376-0.395 per
+    # V(2,2)-cycle here (w = 2/3 Jacobi smooths by 7/9 per sweep)
+    assert max(factors) < 0.42, factors
+
+
+def test_vcycle_contraction_matches_oracle_at_256(msbg, ctx, oracle):
+    """The level-0 blocks of the 256^3 three-level layout (776 blocks,
+    3.18 M unknowns): plain V-cycles and MG-PCG reach 1e-6 in the oracle's
+    iteration counts (13 and 8 in FP64)."""
+    from msbg_rs_b200 import workloads
+    lv = workloads.block_levels(256, 16, 0.35 * 256)
+    act = np.nonzero(lv == 0)[0].astype(np.uint64)
+    P = msbg.Poisson(ctx, 256, 256, 256, 16, act)
+    b = rhs(P.n, 5)
+    for method in (0, 1):
+        x, it, rel, _ = P.solve(b, method=method, tol=1e-6, max_iter=60)
+        _, ohist = oracle.poisson_solve(act.astype(np.int64), 16, 16, 16, 16, b.astype(np.float64), mode=method,
+                                        tol=1e-6, max_iter=60)
+        assert rel <= 1e-6
+        assert abs(len(ohist) - it) <= 1, (method, len(ohist), it)
 
 
 def test_zero_rhs_and_errors(msbg, ctx):
