@@ -354,6 +354,28 @@ def run_ours(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
+    # ---- end to end through the host-array entry point ----------------------
+    # msbg_flip_step: one call per step copies the step's inputs up from the
+    # (page-locked) host arrays, runs the whole step and returns once the new
+    # velocities are in the host output array -- what a host caller of the
+    # C ABI gets per step.  The pipelined figure above overlaps the copies of
+    # neighbouring steps with torch streams around the device-pointer entry
+    # points instead.
+    fstep = msbg.FlipStep(mac, coarse, levels)
+    fargs = (pin_pos.data_ptr(), pin_vel.data_ptr(), pin_mass.data_ptr(), n, R_P, int(msbg.Stencil.MeanCurvature), DT,
+             SWEEPS, ALPHA, pin_out.data_ptr())
+    fstep.step_ptrs(*fargs)  # sizes the step's device arrays
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        fstep.step_ptrs(*fargs)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    abi_ms = _max_over_ranks(dist, f0.elapsed_time(f1) / e2e_steps, dev)
+    fstep.close()
+
     # ---- roofline of the dominant kernel ------------------------------------
     peak, peak_kind = load_peaks()
     dom = max(kernels.items(), key=lambda kv: kv[1][1]) if kernels else ("none", (1, 1.0))
@@ -396,10 +418,16 @@ def run_ours(args, world, rank, local):
                    "p2g_active_blocks": n_active, "smoothed_level0_blocks": n_fine, "r_p": R_P,
                    "sweeps": SWEEPS, "stencil": "19-tap mean curvature", "parallelism": f"replicas x{world}",
                    "l2": "inputs (713 MB) larger than L2, no flush"},
-        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms, "steps": e2e_steps,
-                "copies": "every step: inputs host->device and new velocities device->host, on two copy streams "
-                          "overlapped with the device work of neighbouring steps",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": world * n / (abi_ms * 1e-3), "unit": UNIT, "ms_per_step": abi_ms, "steps": e2e_steps,
+                "api": "msbg_flip_step (C ABI, host arrays in page-locked memory; returns with the new velocities "
+                       "in the host array, in the caller's particle order)",
+                "copies": "every step: positions, velocities and masses host->device (velocities and masses beside "
+                          "the sort), new velocities device->host",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "pipelined_device_api": {
+                    "value": world * n / (e2e_ms * 1e-3), "ms_per_step": e2e_ms,
+                    "copies": "the same bytes on two torch copy streams, overlapped with the device work of "
+                              "neighbouring steps (identical inputs every step)"}},
         "gpu_launches": launches,
         "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
         "kernels_ms_per_step": {k: round(v[1] / prof_steps, 4) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])},
@@ -408,6 +436,15 @@ def run_ours(args, world, rank, local):
         "roofline": roof,
         "clocks": clk,
     }
+    if world == 1 and not args.no_submetrics:
+        # the other two parts of the metric, on their own configurations:
+        # smoother GB/s on the 2048^3 shell and the pressure solve's time to
+        # 1e-6 (plain MG, MG-PCG, learned PCG) on the 256^3 layout
+        del pos, vel, mass, keys, perm, spos, svel, smass, u, u_new
+        mac.close()
+        coarse.close()
+        torch.cuda.empty_cache()
+        line["submetrics"].update(submetric_lines(args, rank, local))
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ft, pos_h, vel_h, mass_h, budget_s=args.cpu_budget)
     if rank == 0:
@@ -417,18 +454,49 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def submetric_lines(args, rank, local):
+    """Smoother and pressure-solve parts of the metric, measured in this
+    process after the FLIP step (world size 1)."""
+    sub = argparse.Namespace(**vars(args))
+    sub.size, sub.steps, sub.warmup, sub.stencil = 2048, 3, 1, "laplacian"
+    sm = run_smoother(sub, 1, rank, local, emit=False)
+    sub = argparse.Namespace(**vars(args))
+    sub.size, sub.steps, sub.warmup = 256, 3, 1
+    po = run_poisson(sub, 1, rank, local, emit=False)
+    m = po["methods"]
+    head = po["learned"]["head"]
+    return {
+        "smoother_shell2048": {
+            "config": sm["config"], "cell_updates_per_s_7tap": sm["value"], "ms_per_10_sweeps_7tap": sm["ms_per_step"],
+            "roofline_7tap": sm["roofline"], "other_stencils": sm["submetrics"]["other_stencils"],
+            "jacobi": sm["submetrics"]["jacobi"], "clocks": sm["clocks"]},
+        "poisson_256": {
+            "config": po["config"], "metric": "time to 1e-6 relative residual (ms), FP64 true residual",
+            "plain_mg_ms": m["plain_mg"]["ms"], "plain_mg_vcycles": m["plain_mg"]["iterations"],
+            "mg_pcg_ms": m["mg_pcg"]["ms"], "mg_pcg_iterations": m["mg_pcg"]["iterations"],
+            "learned_pcg_ms": m[head]["ms"], "learned_pcg_iterations": m[head]["iterations"],
+            "learned_method": head,
+            "plain_mg_over_learned": m["plain_mg"]["ms"] / m[head]["ms"],
+            "mg_pcg_over_learned": m["mg_pcg"]["ms"] / m[head]["ms"],
+            "methods": {k: {"ms": v["ms"], "iterations": v["iterations"]} for k, v in m.items()},
+            "training": {k: po["learned"][k] for k in ("pairs", "adam_steps", "train_s", "loss_first", "loss_last")},
+            "training_outside_timed_region": True,
+            "roofline_jacobi": po["roofline"], "clocks": po["clocks"]},
+    }
+
+
 def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
     """Algorithmic HBM bytes moved by `launches` launches of `kernel` in one
     FLIP transfer step's accounting: 8 B per f32 cell-update for the in-place
-    smoother; 28 B read per particle per face direction for the P2G splat (x,
-    y, z, velocity component, mass, packed footprint; one launch per
-    direction); 24 B written per face-cell of the active blocks for the
-    combine; 12 B read + 12 B written per particle for G2P; 24 B per element
-    per onesweep radix pass (3 passes per sort)."""
+    smoother; 28 B per particle once per P2G for the splat (position, velocity
+    and mass read once: P2G_SPLAT_LAUNCHES launches make one P2G); 24 B
+    written per face-cell of the active blocks for the combine; 12 B read + 12
+    B written per particle for G2P; 24 B per element per onesweep radix pass
+    (3 passes per sort)."""
     if kernel in SWEEP_KERNELS:
         return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
-        return 28.0 * n * launches
+        return 28.0 * n * launches / P2G_SPLAT_LAUNCHES
     if kernel == "p2g_combine_kernel":
         return 24.0 * n_active * 4096 * launches
     if kernel == "g2p_kernel":
@@ -439,6 +507,9 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
         return 28.0 * n * launches
     return None
 
+
+# Launches of the splat kernel per P2G (one per face direction).
+P2G_SPLAT_LAUNCHES = 3
 
 # DRAM bytes (read + write) per launch measured by ncu on a smaller case of
 # the same kernel, per unit of work: p2g_cells_kernel at 128^3 (5,767,168
@@ -483,16 +554,17 @@ def cpu_baseline(ft, pos_h, vel_h, mass_h, budget_s=20.0):
     return {"value": res["value"], "unit": UNIT, "cores": res["threads"], "kind": "port", "sample": res["sample"]}
 
 
-def run_cpu_sample(oracle, ft, budget_s):
+def run_cpu_sample(oracle, ft, budget_s, full=False):
     """Times Morton sort + P2G + downsample + 10 multires sweeps + G2P on the
-    host for the particles of a contiguous run of level-0 blocks."""
+    host for the particles of a contiguous run of level-0 blocks (full: all
+    particles, the whole step)."""
     threads = oracle.num_threads()
     size, bsx = ft.size, ft.bsx
     per_block = 8 * bsx ** 3
-    k = 8
+    k = len(ft.fine_blocks) if full else 8
     results = None
     while True:
-        sel = slice(0, k * per_block)
+        sel = slice(0, ft.n) if full else slice(0, k * per_block)
         pos, vel, mass = ft.pos[sel], ft.vel[sel], ft.mass[sel]
         t = time.perf_counter()
         keys, perm = oracle.morton_sort(pos)
@@ -524,7 +596,7 @@ def run_cpu_sample(oracle, ft, budget_s):
         results = {"value": len(pos) / el, "threads": threads, "seconds": el,
                    "sample": f"{len(pos)} particles ({k} level-0 blocks of {len(ft.fine_blocks)}), full step pipeline, "
                              f"{el:.1f} s"}
-        if el > budget_s / 4 or k * 2 > len(ft.fine_blocks):
+        if full or el > budget_s / 4 or k * 2 > len(ft.fine_blocks):
             return results
         k *= 2
 
@@ -541,18 +613,21 @@ def run_reference(args, world, rank, local):
     from msbg_rs_b200 import workloads
 
     ft = workloads.flip_transfer(size=args.size, bsx=16, seed=2, ppc=8)
+    # every step is the whole step on every particle (the same configuration
+    # as the GPU arm); the warm-up steps are the same work, untimed
     for _ in range(args.warmup):
-        run_cpu_sample(oracle, ft, budget_s=4.0)
-    vals = [run_cpu_sample(oracle, ft, budget_s=args.cpu_budget) for _ in range(args.steps)]
-    v = statistics.median(r["value"] for r in vals)
+        run_cpu_sample(oracle, ft, budget_s=0.0, full=True)
+    vals = [run_cpu_sample(oracle, ft, budget_s=0.0, full=True) for _ in range(args.steps)]
+    step_s = statistics.mean(r["seconds"] for r in vals)
+    v = ft.n / step_s
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ft.n / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": f"FLIP transfer {args.size}^3, 16^3 blocks, 3 levels, 8 particles per level-0 cell",
                    "particles": ft.n, "parallelism": "host CPU"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["threads"], "kind": "port",
-                         "sample": vals[0]["sample"]},
+                         "sample": f"the whole step on all {ft.n} particles, every step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -595,14 +670,15 @@ SWEEP_TRAFFIC_2048 = 160.23e6 + 74.49e6
 SMOOTHER_STENCILS = {0: "7-tap laplacian", 1: "19-tap mean curvature", 2: "25-tap bilaplacian"}
 
 
-def run_smoother(args, world, rank, local):
-    """10 in-place sweeps of the 7-tap stencil over the shell per step."""
+def run_smoother(args, world, rank, local, emit=True):
+    """10 in-place sweeps of the 7-tap stencil over the shell per step.
+    emit=False: no process group, no CPU baseline; returns the line."""
     import torch
 
     msbg = load_package()
     from msbg_rs_b200 import workloads
 
-    dist = _dist_init(world, local)
+    dist = _dist_init(world, local) if emit else None
     dev = torch.device("cuda", local)
     size = args.size or 2048
     sp = workloads.shell_problem(size, 16, seed=1)
@@ -667,8 +743,10 @@ def run_smoother(args, world, rank, local):
             continue
         o_ms, o_k = timed(st, 2, 1)
         ok = sweep_kernel_time(o_k) or (1, float("nan"))
+        o_gbs = 8.0 * cells / (ok[1] / 2 * 1e-3) / 1e9
         others[SMOOTHER_STENCILS[st]] = {"ms_per_10_sweeps": o_ms, "cell_updates_per_s": cells / (o_ms * 1e-3),
-                                         "kernel_gbs_algorithmic": 8.0 * cells / (ok[1] / 2 * 1e-3) / 1e9}
+                                         "kernel_gbs_algorithmic": o_gbs, "frac_of_hbm": o_gbs / peak,
+                                         "kernel": sweep_kernel_name(o_k)}
     # weighted-Jacobi relaxation of the Poisson operator on the same blocks
     P = msbg.Poisson(ctx, size, size, size, 16, sp.active)
     x = torch.empty(P.n, device=dev)
@@ -714,6 +792,10 @@ def run_smoother(args, world, rank, local):
         "roofline": roof,
         "clocks": clk,
     }
+    if not emit:
+        grid.close()
+        ctx.close()
+        return line
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_smoother(sp, stencil, args.cpu_budget)
     if rank == 0:
@@ -769,12 +851,13 @@ def poisson_problem(size=256):
     return active, b
 
 
-def run_poisson(args, world, rank, local):
-    """Time to 1e-6 relative residual, plain V-cycles and MG-PCG."""
+def run_poisson(args, world, rank, local, emit=True):
+    """Time to 1e-6 relative residual, plain V-cycles and MG-PCG.
+    emit=False: no process group, no CPU baseline; returns the line."""
     import torch
 
     msbg = load_package()
-    dist = _dist_init(world, local)
+    dist = _dist_init(world, local) if emit else None
     dev = torch.device("cuda", local)
     size = args.size or 256
     active, bh = poisson_problem(size)
@@ -853,6 +936,7 @@ def run_poisson(args, world, rank, local):
                "loss_first": float(np.mean(hist[:20])) if len(hist) else None,
                "loss_last": float(np.mean(hist[-20:])) if len(hist) else None,
                "rel_error_fresh_pairs": ev,
+               "head": head,
                "speedup_vs_plain_mg": per_method["plain_mg"]["ms"] / per_method[head]["ms"],
                "speedup_vs_mg_pcg": per_method["mg_pcg"]["ms"] / per_method[head]["ms"]}
     peak, peak_kind = load_peaks()
@@ -891,11 +975,15 @@ def run_poisson(args, world, rank, local):
                      "launches": 20, "avg_launch_us": round(jac_us, 2)},
         "clocks": clk,
     }
+    P.close()
+    if not emit:
+        net.close()
+        ctx.close()
+        return line
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_poisson(active, bh, size)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    P.close()
     _finish(dist)
 
 
@@ -1230,6 +1318,8 @@ def main():
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-submetrics", action="store_true",
+                    help="flip: skip the smoother (2048^3 shell) and pressure-solve (256^3) parts of the metric")
     ap.add_argument("--train-rhs", type=int, default=100, help="poisson: right-hand sides generating training pairs")
     ap.add_argument("--problems", type=int, default=64, help="batched: number of problems")
     ap.add_argument("--check", type=int, default=8, help="batched: problems checked against the FP64 oracle")

@@ -63,6 +63,7 @@ typedef struct msbg_grid msbg_grid;
 typedef struct msbg_mac msbg_mac;
 typedef struct msbg_poisson msbg_poisson;
 typedef struct msbg_unet msbg_unet;
+typedef struct msbg_flip msbg_flip;
 
 /* ---- context ---------------------------------------------------------- */
 const char* msbg_status_string(int status);
@@ -249,6 +250,27 @@ int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u,
 /* Scalar trilinear Sampler::sample::<Linear> (math/sample.rs:494-512);
  * align 0 = Corner, 1 = CellCentered. */
 int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, int bc, float* out);
+
+/* ---- one FLIP transfer step through host arrays ------------------------- */
+/* The per-step composition of the crate's transfer entry points that a FLIP
+ * loop makes (bucket_particles + particles_to_grid, fluid/p2g.rs:141-164;
+ * Sweeper::sweep of the x-face mass, solver.rs:166-185; MacSampler::sample +
+ * g2p_blend, fluid/g2p.rs:15-45), with the host<->device copies inside the
+ * call.  levels ([n_levels] = one per block of the MAC grid) gives each
+ * block's resolution level; `coarse` has half the MAC grid's block size and
+ * receives the 2^3 downsample of the x-face mass that feeds the multires
+ * halos of the level-0 sweep. */
+int msbg_flip_create(msbg_mac* mac, msbg_grid* coarse, const uint8_t* levels, size_t n_levels, msbg_flip** out);
+int msbg_flip_destroy(msbg_flip* f);
+/* One step: pos, vel ([n][3] f32) and mass ([n]) are copied up; the particles
+ * are Morton-sorted (msbg_morton_sort_device), splatted (msbg_p2g_sorted_device,
+ * r_p), the x-face mass is smoothed by `sweeps` multires sweeps of `stencil`
+ * (dt) over the level-0 blocks of the new active set, velocities are sampled
+ * back (Clamp) and blended (alpha), and vel_out[i] ([n][3], host) receives the
+ * new velocity of input particle i.  Returns when vel_out is written.  Host
+ * arrays from page-locked memory copy at full PCIe speed. */
+int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float* mass, size_t n, float r_p, int stencil,
+                   float dt, int sweeps, float alpha, float* vel_out);
 
 /* ---- multiresolution transfers (multires/downsample.rs) ----------------- */
 /* downsample_channel_avg (downsample.rs:13-59): every value block of `src`

@@ -94,6 +94,9 @@ SIGNATURES = {
     "msbg_g2p_blend_device": [_P, _P, _P, _P, _SZ, _F, _P],
     "msbg_sample_linear": [_P, _P, _SZ, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_flip_create": [_P, _P, _P, _SZ, C.POINTER(_P)],
+    "msbg_flip_destroy": [_P],
+    "msbg_flip_step": [_P, _P, _P, _P, _SZ, _F, _I, _F, _I, _F, _P],
     "msbg_conv3_forward_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P, _I, _I, _P],
     "msbg_conv3_wgrad_device": [_P, _P, C.c_int64, _I, _I, _I, _P, _P, _P],
     "msbg_unet_create": [_P, _U64, _U64, _U64, _P, _SZ, _U64, C.POINTER(_P)],

@@ -576,11 +576,13 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
         if (l > 0) {
             const PLevelDev& F = P->lv[l - 1];
             const int mf = F.bs - 1;
+            const bool same_grid = F.bs == 2 * L.bs;  // same block grid: the children of block k are in fine block k
             for (int64_t k = 0; k < L.n(); ++k)
                 for (int64_t v = 0; v < N; ++v) {
                     const int64_t q[3] = {coords[l][3 * k] * (int64_t)bs + (v & m), coords[l][3 * k + 1] * (int64_t)bs + ((v >> L.lg) & m),
                                           coords[l][3 * k + 2] * (int64_t)bs + (v >> (2 * L.lg))};
-                    const int32_t fs = slot_at(l - 1, (2 * q[0]) >> F.lg, (2 * q[1]) >> F.lg, (2 * q[2]) >> F.lg);
+                    const int32_t fs = same_grid ? (int32_t)k
+                                                 : slot_at(l - 1, (2 * q[0]) >> F.lg, (2 * q[1]) >> F.lg, (2 * q[2]) >> F.lg);
                     uint8_t a = 0;
                     if (fs >= 0)
                         for (int c = 0; c < 8; ++c) {

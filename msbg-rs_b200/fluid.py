@@ -122,3 +122,46 @@ def g2p_blend(u_old: np.ndarray, u: np.ndarray, u_tilde: np.ndarray, alpha: floa
     a = np.float32(alpha)
     delta = (u.astype(np.float32) - u_tilde.astype(np.float32)).astype(np.float32)
     return ((u_old.astype(np.float32) + delta) * a + u.astype(np.float32) * (np.float32(1.0) - a)).astype(np.float32)
+
+
+class FlipStep:
+    """One FLIP transfer step through host arrays (msbg_flip_step): Morton
+    sort, particles_to_grid (fluid/p2g.rs:141-164), `sweeps` multires sweeps
+    of the x-face mass over the level-0 blocks (solver.rs:166-185),
+    MacSampler::sample + g2p_blend (fluid/g2p.rs:15-45), with the copies in
+    the call.  `levels` holds one level per block of the MAC grid; `coarse`
+    has half its block size."""
+
+    def __init__(self, mac: MacGrid, coarse: SparseGrid, levels):
+        self.mac, self.coarse = mac, coarse
+        self.levels = np.ascontiguousarray(levels, np.uint8)
+        h = C.c_void_p()
+        call("msbg_flip_create", mac.handle, coarse.handle, ptr(self.levels), len(self.levels), C.byref(h))
+        self.handle = h
+
+    def step_ptrs(self, pos_ptr: int, vel_ptr: int, mass_ptr: int, n: int, r_p: float, stencil: int, dt: float,
+                  sweeps: int, alpha: float, out_ptr: int) -> None:
+        """Host addresses (e.g. of page-locked buffers); out gets [n][3]."""
+        call("msbg_flip_step", self.handle, C.c_void_p(pos_ptr), C.c_void_p(vel_ptr), C.c_void_p(mass_ptr), int(n),
+             float(r_p), int(stencil), float(dt), int(sweeps), float(alpha), C.c_void_p(out_ptr))
+
+    def step(self, positions, velocities, mass, r_p: float, stencil: int, dt: float, sweeps: int,
+             alpha: float) -> np.ndarray:
+        p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        v = np.ascontiguousarray(velocities, np.float32).reshape(-1, 3)
+        m = np.ascontiguousarray(mass, np.float32).reshape(-1)
+        out = np.empty_like(v)
+        self.step_ptrs(p.ctypes.data, v.ctypes.data, m.ctypes.data, len(p), r_p, stencil, dt, sweeps, alpha,
+                       out.ctypes.data)
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            call("msbg_flip_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
