@@ -250,6 +250,14 @@ int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u,
 /* Scalar trilinear Sampler::sample::<Linear> (math/sample.rs:494-512);
  * align 0 = Corner, 1 = CellCentered. */
 int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, int bc, float* out);
+/* Sampler::sample / gradient / hessian (math/sample.rs:493-649) beyond the
+ * trilinear value: mode 0 = cubic B-spline value (out[n]), 1 = cubic
+ * gradient (out[n][3]), 2 = cubic Hessian (out[n][6]: fxx, fyy, fzz, fxy, fxz,
+ * fyz), 3 = trilinear gradient at `align` (out[n][3]).  The cubic basis
+ * (math/bspline.rs:4-32) is cell-centred whatever `align` says, with a 4^3
+ * window from gather_map (math/gather.rs:54-158); f32 grids, blocks >= 4^3. */
+int msbg_sample_ext(msbg_grid* grid, const float* pos, size_t n, int mode, int align, int bc, float* out);
+int msbg_sample_ext_device(msbg_grid* grid, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out);
 
 /* ---- one FLIP transfer step through host arrays ------------------------- */
 /* The per-step composition of the crate's transfer entry points that a FLIP

@@ -93,6 +93,8 @@ SIGNATURES = {
     "msbg_g2p_device": [_P, _P, _SZ, _I, _P],
     "msbg_g2p_blend_device": [_P, _P, _P, _P, _SZ, _F, _P],
     "msbg_sample_linear": [_P, _P, _SZ, _I, _I, _P],
+    "msbg_sample_ext": [_P, _P, _SZ, _I, _I, _I, _P],
+    "msbg_sample_ext_device": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
     "msbg_flip_create": [_P, _P, _P, _SZ, C.POINTER(_P)],
     "msbg_flip_destroy": [_P],

@@ -122,6 +122,168 @@ __global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, i
     }
 }
 
+// gather_map (math/gather.rs:54-158) for a window of SPAN = dmax + 1 (2 or
+// 4) anchored at (ix0, iy0, iz0): the one-block fast path, else the 2x2x2
+// block slots from the clamped anchor block and per-axis boundary resolution.
+template <int SPAN>
+__device__ void gather_window_dev(const SampleGrid& g, int32_t ix0, int32_t iy0, int32_t iz0, int bc, float* out) {
+    constexpr int DMAX = SPAN - 1;
+    const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
+    if (ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + DMAX < g.sx && iy0 + DMAX < g.sy && iz0 + DMAX < g.sz) {
+        const int vx0 = ix0 & mask, vy0 = iy0 & mask, vz0 = iz0 & mask;
+        if (vx0 + DMAX < bsx && vy0 + DMAX < bsx && vz0 + DMAX < bsx) {
+            const uint64_t bid = (uint64_t)(ix0 >> lg) + (uint64_t)(iy0 >> lg) * g.nx + (uint64_t)(iz0 >> lg) * g.nx * g.ny;
+            const int32_t code = block_code(g, bid);
+            int s = 0;
+#pragma unroll
+            for (int k = 0; k < SPAN; ++k)
+#pragma unroll
+                for (int j = 0; j < SPAN; ++j)
+#pragma unroll
+                    for (int i = 0; i < SPAN; ++i)
+                        out[s++] = code_value(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
+            return;
+        }
+    }
+    const int64_t bx0 = min(max((int64_t)(ix0 >> lg), (int64_t)0), g.nx - 1);
+    const int64_t by0 = min(max((int64_t)(iy0 >> lg), (int64_t)0), g.ny - 1);
+    const int64_t bz0 = min(max((int64_t)(iz0 >> lg), (int64_t)0), g.nz - 1);
+    int32_t codes[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int64_t bxx = min(bx0 + (s & 1), g.nx - 1), byy = min(by0 + ((s >> 1) & 1), g.ny - 1),
+                      bzz = min(bz0 + (s >> 2), g.nz - 1);
+        codes[s] = block_code(g, (uint64_t)bxx + (uint64_t)byy * g.nx + (uint64_t)bzz * g.nx * g.ny);
+    }
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SPAN; ++k) {
+        int32_t rz;
+        const bool okz = resolve_axis(iz0 + k, g.sz - 1, bc, &rz);
+#pragma unroll
+        for (int j = 0; j < SPAN; ++j) {
+            int32_t ry;
+            const bool oky = resolve_axis(iy0 + j, g.sy - 1, bc, &ry);
+#pragma unroll
+            for (int i = 0; i < SPAN; ++i) {
+                int32_t rx;
+                const bool okx = resolve_axis(ix0 + i, g.sx - 1, bc, &rx);
+                if (okx && oky && okz) {
+                    const int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) |
+                                         ((((rz >> lg) - bz0) & 1) << 2));
+                    out[s] = code_value(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
+                } else {
+                    out[s] = g.empty;
+                }
+                ++s;
+            }
+        }
+    }
+}
+
+// math/bspline.rs:4-32 uniform cubic B-spline weights, first and second
+// derivative weights (f32, left to right; built without contraction).
+__device__ __forceinline__ void cubic_w_dev(float t, float w[4]) {
+    const float m = 1.0f - t, s6 = 1.0f / 6.0f, t3 = 2.0f / 3.0f;
+    w[0] = ((s6 * m) * m) * m;
+    w[1] = t3 - ((0.5f * t) * t) * (2.0f - t);
+    w[2] = t3 - ((0.5f * m) * m) * (1.0f + t);
+    w[3] = ((s6 * t) * t) * t;
+}
+__device__ __forceinline__ void cubic_dw_dev(float t, float w[4]) {
+    const float m = 1.0f - t;
+    w[0] = ((-m) * m) / 2.0f;
+    w[1] = (0.5f * t) * t - (2.0f - t) * t;
+    w[2] = m * (t + 1.0f) - (0.5f * m) * m;
+    w[3] = (t * t) / 2.0f;
+}
+__device__ __forceinline__ void cubic_d2w_dev(float t, float w[4]) {
+    w[0] = 1.0f - t;
+    w[1] = 3.0f * t - 2.0f;
+    w[2] = 1.0f - 3.0f * t;
+    w[3] = t;
+}
+// (f * w).reduce_sum() of one window row: lanes added in order
+__device__ __forceinline__ float row_dot_dev(const float* f, const float w[4]) {
+    return ((f[0] * w[0] + f[1] * w[1]) + f[2] * w[2]) + f[3] * w[3];
+}
+
+// Sample for SparseGrid (math/sample.rs:493-649).  mode 0: cubic B-spline
+// value -> out[n]; 1: cubic gradient -> out[n][3]; 2: cubic Hessian (fxx,
+// fyy, fzz, fxy, fxz, fyz) -> out[n][6]; 3: trilinear gradient
+// (trilinear_value_grad, sample.rs:215-237) at `align` -> out[n][3].  The
+// cubic basis is cell-centred whatever the alignment: window base
+// floor(p - 0.5) - 1, t = frac(p - 0.5).  One thread per position.
+__global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, size_t n, int mode, int align, int bc,
+                                  float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        if (mode == 3) {
+            if (align == 1) { x = x - 0.5f; y = y - 0.5f; z = z - 0.5f; }
+            const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+            float c[8];
+            gather_window_dev<2>(g, (int32_t)fx, (int32_t)fy, (int32_t)fz, bc, c);
+            const float u = x - fx, v = y - fy, w = z - fz;
+            const float f01234567 = ((((((c[7] - c[6]) - c[5]) + c[4]) - c[3]) + c[2]) + c[1]) - c[0];
+            const float f01234567u = f01234567 * u;
+            const float f01234567uf6420 = (((f01234567u + c[6]) - c[4]) - c[2]) + c[0];
+            const float f5410 = ((c[5] - c[4]) - c[1]) + c[0];
+            const float f3210 = ((c[3] - c[2]) - c[1]) + c[0];
+            out[3 * i] = fmaf(f01234567 * v + f5410, w, (f3210 * v + c[1]) - c[0]);
+            out[3 * i + 1] = fmaf(f01234567uf6420, w, (f3210 * u + c[2]) - c[0]);
+            out[3 * i + 2] = fmaf(f01234567uf6420, v, (f5410 * u + c[4]) - c[0]);
+            continue;
+        }
+        x = x - 0.5f; y = y - 0.5f; z = z - 0.5f;
+        const float xf = floorf(x), yf = floorf(y), zf = floorf(z);
+        const float tx = x - xf, ty = y - yf, tz = z - zf;
+        float win[64];
+        gather_window_dev<4>(g, (int32_t)xf - 1, (int32_t)yf - 1, (int32_t)zf - 1, bc, win);
+        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4], ddx[4], ddy[4], ddz[4];
+        cubic_w_dev(tx, wx); cubic_w_dev(ty, wy); cubic_w_dev(tz, wz);
+        cubic_dw_dev(tx, dx); cubic_dw_dev(ty, dy); cubic_dw_dev(tz, dz);
+        cubic_d2w_dev(tx, ddx); cubic_d2w_dev(ty, ddy); cubic_d2w_dev(tz, ddz);
+        float val = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        float fxx = 0.0f, fyy = 0.0f, fzz = 0.0f, fxy = 0.0f, fxz = 0.0f, fyz = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float* f = win + 16 * k + 4 * j;
+                const float sx = row_dot_dev(f, wx);
+                if (mode == 0) {
+                    val = fmaf(sx, wy[j] * wz[k], val);
+                } else if (mode == 1) {
+                    const float sxp = row_dot_dev(f, dx);
+                    const float wyz = wy[j] * wz[k];
+                    val = fmaf(sx, wyz, val);
+                    gx = fmaf(sxp, wyz, gx);
+                    gy = fmaf(sx, dy[j] * wz[k], gy);
+                    gz = fmaf(sx, wy[j] * dz[k], gz);
+                } else {
+                    const float sxp = row_dot_dev(f, dx), sxpp = row_dot_dev(f, ddx);
+                    const float wyz = wy[j] * wz[k], wpyz = dy[j] * wz[k], wypz = wy[j] * dz[k];
+                    const float wppyz = ddy[j] * wz[k], wyppz = wy[j] * ddz[k], wpyzp = dy[j] * dz[k];
+                    fxx = fmaf(sxpp, wyz, fxx);
+                    fyy = fmaf(sx, wppyz, fyy);
+                    fzz = fmaf(sx, wyppz, fzz);
+                    fxy = fmaf(sxp, wpyz, fxy);
+                    fxz = fmaf(sxp, wypz, fxz);
+                    fyz = fmaf(sx, wpyzp, fyz);
+                }
+            }
+        if (mode == 0) out[i] = val;
+        else if (mode == 1) {
+            out[3 * i] = gx;
+            out[3 * i + 1] = gy;
+            out[3 * i + 2] = gz;
+        } else {
+            float* h = out + 6 * i;
+            h[0] = fxx; h[1] = fyy; h[2] = fzz; h[3] = fxy; h[4] = fxz; h[5] = fyz;
+        }
+    }
+}
+
 // One component's sample when its 2x2x2 corners lie inside the domain
 // (gather_map's interior case, no boundary condition applies): the code of
 // the block of corner (0, 0, 0) and, for corners in the next block along an
@@ -479,6 +641,44 @@ int msbg_sample_linear(msbg_grid* g, const float* pos, size_t n, int align, int 
     sample_linear_kernel<<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout);
     after_launch(g->ctx, "sample_linear_kernel");
     CUDA_CHECK(cudaMemcpyAsync(out, dout, 4 * n, cudaMemcpyDeviceToHost, g->ctx->stream));
+    sync(g->ctx);
+    MSBG_API_END
+}
+
+static int sample_width(int mode) { return mode == 0 ? 1 : mode == 2 ? 6 : 3; }
+
+int msbg_sample_ext_device(msbg_grid* g, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(g && ((d_pos && d_out) || !n), "null argument");
+    MSBG_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0 (cubic value), 1 (cubic gradient), 2 (Hessian) or 3 (trilinear gradient)");
+    MSBG_REQUIRE(align == 0 || align == 1, "align must be 0 (Corner) or 1 (CellCentered)");
+    MSBG_REQUIRE(bc >= 0 && bc <= 2, "bad boundary condition");
+    MSBG_REQUIRE(g->bsx >= 4, "cubic sampling needs blocks of at least 4^3 cells");
+    if (!n) return MSBG_OK;
+    set_device(g->ctx);
+    SampleGrid s = sample_grid(g);
+    begin_launch(g->ctx);
+    sample_ext_kernel<<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out);
+    after_launch(g->ctx, "sample_ext_kernel");
+    MSBG_API_END
+}
+
+int msbg_sample_ext(msbg_grid* g, const float* pos, size_t n, int mode, int align, int bc, float* out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(g && ((pos && out) || !n), "null argument");
+    MSBG_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0 (cubic value), 1 (cubic gradient), 2 (Hessian) or 3 (trilinear gradient)");
+    if (!n) return MSBG_OK;
+    set_device(g->ctx);
+    const int w = sample_width(mode);
+    ScratchLayout L;
+    size_t op = L.add<float>(3 * n), oo = L.add<float>((size_t)w * n);
+    char* base = scratch(g->ctx, L);
+    float* dp = ScratchLayout::at<float>(base, op);
+    float* dout = ScratchLayout::at<float>(base, oo);
+    CUDA_CHECK(cudaMemcpyAsync(dp, pos, 12 * n, cudaMemcpyHostToDevice, g->ctx->stream));
+    const int st = msbg_sample_ext_device(g, dp, n, mode, align, bc, dout);
+    if (st != MSBG_OK) MSBG_THROW(st, msbg_last_error());
+    CUDA_CHECK(cudaMemcpyAsync(out, dout, 4 * (size_t)w * n, cudaMemcpyDeviceToHost, g->ctx->stream));
     sync(g->ctx);
     MSBG_API_END
 }

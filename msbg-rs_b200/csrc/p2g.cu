@@ -508,6 +508,318 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
 }
 
+// Splat for r_p = 2 (M = 2): all three face directions in one launch, CTA
+// 3k + d taking particle block k and direction d, so a block's three CTAs run
+// side by side and read its particles from L2 once.  Tiles, colours, the
+// tile-order waits and the FP64 window are those of p2g_cells_kernel; the
+// per-cell work differs.  With r_p = 2 the clipped footprint of a particle
+// in cell c spans cells [c-2+a, c+1+a] along each lane axis (a = 0 or 1 by
+// the side of the cell centre the particle lies on) and faces [c-2, c+1]
+// along the face axis, except when a coordinate lies exactly on a cell
+// centre (lane axes) or a face plane (face axis).  The cell's regular
+// particles are grouped by (a_U, a_V); within a group, 16 lanes cover the
+// 4 x 4 footprint rows of one particle and the two half-warps take two
+// particles at a time, each lane keeping the 4 faces of its row in FP64
+// registers, so every evaluated term is inside the footprint.  After each
+// group the half-warp sums are added (lower half first) and written into
+// the window.  The cell's other particles then go through the lane-bit path
+// of p2g_cells_kernel, adding straight into the window.  Every term is the
+// reference's f32 operation sequence (p2g.rs:263-330); the sums are FP64 in
+// a fixed order.
+template <int BSX, int DIR>
+__device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb, double* st, uint32_t* s_done,
+                                              const uint16_t* s_order, uint32_t* s_next) {
+    constexpr int M = 2;
+    constexpr int W = BSX + 2 * M;
+    constexpr int WW = W * W * W;
+    constexpr int WIN = 2 * M + 1;
+    constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
+    constexpr int NNB = WIN * WIN * WIN;
+    constexpr int CAP = SplatCap<BSX, M>::v;
+    constexpr int NR = (NNB + 31) / 32;
+    constexpr int F = DIR, U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2;
+    const int tid = threadIdx.x, lane = tid & 31;
+    float4* wslot = reinterpret_cast<float4*>(st + 2 * WW) + (size_t)(tid >> 5) * 2 * CAP;
+    const uint64_t key = a.pb_key[k_pb];
+    const int32_t b0[3] = {(int32_t)compact3(key) * BSX, (int32_t)compact3(key >> 1) * BSX,
+                           (int32_t)compact3(key >> 2) * BSX};
+    const int32_t* cb = a.cell_begin + (size_t)k_pb * BSX * BSX * BSX;
+    const int32_t* ce = a.cell_end + (size_t)k_pb * BSX * BSX * BSX;
+    const float* __restrict__ pv = a.pv[DIR];
+    const uint64_t* __restrict__ lmask = a.lane_mask[DIR];
+    const float inv_r2 = a.inv_r2, r_p = a.r_p;
+    // this lane's footprint row inside a group: (i, j) along (U, V)
+    const int li = lane & 3, lj = (lane >> 2) & 3;
+    const bool lower = lane < 16;
+    while (true) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(s_next, 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= (uint32_t)NT) break;
+        const int t = s_order[q];
+        const int tc[3] = {t % T, (t / T) % T, t / (T * T)};
+        const int ci = tc[0] % K + K * (tc[1] % K + K * (tc[2] % K));
+        int cbeg = 0, cend = 0;
+        if (lane < 8) {
+            const uint32_t lm = (uint32_t)morton3(2 * tc[0] + (lane & 1), 2 * tc[1] + ((lane >> 1) & 1), 2 * tc[2] + (lane >> 2));
+            cbeg = cb[lm];
+            cend = ce[lm];
+        }
+        uint32_t nbi[(NR + 1) / 2];
+#pragma unroll
+        for (int k = 0; k < (NR + 1) / 2; ++k) nbi[k] = 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            const int o = lane + 32 * k;
+            const int nx = tc[0] + o % WIN - M, ny = tc[1] + (o / WIN) % WIN - M, nz = tc[2] + o / (WIN * WIN) - M;
+            const bool dep = o < NNB && nx >= 0 && ny >= 0 && nz >= 0 && nx < T && ny < T && nz < T &&
+                             nx % K + K * (ny % K + K * (nz % K)) < ci;
+            if (dep) nbi[k >> 1] &= ~(0xffffu << (16 * (k & 1))) | ((uint32_t)(nx + T * (ny + T * nz)) << (16 * (k & 1)));
+        }
+        bool deps_pending = true;
+        auto wait_deps = [&]() {
+            uint64_t t0 = 0;
+            uint32_t spins = 0, sleep_ns = 32;
+            while (true) {
+                bool ready = true;
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const uint32_t idx = (nbi[k >> 1] >> (16 * (k & 1))) & 0xffffu;
+                    if (idx != 0xffffu) {
+                        if (*(volatile uint32_t*)&s_done[idx]) nbi[k >> 1] |= 0xffffu << (16 * (k & 1));
+                        else ready = false;
+                    }
+                }
+                if (__all_sync(0xffffffffu, ready)) break;
+                __nanosleep(sleep_ns);
+                sleep_ns = sleep_ns < 512 ? 2 * sleep_ns : 512;
+                if ((++spins & 63u) == 0) {
+                    const uint64_t now = globaltimer_ns();
+                    if (!t0) t0 = now;
+                    else if (now - t0 > kWaitLimitNs) {
+                        if (lane == 0) atomicOr(a.status, 4);
+                        break;
+                    }
+                }
+            }
+            __threadfence_block();
+            deps_pending = false;
+        };
+        const int e_tile = (int)__reduce_max_sync(0xffffffffu, lane < 8 ? (uint32_t)cend : 0u);
+        int st_lo = 0, st_hi = 0;
+        for (int sub = 0; sub < 8; ++sub) {
+            const int b = __shfl_sync(0xffffffffu, cbeg, sub), e = __shfl_sync(0xffffffffu, cend, sub);
+            if (b >= e) continue;
+            int cell[3];
+            cell[0] = 2 * tc[0] + (sub & 1);
+            cell[1] = 2 * tc[1] + ((sub >> 1) & 1);
+            cell[2] = 2 * tc[2] + (sub >> 2);
+            // face positions along F (faces -2 .. +1 of the cell, in pairs)
+            uint64_t gf2[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                gf2[h] = f2_pack((float)(b0[F] - M + cell[F] + 2 * h), (float)(b0[F] - M + cell[F] + 2 * h + 1));
+            for (int p0 = b; p0 < e;) {
+                if (p0 < st_lo || p0 >= st_hi) {
+                    __syncwarp();
+                    st_lo = p0;
+                    st_hi = min(p0 + CAP, e_tile);
+#pragma unroll
+                    for (int k = 0; k < CAP / 32; ++k) {
+                        const int pl = st_lo + lane + 32 * k;
+                        if (pl < st_hi) {
+                            const uint64_t fb = lmask[pl];
+                            const float m = a.pm[pl];
+                            const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
+                            // footprint starts and ends exactly as the reference computes them
+                            int cat = 4;
+                            {
+                                const int cU = pp[U] > 0.0f ? (int)pp[U] : 0, cV = pp[V] > 0.0f ? (int)pp[V] : 0,
+                                          cF = pp[F] > 0.0f ? (int)pp[F] : 0;
+                                const int sU = (int)ceilf((pp[U] - r_p) - 0.5f), eU = (int)floorf((pp[U] + r_p) - 0.5f);
+                                const int sV = (int)ceilf((pp[V] - r_p) - 0.5f), eV = (int)floorf((pp[V] + r_p) - 0.5f);
+                                const int sF = (int)ceilf((pp[F] - r_p) - 1.0f), eF = (int)floorf((pp[F] + r_p) - 1.0f);
+                                const int aU = sU - cU + 2, aV = sV - cV + 2;
+                                if (eU - sU == 3 && eV - sV == 3 && sF == cF - 2 && eF == cF + 1 && (unsigned)aU <= 1u &&
+                                    (unsigned)aV <= 1u)
+                                    cat = aU | (aV << 1);
+                            }
+                            wslot[pl - st_lo] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
+                            wslot[CAP + pl - st_lo] = make_float4(m * pv[pl], __uint_as_float((uint32_t)fb),
+                                                                  __uint_as_float((uint32_t)(fb >> 32)), __int_as_float(cat));
+                        }
+                    }
+                    __syncwarp();
+                }
+                const int pend = min(e, st_hi);
+                for (int c0 = p0; c0 < pend; c0 += 32) {
+                    const int my = c0 + lane < pend ? __float_as_int(wslot[CAP + c0 + lane - st_lo].w) : 7;
+#pragma unroll 1
+                    for (int g = 0; g < 4; ++g) {
+                        uint32_t gm = __ballot_sync(0xffffffffu, my == g);
+                        if (!gm) continue;
+                        // this lane's row: lane-axis offsets -2 + a + (i, j) from the cell
+                        const int su = cell[U] + (g & 1) + li, sv = cell[V] + (g >> 1) + lj;
+                        const float gu = (float)(b0[U] - M + su), gv = (float)(b0[V] - M + sv);
+                        double am[4], av[4];
+#pragma unroll
+                        for (int s = 0; s < 4; ++s) am[s] = av[s] = 0.0;
+                        while (gm) {
+                            const int j1 = __ffs(gm) - 1;
+                            gm &= gm - 1;
+                            const int j2 = gm ? __ffs(gm) - 1 : -1;
+                            if (gm) gm &= gm - 1;
+                            const bool on = lower || j2 >= 0;
+                            const int jj = c0 - st_lo + (lower || j2 < 0 ? j1 : j2);
+                            const float4 P = wslot[jj];
+                            const float4 R = wslot[CAP + jj];
+                            const float m_p = P.w, scale_mom = R.x;
+                            const float du = gu - P.x, dv = gv - P.y;
+                            const uint64_t pf2 = f2_pack(P.z, P.z);
+                            float hoist0 = 0.0f, hoist1 = 0.0f;
+                            if (DIR == 0) hoist0 = dv * dv + du * du;
+                            else { hoist0 = dv * dv; hoist1 = du * du; }
+                            const uint64_t h02 = f2_pack(hoist0, hoist0), h12 = f2_pack(hoist1, hoist1);
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const uint64_t df = f2_sub(gf2[h], pf2);
+                                float d0, d1;
+                                f2_unpack(df, d0, d1);
+                                const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
+                                uint64_t dist;
+                                if (DIR == 0) dist = f2_add(sq, h02);
+                                else if (DIR == 1) dist = f2_add(h12, f2_add(h02, sq));
+                                else dist = f2_add(h12, f2_add(sq, h02));
+                                const uint64_t df2 = f2_add(f2_add(dist, df), f2_pack(0.25f, 0.25f));
+                                float e0, e1;
+                                f2_unpack(df2, e0, e1);
+                                const uint64_t tt = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
+                                float w0, w1;
+                                f2_unpack(tt, w0, w1);
+                                w0 = on ? fmaxf(w0, 0.0f) : 0.0f;
+                                w1 = on ? fmaxf(w1, 0.0f) : 0.0f;
+                                uint64_t w = f2_pack(w0, w1);
+                                w = f2_mul(f2_mul(w, w), w);
+                                float tm0, tm1, tv0, tv1;
+                                f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
+                                f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
+                                am[2 * h] += (double)tm0;
+                                av[2 * h] += (double)tv0;
+                                am[2 * h + 1] += (double)tm1;
+                                av[2 * h + 1] += (double)tv1;
+                            }
+                        }
+#pragma unroll
+                        for (int s = 0; s < 4; ++s) {
+                            am[s] += __shfl_down_sync(0xffffffffu, am[s], 16);
+                            av[s] += __shfl_down_sync(0xffffffffu, av[s], 16);
+                        }
+                        if (deps_pending) wait_deps();
+                        if (lower) {
+#pragma unroll
+                            for (int s = 0; s < 4; ++s) {
+                                int sc[3];
+                                sc[F] = cell[F] + s;  // faces -2 .. +1: staging cell[F] + M - 2 + s
+                                sc[U] = su;
+                                sc[V] = sv;
+                                const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                                st[si] += am[s];
+                                st[WW + si] += av[s];
+                            }
+                        }
+                        __syncwarp();
+                    }
+                    // the chunk's other particles: lanes take the 5 x 5 rows
+                    // around the cell, faces by the lane bits
+                    uint32_t rm = __ballot_sync(0xffffffffu, my == 4);
+                    while (rm) {
+                        const int jr = __ffs(rm) - 1;
+                        rm &= rm - 1;
+                        if (deps_pending) wait_deps();
+                        const float4 P = wslot[c0 + jr - st_lo];
+                        const float4 R = wslot[CAP + c0 + jr - st_lo];
+                        const uint32_t f_lo = __float_as_uint(R.y), f_hi = __float_as_uint(R.z);
+                        const bool on = lane < WIN * WIN;
+                        const uint32_t lanebit = on ? ((f_lo >> lane) & 1u) : 0u;
+                        const uint32_t fbits = (f_hi >> 24) & (0u - lanebit);
+                        const int su = cell[U] + lane % WIN, sv = cell[V] + lane / WIN;
+                        const float du = (float)(b0[U] - M + su) - P.x, dv = (float)(b0[V] - M + sv) - P.y;
+                        float hoist0 = 0.0f, hoist1 = 0.0f;
+                        if (DIR == 0) hoist0 = dv * dv + du * du;
+                        else { hoist0 = dv * dv; hoist1 = du * du; }
+                        if (on) {
+#pragma unroll
+                            for (int s = 0; s < WIN; ++s) {
+                                const int sf = cell[F] + s - 1;
+                                if (sf < 0 || sf >= W || !((fbits >> s) & 1u)) continue;
+                                const float df = (float)(b0[F] - M + sf) - P.z;
+                                const float sq = df * df;
+                                float dist;
+                                if (DIR == 0) dist = sq + hoist0;
+                                else if (DIR == 1) dist = hoist1 + (hoist0 + sq);
+                                else dist = hoist1 + (sq + hoist0);
+                                const float df2 = (dist + df) + 0.25f;
+                                float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
+                                w = (w * w) * w;
+                                int sc[3];
+                                sc[F] = sf;
+                                sc[U] = su;
+                                sc[V] = sv;
+                                const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                                st[si] += (double)(w * P.w);
+                                st[WW + si] += (double)(w * R.x);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+                p0 = pend;
+            }
+        }
+        __syncwarp();
+        __threadfence_block();
+        if (lane == 0) *(volatile uint32_t*)&s_done[t] = 1u;
+    }
+    __syncthreads();
+    double* out = a.partial + ((size_t)k_pb * 3 + DIR) * 2 * WW;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
+}
+
+template <int BSX>
+__global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_r2_kernel(SplatArgs a) {
+    constexpr int M = 2;
+    constexpr int W = BSX + 2 * M;
+    constexpr int WW = W * W * W;
+    constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
+    extern __shared__ double st[];  // [2][W^3]: mass, momentum; then per-warp particle slots
+    __shared__ uint32_t s_done[NT];
+    __shared__ uint16_t s_order[NT];
+    __shared__ uint32_t s_next;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
+    for (int t = tid; t < NT; t += blockDim.x) {
+        s_done[t] = 0;
+        const int tx = t % T, ty = (t / T) % T, tz = t / (T * T);
+        const int cx = tx % K, cy = ty % K, cz = tz % K;
+        const int ci = cx + K * (cy + K * cz);
+        int base = 0;
+        for (int c = 0; c < ci; ++c) {
+            const int ox = c % K, oy = (c / K) % K, oz = c / (K * K);
+            base += ((T - ox + K - 1) / K) * ((T - oy + K - 1) / K) * ((T - oz + K - 1) / K);
+        }
+        const int ntx = (T - cx + K - 1) / K, nty = (T - cy + K - 1) / K;
+        s_order[base + (tx / K) + ntx * ((ty / K) + nty * (tz / K))] = (uint16_t)t;
+    }
+    if (tid == 0) s_next = 0;
+    __syncthreads();
+    const int k_pb = blockIdx.x / 3;
+    switch (blockIdx.x % 3) {
+        case 0: splat_r2_body<BSX, 0>(a, k_pb, st, s_done, s_order, &s_next); break;
+        case 1: splat_r2_body<BSX, 1>(a, k_pb, st, s_done, s_order, &s_next); break;
+        default: splat_r2_body<BSX, 2>(a, k_pb, st, s_done, s_order, &s_next); break;
+    }
+}
+
 // OR of the footprint masks over each particle block's particles, expanded to
 // candidate block ids (n_blocks = "none").
 __global__ void pb_candidates_kernel(const uint32_t* fmask, const uint64_t* pb_starts, const uint64_t* pb_key, size_t npb,
@@ -580,6 +892,21 @@ static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
 
 template <int BSX, int M>
 static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
+    if (M == 2 && a.r_p == 2.0f) {
+        constexpr int W = BSX + 2 * 2;
+        constexpr int T = BSX / 2, NT = T * T * T;
+        constexpr int WARPS = NT < kSplatWarps ? NT : kSplatWarps;
+        const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 2 * SplatCap<BSX, 2>::v * sizeof(float4);
+        static bool attr = false;
+        if (!attr) {
+            CUDA_CHECK(cudaFuncSetAttribute(p2g_r2_kernel<BSX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr = true;
+        }
+        begin_launch(ctx);
+        p2g_r2_kernel<BSX><<<(unsigned)(3 * npb), 32 * WARPS, smem, ctx->stream>>>(a);
+        after_launch(ctx, "p2g_r2_kernel");
+        return;
+    }
     launch_splat_dir<BSX, M, 0>(ctx, a, npb);
     launch_splat_dir<BSX, M, 1>(ctx, a, npb);
     launch_splat_dir<BSX, M, 2>(ctx, a, npb);

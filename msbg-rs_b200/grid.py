@@ -295,6 +295,15 @@ class SparseGrid:
         call("msbg_sample_linear", self.handle, ptr(p), len(p), int(align), int(bc), ptr(out))
         return out
 
+    def sample_ext(self, pos: np.ndarray, mode: int, align: int, bc: int) -> np.ndarray:
+        """Cubic value (mode 0), cubic gradient (1), Hessian (2) or trilinear
+        gradient (3) (math/sample.rs:493-649)."""
+        p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        w = {0: 1, 1: 3, 2: 6, 3: 3}[int(mode)]
+        out = np.empty((len(p), w), np.float32)
+        call("msbg_sample_ext", self.handle, ptr(p), len(p), int(mode), int(align), int(bc), ptr(out))
+        return out[:, 0] if w == 1 else out
+
     def close(self) -> None:
         if self.handle and self._owned:
             call("msbg_grid_destroy", self.handle)

@@ -828,6 +828,153 @@ static float sample_linear(const Grid& g, const Dummies& dm, float x, float y, f
     return lerp(c0, c1, w);
 }
 
+// math/gather.rs:54-158 gather_map for a window of span = dmax + 1 (2 or 4)
+// anchored at (ix0, iy0, iz0): the one-block fast path, else 2x2x2 block
+// slots from the clamped anchor block and per-axis boundary resolution.
+static void gather_window(const Grid& g, const Dummies& dm, int32_t ix0, int32_t iy0, int32_t iz0, int bc, int span,
+                          float* out) {
+    const int bsx = g.bsx, lg = ilog2(bsx), mask = bsx - 1, dmax = span - 1;
+    if (ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && (int64_t)ix0 + dmax < (int64_t)g.sx && (int64_t)iy0 + dmax < (int64_t)g.sy &&
+        (int64_t)iz0 + dmax < (int64_t)g.sz) {
+        int vx0 = ix0 & mask, vy0 = iy0 & mask, vz0 = iz0 & mask;
+        if (vx0 + dmax < bsx && vy0 + dmax < bsx && vz0 + dmax < bsx) {
+            int64_t bid = (ix0 >> lg) + (int64_t)(iy0 >> lg) * g.nx + (int64_t)(iz0 >> lg) * g.nxy;
+            const float* p = block_data_ptr(g, dm, bid);
+            int s = 0;
+            for (int k = 0; k < span; ++k)
+                for (int j = 0; j < span; ++j)
+                    for (int i = 0; i < span; ++i) out[s++] = p[(vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg))];
+            return;
+        }
+    }
+    int64_t bx0 = std::min<int64_t>(std::max<int64_t>(ix0 >> lg, 0), g.nx - 1);
+    int64_t by0 = std::min<int64_t>(std::max<int64_t>(iy0 >> lg, 0), g.ny - 1);
+    int64_t bz0 = std::min<int64_t>(std::max<int64_t>(iz0 >> lg, 0), g.nz - 1);
+    const float* slots[8];
+    for (int sz_ = 0; sz_ < 2; ++sz_)
+        for (int sy_ = 0; sy_ < 2; ++sy_)
+            for (int sx_ = 0; sx_ < 2; ++sx_) {
+                int64_t bxx = std::min<int64_t>(bx0 + sx_, g.nx - 1), byy = std::min<int64_t>(by0 + sy_, g.ny - 1),
+                        bzz = std::min<int64_t>(bz0 + sz_, g.nz - 1);
+                slots[sx_ | (sy_ << 1) | (sz_ << 2)] = block_data_ptr(g, dm, bxx + byy * g.nx + bzz * g.nxy);
+            }
+    int s = 0;
+    for (int k = 0; k < span; ++k) {
+        int32_t rz; bool okz = resolve_axis(iz0 + k, (int32_t)g.sz - 1, bc, &rz);
+        for (int j = 0; j < span; ++j) {
+            int32_t ry; bool oky = resolve_axis(iy0 + j, (int32_t)g.sy - 1, bc, &ry);
+            for (int i = 0; i < span; ++i) {
+                int32_t rx; bool okx = resolve_axis(ix0 + i, (int32_t)g.sx - 1, bc, &rx);
+                if (okx && oky && okz) {
+                    int sl = (int)(((rx >> lg) - bx0) | (((ry >> lg) - by0) << 1) | (((rz >> lg) - bz0) << 2));
+                    out[s] = slots[sl][(rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg))];
+                } else {
+                    out[s] = g.empty_value;
+                }
+                ++s;
+            }
+        }
+    }
+}
+
+// math/bspline.rs:4-32 uniform cubic B-spline weights and their first and
+// second derivatives (f32, left to right, no contraction).
+static void cubic_w(float t, float w[4]) {
+    const float m = 1.0f - t, s6 = 1.0f / 6.0f, t3 = 2.0f / 3.0f;
+    w[0] = ((s6 * m) * m) * m;
+    w[1] = t3 - ((0.5f * t) * t) * (2.0f - t);
+    w[2] = t3 - ((0.5f * m) * m) * (1.0f + t);
+    w[3] = ((s6 * t) * t) * t;
+}
+static void cubic_dw(float t, float w[4]) {
+    const float m = 1.0f - t;
+    w[0] = ((-m) * m) / 2.0f;
+    w[1] = (0.5f * t) * t - (2.0f - t) * t;
+    w[2] = m * (t + 1.0f) - (0.5f * m) * m;
+    w[3] = (t * t) / 2.0f;
+}
+static void cubic_d2w(float t, float w[4]) {
+    w[0] = 1.0f - t;
+    w[1] = 3.0f * t - 2.0f;
+    w[2] = 1.0f - 3.0f * t;
+    w[3] = t;
+}
+// (f * w).reduce_sum() of a row of 4 (ordered lane sum)
+static inline float row_dot(const float* f, const float w[4]) {
+    return ((f[0] * w[0] + f[1] * w[1]) + f[2] * w[2]) + f[3] * w[3];
+}
+
+// sample.rs:493-649 Sample for SparseGrid, cubic B-spline (cell-centred
+// regardless of alignment; window base floor(x - 0.5) - 1, t = frac) and the
+// trilinear gradient (sample.rs:215-237).  mode 0: cubic value -> out[n];
+// 1: cubic gradient -> out[n][3]; 2: Hessian (fxx, fyy, fzz, fxy, fxz, fyz) ->
+// out[n][6]; 3: trilinear gradient at the given alignment -> out[n][3].
+void or_sample_ext(const OracleGrid* og, const float* pos, int64_t n, int mode, int align, int bc, float* out) {
+    Grid g = to_grid(og);
+    Dummies dm(g);
+    for (int64_t i = 0; i < n; ++i) {
+        float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        if (mode == 3) {
+            if (align == 1) { x = x - 0.5f; y = y - 0.5f; z = z - 0.5f; }
+            const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+            float c[8];
+            gather_window(g, dm, (int32_t)fx, (int32_t)fy, (int32_t)fz, bc, 2, c);
+            const float u = x - fx, v = y - fy, w = z - fz;
+            const float f01234567 = ((((((c[7] - c[6]) - c[5]) + c[4]) - c[3]) + c[2]) + c[1]) - c[0];
+            const float f01234567u = f01234567 * u;
+            const float f01234567uf6420 = (((f01234567u + c[6]) - c[4]) - c[2]) + c[0];
+            const float f5410 = ((c[5] - c[4]) - c[1]) + c[0];
+            const float f3210 = ((c[3] - c[2]) - c[1]) + c[0];
+            out[3 * i] = fmaf(f01234567 * v + f5410, w, ((f3210 * v + c[1]) - c[0]));
+            out[3 * i + 1] = fmaf(f01234567uf6420, w, ((f3210 * u + c[2]) - c[0]));
+            out[3 * i + 2] = fmaf(f01234567uf6420, v, ((f5410 * u + c[4]) - c[0]));
+            continue;
+        }
+        x = x - 0.5f; y = y - 0.5f; z = z - 0.5f;
+        const float xf = floorf(x), yf = floorf(y), zf = floorf(z);
+        const float tx = x - xf, ty = y - yf, tz = z - zf;
+        float win[64];
+        gather_window(g, dm, (int32_t)xf - 1, (int32_t)yf - 1, (int32_t)zf - 1, bc, 4, win);
+        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4], ddx[4], ddy[4], ddz[4];
+        cubic_w(tx, wx); cubic_w(ty, wy); cubic_w(tz, wz);
+        cubic_dw(tx, dx); cubic_dw(ty, dy); cubic_dw(tz, dz);
+        cubic_d2w(tx, ddx); cubic_d2w(ty, ddy); cubic_d2w(tz, ddz);
+        float val = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        float fxx = 0.0f, fyy = 0.0f, fzz = 0.0f, fxy = 0.0f, fxz = 0.0f, fyz = 0.0f;
+        for (int k = 0; k < 4; ++k)
+            for (int j = 0; j < 4; ++j) {
+                const float* f = win + 16 * k + 4 * j;
+                const float sx = row_dot(f, wx);
+                if (mode == 0) {
+                    val = fmaf(sx, wy[j] * wz[k], val);
+                } else if (mode == 1) {
+                    const float sxp = row_dot(f, dx);
+                    const float wyz = wy[j] * wz[k];
+                    val = fmaf(sx, wyz, val);
+                    gx = fmaf(sxp, wyz, gx);
+                    gy = fmaf(sx, dy[j] * wz[k], gy);
+                    gz = fmaf(sx, wy[j] * dz[k], gz);
+                } else {
+                    const float sxp = row_dot(f, dx), sxpp = row_dot(f, ddx);
+                    const float wyz = wy[j] * wz[k], wpyz = dy[j] * wz[k], wypz = wy[j] * dz[k];
+                    const float wppyz = ddy[j] * wz[k], wyppz = wy[j] * ddz[k], wpyzp = dy[j] * dz[k];
+                    fxx = fmaf(sxpp, wyz, fxx);
+                    fyy = fmaf(sx, wppyz, fyy);
+                    fzz = fmaf(sx, wyppz, fzz);
+                    fxy = fmaf(sxp, wpyz, fxy);
+                    fxz = fmaf(sxp, wypz, fxz);
+                    fyz = fmaf(sx, wpyzp, fyz);
+                }
+            }
+        if (mode == 0) out[i] = val;
+        else if (mode == 1) { out[3 * i] = gx; out[3 * i + 1] = gy; out[3 * i + 2] = gz; }
+        else {
+            float* h = out + 6 * i;
+            h[0] = fxx; h[1] = fyy; h[2] = fzz; h[3] = fxy; h[4] = fxz; h[5] = fyz;
+        }
+    }
+}
+
 // Scalar trilinear Sampler::sample::<Linear> (sample.rs:494-512) with the
 // given alignment (0 Corner, 1 CellCentered).
 void or_sample_linear(const OracleGrid* og, const float* pos, int64_t n, int align, int bc, float* out) {

@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
                                     C.c_float, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         _lib.or_mac_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         _lib.or_sample_linear.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p]
+        _lib.or_sample_ext.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_void_p]
         _lib.or_g2p_blend.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p]
         _lib.or_divergence.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
         _lib.or_downsample_avg.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
@@ -236,6 +237,20 @@ def sample_linear(host, pos, align, bc) -> np.ndarray:
     out = np.empty(len(p), np.float32)
     lib().or_sample_linear(v.ref(), _p(p), len(p), int(align), int(bc), _p(out))
     return out
+
+
+SAMPLE_WIDTH = {0: 1, 1: 3, 2: 6, 3: 3}
+
+
+def sample_ext(host, pos, mode, bc, align=0) -> np.ndarray:
+    """Sample for SparseGrid (math/sample.rs:493-649): mode 0 cubic value,
+    1 cubic gradient [n][3], 2 cubic Hessian [n][6] (fxx, fyy, fzz, fxy, fxz,
+    fyz), 3 trilinear gradient [n][3] at `align` (0 Corner, 1 CellCentered)."""
+    v = GridView(host)
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    out = np.empty((len(p), SAMPLE_WIDTH[mode]), np.float32)
+    lib().or_sample_ext(v.ref(), _p(p), len(p), int(mode), int(align), int(bc), _p(out))
+    return out[:, 0] if mode == 0 else out
 
 
 def mac_sample(vx, vy, vz, pos, bc) -> np.ndarray:

@@ -145,6 +145,22 @@ def test_p2g_edge_cases(msbg, ctx, oracle):
     check_p2g(msbg, ctx, oracle, pos, vel, np.ones(len(pos), np.float32), 32, 16, 2.0)
 
 
+def test_p2g_plane_and_centre_positions(msbg, ctx, oracle):
+    """Coordinates exactly on cell centres (x.5) and face planes (integers),
+    alone and mixed with regular ones, and one cell holding 300 particles
+    (more than a warp stages at once): the cases the r_p = 2 splat sends down
+    its general path or across staging refills."""
+    r = np.random.default_rng(21)
+    base = r.integers(1, 30, (600, 3)).astype(np.float32)
+    frac = r.choice(np.array([0.0, 0.5, 0.25, 0.75, 0.9999], np.float32), (600, 3))
+    dense = np.float32([9, 9, 9]) + r.uniform(0, 1, (300, 3)).astype(np.float32)
+    pos = np.concatenate([base + frac, dense]).astype(np.float32)
+    vel = r.normal(size=pos.shape).astype(np.float32)
+    mass = r.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    check_p2g(msbg, ctx, oracle, pos, vel, mass, 32, 16, 2.0)
+    check_p2g(msbg, ctx, oracle, pos, vel, mass, 32, 8, 2.0)
+
+
 def test_p2g_deterministic(msbg, ctx):
     pos, vel, mass = make_particles(30000, 64, 9)
     runs = []

@@ -30,7 +30,7 @@ def test_smoother_goldens(msbg, oracle, goldens):
 
 
 def test_interp_goldens(msbg, oracle, goldens):
-    """tests/difftest_interp.rs:84-91, trilinear value column (Corner, Clamp)."""
+    """tests/difftest_interp.rs:84-91: all 14 columns (Corner, Clamp)."""
     G = goldens["interp"]
     g = msbg.HostGrid("interp", 48, 48, 48, 0.0, 1.0, 16)
     zz, yy, xx = np.meshgrid(np.arange(48), np.arange(48), np.arange(48), indexing="ij")
@@ -39,9 +39,15 @@ def test_interp_goldens(msbg, oracle, goldens):
         bx, by, bz = g.get_block_coords_by_id(bid)
         g.ensure_block(bid)
         g.blocks[bid][:] = dense[bz * 16:(bz + 1) * 16, by * 16:(by + 1) * 16, bx * 16:(bx + 1) * 16].reshape(-1)
-    got = oracle.sample_linear(g, np.array(G["positions"], np.float32), 0, CLAMP)
-    want = np.array([row[0] for row in G["golden"]], np.float32)
-    np.testing.assert_allclose(got, want, atol=G["tol"], rtol=0)
+    pos = np.array(G["positions"], np.float32)
+    gold = np.array(G["golden"], np.float32)
+    np.testing.assert_allclose(oracle.sample_linear(g, pos, 0, CLAMP), gold[:, 0], atol=G["tol"], rtol=0)
+    # columns 1-13: trilinear gradient, cubic B-spline value, gradient and
+    # Hessian (sample_all, difftest_interp.rs:65-73)
+    np.testing.assert_allclose(oracle.sample_ext(g, pos, 3, CLAMP, align=0), gold[:, 1:4], atol=G["tol"], rtol=0)
+    np.testing.assert_allclose(oracle.sample_ext(g, pos, 0, CLAMP), gold[:, 4], atol=G["tol"], rtol=0)
+    np.testing.assert_allclose(oracle.sample_ext(g, pos, 1, CLAMP), gold[:, 5:8], atol=G["tol"], rtol=0)
+    np.testing.assert_allclose(oracle.sample_ext(g, pos, 2, CLAMP), gold[:, 8:14], atol=G["tol"], rtol=0)
 
 
 def fnv1a(h, data: bytes):
