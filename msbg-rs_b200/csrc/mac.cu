@@ -125,6 +125,9 @@ __global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, i
 // gather_map (math/gather.rs:54-158) for a window of SPAN = dmax + 1 (2 or
 // 4) anchored at (ix0, iy0, iz0): the one-block fast path, else the 2x2x2
 // block slots from the clamped anchor block and per-axis boundary resolution.
+// A Neumann window far outside the domain can reflect to a block before the
+// anchor block, where the crate's slot index leaves the 2x2x2 slots
+// (undefined there); slot offsets are taken mod 2.
 template <int SPAN>
 __device__ void gather_window_dev(const SampleGrid& g, int32_t ix0, int32_t iy0, int32_t iz0, int bc, float* out) {
     constexpr int DMAX = SPAN - 1;

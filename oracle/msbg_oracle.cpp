@@ -811,7 +811,8 @@ static float sample_linear(const Grid& g, const Dummies& dm, float x, float y, f
                 for (int i = 0; i < 2; ++i) {
                     int32_t rx; bool okx = resolve_axis(ix0 + i, (int32_t)g.sx - 1, bc, &rx);
                     if (okx && oky && okz) {
-                        int sl = (int)(((rx >> lg) - bx0) | (((ry >> lg) - by0) << 1) | (((rz >> lg) - bz0) << 2));
+                        // slot offsets mod 2 (see gather_window)
+                        int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) | ((((rz >> lg) - bz0) & 1) << 2));
                         c[s] = slots[sl][(rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg))];
                     } else {
                         c[s] = g.empty_value;
@@ -866,7 +867,11 @@ static void gather_window(const Grid& g, const Dummies& dm, int32_t ix0, int32_t
             for (int i = 0; i < span; ++i) {
                 int32_t rx; bool okx = resolve_axis(ix0 + i, (int32_t)g.sx - 1, bc, &rx);
                 if (okx && oky && okz) {
-                    int sl = (int)(((rx >> lg) - bx0) | (((ry >> lg) - by0) << 1) | (((rz >> lg) - bz0) << 2));
+                    // A Neumann window far outside the domain can reflect to
+                    // a block before the anchor block, where the crate's slot
+                    // index leaves the 2x2x2 slots (undefined there); the
+                    // offsets are taken mod 2, as on the device.
+                    int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) | ((((rz >> lg) - bz0) & 1) << 2));
                     out[s] = slots[sl][(rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg))];
                 } else {
                     out[s] = g.empty_value;
