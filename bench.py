@@ -399,8 +399,8 @@ def run_ours(args, world, rank, local):
             pk = 4.0 * sms * mhz * 1e6 / 1e9
             roof["issue"] = {"inst_per_particle_per_launch": round(ipu, 1), "achieved_ginst_s": round(ach, 1),
                              "peak_ginst_s": round(pk, 1), "frac": round(ach / pk, 4),
-                             "source": "warp instructions per particle from ncu at 128^3; peak = 4 per SM per clock "
-                                       "at the sampled SM clock"}
+                             "source": "warp instructions per particle and launch from ncu at 128^3; peak = 4 per "
+                                       "SM per clock at the sampled SM clock"}
     sweep_k = sweep_kernel_time(kernels)
     smoother = None
     if sweep_k:
@@ -497,6 +497,8 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
         return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
         return 28.0 * n * launches / P2G_SPLAT_LAUNCHES
+    if kernel == "p2g_r2_kernel":
+        return 28.0 * n * launches
     if kernel == "p2g_combine_kernel":
         return 24.0 * n_active * 4096 * launches
     if kernel == "g2p_kernel":
@@ -508,7 +510,8 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
     return None
 
 
-# Launches of the splat kernel per P2G (one per face direction).
+# Launches of the general splat kernel per P2G (one per face direction; the
+# r_p = 2 kernel does the three directions in one launch).
 P2G_SPLAT_LAUNCHES = 3
 
 # DRAM bytes (read + write) per launch measured by ncu on a smaller case of
@@ -516,12 +519,16 @@ P2G_SPLAT_LAUNCHES = 3
 # particles, one direction per launch) read 167.28 MB and wrote 3.96 MB
 # (profiles/p2g_cells_kernel_flip128.txt); traffic grows with the particle
 # count, so it is scaled by particles.
-TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.28e6 + 3.96e6) / 5767168}
+TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.28e6 + 3.96e6) / 5767168,
+                    # r_p = 2 kernel, all three directions in one launch at 128^3
+                    # (profiles/p2g_r2_kernel_flip128.txt): 306.61 MB read, 47.86 MB written
+                    "p2g_r2_kernel": (306.61e6 + 47.86e6) / 5767168}
 
 # Warp instructions per unit of work from the same capture (575,950,823 per
 # launch at 128^3): the splat is bound by instruction issue, not by DRAM, so
 # its second roofline is issue slots (4 warp instructions per SM per clock).
-INST_PER_UNIT = {"p2g_cells_kernel": 575950823 / 5767168}
+INST_PER_UNIT = {"p2g_cells_kernel": 575950823 / 5767168,
+                 "p2g_r2_kernel": 1492421629 / 5767168}
 
 
 # The smoother's sweep kernels (one of them runs, by element type and halo).

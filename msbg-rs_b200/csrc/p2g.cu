@@ -508,6 +508,12 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
 }
 
+// Warps of an r_p = 2 splat CTA and the particles each warp stages at once.
+constexpr int kSplatR2Warps = 20;
+template <int BSX> struct SplatR2Cap {
+    static constexpr int v = SplatCap<BSX, 2>::v;
+};
+
 // Splat for r_p = 2 (M = 2): all three face directions in one launch, CTA
 // 3k + d taking particle block k and direction d, so a block's three CTAs run
 // side by side and read its particles from L2 once.  Tiles, colours, the
@@ -517,12 +523,12 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
 // the side of the cell centre the particle lies on) and faces [c-2, c+1]
 // along the face axis, except when a coordinate lies exactly on a cell
 // centre (lane axes) or a face plane (face axis).  The cell's regular
-// particles are grouped by (a_U, a_V); within a group, 16 lanes cover the
-// 4 x 4 footprint rows of one particle and the two half-warps take two
-// particles at a time, each lane keeping the 4 faces of its row in FP64
-// registers, so every evaluated term is inside the footprint.  After each
-// group the half-warp sums are added (lower half first) and written into
-// the window.  The cell's other particles then go through the lane-bit path
+// particles are grouped by (a_U, a_V); within a group the warp takes one
+// particle at a time, lane (i, j, h) evaluating faces 2h and 2h + 1 of
+// footprint row (i, j), so every evaluated term is inside the footprint and
+// every lane owns its faces: each lane keeps its two face sums in FP64
+// registers over the group and adds them into the window after the group.
+// The cell's other particles then go through the lane-bit path
 // of p2g_cells_kernel, adding straight into the window.  Every term is the
 // reference's f32 operation sequence (p2g.rs:263-330); the sums are FP64 in
 // a fixed order.
@@ -535,7 +541,7 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
     constexpr int WIN = 2 * M + 1;
     constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
     constexpr int NNB = WIN * WIN * WIN;
-    constexpr int CAP = SplatCap<BSX, M>::v;
+    constexpr int CAP = SplatR2Cap<BSX>::v;
     constexpr int NR = (NNB + 31) / 32;
     constexpr int F = DIR, U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -548,9 +554,9 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
     const float* __restrict__ pv = a.pv[DIR];
     const uint64_t* __restrict__ lmask = a.lane_mask[DIR];
     const float inv_r2 = a.inv_r2, r_p = a.r_p;
-    // this lane's footprint row inside a group: (i, j) along (U, V)
-    const int li = lane & 3, lj = (lane >> 2) & 3;
-    const bool lower = lane < 16;
+    // this lane's footprint row inside a group, (i, j) along (U, V), and
+    // which two of the particle's four faces along F it evaluates
+    const int li = lane & 3, lj = (lane >> 2) & 3, half = lane >> 4;
     while (true) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(s_next, 1u);
@@ -614,11 +620,9 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
             cell[0] = 2 * tc[0] + (sub & 1);
             cell[1] = 2 * tc[1] + ((sub >> 1) & 1);
             cell[2] = 2 * tc[2] + (sub >> 2);
-            // face positions along F (faces -2 .. +1 of the cell, in pairs)
-            uint64_t gf2[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                gf2[h] = f2_pack((float)(b0[F] - M + cell[F] + 2 * h), (float)(b0[F] - M + cell[F] + 2 * h + 1));
+            // this lane's two face positions along F: offsets -2 + 2 half and
+            // -1 + 2 half from the cell
+            const uint64_t gf2 = f2_pack((float)(b0[F] - M + cell[F] + 2 * half), (float)(b0[F] - M + cell[F] + 2 * half + 1));
             for (int p0 = b; p0 < e;) {
                 if (p0 < st_lo || p0 >= st_hi) {
                     __syncwarp();
@@ -658,74 +662,58 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                     for (int g = 0; g < 4; ++g) {
                         uint32_t gm = __ballot_sync(0xffffffffu, my == g);
                         if (!gm) continue;
-                        // this lane's row: lane-axis offsets -2 + a + (i, j) from the cell
+                        // this lane's row: lane-axis offsets -2 + a + (i, j)
+                        // from the cell; its faces: F offsets -2 + 2 half, +1
                         const int su = cell[U] + (g & 1) + li, sv = cell[V] + (g >> 1) + lj;
                         const float gu = (float)(b0[U] - M + su), gv = (float)(b0[V] - M + sv);
-                        double am[4], av[4];
-#pragma unroll
-                        for (int s = 0; s < 4; ++s) am[s] = av[s] = 0.0;
+                        double am0 = 0.0, am1 = 0.0, av0 = 0.0, av1 = 0.0;
                         while (gm) {
-                            const int j1 = __ffs(gm) - 1;
+                            const int jj = c0 - st_lo + __ffs(gm) - 1;
                             gm &= gm - 1;
-                            const int j2 = gm ? __ffs(gm) - 1 : -1;
-                            if (gm) gm &= gm - 1;
-                            const bool on = lower || j2 >= 0;
-                            const int jj = c0 - st_lo + (lower || j2 < 0 ? j1 : j2);
                             const float4 P = wslot[jj];
                             const float4 R = wslot[CAP + jj];
                             const float m_p = P.w, scale_mom = R.x;
                             const float du = gu - P.x, dv = gv - P.y;
-                            const uint64_t pf2 = f2_pack(P.z, P.z);
                             float hoist0 = 0.0f, hoist1 = 0.0f;
                             if (DIR == 0) hoist0 = dv * dv + du * du;
                             else { hoist0 = dv * dv; hoist1 = du * du; }
-                            const uint64_t h02 = f2_pack(hoist0, hoist0), h12 = f2_pack(hoist1, hoist1);
-#pragma unroll
-                            for (int h = 0; h < 2; ++h) {
-                                const uint64_t df = f2_sub(gf2[h], pf2);
-                                float d0, d1;
-                                f2_unpack(df, d0, d1);
-                                const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
-                                uint64_t dist;
-                                if (DIR == 0) dist = f2_add(sq, h02);
-                                else if (DIR == 1) dist = f2_add(h12, f2_add(h02, sq));
-                                else dist = f2_add(h12, f2_add(sq, h02));
-                                const uint64_t df2 = f2_add(f2_add(dist, df), f2_pack(0.25f, 0.25f));
-                                float e0, e1;
-                                f2_unpack(df2, e0, e1);
-                                const uint64_t tt = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
-                                float w0, w1;
-                                f2_unpack(tt, w0, w1);
-                                w0 = on ? fmaxf(w0, 0.0f) : 0.0f;
-                                w1 = on ? fmaxf(w1, 0.0f) : 0.0f;
-                                uint64_t w = f2_pack(w0, w1);
-                                w = f2_mul(f2_mul(w, w), w);
-                                float tm0, tm1, tv0, tv1;
-                                f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
-                                f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
-                                am[2 * h] += (double)tm0;
-                                av[2 * h] += (double)tv0;
-                                am[2 * h + 1] += (double)tm1;
-                                av[2 * h + 1] += (double)tv1;
-                            }
-                        }
-#pragma unroll
-                        for (int s = 0; s < 4; ++s) {
-                            am[s] += __shfl_down_sync(0xffffffffu, am[s], 16);
-                            av[s] += __shfl_down_sync(0xffffffffu, av[s], 16);
+                            const uint64_t df = f2_sub(gf2, f2_pack(P.z, P.z));
+                            float d0, d1;
+                            f2_unpack(df, d0, d1);
+                            const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
+                            const uint64_t h02 = f2_pack(hoist0, hoist0);
+                            uint64_t dist;
+                            if (DIR == 0) dist = f2_add(sq, h02);
+                            else if (DIR == 1) dist = f2_add(f2_pack(hoist1, hoist1), f2_add(h02, sq));
+                            else dist = f2_add(f2_pack(hoist1, hoist1), f2_add(sq, h02));
+                            const uint64_t df2 = f2_add(f2_add(dist, df), f2_pack(0.25f, 0.25f));
+                            float e0, e1;
+                            f2_unpack(df2, e0, e1);
+                            const uint64_t tt = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
+                            float w0, w1;
+                            f2_unpack(tt, w0, w1);
+                            uint64_t w = f2_pack(fmaxf(w0, 0.0f), fmaxf(w1, 0.0f));
+                            w = f2_mul(f2_mul(w, w), w);
+                            float tm0, tm1, tv0, tv1;
+                            f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
+                            f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
+                            am0 += (double)tm0;
+                            av0 += (double)tv0;
+                            am1 += (double)tm1;
+                            av1 += (double)tv1;
                         }
                         if (deps_pending) wait_deps();
-                        if (lower) {
-#pragma unroll
-                            for (int s = 0; s < 4; ++s) {
-                                int sc[3];
-                                sc[F] = cell[F] + s;  // faces -2 .. +1: staging cell[F] + M - 2 + s
-                                sc[U] = su;
-                                sc[V] = sv;
-                                const int si = (sc[2] * W + sc[1]) * W + sc[0];
-                                st[si] += am[s];
-                                st[WW + si] += av[s];
-                            }
+                        {
+                            int sc[3];
+                            sc[F] = cell[F] + 2 * half;  // faces -2 + 2 half: staging cell[F] + M - 2 + 2 half
+                            sc[U] = su;
+                            sc[V] = sv;
+                            const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                            constexpr int step = F == 0 ? 1 : F == 1 ? W : W * W;
+                            st[si] += am0;
+                            st[WW + si] += av0;
+                            st[si + step] += am1;
+                            st[WW + si + step] += av1;
                         }
                         __syncwarp();
                     }
@@ -786,7 +774,7 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
 }
 
 template <int BSX>
-__global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_r2_kernel(SplatArgs a) {
+__global__ void __launch_bounds__(32 * kSplatR2Warps, 1) p2g_r2_kernel(SplatArgs a) {
     constexpr int M = 2;
     constexpr int W = BSX + 2 * M;
     constexpr int WW = W * W * W;
@@ -895,8 +883,8 @@ static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     if (M == 2 && a.r_p == 2.0f) {
         constexpr int W = BSX + 2 * 2;
         constexpr int T = BSX / 2, NT = T * T * T;
-        constexpr int WARPS = NT < kSplatWarps ? NT : kSplatWarps;
-        const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 2 * SplatCap<BSX, 2>::v * sizeof(float4);
+        constexpr int WARPS = NT < kSplatR2Warps ? NT : kSplatR2Warps;
+        const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 2 * SplatR2Cap<BSX>::v * sizeof(float4);
         static bool attr = false;
         if (!attr) {
             CUDA_CHECK(cudaFuncSetAttribute(p2g_r2_kernel<BSX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
