@@ -259,6 +259,37 @@ int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, i
 int msbg_sample_ext(msbg_grid* grid, const float* pos, size_t n, int mode, int align, int bc, float* out);
 int msbg_sample_ext_device(msbg_grid* grid, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out);
 
+/* ---- surface reconstruction from particles (particles/mod.rs:220-302) ---- */
+/* splat (particles/splat.rs:92-319) of device positions d_pos [n][3] into
+ * `grid` (Density u16 or f32, empty value 0, full value 1; extents multiples
+ * of bsx; r_particle + nb_dist < bsx - 1/2): the footprint blocks of the
+ * particles (reach r_scan = r_particle + nb_dist, particles/active.rs:15-47)
+ * are allocated and filled with the full value, and every voxel within r_scan
+ * of a particle takes the minimum of dist_sq / r_scan^2 (Density: rounded to
+ * u16, channel.rs:392-417).  The sorted active bids go to active_out
+ * (capacity cap, at least the grid's block count is always enough). */
+int msbg_surface_splat_device(msbg_grid* grid, const float* d_pos, size_t n, float r_particle, float nb_dist,
+                              uint64_t* active_out, size_t cap, size_t* n_active_out);
+/* finalize (particles/finalize.rs:35-71) of the listed value blocks in place:
+ * the splatted ratio becomes 1 - clamp(sqrt(ratio) r_scan / (2 r_particle +
+ * nb_dist), 0, 1), or 0 where it is >= 0.999 (untouched). */
+int msbg_surface_finalize(msbg_grid* grid, const uint64_t* active, size_t n, float r_particle, float nb_dist);
+/* reconstruct_and_smooth (particles/mod.rs:279-302) from host positions:
+ * splat, finalize, then `iterations` mean-curvature sweeps of step dt with
+ * [0, 1] clamping over the active blocks (the PLY loading and placement of the
+ * crate's pipeline are left to the caller: see msbg_place_instances). */
+int msbg_reconstruct_and_smooth(msbg_grid* grid, const float* pos, size_t n, float r_particle, float nb_dist,
+                                int iterations, float dt, uint64_t* active_out, size_t cap, size_t* n_active_out);
+/* place (particles/sort.rs:31-144): n_instances copies of the base cloud
+ * ([n_base][3], host), instance i at 0.2 smax + 0.6 smax (b_i - bbox_min) /
+ * span_max scaled by smin * factor / span_max, kept inside the domain bounds
+ * (particles/mod.rs DomainBounds) and the grid; the kept positions go to
+ * pos_out ([cap][3], host, instance-major) and their count to *n_out
+ * (pos_out null: count only). */
+int msbg_place_instances(msbg_ctx* ctx, const float* base, size_t n_base, const float* bbox_min, float span_max,
+                         uint64_t sx, uint64_t sy, uint64_t sz, float instance_scale_factor, size_t n_instances,
+                         float* pos_out, size_t cap, size_t* n_out);
+
 /* ---- one FLIP transfer step through host arrays ------------------------- */
 /* The per-step composition of the crate's transfer entry points that a FLIP
  * loop makes (bucket_particles + particles_to_grid, fluid/p2g.rs:141-164;

@@ -19,6 +19,8 @@ from .fluid import (FlipStep, MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend
                     particles_to_grid_device, particles_to_grid_sorted_device)
 from .multires import downsample_channel_avg
 from .sampler import CELL_CENTERED, CORNER, CUBIC_BSPLINE, LINEAR, Sampler
+from . import surface
+from .surface import SurfaceConfig, reconstruct_and_smooth
 from .poisson import HYBRID, LEARNED, LEARNED_LEAD, LEARNED_MG, MG, PCG, Poisson
 from .learned import UNet
 from .batch import Batch
@@ -31,6 +33,6 @@ __all__ = [
     "BucketPlan", "bucket_indices", "morton3", "morton3_host", "morton_sort", "sort_block_list_morton",
     "FlipStep", "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
     "particles_to_grid_device", "particles_to_grid_sorted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
-    "Sampler", "LINEAR", "CUBIC_BSPLINE", "CORNER", "CELL_CENTERED",
+    "surface", "SurfaceConfig", "reconstruct_and_smooth", "Sampler", "LINEAR", "CUBIC_BSPLINE", "CORNER", "CELL_CENTERED",
     "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch",
 ]

@@ -96,6 +96,10 @@ SIGNATURES = {
     "msbg_sample_ext": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_sample_ext_device": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_surface_splat_device": [_P, _P, _SZ, _F, _F, _P, _SZ, _SZP],
+    "msbg_surface_finalize": [_P, _P, _SZ, _F, _F],
+    "msbg_reconstruct_and_smooth": [_P, _P, _SZ, _F, _F, _I, _F, _P, _SZ, _SZP],
+    "msbg_place_instances": [_P, _P, _SZ, _P, _F, _U64, _U64, _U64, _F, _SZ, _P, _SZ, _SZP],
     "msbg_flip_create": [_P, _P, _P, _SZ, C.POINTER(_P)],
     "msbg_flip_destroy": [_P],
     "msbg_flip_step": [_P, _P, _P, _P, _SZ, _F, _I, _F, _I, _F, _P],

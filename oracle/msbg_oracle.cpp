@@ -1489,3 +1489,160 @@ int or_poisson_solve(const int64_t* active, int64_t n_active, int64_t nx, int64_
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Surface reconstruction from particles (particles/{sort,splat,finalize}.rs).
+// ===========================================================================
+extern "C" {
+
+// particles/sort.rs:31-144 place: instance i of the base cloud has origin
+// 0.2 smax + 0.6 smax bs (b_i - bbox) and scale smin * factor * bs (bs =
+// 1 / span_max); each base point j is placed at origin + scale (b_j - bbox),
+// kept when inside the domain bounds and its truncated cell inside the grid.
+// Positions come out instance-major; bids are their centre blocks.  Writes
+// at most cap particles; returns the number placed.
+int64_t or_place(const float* base, int64_t n_base, const float* bbox_min, float span_max, int64_t sx, int64_t sy,
+                 int64_t sz, int bsx, float factor, int64_t n_instances, const float* dom_min, const float* dom_max,
+                 float* pos_out, int64_t* bids_out, int64_t cap) {
+    const int64_t nx = (sx + bsx - 1) / bsx, ny = (sy + bsx - 1) / bsx;
+    const int lg = ilog2(bsx);
+    const float base_scale = 1.0f / span_max;
+    const float smin = (float)std::min(sx, std::min(sy, sz)), smax = (float)std::max(sx, std::max(sy, sz));
+    const float scale = smin * factor;
+    const float inst_scale = scale * base_scale;
+    const int64_t dims[3] = {sx, sy, sz};
+    int64_t c = 0;
+    for (int64_t i = 0; i < n_instances; ++i) {
+        const float* bi = base + 3 * i;
+        float origin[3];
+        for (int a = 0; a < 3; ++a) origin[a] = 0.2f * smax + ((0.6f * smax) * base_scale) * (bi[a] - bbox_min[a]);
+        for (int64_t j = 0; j < n_base; ++j) {
+            const float* bj = base + 3 * j;
+            float p[3];
+            bool in = true;
+            for (int a = 0; a < 3; ++a) {
+                p[a] = origin[a] + inst_scale * (bj[a] - bbox_min[a]);
+                if (!(p[a] >= dom_min[a] && p[a] <= dom_max[a])) in = false;
+            }
+            if (!in) continue;
+            int32_t ip[3];
+            for (int a = 0; a < 3; ++a) {
+                ip[a] = (int32_t)p[a];
+                if (ip[a] < 0 || ip[a] >= dims[a]) in = false;
+            }
+            if (!in) continue;
+            if (c < cap) {
+                for (int a = 0; a < 3; ++a) pos_out[3 * c + a] = p[a];
+                bids_out[c] = (int64_t)(ip[0] >> lg) + (int64_t)(ip[1] >> lg) * nx + (int64_t)(ip[2] >> lg) * nx * ny;
+            }
+            ++c;
+        }
+    }
+    return c;
+}
+
+// particles/active.rs:15-47 footprint union with r_scan = r_particle +
+// nb_dist: sorted unique bids; returns the count (out may be NULL).
+int64_t or_surface_active(const float* pos, int64_t n, int64_t sx, int64_t sy, int64_t sz, int bsx, float r_scan,
+                          int64_t* out) {
+    int64_t nx = (sx + bsx - 1) / bsx, ny = (sy + bsx - 1) / bsx, nz = (sz + bsx - 1) / bsx;
+    std::vector<uint8_t> mark((size_t)(nx * ny * nz), 0);
+    const float rs = r_scan / (float)bsx;
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t x1, x2, y1, y2, z1, z2;
+        footprint_axis(pos[3 * i], rs, bsx, nx, &x1, &x2);
+        footprint_axis(pos[3 * i + 1], rs, bsx, ny, &y1, &y2);
+        footprint_axis(pos[3 * i + 2], rs, bsx, nz, &z1, &z2);
+        for (int32_t bz = z1; bz <= z2; ++bz)
+            for (int32_t by = y1; by <= y2; ++by)
+                for (int32_t bx = x1; bx <= x2; ++bx) mark[bx + by * nx + bz * nx * ny] = 1;
+    }
+    int64_t c = 0;
+    for (int64_t b = 0; b < nx * ny * nz; ++b)
+        if (mark[b]) { if (out) out[c] = b; ++c; }
+    return c;
+}
+
+// particles/splat.rs:92-319 splat into active blocks filled with the full
+// value: per particle, over its footprint voxels [ceil(p - r - 1/2),
+// floor(p + r - 1/2)] (r = r_scan, clipped to its block's staging window),
+// dist_sq = dx dx + (dz dz + dy dy) with d = voxel - (p - 1/2); where dist_sq
+// <= r^2 the voxel takes min(old, q), q = dist_sq / r^2 (f32 storage) or
+// round(dist_sq / r^2 * 65535) (Density, u16; channel.rs:392-417).  Voxels
+// outside the domain or in blocks outside `active` are skipped (the
+// reference's commit skips them).  The reference stages per block and
+// commits by colour; min is order-independent, so a direct scatter-min gives
+// the same grid.  out is [n_active][bsx^3] f32 (values of u16 as floats
+// when density != 0).
+void or_density_splat(const float* pos, int64_t n, int64_t sx, int64_t sy, int64_t sz, int bsx, float r_particle,
+                      float nb_dist, int density, const int64_t* active, int64_t n_active, float* out) {
+    const int64_t nx = (sx + bsx - 1) / bsx, ny = (sy + bsx - 1) / bsx, nz = (sz + bsx - 1) / bsx;
+    const int lg = ilog2(bsx), msk = bsx - 1;
+    const int64_t N = (int64_t)bsx * bsx * bsx;
+    std::vector<int64_t> slot((size_t)(nx * ny * nz), -1);
+    for (int64_t k = 0; k < n_active; ++k) slot[active[k]] = k;
+    const float r_scan = r_particle + nb_dist;
+    const float dmax = r_scan * r_scan, inv = 1.0f / dmax;
+    const int m = (int)ceilf(r_scan);
+    std::vector<uint32_t> q((size_t)(n_active * N), density ? 65535u : 0x3f800000u);  // full: u16 max or 1.0f
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = pos + 3 * i;
+        int32_t b0[3];
+        for (int a = 0; a < 3; ++a) b0[a] = ((int32_t)p[a] >> lg) << lg;
+        int32_t lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(std::max((int32_t)ceilf((p[a] - r_scan) - 0.5f), b0[a] - m), b0[a] + bsx + m - 1);
+            hi[a] = std::min(std::max((int32_t)floorf((p[a] + r_scan) - 0.5f), b0[a] - m), b0[a] + bsx + m - 1);
+        }
+        const float px0 = p[0] - 0.5f, py0 = p[1] - 0.5f, pz0 = p[2] - 0.5f;
+        for (int32_t iz = lo[2]; iz <= hi[2]; ++iz) {
+            const float dz = (float)iz - pz0, dz2 = dz * dz;
+            for (int32_t iy = lo[1]; iy <= hi[1]; ++iy) {
+                const float dy = (float)iy - py0, dyz = dz2 + dy * dy;
+                for (int32_t ix = lo[0]; ix <= hi[0]; ++ix) {
+                    const float dx = (float)ix - px0;
+                    const float d2 = dx * dx + dyz;
+                    if (!(d2 <= dmax)) continue;
+                    if (ix < 0 || iy < 0 || iz < 0 || ix >= sx || iy >= sy || iz >= sz) continue;
+                    const int64_t s = slot[(ix >> lg) + (int64_t)(iy >> lg) * nx + (int64_t)(iz >> lg) * nx * ny];
+                    if (s < 0) continue;
+                    const float t = d2 * inv;
+                    uint32_t v;
+                    if (density) v = (uint32_t)(int32_t)roundf(t * 65535.0f) & 0xffffu;
+                    else memcpy(&v, &t, 4);
+                    uint32_t& o = q[(size_t)(s * N + ((ix & msk) | ((iy & msk) << lg) | ((iz & msk) << (2 * lg))))];
+                    if (v < o) o = v;
+                }
+            }
+        }
+    }
+    for (size_t k = 0; k < q.size(); ++k) {
+        if (density) out[k] = (float)q[k];
+        else memcpy(&out[k], &q[k], 4);
+    }
+}
+
+// particles/finalize.rs:35-71 in place on [n][bsx^3] values (u16 values as
+// floats when density != 0): ratio (dequantised), touched = ratio < 0.999,
+// f = 1 - clamp((sqrt(ratio r^2) - r_p + r_p) / (2 r_p + nb), 0, 1), 0 when
+// untouched; stored back (Density: round(f * 65535)).
+void or_density_finalize(float* vals, int64_t n, int density, float r_particle, float nb_dist) {
+    const float r_scan = r_particle + nb_dist, dmax = r_scan * r_scan;
+    const float denom = 2.0f * r_particle + nb_dist;
+    for (int64_t k = 0; k < n; ++k) {
+        const float ratio = density ? density_to_f32((uint16_t)vals[k]) : vals[k];
+        const bool touched = ratio < 0.999f;
+        const float dist = sqrtf(ratio * dmax) - r_particle;
+        float t = (dist + r_particle) / denom;
+        t = std::min(std::max(t, 0.0f), 1.0f);
+        const float f = touched ? 1.0f - t : 0.0f;
+        if (density) {
+            const float r = roundf(f * 65535.0f);
+            vals[k] = (float)(uint16_t)(int32_t)r;
+        } else {
+            vals[k] = f;
+        }
+    }
+}
+
+}  // extern "C"

@@ -59,6 +59,15 @@ def lib() -> C.CDLL:
         _lib.or_mac_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         _lib.or_sample_linear.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p]
         _lib.or_sample_ext.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        _lib.or_place.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_float, C.c_int64, C.c_int64, C.c_int64, C.c_int,
+                                  C.c_float, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+        _lib.or_place.restype = C.c_int64
+        _lib.or_surface_active.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_float,
+                                           C.c_void_p]
+        _lib.or_surface_active.restype = C.c_int64
+        _lib.or_density_splat.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_float,
+                                          C.c_float, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+        _lib.or_density_finalize.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_float, C.c_float]
         _lib.or_g2p_blend.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p]
         _lib.or_divergence.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
         _lib.or_downsample_avg.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
@@ -251,6 +260,58 @@ def sample_ext(host, pos, mode, bc, align=0) -> np.ndarray:
     out = np.empty((len(p), SAMPLE_WIDTH[mode]), np.float32)
     lib().or_sample_ext(v.ref(), _p(p), len(p), int(mode), int(align), int(bc), _p(out))
     return out[:, 0] if mode == 0 else out
+
+
+def domain_bounds(sx, sy, sz):
+    """DomainBounds::new (particles/mod.rs): align24(0.005), align24(size - 0.005)."""
+    scale = 16_777_215.0 / 32_768.0
+
+    def align24(x):
+        return np.float32(np.floor(scale * x + 0.5) / scale)
+
+    return (np.array([align24(0.005)] * 3, np.float32),
+            np.array([align24(float(v) - 0.005) for v in (sx, sy, sz)], np.float32))
+
+
+def place(base, bbox_min, span_max, sx, sy, sz, bsx, factor, n_instances):
+    """particles/sort.rs:31-144 place: (positions [n][3] f32, centre bids)."""
+    b = np.ascontiguousarray(base, np.float32).reshape(-1, 3)
+    bb = np.ascontiguousarray(bbox_min, np.float32)
+    lo, hi = domain_bounds(sx, sy, sz)
+    n = lib().or_place(_p(b), len(b), _p(bb), float(span_max), sx, sy, sz, bsx, float(factor), int(n_instances),
+                       _p(lo), _p(hi), None, None, 0)
+    pos = np.zeros((n, 3), np.float32)
+    bids = np.zeros(n, np.int64)
+    lib().or_place(_p(b), len(b), _p(bb), float(span_max), sx, sy, sz, bsx, float(factor), int(n_instances), _p(lo),
+                   _p(hi), _p(pos), _p(bids), n)
+    return pos, bids
+
+
+def surface_active(pos, sx, sy, sz, bsx, r_scan) -> np.ndarray:
+    """Footprint block union of the surface splat (reach r_scan)."""
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    c = lib().or_surface_active(_p(p), len(p), sx, sy, sz, bsx, float(r_scan), None)
+    out = np.zeros(c, np.int64)
+    lib().or_surface_active(_p(p), len(p), sx, sy, sz, bsx, float(r_scan), _p(out))
+    return out
+
+
+def density_splat(pos, sx, sy, sz, bsx, r_particle, nb_dist, density, active) -> np.ndarray:
+    """particles/splat.rs:92-319 min-splat into the active blocks (filled with
+    the full value first): [n_active][bsx^3], u16 values (density) or f32."""
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    a = np.ascontiguousarray(active, np.int64)
+    out = np.zeros((len(a), bsx ** 3), np.float32)
+    lib().or_density_splat(_p(p), len(p), sx, sy, sz, bsx, float(r_particle), float(nb_dist), int(bool(density)), _p(a),
+                           len(a), _p(out))
+    return out.astype(np.uint16) if density else out
+
+
+def density_finalize(vals, density, r_particle, nb_dist) -> np.ndarray:
+    """particles/finalize.rs:35-71 on splatted values (u16 or f32)."""
+    v = np.ascontiguousarray(vals, np.float32).copy()
+    lib().or_density_finalize(_p(v), v.size, int(bool(density)), float(r_particle), float(nb_dist))
+    return v.astype(np.uint16) if density else v
 
 
 def mac_sample(vx, vy, vz, pos, bc) -> np.ndarray:

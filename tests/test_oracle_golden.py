@@ -330,3 +330,65 @@ def test_poisson_oracle_converges(oracle):
     cells = oracle.poisson_levels(active, nx, nx, nx, 8)
     assert list(cells[:3]) == [len(active) * 512, len(active) * 64, len(active) * 8]
     assert cells[-1] <= 1024
+
+
+# ---- surface reconstruction (particles/splat.rs, finalize.rs) --------------
+R_PARTICLE, NB_DIST = 2.0, 2.0  # SurfaceConfig of the crate's splat tests
+
+
+def _splat_voxels(oracle, pts, s=32, bsx=16):
+    pts = np.array(pts, np.float32)
+    act = oracle.surface_active(pts, s, s, s, bsx, R_PARTICLE + NB_DIST)
+    vals = oracle.density_splat(pts, s, s, s, bsx, R_PARTICLE, NB_DIST, True, act)
+    nb = s // bsx
+
+    def get(x, y, z):
+        b = (x // bsx) + (y // bsx) * nb + (z // bsx) * nb * nb
+        k = np.searchsorted(act, b)
+        if k >= len(act) or act[k] != b:
+            return 0  # absent block: the grid's empty Density(0)
+        return int(vals[k][(x % bsx) + (y % bsx) * bsx + (z % bsx) * bsx * bsx])
+    return act, get
+
+
+def test_density_splat_known_answers(oracle):
+    """particles/splat.rs:371-459 (splat_01, 02, 04, 05, 06)."""
+    _, get = _splat_voxels(oracle, [[8.0, 8.0, 8.0]])
+    assert get(8, 8, 8) == 3072  # distSq 0.75
+    assert get(5, 8, 8) == round((6.75 / 16.0) * 65535.0)
+    assert get(1, 8, 8) == 65535
+    assert get(4, 8, 8) == int(np.floor(np.float32(12.75 / 16.0) * np.float32(65535.0) + np.float32(0.5)))
+    assert get(0, 8, 8) == 65535
+    act, get = _splat_voxels(oracle, [[15.5, 8.0, 8.0]])
+    assert 1 in act
+    assert get(16, 8, 8) == round((1.5 / 16.0) * 65535.0)
+    _, get = _splat_voxels(oracle, [[0.1, 0.1, 0.1]])
+    assert get(0, 0, 0) != 65535
+    _, get = _splat_voxels(oracle, [[16.0, 16.0, 16.0]])
+    assert get(21, 16, 16) == 65535 and get(20, 16, 16) == 65535
+
+
+def test_density_splat_min_order_independent(oracle):
+    """particles/splat.rs:411-431 (splat_03): min is order-independent."""
+    a = [[10.0, 8.0, 8.0], [12.0, 8.0, 8.0]]
+    act1, _ = _splat_voxels(oracle, a)
+    v1 = oracle.density_splat(np.array(a, np.float32), 32, 32, 32, 16, R_PARTICLE, NB_DIST, True, act1)
+    v2 = oracle.density_splat(np.array(a[::-1], np.float32), 32, 32, 32, 16, R_PARTICLE, NB_DIST, True, act1)
+    assert np.array_equal(v1, v2)
+
+
+def test_density_finalize_known_answers(oracle):
+    """particles/finalize.rs:106-175 (finalize_01 .. 04)."""
+    r = 16.0
+    vals = np.array([0, round(2.5 * 2.5 / r * 65535.0), 65468, 65535,
+                     round(0.9989 * 65535.0), round(0.9991 * 65535.0)], np.float32)
+    out = oracle.density_finalize(vals, True, R_PARTICLE, NB_DIST).astype(np.float32) / np.float32(65535.0)
+    assert abs(out[0] - 1.0) < 1e-4
+    assert abs(out[1] - (1.0 - (0.5 + 2.0) / 6.0)) < 1e-4
+    ratio = np.float32(65468.0) / np.float32(65535.0)
+    assert abs(out[2] - (1.0 - np.sqrt(ratio * r) / 6.0)) < 1e-4
+    assert out[3] == 0.0
+    assert out[4] > 0.0 and out[5] == 0.0
+    mixed = np.array([((x + y + z) % 17) / 17.0 * 65535.0 for z in range(16) for y in range(16) for x in range(16)])
+    fin = oracle.density_finalize(np.round(mixed).astype(np.float32), True, R_PARTICLE, NB_DIST)
+    assert fin.min() >= 0 and fin.max() <= 65535
