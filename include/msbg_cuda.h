@@ -64,6 +64,7 @@ typedef struct msbg_mac msbg_mac;
 typedef struct msbg_poisson msbg_poisson;
 typedef struct msbg_unet msbg_unet;
 typedef struct msbg_flip msbg_flip;
+typedef struct msbg_blockmap msbg_blockmap;
 
 /* ---- context ---------------------------------------------------------- */
 const char* msbg_status_string(int status);
@@ -102,6 +103,12 @@ int msbg_grid_dims(const msbg_grid* grid, uint64_t out[8]);
 int msbg_grid_ensure_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
 /* set_full_block / set_empty_block (sparse_grid.rs:248-262): only for bids
  * that are not value blocks (MSBG_ERR_ARG otherwise). */
+/* ensure_blocks_parallel (sparse_grid.rs:326-355) from a device list: the
+ * blocks of d_bids (duplicates allowed) that are not value blocks become value
+ * blocks holding the empty value; existing blocks keep their data.  Lookups,
+ * deduplication and table updates run on the device; only the new ids are
+ * read back.  d_slots_out (optional, device, [n]) receives every id's slot. */
+int msbg_grid_ensure_blocks_device(msbg_grid* g, const uint64_t* d_bids, size_t n, int32_t* d_slots_out);
 int msbg_grid_set_full_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
 int msbg_grid_set_empty_blocks(msbg_grid* grid, const uint64_t* bids, size_t n);
 /* set_empty_value / set_full_value (sparse_grid.rs:232-245). */
@@ -258,6 +265,31 @@ int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, i
  * window from gather_map (math/gather.rs:54-158); f32 grids, blocks >= 4^3. */
 int msbg_sample_ext(msbg_grid* grid, const float* pos, size_t n, int mode, int align, int bc, float* out);
 int msbg_sample_ext_device(msbg_grid* grid, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out);
+
+/* ---- BlockMap in device memory (blockmap.rs:35-209) ---------------------- */
+/* Open-addressing hash of 64-bit block ids to 32-bit values, probed linearly
+ * from (key * 0x9e3779b97f4a7c15) & mask; capacity a power of two >= 4
+ * (with_capacity), doubled when live entries plus tombstones would pass 3/4.
+ * Keys 2^64 - 1 and 2^64 - 2 are the EMPTY and TOMBSTONE sentinels and are
+ * rejected (MSBG_ERR_ARG).  Batches take device arrays. */
+int msbg_blockmap_create(msbg_ctx* ctx, uint64_t capacity, msbg_blockmap** out);
+int msbg_blockmap_destroy(msbg_blockmap* m);
+/* len() and capacity(). */
+int msbg_blockmap_len(msbg_blockmap* m, uint64_t* len_out, uint64_t* capacity_out);
+/* insert (blockmap.rs:101-127) of n (key, value) pairs; for a key given twice
+ * the later value wins, as inserting the batch in order would. */
+int msbg_blockmap_insert_device(msbg_blockmap* m, const uint64_t* d_keys, const uint32_t* d_vals, size_t n);
+/* update(key, 1, |c| c + 1) (blockmap.rs:153-175) for every key of the batch:
+ * the per-key counts of bucket_indices' histogram (particles/sort.rs:174-200). */
+int msbg_blockmap_update_add_device(msbg_blockmap* m, const uint64_t* d_keys, size_t n);
+/* get (blockmap.rs:86-99): d_out[i] = value of d_keys[i], or `missing`. */
+int msbg_blockmap_get_device(msbg_blockmap* m, const uint64_t* d_keys, size_t n, uint32_t missing, uint32_t* d_out);
+/* remove (blockmap.rs:129-151): keys become tombstones. */
+int msbg_blockmap_remove_device(msbg_blockmap* m, const uint64_t* d_keys, size_t n);
+/* sorted_pairs (blockmap.rs:177-187): the live entries by ascending key into
+ * device arrays of capacity cap; *n_out = len() (keys_out null: count only). */
+int msbg_blockmap_sorted_pairs_device(msbg_blockmap* m, uint64_t* d_keys_out, uint32_t* d_vals_out, size_t cap,
+                                      size_t* n_out);
 
 /* ---- surface reconstruction from particles (particles/mod.rs:220-302) ---- */
 /* splat (particles/splat.rs:92-319) of device positions d_pos [n][3] into

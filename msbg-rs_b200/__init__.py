@@ -24,6 +24,7 @@ from .surface import SurfaceConfig, reconstruct_and_smooth
 from .poisson import HYBRID, LEARNED, LEARNED_LEAD, LEARNED_MG, MG, PCG, Poisson
 from .learned import UNet
 from .batch import Batch
+from .blockmap import BlockMap
 
 MsbgError = _lib.MsbgError
 CLAMP, NEUMANN, DIRICHLET = _lib.MSBG_CLAMP, _lib.MSBG_NEUMANN, _lib.MSBG_DIRICHLET
@@ -34,5 +35,5 @@ __all__ = [
     "FlipStep", "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
     "particles_to_grid_device", "particles_to_grid_sorted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
     "surface", "SurfaceConfig", "reconstruct_and_smooth", "Sampler", "LINEAR", "CUBIC_BSPLINE", "CORNER", "CELL_CENTERED",
-    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch",
+    "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch", "BlockMap",
 ]

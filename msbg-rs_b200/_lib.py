@@ -55,6 +55,7 @@ SIGNATURES = {
     "msbg_grid_destroy": [_P],
     "msbg_grid_dims": [_P, _U64P],
     "msbg_grid_ensure_blocks": [_P, _P, _SZ],
+    "msbg_grid_ensure_blocks_device": [_P, _P, _SZ, _P],
     "msbg_grid_set_full_blocks": [_P, _P, _SZ],
     "msbg_grid_set_empty_blocks": [_P, _P, _SZ],
     "msbg_grid_set_values": [_P, _F, _F],
@@ -96,6 +97,14 @@ SIGNATURES = {
     "msbg_sample_ext": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_sample_ext_device": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_blockmap_create": [_P, _U64, C.POINTER(_P)],
+    "msbg_blockmap_destroy": [_P],
+    "msbg_blockmap_len": [_P, _U64P, _U64P],
+    "msbg_blockmap_insert_device": [_P, _P, _P, _SZ],
+    "msbg_blockmap_update_add_device": [_P, _P, _SZ],
+    "msbg_blockmap_get_device": [_P, _P, _SZ, C.c_uint32, _P],
+    "msbg_blockmap_remove_device": [_P, _P, _SZ],
+    "msbg_blockmap_sorted_pairs_device": [_P, _P, _P, _SZ, _SZP],
     "msbg_surface_splat_device": [_P, _P, _SZ, _F, _F, _P, _SZ, _SZP],
     "msbg_surface_finalize": [_P, _P, _SZ, _F, _F],
     "msbg_reconstruct_and_smooth": [_P, _P, _SZ, _F, _F, _I, _F, _P, _SZ, _SZP],

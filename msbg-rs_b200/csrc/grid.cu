@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "grid.cuh"
+#include "sort.cuh"
 #include "sweep.cuh"
 
 namespace msbg {
@@ -242,6 +243,135 @@ void grid_ensure(msbg_grid* g, const uint64_t* bids, size_t n, int32_t* slots) {
         sync(g->ctx);
         (void)first_new;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Block materialisation from a device list (ensure_blocks_parallel,
+// sparse_grid.rs:326-355): the table lookups, the deduplication and the
+// table updates run on the device; only the ids of the blocks that are new
+// come back to the host (to keep its mirror of the table), so a block set
+// that changes every step costs one small read instead of a rebuild and
+// upload of the whole table.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int32_t dev_code(const int32_t* dense, const DevHash& h, uint64_t bid) {
+    return dense ? dense[bid] : hash_find(h, bid);
+}
+
+// flags[i] = 1 for the first of each run of equal (sorted) ids whose block is
+// not a value block yet; bad = an id out of range.
+__global__ void ens_new_kernel(const uint64_t* __restrict__ sorted, size_t n, uint64_t n_blocks, const int32_t* dense,
+                               DevHash h, uint32_t* __restrict__ flags, int* __restrict__ bad) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t b = sorted[i];
+        if (b >= n_blocks) {
+            atomicExch(bad, 1);
+            flags[i] = 0;
+            continue;
+        }
+        flags[i] = (i == 0 || sorted[i - 1] != b) && dev_code(dense, h, b) < 0 ? 1u : 0u;
+    }
+}
+
+__global__ void ens_compact_kernel(const uint64_t* __restrict__ sorted, size_t n, const uint32_t* __restrict__ flags,
+                                   const uint32_t* __restrict__ off, uint64_t* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (flags[i]) out[off[i]] = sorted[i];
+}
+
+// New blocks get slots first_slot + rank: written into the dense table, or
+// inserted into the hash (linear probing from hash_slot; a full dummy's entry
+// takes the slot), and listed for the fill.
+__global__ void ens_insert_kernel(const uint64_t* __restrict__ fresh, size_t n, int32_t first_slot, int32_t* dense,
+                                  unsigned long long* hkeys, int32_t* hvals, uint32_t hmask, int hshift,
+                                  int32_t* __restrict__ fresh_slots) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const unsigned long long b = fresh[i];
+        const int32_t s = first_slot + (int32_t)i;
+        fresh_slots[i] = s;
+        if (dense) dense[b] = s;
+        if (hkeys) {
+            uint32_t j = hash_slot(b, hshift);
+            for (uint32_t probe = 0; probe <= hmask; ++probe) {
+                const unsigned long long k = atomicCAS(hkeys + j, (unsigned long long)kHashEmpty, b);
+                if (k == kHashEmpty || k == b) {
+                    hvals[j] = s;
+                    break;
+                }
+                j = (j + 1) & hmask;
+            }
+        }
+    }
+}
+
+__global__ void ens_slots_kernel(const uint64_t* __restrict__ bids, size_t n, const int32_t* dense, DevHash h,
+                                 int32_t* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = dev_code(dense, h, bids[i]);
+}
+
+void grid_ensure_device(msbg_grid* g, const uint64_t* d_bids, size_t n, int32_t* d_slots_out) {
+    msbg_ctx* ctx = g->ctx;
+    if (!n) return;
+    MSBG_REQUIRE(n < (1ULL << 32), "at most 2^32 - 1 block ids per call");
+    const int32_t* dense = device_dense(g);
+    DevHash h = device_hash(g);
+    DevBuf tmp;  // private: callers may hold the context arena
+    const size_t b_sorted = (n * 8 + 255) & ~size_t(255), b_perm = (n * 4 + 255) & ~size_t(255);
+    const size_t b_flags = b_perm, b_off = b_perm, b_fresh = b_sorted;
+    const size_t b_rs = (std::max(radix_sort_scratch_bytes(n), scan_scratch_bytes(n)) + 255) & ~size_t(255);
+    tmp.reserve(b_sorted + b_perm + b_flags + b_off + b_fresh + b_rs + 256);
+    char* p = (char*)tmp.p;
+    uint64_t* sorted = (uint64_t*)p; p += b_sorted;
+    uint32_t* perm = (uint32_t*)p;   p += b_perm;
+    uint32_t* flags = (uint32_t*)p;  p += b_flags;
+    uint32_t* off = (uint32_t*)p;    p += b_off;
+    uint64_t* fresh = (uint64_t*)p;  p += b_fresh;
+    char* rs = p;                    p += b_rs;
+    int* words = (int*)p;            // [0] bad, [1..] scan total
+    CUDA_CHECK(cudaMemsetAsync(words, 0, 16, ctx->stream));
+    radix_sort_pairs(ctx, d_bids, nullptr, sorted, perm, n, ilog2i(g->n_blocks + 1) + 1, rs);
+    const unsigned grid = (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 148 * 16);
+    begin_launch(ctx);
+    ens_new_kernel<<<grid, 256, 0, ctx->stream>>>(sorted, n, g->n_blocks, dense, h, flags, words);
+    after_launch(ctx, "ens_new_kernel");
+    exclusive_scan_u32(ctx, flags, off, n, (uint32_t*)(words + 1), rs);
+    begin_launch(ctx);
+    ens_compact_kernel<<<grid, 256, 0, ctx->stream>>>(sorted, n, flags, off, fresh);
+    after_launch(ctx, "ens_compact_kernel");
+    int hw[2] = {0, 0};
+    read_small(ctx, hw, words, 8);
+    MSBG_REQUIRE(!hw[0], "block id out of range");
+    const size_t nf = (size_t)(uint32_t)hw[1];
+    if (nf) {
+        std::vector<uint64_t> fresh_h(nf);
+        read_small(ctx, fresh_h.data(), fresh, nf * 8);
+        const int32_t first = (int32_t)g->slot_bid.size();
+        for (size_t i = 0; i < nf; ++i) {
+            g->slot_bid.push_back(fresh_h[i]);
+            g->map[fresh_h[i]] = first + (int32_t)i;
+        }
+        g->version++;
+        grid_reserve(g, g->n_slots());
+        // the hash stays below half load: insert in place, else rebuild it on next use
+        const bool hash_in_place = !g->hash_dirty && g->map.size() * 2 <= (size_t)g->hmask + 1;
+        if (!hash_in_place) g->hash_dirty = true;
+        int32_t* fresh_slots = (int32_t*)perm;  // the permutation is no longer needed
+        begin_launch(ctx);
+        ens_insert_kernel<<<(unsigned)std::min<size_t>(div_up(nf, 256), 148 * 16), 256, 0, ctx->stream>>>(
+            fresh, nf, first, dense && !g->dense_dirty ? const_cast<int32_t*>(dense) : nullptr,
+            hash_in_place ? g->hkeys.as<unsigned long long>() : nullptr, g->hvals.as<int32_t>(), g->hmask, g->hshift,
+            fresh_slots);
+        after_launch(ctx, "ens_insert_kernel");
+        grid_fill_slots(g, fresh_slots, nf, g->empty_value);
+    }
+    if (d_slots_out) {
+        const int32_t* dense2 = device_dense(g);
+        DevHash h2 = device_hash(g);
+        begin_launch(ctx);
+        ens_slots_kernel<<<grid, 256, 0, ctx->stream>>>(d_bids, n, dense2, h2, d_slots_out);
+        after_launch(ctx, "ens_slots_kernel");
+    }
+    sync(ctx);  // tmp dies at return
 }
 
 // ---------------------------------------------------------------------------
@@ -627,6 +757,14 @@ int msbg_grid_ensure_blocks(msbg_grid* g, const uint64_t* bids, size_t n) {
     MSBG_REQUIRE(g && (bids || !n), "null argument");
     set_device(g->ctx);
     grid_ensure(g, bids, n, nullptr);
+    MSBG_API_END
+}
+
+int msbg_grid_ensure_blocks_device(msbg_grid* g, const uint64_t* d_bids, size_t n, int32_t* d_slots_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(g && (d_bids || !n), "null argument");
+    set_device(g->ctx);
+    grid_ensure_device(g, d_bids, n, d_slots_out);
     MSBG_API_END
 }
 

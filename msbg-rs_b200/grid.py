@@ -295,6 +295,11 @@ class SparseGrid:
         call("msbg_sample_linear", self.handle, ptr(p), len(p), int(align), int(bc), ptr(out))
         return out
 
+    def ensure_blocks_device(self, d_bids, d_slots_out=None) -> None:
+        """ensure_blocks_parallel (sparse_grid.rs:326-355) from a device (torch)
+        array of block ids; optionally writes every id's slot."""
+        call("msbg_grid_ensure_blocks_device", self.handle, ptr(d_bids), int(d_bids.numel()), ptr(d_slots_out))
+
     def sample_ext(self, pos: np.ndarray, mode: int, align: int, bc: int) -> np.ndarray:
         """Cubic value (mode 0), cubic gradient (1), Hessian (2) or trilinear
         gradient (3) (math/sample.rs:493-649)."""
