@@ -175,9 +175,12 @@ void grid_reserve(msbg_grid* g, size_t need) {
     cap = std::max<size_t>(cap, 8);
     void* p = nullptr;
     CUDA_CHECK(cudaMalloc(&p, cap * g->block_elems * g->esize));
-    if (g->payload.p && g->n_slots())
-        CUDA_CHECK(cudaMemcpyAsync(p, g->payload.p, g->n_slots() * g->block_elems * g->esize,
-                                   cudaMemcpyDeviceToDevice, g->ctx->stream));
+    // Callers list the new slots before reserving them, so only the old
+    // capacity holds data to keep.
+    const size_t keep = std::min(g->n_slots(), g->cap_slots);
+    if (g->payload.p && keep)
+        CUDA_CHECK(cudaMemcpyAsync(p, g->payload.p, keep * g->block_elems * g->esize, cudaMemcpyDeviceToDevice,
+                                   g->ctx->stream));
     sync(g->ctx);
     g->payload.release();
     g->payload.p = p;
