@@ -266,6 +266,24 @@ int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, i
 int msbg_sample_ext(msbg_grid* grid, const float* pos, size_t n, int mode, int align, int bc, float* out);
 int msbg_sample_ext_device(msbg_grid* grid, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out);
 
+/* ---- refinement map (multires/refinement.rs) ---------------------------- */
+/* regularize_refinement_map (refinement.rs:63-107): the 2:1 rule on a
+ * per-block level map ([nx*ny*nz] u8, 0 = finest), in place; n_levels - 2
+ * passes, each moving a block at level >= ll whose finest neighbour (26
+ * neighbours) is at ll - 1 up to level ll. */
+int msbg_regularize_refinement_map(msbg_ctx* ctx, uint8_t* levels, uint64_t nx, uint64_t ny, uint64_t nz, int n_levels);
+int msbg_regularize_refinement_map_device(msbg_ctx* ctx, uint8_t* d_levels, uint64_t nx, uint64_t ny, uint64_t nz,
+                                          int n_levels);
+/* compute_block_topology (refinement.rs:124-208, levelMg 0): flags_out[bid] =
+ * user_flags[bid] (optional) | DOM_BORDER (1 << 1) on the block grid's faces |
+ * FINE_COARSE (1 << 3) next to a coarser block | COARSE_FINE (1 << 2) next to
+ * a finer one; the FINE_COARSE blocks of level l in block order go to
+ * fine_coarse_out + l * n_blocks (optional) and their count to
+ * fine_coarse_counts[l]; *n_exists_out counts user EXISTS (1 << 12) blocks. */
+int msbg_block_topology(msbg_ctx* ctx, const uint8_t* levels, uint64_t nx, uint64_t ny, uint64_t nz, int n_levels,
+                        const uint16_t* user_flags, uint16_t* flags_out, uint64_t* fine_coarse_out,
+                        uint64_t* fine_coarse_counts, uint64_t* n_exists_out);
+
 /* ---- BlockMap in device memory (blockmap.rs:35-209) ---------------------- */
 /* Open-addressing hash of 64-bit block ids to 32-bit values, probed linearly
  * from (key * 0x9e3779b97f4a7c15) & mask; capacity a power of two >= 4

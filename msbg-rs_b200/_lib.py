@@ -97,6 +97,9 @@ SIGNATURES = {
     "msbg_sample_ext": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_sample_ext_device": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_downsample_avg": [_P, _P],
+    "msbg_regularize_refinement_map": [_P, _P, _U64, _U64, _U64, _I],
+    "msbg_regularize_refinement_map_device": [_P, _P, _U64, _U64, _U64, _I],
+    "msbg_block_topology": [_P, _P, _U64, _U64, _U64, _I, _P, _P, _P, _P, _U64P],
     "msbg_blockmap_create": [_P, _U64, C.POINTER(_P)],
     "msbg_blockmap_destroy": [_P],
     "msbg_blockmap_len": [_P, _U64P, _U64P],

@@ -1646,3 +1646,76 @@ void or_density_finalize(float* vals, int64_t n, int density, float r_particle, 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Refinement map (multires/refinement.rs).
+// ===========================================================================
+extern "C" {
+
+// refinement.rs:63-107 regularize_refinement_map: passes ll = 1 .. n_levels-2;
+// a block at level >= ll whose minimum neighbour level (26-neighbourhood, in
+// range; starting from n_levels - 1) is ll - 1 moves to level ll.
+void or_regularize_refinement_map(uint8_t* map, int64_t nx, int64_t ny, int64_t nz, int n_levels) {
+    if (n_levels <= 2) return;
+    const int64_t n = nx * ny * nz;
+    std::vector<uint8_t> prev(map, map + n);
+    for (int ll = 1; ll <= n_levels - 2; ++ll) {
+        for (int64_t bid = 0; bid < n; ++bid) {
+            const uint8_t level = prev[bid];
+            uint8_t out = level;
+            if (level >= ll) {
+                const int64_t bx = bid % nx, by = (bid / nx) % ny, bz = bid / (nx * ny);
+                uint8_t level2 = (uint8_t)(n_levels - 1);
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            if (!dx && !dy && !dz) continue;
+                            const int64_t X = bx + dx, Y = by + dy, Z = bz + dz;
+                            if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+                            level2 = std::min(level2, prev[X + Y * nx + Z * nx * ny]);
+                        }
+                if (level2 == ll - 1) out = (uint8_t)ll;
+            }
+            map[bid] = out;
+        }
+        std::copy(map, map + n, prev.begin());
+    }
+}
+
+// refinement.rs:124-208 compute_block_topology (levelMg == 0): per block the
+// user flags plus DOM_BORDER (1 << 1) on the block grid's faces, FINE_COARSE
+// (1 << 3) when a neighbour is coarser, COARSE_FINE (1 << 2) when one is
+// finer; the FINE_COARSE blocks of each level in bid order; the number of
+// EXISTS (1 << 12) blocks.  fc_out is [n_levels][n] (each row holds the list
+// of its level, fc_count[l] entries).
+uint64_t or_block_topology(const uint8_t* map, int64_t nx, int64_t ny, int64_t nz, int n_levels, const uint16_t* user,
+                           uint16_t* flags_out, int64_t* fc_out, int64_t* fc_count) {
+    const int64_t n = nx * ny * nz;
+    for (int l = 0; l < n_levels; ++l) fc_count[l] = 0;
+    uint64_t n_act = 0;
+    for (int64_t bid = 0; bid < n; ++bid) {
+        const uint8_t level = map[bid];
+        uint16_t f = user ? user[bid] : 0;
+        const int64_t bx = bid % nx, by = (bid / nx) % ny, bz = bid / (nx * ny);
+        if (bx == 0 || bx == nx - 1 || by == 0 || by == ny - 1 || bz == 0 || bz == nz - 1) f |= 1u << 1;
+        uint8_t lmax = 0, lmin = (uint8_t)(n_levels - 1);
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!dx && !dy && !dz) continue;
+                    const int64_t X = bx + dx, Y = by + dy, Z = bz + dz;
+                    if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+                    const uint8_t l2 = map[X + Y * nx + Z * nx * ny];
+                    lmax = std::max(lmax, l2);
+                    lmin = std::min(lmin, l2);
+                }
+        if (lmax > level) f |= 1u << 3;
+        if (lmin < level) f |= 1u << 2;
+        if (f & (1u << 3)) fc_out[(int64_t)level * n + fc_count[level]++] = bid;
+        if (f & (1u << 12)) ++n_act;
+        flags_out[bid] = f;
+    }
+    return n_act;
+}
+
+}  // extern "C"

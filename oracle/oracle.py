@@ -59,6 +59,10 @@ def lib() -> C.CDLL:
         _lib.or_mac_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         _lib.or_sample_linear.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p]
         _lib.or_sample_ext.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        _lib.or_regularize_refinement_map.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int]
+        _lib.or_block_topology.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]
+        _lib.or_block_topology.restype = C.c_uint64
         _lib.or_place.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_float, C.c_int64, C.c_int64, C.c_int64, C.c_int,
                                   C.c_float, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
         _lib.or_place.restype = C.c_int64
@@ -260,6 +264,27 @@ def sample_ext(host, pos, mode, bc, align=0) -> np.ndarray:
     out = np.empty((len(p), SAMPLE_WIDTH[mode]), np.float32)
     lib().or_sample_ext(v.ref(), _p(p), len(p), int(mode), int(align), int(bc), _p(out))
     return out[:, 0] if mode == 0 else out
+
+
+def regularize_refinement_map(levels, nx, ny, nz, n_levels) -> np.ndarray:
+    """multires/refinement.rs:63-107 (a copy is regularised)."""
+    m = np.ascontiguousarray(levels, np.uint8).copy()
+    lib().or_regularize_refinement_map(_p(m), nx, ny, nz, int(n_levels))
+    return m
+
+
+def block_topology(levels, nx, ny, nz, n_levels, user_flags=None):
+    """multires/refinement.rs:124-208: (flags [n] u16, fine-coarse lists per
+    level, EXISTS count)."""
+    m = np.ascontiguousarray(levels, np.uint8)
+    n = len(m)
+    u = None if user_flags is None else np.ascontiguousarray(user_flags, np.uint16)
+    flags = np.zeros(n, np.uint16)
+    fc = np.zeros((n_levels, n), np.int64)
+    cnt = np.zeros(n_levels, np.int64)
+    n_act = lib().or_block_topology(_p(m), nx, ny, nz, int(n_levels), None if u is None else _p(u), _p(flags), _p(fc),
+                                    _p(cnt))
+    return flags, [fc[l, : cnt[l]].copy() for l in range(n_levels)], int(n_act)
 
 
 def domain_bounds(sx, sy, sz):

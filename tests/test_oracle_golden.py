@@ -392,3 +392,37 @@ def test_density_finalize_known_answers(oracle):
     mixed = np.array([((x + y + z) % 17) / 17.0 * 65535.0 for z in range(16) for y in range(16) for x in range(16)])
     fin = oracle.density_finalize(np.round(mixed).astype(np.float32), True, R_PARTICLE, NB_DIST)
     assert fin.min() >= 0 and fin.max() <= 65535
+
+
+# ---- refinement map (multires/refinement.rs:210-330 tests) ------------------
+DOM_BORDER, COARSE_FINE, FINE_COARSE = 1 << 1, 1 << 2, 1 << 3
+
+
+def test_refinement_known_answers(oracle):
+    n = 4
+    for lv in (0, 2):  # test_ref_01: uniform maps unchanged
+        m = np.full(n ** 3, lv, np.uint8)
+        assert np.array_equal(oracle.regularize_refinement_map(m, n, n, n, 3), m)
+    m = np.full(n ** 3, 1, np.uint8)  # test_ref_02: a single fine block
+    m[21] = 0
+    m = oracle.regularize_refinement_map(m, n, n, n, 3)
+    flags, fc, _ = oracle.block_topology(m, n, n, n, 3)
+    assert m[21] == 0 and flags[21] & FINE_COARSE and not flags[21] & COARSE_FINE
+    assert fc[0].tolist() == [21]
+    assert m[63] == 1 and not flags[63] & (FINE_COARSE | COARSE_FINE)
+    m = np.full(n ** 3, 2, np.uint8)  # test_ref_03: a jump of 2 becomes a staircase
+    m[21] = 0
+    m = oracle.regularize_refinement_map(m, n, n, n, 3)
+    lv = m.reshape(n, n, n)
+    for z in range(n):
+        for y in range(n):
+            for x in range(n):
+                nb = lv[max(z - 1, 0):z + 2, max(y - 1, 0):y + 2, max(x - 1, 0):x + 2]
+                assert np.abs(nb.astype(int) - int(lv[z, y, x])).max() <= 1
+    flags, _, _ = oracle.block_topology(np.zeros(n ** 3, np.uint8), n, n, n, 3)  # test_ref_04
+    assert flags[0] & DOM_BORDER and flags[n ** 3 - 1] & DOM_BORDER and not flags[21] & DOM_BORDER
+    z = np.zeros(n ** 3, np.uint8)  # test_ref_05 / 06: small level counts, idempotent
+    assert np.array_equal(oracle.regularize_refinement_map(z, n, n, n, 1), z)
+    assert np.array_equal(oracle.regularize_refinement_map(z, n, n, n, 2), z)
+    once = oracle.regularize_refinement_map(z, n, n, n, 3)
+    assert np.array_equal(oracle.regularize_refinement_map(once, n, n, n, 3), once)
