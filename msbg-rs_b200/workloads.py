@@ -221,7 +221,7 @@ class PhaseField:
         return len(self.mass)
 
 
-def phase_field(size: int = 512, seed: int = 5, ppc: int = 8, band: float = 12.0) -> PhaseField:
+def phase_field(size: int = 512, seed: int = 5, ppc: int = 8, band: float = 12.0, particles: bool = True) -> PhaseField:
     bsx = 16
     nb = size // bsx
     c = size / 2.0
@@ -253,6 +253,9 @@ def phase_field(size: int = 512, seed: int = 5, ppc: int = 8, band: float = 12.0
     for s in range(0, len(cc), chunk):
         ph[s:s + chunk] = phi(cc[s:s + chunk])
     phase = (0.5 * (1.0 - np.tanh(ph / 2.0))).astype(np.float32).reshape(len(fine), bsx ** 3)
+    if not particles:
+        e = np.empty((0, 3), np.float32)
+        return PhaseField(size, lv, fine, phase, e, e, np.empty(0, np.float32))
     inband = np.abs(ph) < band
     origin = np.repeat(cc[inband] - 0.5, ppc, axis=0).astype(np.float32)
     rng = np.random.default_rng(seed + 1)

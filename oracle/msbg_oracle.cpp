@@ -1000,6 +1000,7 @@ void or_mac_sample(const OracleGrid* vx, const OracleGrid* vy, const OracleGrid*
     for (int a = 0; a < 3; ++a) {
         Grid g = to_grid(v[a]);
         Dummies dm(g);
+#pragma omp parallel for schedule(static) if (n > 100000)
         for (int64_t i = 0; i < n; ++i) {
             float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
             if (a == 0) px = px - 0.5f;
