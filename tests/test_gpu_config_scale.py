@@ -142,10 +142,12 @@ def test_learned_solve_256_reaches_1e6(msbg, ctx, oracle):
     P.set_preconditioner(net)
     P.train_preconditioner(n_rhs=20, mg_iters=40, steps_per_rhs=40, pool=64, lr=1e-3, target=1, seed=7)
     P.set_network_lead(1)
-    x, it, rel, _ = P.solve(b, method=msbg.LEARNED_LEAD, tol=1e-6, max_iter=200)
+    # the FP64 solution: rounding x to f32 alone would leave ~1e-5 here
+    x64 = torch.zeros(P.n, dtype=torch.float64, device="cuda")
+    it, rel, _ = P.solve_device(x64, torch.from_numpy(b).cuda(), method=msbg.LEARNED_LEAD, tol=1e-6, max_iter=200)
     assert rel <= 1e-6 and it < 200
     nb = size // 16
-    ax = oracle.poisson_matvec(active.astype(np.int64), nb, nb, nb, 16, x.astype(np.float64))
+    ax = oracle.poisson_matvec(active.astype(np.int64), nb, nb, nb, 16, x64.cpu().numpy())
     bb = b.astype(np.float64)
     assert np.linalg.norm(bb - ax) / np.linalg.norm(bb) <= 1.5e-6
     P.close()
