@@ -230,7 +230,7 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
 // scratch arrays [3][HSX].
 template <int BSX> struct Compact;
 
-template <class E, int BSX, int ST, bool COMPACT = false, bool CG = false>
+template <class E, int BSX, int ST, bool COMPACT = false>
 __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const int32_t* nb, int pi, int8_t* ok, int8_t* dd,
                               int8_t* ll) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
@@ -276,10 +276,7 @@ __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const i
                 const int c = nb[dd[hx] + 3 * dd[HSX + hy] + 9 * dd[2 * HSX + hz]];
                 const int lx = ll[hx], ly = ll[HSX + hy], lz = ll[2 * HSX + hz];
                 if (c >= 0) {
-                    // CG: blocks another CTA of the same launch may have updated,
-                    // read through L2 (L1 is not coherent across SMs)
-                    const typename E::T* src = payload + (size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)));
-                    v = E::load(CG ? __ldcg(src) : *src);
+                    v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
                 } else if (c == kCodeFull) {
                     v = a.full;
                 } else if (c <= kCodeCoarse0) {
@@ -658,7 +655,7 @@ template <int BSX> struct Compact {
 };
 
 // Issues the staging of an interior block (one-cell halo) in the compact layout.
-template <int BSX, int ST, int NT = BSX * BSX, bool CG = false>
+template <int BSX, int ST, int NT = BSX * BSX>
 __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
     using CL = Compact<BSX>;
     constexpr int H = CL::H;
@@ -770,9 +767,7 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
                 const int ly = sy < 0 ? BSX - 1 : 0, hy = sy < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
                 float* d = h + CL::MAIN + side * CL::XS + (j + 1) * CL::XP + 3 + hy;
                 if (c >= 0) {
-                    const float* src = a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly;
-                    if (CG) *d = __ldcg(src);  // 4-byte cp.async goes through L1
-                    else cp_async4(d, src);
+                    cp_async4(d, a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly);
                 } else if (c <= kCodeCoarse0) {
                     constexpr int CLG = LG - 1;
                     const int lx = sx < 0 ? BSX - 1 : 0;
@@ -1030,141 +1025,6 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     cp_async_wait<0>();
 }
 
-// All the colour phases of all the sweeps of a call in one launch.  Items
-// are (sweep t, block) pairs in sweep-major, colour-major, Morton order, and
-// each CTA claims the next item from a counter, so every item a running CTA
-// waits for was claimed earlier by a running CTA.  A block of colour c in
-// sweep t reads its neighbours of lower colours after their update in sweep
-// t and its neighbours of higher colours before it (the crate's colour
-// order, solver.rs:187-217), so the item waits until every swept neighbour
-// of lower colour has completed t + 1 sweeps and every one of higher colour
-// t sweeps (per-slot progress words, released after the block's stores).
-// The next item's staging is issued while the current block is computed
-// when its neighbours are already done, else after the current block is
-// published.  Blocks other CTAs update are read through L2.  A wait that
-// runs past kWaitLimitNs sets bit 8 of the status word, and every CTA stops
-// at its next wait once the bit is set (after its copies in flight have
-// landed); the sweep is then incomplete and the next call that reads the
-// status word reports it.
-template <int BSX, int ST, bool CLAMP>
-__global__ void __launch_bounds__(CompactThreads<BSX, ST>::v, BSX == 16 ? 4 : 1)
-sweep_flow_kernel(SweepArgs a, const int32_t* __restrict__ order, int n, int iters, int* prog, unsigned int* counter,
-                  int* status) {
-    using CL = Compact<BSX>;
-    constexpr int NT = CompactThreads<BSX, ST>::v;
-    extern __shared__ float4 h4[];
-    float* hb = reinterpret_cast<float*>(h4);
-    __shared__ int32_t nbs[2][27];
-    __shared__ int32_t flg[2], pis[2], col[2];
-    __shared__ int itm[2];
-    __shared__ int8_t ok[3][BSX + 2], dd[3][BSX + 2], ll[3][BSX + 2];
-    __shared__ int s_stop;
-    const int tid = threadIdx.x;
-    const int total = n * iters;
-    auto claim = [&](int b) {
-        if (tid == 0) itm[b] = (int)atomicAdd(counter, 1u);
-        __syncthreads();
-        const int w = itm[b];
-        if (w < total) {
-            const int pi = order[w % n];
-            if (tid < 27) nbs[b][tid] = a.nbr[(size_t)pi * 27 + tid];
-            if (tid == 27) {
-                const int32_t* bx = a.bxyz + (size_t)pi * 4;
-                flg[b] = bx[3];
-                pis[b] = pi;
-                col[b] = (bx[0] & 1) | ((bx[1] & 1) << 1) | ((bx[2] & 1) << 2);
-            }
-        }
-        __syncthreads();
-    };
-    // every swept neighbour has completed the sweeps item b needs
-    auto ready = [&](int b) -> bool {
-        bool good = true;
-        if (tid < 27 && tid != 13) {
-            const int c = nbs[b][tid];
-            if (c >= 0) {
-                const int t = itm[b] / n;
-                const int nc = col[b] ^ ((tid % 3 != 1) | (((tid / 3) % 3 != 1) << 1) | ((tid / 9 != 1) << 2));
-                const int need = nc < col[b] ? t + 1 : t;
-                good = *(volatile int*)(prog + c) >= need;
-            }
-        }
-        __threadfence();
-        return __syncthreads_and(good) != 0;
-    };
-    // false: a wait gave up (here or in another CTA); the kernel then stops
-    auto wait_ready = [&](int b) -> bool {
-        uint64_t t0 = 0;
-        for (uint32_t spins = 0;; ++spins) {
-            if (ready(b)) return true;
-            if (tid == 0) {
-                int stop = (*(volatile int*)status & 8) ? 1 : 0;
-                if (!stop && (spins & 15u) == 15u) {
-                    const uint64_t now = globaltimer_ns();
-                    if (!t0) t0 = now;
-                    else if (now - t0 > kWaitLimitNs) {
-                        atomicOr(status, 8);
-                        stop = 1;
-                    }
-                }
-                s_stop = stop;
-            }
-            __syncthreads();
-            if (s_stop) return false;
-            __nanosleep(128);
-        }
-    };
-    auto stage = [&](int b) {  // issues (interior) or performs (edge) the staging of item b into buffer b
-        if (flg[b] & 1) issue_compact<BSX, ST, NT, true>(a, hb + b * CL::BUF, nbs[b]);
-        else stage_general<ElemF32, BSX, ST, true, true>(a, hb + b * CL::BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
-        cp_async_commit();
-    };
-    claim(0);
-    if (itm[0] >= total) return;
-    if (!wait_ready(0)) return;
-    stage(0);
-    int b = 0;
-    while (true) {
-        const int bn = b ^ 1;
-        claim(bn);
-        const bool more = itm[bn] < total;
-        bool early = false;
-        if (more && ready(bn)) {
-            stage(bn);
-            early = true;
-        } else {
-            cp_async_commit();  // an empty group keeps the wait count below uniform
-        }
-        cp_async_wait<1>();  // the current block's copies have landed
-        __syncthreads();
-        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
-        else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            atomicExch(prog + nbs[b][13], itm[b] / n + 1);
-        }
-        if (!more) break;
-        if (!early) {
-            if (!wait_ready(bn)) break;  // nothing of bn is in flight
-            stage(bn);
-        }
-        b = bn;
-    }
-    cp_async_wait<0>();
-}
-
-// Progress words of a flowing sweep: INT_MAX for every slot (blocks that are
-// not swept never hold anything up), then 0 for the swept blocks.
-__global__ void flow_init_kernel(int* prog, size_t n_slots, const int32_t* __restrict__ nbr, int n, unsigned int* counter) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_slots; i += (size_t)gridDim.x * blockDim.x)
-        prog[i] = 0x7fffffff;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
-}
-__global__ void flow_zero_kernel(int* prog, const int32_t* __restrict__ nbr, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) prog[nbr[(size_t)i * 27 + 13]] = 0;
-}
-
 // Copies the x-planes (x = 0 and x = bsx-1) of the listed slots into the side
 // buffer: [slot][plane][z][y].
 template <class E, int BSX>
@@ -1218,37 +1078,6 @@ static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* ord
     begin_launch(ctx);
     sweep_compact_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
     after_launch(ctx, "sweep_compact_kernel");
-}
-
-template <int BSX, int ST, bool CLAMP>
-static void launch_flow(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n, int iters, int* prog,
-                        unsigned int* counter) {
-    const size_t smem = 2 * sizeof(float) * Compact<BSX>::BUF;
-    static bool attr = false;
-    if (!attr) {
-        CUDA_CHECK(cudaFuncSetAttribute(sweep_flow_kernel<BSX, ST, CLAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CUDA_CHECK(cudaFuncSetAttribute(sweep_flow_kernel<BSX, ST, CLAMP>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        (int)cudaSharedmemCarveoutMaxShared));
-        attr = true;
-    }
-    const int threads = CompactThreads<BSX, ST>::v;
-    int per_sm = 0;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_flow_kernel<BSX, ST, CLAMP>, threads, smem));
-    int sms = 0;
-    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    const long total = (long)n * iters;
-    const int grid = (int)std::max<long>(1, std::min<long>(total, (long)std::max(per_sm, 1) * sms));
-    begin_launch(ctx);
-    sweep_flow_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n, iters, prog, counter,
-                                                                                       ctx->status.as<int>());
-    after_launch(ctx, "sweep_flow_kernel");
-}
-
-template <int BSX, int ST>
-static void launch_flow_c(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n, int iters, int* prog,
-                          unsigned int* counter) {
-    if (a.clamp01) launch_flow<BSX, ST, true>(ctx, a, order, n, iters, prog, counter);
-    else launch_flow<BSX, ST, false>(ctx, a, order, n, iters, prog, counter);
 }
 
 template <class E, int BSX, int ST>
@@ -1459,35 +1288,6 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
         else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
     }
     const int32_t* order = plan->order.as<int32_t>();
-    // f32 with a one-cell halo on 8^3 or 16^3 blocks: every colour phase of
-    // every sweep in one launch (sweep_flow_kernel)
-    if (g->dtype == MSBG_F32 && (g->bsx == 8 || g->bsx == 16) && stencil != MSBG_BILAPLACIAN) {
-        MSBG_REQUIRE((long)plan->n * iterations < (1L << 31), "too many (sweep, block) items for one launch");
-        const size_t slots = g->n_slots();
-        if (plan->flow_slots < slots) {
-            plan->flow.reserve(slots * 4 + 256);
-            plan->flow_slots = slots;
-        }
-        int* prog = plan->flow.as<int>();
-        unsigned int* counter = reinterpret_cast<unsigned int*>(plan->flow.as<char>() + ((slots * 4 + 127) & ~size_t(127)));
-        begin_launch(g->ctx);
-        flow_init_kernel<<<(unsigned)std::min<size_t>((slots + 255) / 256 + 1, 148 * 8), 256, 0, g->ctx->stream>>>(
-            prog, slots, a.nbr, (int)plan->n, counter);
-        after_launch(g->ctx, "flow_init_kernel");
-        begin_launch(g->ctx);
-        flow_zero_kernel<<<(unsigned)std::min<size_t>((plan->n + 255) / 256, 148 * 8), 256, 0, g->ctx->stream>>>(
-            prog, a.nbr, (int)plan->n);
-        after_launch(g->ctx, "flow_zero_kernel");
-        const int n = (int)plan->n;
-        if (stencil == MSBG_LAPLACIAN) {
-            if (g->bsx == 16) launch_flow_c<16, MSBG_LAPLACIAN>(g->ctx, a, order, n, iterations, prog, counter);
-            else launch_flow_c<8, MSBG_LAPLACIAN>(g->ctx, a, order, n, iterations, prog, counter);
-        } else {
-            if (g->bsx == 16) launch_flow_c<16, MSBG_MEAN_CURVATURE>(g->ctx, a, order, n, iterations, prog, counter);
-            else launch_flow_c<8, MSBG_MEAN_CURVATURE>(g->ctx, a, order, n, iterations, prog, counter);
-        }
-        return;
-    }
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < 8; ++c) {
             int cnt = plan->color_off[c + 1] - plan->color_off[c];

@@ -24,8 +24,6 @@ struct SweepPlan {
     size_t n_xslots = 0;
     DevBuf xface;   // f32 [n_slots][2][bsx^2]: x = 0 and x = bsx-1 planes, [z][y]
     size_t xface_slots = 0;
-    DevBuf flow;    // one-launch sweeps: int32 progress word per slot, then the item counter
-    size_t flow_slots = 0;
 };
 
 }  // namespace msbg
