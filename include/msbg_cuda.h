@@ -47,6 +47,11 @@ extern "C" {
 #define MSBG_U16 1  /* `Density`: u16, value = q / 65535, store rounds      */
                     /* half away from zero (stencil.rs:160-174)            */
 #define MSBG_BF16 2 /* bf16 payload, store rounds to nearest even           */
+#define MSBG_U8 3   /* `Density8`: u8, value = q / 255 (sample.rs:64-70);   */
+                    /* writes round(v * 255) (channel.rs:378-382); sweeps  */
+                    /* store sqrt-compressed with stochastic rounding      */
+                    /* (stencil.rs:176-192)                                */
+#define MSBG_F16 4  /* IEEE binary16 payload, store rounds to nearest even  */
 
 /* Stencil of a sweep (solver.rs:44-51). */
 #define MSBG_LAPLACIAN 0       /* 7-tap,  laplacian.rs:16-70               */
@@ -152,6 +157,21 @@ int msbg_halo_gather_device(msbg_grid* grid, const uint64_t* d_bids, size_t n, i
  * active list or the grid's block set changes. */
 int msbg_sweep(msbg_grid* grid, const uint64_t* active, size_t n, int stencil, float dt,
                int iterations, int clamp01);
+/* The same sweep with the Density8 store's generator made explicit: the
+ * store of chunk k (counting every chunk the sweeper stored since it was
+ * seeded: sweeps, then colours, then blocks in plan order, then chunks of
+ * `lanes` elements in block order) draws from SimdRng::<lanes>::seed(seed)
+ * after k + 1 steps (stencil.rs:103-132).  *stream_pos holds k at the first
+ * store of this call and is advanced past the last; a fresh sweeper starts at
+ * 0.  One rayon thread of the reference (slot 0, seed 0xdeadbeef,
+ * solver.rs:109-119) draws exactly this stream.  lanes is the reference
+ * build's SIMD width (4, 8 or 16) and must divide the block size.
+ * msbg_sweep on a Density8 grid is this call with seed 0xdeadbeef, lanes 16
+ * (the block size when that is smaller) and position 0 (apply_pde's fresh
+ * sweeper).  Other dtypes ignore the
+ * generator (their stores are deterministic) and leave *stream_pos alone. */
+int msbg_sweep_stochastic(msbg_grid* grid, const uint64_t* active, size_t n, int stencil, float dt,
+                          int iterations, int clamp01, uint32_t seed, int lanes, uint64_t* stream_pos);
 /* Multiresolution sweep: the halo of each fine block reads coarser
  * neighbours (levels[b] > levels[bid]) from `coarse` at the fine coordinate
  * >> 1 (fill_multires, multires/halo.rs:187-358); absent blocks read 0.
@@ -255,14 +275,16 @@ int msbg_g2p_device(msbg_mac* mac, const float* d_pos, size_t n, int bc, float* 
 int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u, const float* d_u_tilde,
                           size_t n, float alpha, float* d_out);
 /* Scalar trilinear Sampler::sample::<Linear> (math/sample.rs:494-512);
- * align 0 = Corner, 1 = CellCentered. */
+ * align 0 = Corner, 1 = CellCentered.  Any storage type: samples are read
+ * through Dequant (math/sample.rs:45-70; Density8 linearly, q / 255). */
 int msbg_sample_linear(msbg_grid* grid, const float* pos, size_t n, int align, int bc, float* out);
 /* Sampler::sample / gradient / hessian (math/sample.rs:493-649) beyond the
  * trilinear value: mode 0 = cubic B-spline value (out[n]), 1 = cubic
  * gradient (out[n][3]), 2 = cubic Hessian (out[n][6]: fxx, fyy, fzz, fxy, fxz,
  * fyz), 3 = trilinear gradient at `align` (out[n][3]).  The cubic basis
  * (math/bspline.rs:4-32) is cell-centred whatever `align` says, with a 4^3
- * window from gather_map (math/gather.rs:54-158); f32 grids, blocks >= 4^3. */
+ * window from gather_map (math/gather.rs:54-158); any storage type (read
+ * through Dequant as above), blocks >= 4^3. */
 int msbg_sample_ext(msbg_grid* grid, const float* pos, size_t n, int mode, int align, int bc, float* out);
 int msbg_sample_ext_device(msbg_grid* grid, const float* d_pos, size_t n, int mode, int align, int bc, float* d_out);
 
@@ -500,15 +522,21 @@ int msbg_unet_train_step_device(msbg_unet* net, const float* d_r, const float* d
  * touch at any level).  Problem p's level-0 cells are a contiguous range of
  * its group's vectors (msbg_batch_problem), blocks in ascending id order.
  * msbg_batch_buffers gives the group's device right-hand side (f32) and
- * solution (FP64).  tune != 0 autotunes the launch shapes of the Jacobi and
- * residual kernels per level (msbg_batch_tuning: per level the chosen shape
- * indices (Jacobi, residual) and the level's cells).  msbg_batch_solve runs
- * MG-preconditioned CG with per-problem scalars on the device; one cycle of
+ * solution (FP64).  tune != 0 autotunes every level but the coarsest: the
+ * z-planes per CTA (2, 4, 8 or 16) of the 16^3 tile kernel on levels of whole
+ * 16^3 blocks, the launch shapes (threads, CTAs per SM) of the Jacobi and
+ * residual kernels elsewhere (msbg_batch_tuning: per level cfg_out[3l..3l+2]
+ * = Jacobi shape index, residual shape index, tile z-planes or 0, and the
+ * level's cells; cap counts levels).  msbg_batch_solve runs
+ * MG-preconditioned CG with per-problem scalars on the device.  A cycle is
  * iters_per_cycle iterations over all problems plus the FP64 residual
- * replacement is a single CUDA graph launch; it stops when every problem
- * reaches relative residual tol (true residual of the FP64 solution) or
- * after max_cycles.  iters_out and rel_out are per problem.
- * msbg_poisson_autotune tunes a single solve's hierarchy the same way. */
+ * replacement; the whole solve is a single CUDA graph launch whose
+ * device-side while loop (a conditional graph node) runs cycles until every
+ * problem reaches relative residual tol (true residual of the FP64 solution)
+ * or max_cycles have run; the host waits once, at the end.  iters_out and
+ * rel_out are per problem, cycles_out the cycles the loop ran.
+ * msbg_poisson_autotune tunes a single solve's hierarchy the same way
+ * (cfg_out as above; cap counts ints). */
 typedef struct msbg_batch msbg_batch;
 int msbg_batch_create(msbg_ctx* ctx, int n_problems, const int* bsx, const uint64_t* dims, const uint64_t* const* active,
                       const size_t* n_active, int tune, msbg_batch** out);
@@ -524,6 +552,12 @@ int msbg_batch_tuning(const msbg_batch* batch, int group, int* cfg_out, uint64_t
 int msbg_batch_solve(msbg_batch* batch, double tol, int iters_per_cycle, int max_cycles, int zero_x, int* iters_out,
                      double* rel_out, int* cycles_out);
 int msbg_poisson_autotune(msbg_poisson* p, int* cfg_out, size_t cap, size_t* n_levels);
+/* Sets the first n_levels levels' choices (cfg as msbg_poisson_autotune
+ * writes it: Jacobi shape, residual shape, tile per level), e.g. a tuning
+ * saved from an earlier run.  Tile 1 is the quad tile (one 64-thread CTA per
+ * 16^3 block, four cells per thread), 2/4/8/16 the slab tile with that many
+ * z-planes per 256-thread CTA; every choice computes the same bits. */
+int msbg_poisson_set_tuning(msbg_poisson* p, const int* cfg, size_t n_levels);
 
 #ifdef __cplusplus
 }

@@ -20,7 +20,7 @@ MSBG_ERR_CUDA = 4
 MSBG_ERR_STATE = 5
 MSBG_ERR_NUMERIC = 6
 
-MSBG_F32, MSBG_U16, MSBG_BF16 = 0, 1, 2
+MSBG_F32, MSBG_U16, MSBG_BF16, MSBG_U8, MSBG_F16 = 0, 1, 2, 3, 4
 MSBG_LAPLACIAN, MSBG_MEAN_CURVATURE, MSBG_BILAPLACIAN = 0, 1, 2
 MSBG_CLAMP, MSBG_NEUMANN, MSBG_DIRICHLET = 0, 1, 2
 
@@ -70,6 +70,7 @@ SIGNATURES = {
     "msbg_halo_gather": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_halo_gather_device": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_sweep": [_P, _P, _SZ, _I, _F, _I, _I],
+    "msbg_sweep_stochastic": [_P, _P, _SZ, _I, _F, _I, _I, C.c_uint32, _I, _P],
     "msbg_sweep_multires": [_P, _P, _P, _P, _SZ, _I, _F, _I, _I],
     "msbg_morton3": [_P, _P, _SZ, _P],
     "msbg_sort_block_list_morton": [_P, _P, _SZ, _U64, _U64, _P, _SZ, _I],
@@ -142,6 +143,7 @@ SIGNATURES = {
     "msbg_poisson_set_preconditioner": [_P, _P],
     "msbg_poisson_set_network_lead": [_P, _I],
     "msbg_poisson_autotune": [_P, _P, _SZ, _SZP],
+    "msbg_poisson_set_tuning": [_P, _P, _SZ],
     "msbg_batch_create": [_P, _I, _P, _P, _P, _P, _I, C.POINTER(_P)],
     "msbg_batch_destroy": [_P],
     "msbg_batch_groups": [_P, C.POINTER(_I)],

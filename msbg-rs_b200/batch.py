@@ -1,6 +1,7 @@
 """Batched Poisson solves (the C ABI's msbg_batch_*): many independent sparse
-problems solved together, one CUDA graph launch per solver cycle, launch
-shapes autotuned per level.  No counterpart in the crate, which has no
+problems solved together in one CUDA graph launch whose device-side loop runs
+solver cycles until every problem converges, launch shapes autotuned per
+level.  No counterpart in the crate, which has no
 pressure solver."""
 from __future__ import annotations
 
@@ -54,12 +55,13 @@ class Batch:
         return out
 
     def tuning(self, g):
-        """Per level of group g: chosen (Jacobi, residual) launch-shape indices and cells."""
-        cfg = np.zeros(2 * 64, np.int32)
+        """Per level of group g: the chosen (Jacobi shape index, residual shape
+        index, tile z-planes or 0) and the level's cells."""
+        cfg = np.zeros(3 * 64, np.int32)
         cells = np.zeros(64, np.uint64)
         n = C.c_size_t()
         call("msbg_batch_tuning", self.handle, int(g), ptr(cfg), ptr(cells), 64, C.byref(n))
-        return cfg[: 2 * n.value].reshape(-1, 2), cells[: n.value]
+        return cfg[: 3 * n.value].reshape(-1, 3), cells[: n.value]
 
     def solve(self, tol=1e-8, iters_per_cycle=8, max_cycles=100, zero_x=True):
         """(iterations per problem, relative residual per problem, cycles)."""

@@ -2,6 +2,7 @@
 // context (stream + scratch arena + launch counter) and small device helpers.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -291,7 +292,69 @@ struct ElemBF16 {
     }
 };
 
-inline size_t dtype_size(int dtype) { return dtype == MSBG_F32 ? 4 : 2; }
+struct ElemU8 {  // `Density8`: read linearly as q / 255 (sample.rs:64-70)
+    using T = uint8_t;
+    __device__ static float load(T v) { return __fmul_rn((float)v, 1.0f / 255.0f); }
+    // Quant::from_unit (channel.rs:378-382): round(v * 255), saturating
+    __device__ static T store(float v) {
+        float r = roundf(__fmul_rn(v, 255.0f));
+        r = r > 0.0f ? r : 0.0f;
+        r = r < 255.0f ? r : 255.0f;
+        return (T)r;
+    }
+};
+struct ElemF16 {  // IEEE binary16 bits, store rounds to nearest even
+    using T = uint16_t;
+    __device__ static float load(T v) { return __half2float(__ushort_as_half(v)); }
+    __device__ static T store(float v) { return __half_as_ushort(__float2half_rn(v)); }
+};
+
+// The sweep's write-back (StoreBack::store_chunk, stencil.rs:142-192).  Every
+// type but Density8 stores deterministically; Density8 compresses with sqrt
+// and rounds stochastically against the lane generator's next draw (the
+// SimdRng state after its multiply, stencil.rs:125-131, 176-192).  `state`
+// is that state for this element's chunk and lane.
+template <class E> struct StoreBack {
+    __device__ static typename E::T store(float v, uint32_t) { return E::store(v); }
+};
+template <> struct StoreBack<ElemU8> {
+    __device__ static uint8_t store(float v, uint32_t state) {
+        const float vf = __fmul_rn(__fsqrt_rn(v), 255.0f);
+        const float fl = floorf(vf);
+        const float frac = __fsub_rn(vf, fl);
+        const float u = __fsub_rn(__uint_as_float((state >> 9) | 0x3f800000u), 1.0f);
+        const float r = u < frac ? __fadd_rn(fl, 1.0f) : fl;
+        // the float -> i32 conversion of the x86 build (invalid or out of
+        // range gives INT_MIN), then the wrapping i32 -> u8 cast
+        const int32_t i = (r >= -2147483648.0f && r < 2147483648.0f) ? (int32_t)r : INT32_MIN;
+        return (uint8_t)(i & 0xff);
+    }
+};
+
+// Lane seeds of the stochastic-rounding generator (SimdRng::seed,
+// stencil.rs:108-121): a murmur finaliser over seed ^ lane * 0x9e3779b9,
+// zero replaced by 0xdeadbeef.
+__host__ __device__ inline uint32_t sr_lane_seed(uint32_t seed, uint32_t lane) {
+    uint32_t h = seed ^ (lane * 0x9e3779b9u);
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h ? h : 0xdeadbeefu;
+}
+// 16807^e mod 2^32: the generator state after e draws is seed * 16807^e.
+__host__ __device__ inline uint32_t sr_pow(uint64_t e) {
+    uint32_t r = 1u, b = 16807u;
+    while (e) {
+        if (e & 1) r *= b;
+        b *= b;
+        e >>= 1;
+    }
+    return r;
+}
+
+inline size_t dtype_size(int dtype) { return dtype == MSBG_F32 ? 4 : dtype == MSBG_U8 ? 1 : 2; }
 
 // Host-side conversions of a float constant to the stored representation and
 // back (the value a dummy block reads after dequantisation).

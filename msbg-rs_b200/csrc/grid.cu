@@ -110,6 +110,13 @@ float quantize_roundtrip(int dtype, float v) {
         memcpy(&f, &u, 4);
         return f;
     }
+    if (dtype == MSBG_U8) {
+        float r = roundf(v * 255.0f);
+        r = r > 0.0f ? r : 0.0f;
+        r = r < 255.0f ? r : 255.0f;
+        return (float)(uint8_t)r * (1.0f / 255.0f);
+    }
+    if (dtype == MSBG_F16) return __half2float(__float2half_rn(v));
     return v;
 }
 
@@ -208,6 +215,10 @@ void grid_fill_slots(msbg_grid* g, const int32_t* d_slots, size_t count, float v
         fill_slots_kernel<ElemF32><<<grid, 256, 0, g->ctx->stream>>>((float*)g->payload.p, d_slots, count, g->block_elems, value);
     else if (g->dtype == MSBG_U16)
         fill_slots_kernel<ElemU16><<<grid, 256, 0, g->ctx->stream>>>((uint16_t*)g->payload.p, d_slots, count, g->block_elems, value);
+    else if (g->dtype == MSBG_U8)
+        fill_slots_kernel<ElemU8><<<grid, 256, 0, g->ctx->stream>>>((uint8_t*)g->payload.p, d_slots, count, g->block_elems, value);
+    else if (g->dtype == MSBG_F16)
+        fill_slots_kernel<ElemF16><<<grid, 256, 0, g->ctx->stream>>>((uint16_t*)g->payload.p, d_slots, count, g->block_elems, value);
     else
         fill_slots_kernel<ElemBF16><<<grid, 256, 0, g->ctx->stream>>>((uint16_t*)g->payload.p, d_slots, count, g->block_elems, value);
     after_launch(g->ctx, "fill_slots_kernel");
@@ -416,6 +427,8 @@ template <class T> static T host_store(int dtype, float v) {
     } else {
         float q = quantize_roundtrip(dtype, v);
         if (dtype == MSBG_U16) return (T)lrintf(q * 65535.0f);
+        if (dtype == MSBG_U8) return (T)lrintf(q * 255.0f);
+        if (dtype == MSBG_F16) return (T)__half_as_ushort(__float2half_rn(q));
         uint32_t u;
         memcpy(&u, &q, 4);
         return (T)(u >> 16);
@@ -443,6 +456,8 @@ static void write_blocks(msbg_grid* g, const uint64_t* bids, size_t n, const voi
     begin_launch(g->ctx);
     if (g->esize == 4)
         scatter_blocks_kernel<uint32_t><<<grid, 256, 0, g->ctx->stream>>>((uint32_t*)g->payload.p, d_slots, (const uint32_t*)src, n, g->block_elems);
+    else if (g->esize == 1)
+        scatter_blocks_kernel<uint8_t><<<grid, 256, 0, g->ctx->stream>>>((uint8_t*)g->payload.p, d_slots, (const uint8_t*)src, n, g->block_elems);
     else
         scatter_blocks_kernel<uint16_t><<<grid, 256, 0, g->ctx->stream>>>((uint16_t*)g->payload.p, d_slots, (const uint16_t*)src, n, g->block_elems);
     after_launch(g->ctx, "scatter_blocks_kernel");
@@ -470,6 +485,10 @@ static void read_blocks(msbg_grid* g, const uint64_t* bids, size_t n, void* out,
         gather_blocks_kernel<uint32_t><<<grid, 256, 0, g->ctx->stream>>>(
             (const uint32_t*)g->payload.p, d_codes, (uint32_t*)dst, n, g->block_elems,
             host_store<uint32_t>(g->dtype, g->empty_value), host_store<uint32_t>(g->dtype, g->full_value));
+    else if (g->esize == 1)
+        gather_blocks_kernel<uint8_t><<<grid, 256, 0, g->ctx->stream>>>(
+            (const uint8_t*)g->payload.p, d_codes, (uint8_t*)dst, n, g->block_elems,
+            host_store<uint8_t>(g->dtype, g->empty_value), host_store<uint8_t>(g->dtype, g->full_value));
     else
         gather_blocks_kernel<uint16_t><<<grid, 256, 0, g->ctx->stream>>>(
             (const uint16_t*)g->payload.p, d_codes, (uint16_t*)dst, n, g->block_elems,
@@ -583,6 +602,8 @@ static void halo_gather(msbg_grid* g, const uint64_t* d_bids, size_t n, int halo
     a.full = quantize_roundtrip(g->dtype, g->full_value);
     if (g->dtype == MSBG_F32) launch_halo_gather<ElemF32>(g, a, d_bids, n, halo, full, bc, d_out);
     else if (g->dtype == MSBG_U16) launch_halo_gather<ElemU16>(g, a, d_bids, n, halo, full, bc, d_out);
+    else if (g->dtype == MSBG_U8) launch_halo_gather<ElemU8>(g, a, d_bids, n, halo, full, bc, d_out);
+    else if (g->dtype == MSBG_F16) launch_halo_gather<ElemF16>(g, a, d_bids, n, halo, full, bc, d_out);
     else launch_halo_gather<ElemBF16>(g, a, d_bids, n, halo, full, bc, d_out);
 }
 
@@ -717,7 +738,7 @@ int msbg_grid_create(msbg_ctx* ctx, uint64_t sx, uint64_t sy, uint64_t sz, int b
     MSBG_API_BEGIN
     MSBG_REQUIRE(ctx && out, "null argument");
     MSBG_REQUIRE(is_pow2((uint64_t)bsx) && bsx <= 32, "bsx must be a power of two <= 32");
-    MSBG_REQUIRE(dtype >= MSBG_F32 && dtype <= MSBG_BF16, "bad dtype");
+    MSBG_REQUIRE(dtype >= MSBG_F32 && dtype <= MSBG_F16, "bad dtype");
     MSBG_REQUIRE(sx > 0 && sy > 0 && sz > 0 && sx < (1ULL << 31) && sy < (1ULL << 31) && sz < (1ULL << 31),
                  "domain extents must be in [1, 2^31)");
     set_device(ctx);

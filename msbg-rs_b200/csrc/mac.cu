@@ -20,7 +20,8 @@ void mac_ensure(msbg_mac* m, const uint64_t* bids, size_t n, int32_t* slots) {
 }
 
 struct SampleGrid {
-    const float* payload;
+    const float* payload;  // f32 grids (the G2P path); null otherwise
+    const void* raw;       // the payload in the grid's storage type
     const int32_t* dense;  // bid -> code, or null (use the hash)
     DevHash hash;
     int64_t nx, ny, nz;
@@ -29,22 +30,29 @@ struct SampleGrid {
     float empty, full;
 };
 
-static SampleGrid sample_grid(msbg_grid* g) {
-    MSBG_REQUIRE(g->dtype == MSBG_F32, "sampling needs an f32 grid");
+// any_dtype: the Sampler of any InterpElem (sample.rs:45-70 Dequant) reads
+// every storage type; the MAC velocity paths need f32.
+static SampleGrid sample_grid(msbg_grid* g, bool any_dtype = false) {
+    MSBG_REQUIRE(any_dtype || g->dtype == MSBG_F32, "sampling needs an f32 grid");
     SampleGrid s;
-    s.payload = g->payload.as<float>();
+    s.payload = g->dtype == MSBG_F32 ? g->payload.as<float>() : nullptr;
+    s.raw = g->payload.p;
     s.hash = device_hash(g);
     s.dense = device_dense(g);
     s.nx = (int64_t)g->nx; s.ny = (int64_t)g->ny; s.nz = (int64_t)g->nz;
     s.sx = (int32_t)g->sx; s.sy = (int32_t)g->sy; s.sz = (int32_t)g->sz;
     s.lg = g->lg;
-    s.empty = g->empty_value;
-    s.full = g->full_value;
+    s.empty = quantize_roundtrip(g->dtype, g->empty_value);
+    s.full = quantize_roundtrip(g->dtype, g->full_value);
     return s;
 }
 
+template <class E = ElemF32>
 __device__ __forceinline__ float code_value(const SampleGrid& g, int32_t code, int vid) {
-    if (code >= 0) return g.payload[((size_t)code << (3 * g.lg)) + vid];
+    if (code >= 0) {
+        if constexpr (std::is_same<E, ElemF32>::value) return g.payload[((size_t)code << (3 * g.lg)) + vid];
+        else return E::load(static_cast<const typename E::T*>(g.raw)[((size_t)code << (3 * g.lg)) + vid]);
+    }
     return code == kCodeFull ? g.full : g.empty;
 }
 
@@ -56,6 +64,7 @@ __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(
 
 // gather_map (math/gather.rs:54-158, dmax = 1) + trilinear_value (sample.rs:203-211)
 // at a position already in the grid's node frame.
+template <class E = ElemF32>
 __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float z, int bc) {
     const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
@@ -71,7 +80,7 @@ __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float 
             for (int k = 0; k < 2; ++k)
                 for (int j = 0; j < 2; ++j)
                     for (int i = 0; i < 2; ++i)
-                        c[s++] = code_value(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
+                        c[s++] = code_value<E>(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
             fast = true;
         }
     }
@@ -98,7 +107,7 @@ __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float 
                     if (okx && oky && okz) {
                         const int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) |
                                              ((((rz >> lg) - bz0) & 1) << 2));
-                        c[s] = code_value(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
+                        c[s] = code_value<E>(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
                     } else {
                         c[s] = g.empty;
                     }
@@ -114,11 +123,12 @@ __device__ float sample_linear_dev(const SampleGrid& g, float x, float y, float 
     return lerpf(c0, c1, w);
 }
 
+template <class E>
 __global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, int align, int bc, float* out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
         if (align == 1) { x = x - 0.5f; y = y - 0.5f; z = z - 0.5f; }
-        out[i] = sample_linear_dev(g, x, y, z, bc);
+        out[i] = sample_linear_dev<E>(g, x, y, z, bc);
     }
 }
 
@@ -128,7 +138,7 @@ __global__ void sample_linear_kernel(SampleGrid g, const float* pos, size_t n, i
 // A Neumann window far outside the domain can reflect to a block before the
 // anchor block, where the crate's slot index leaves the 2x2x2 slots
 // (undefined there); slot offsets are taken mod 2.
-template <int SPAN>
+template <int SPAN, class E = ElemF32>
 __device__ void gather_window_dev(const SampleGrid& g, int32_t ix0, int32_t iy0, int32_t iz0, int bc, float* out) {
     constexpr int DMAX = SPAN - 1;
     const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
@@ -144,7 +154,7 @@ __device__ void gather_window_dev(const SampleGrid& g, int32_t ix0, int32_t iy0,
                 for (int j = 0; j < SPAN; ++j)
 #pragma unroll
                     for (int i = 0; i < SPAN; ++i)
-                        out[s++] = code_value(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
+                        out[s++] = code_value<E>(g, code, (vx0 + i) | ((vy0 + j) << lg) | ((vz0 + k) << (2 * lg)));
             return;
         }
     }
@@ -174,7 +184,7 @@ __device__ void gather_window_dev(const SampleGrid& g, int32_t ix0, int32_t iy0,
                 if (okx && oky && okz) {
                     const int sl = (int)((((rx >> lg) - bx0) & 1) | ((((ry >> lg) - by0) & 1) << 1) |
                                          ((((rz >> lg) - bz0) & 1) << 2));
-                    out[s] = code_value(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
+                    out[s] = code_value<E>(g, codes[sl], (rx & mask) | ((ry & mask) << lg) | ((rz & mask) << (2 * lg)));
                 } else {
                     out[s] = g.empty;
                 }
@@ -217,6 +227,7 @@ __device__ __forceinline__ float row_dot_dev(const float* f, const float w[4]) {
 // (trilinear_value_grad, sample.rs:215-237) at `align` -> out[n][3].  The
 // cubic basis is cell-centred whatever the alignment: window base
 // floor(p - 0.5) - 1, t = frac(p - 0.5).  One thread per position.
+template <class E>
 __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, size_t n, int mode, int align, int bc,
                                   float* __restrict__ out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -225,7 +236,7 @@ __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, s
             if (align == 1) { x = x - 0.5f; y = y - 0.5f; z = z - 0.5f; }
             const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
             float c[8];
-            gather_window_dev<2>(g, (int32_t)fx, (int32_t)fy, (int32_t)fz, bc, c);
+            gather_window_dev<2, E>(g, (int32_t)fx, (int32_t)fy, (int32_t)fz, bc, c);
             const float u = x - fx, v = y - fy, w = z - fz;
             const float f01234567 = ((((((c[7] - c[6]) - c[5]) + c[4]) - c[3]) + c[2]) + c[1]) - c[0];
             const float f01234567u = f01234567 * u;
@@ -241,7 +252,7 @@ __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, s
         const float xf = floorf(x), yf = floorf(y), zf = floorf(z);
         const float tx = x - xf, ty = y - yf, tz = z - zf;
         float win[64];
-        gather_window_dev<4>(g, (int32_t)xf - 1, (int32_t)yf - 1, (int32_t)zf - 1, bc, win);
+        gather_window_dev<4, E>(g, (int32_t)xf - 1, (int32_t)yf - 1, (int32_t)zf - 1, bc, win);
         float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4], ddx[4], ddy[4], ddz[4];
         cubic_w_dev(tx, wx); cubic_w_dev(ty, wy); cubic_w_dev(tz, wz);
         cubic_dw_dev(tx, dx); cubic_dw_dev(ty, dy); cubic_dw_dev(tz, dz);
@@ -633,7 +644,7 @@ int msbg_sample_linear(msbg_grid* g, const float* pos, size_t n, int align, int 
     MSBG_REQUIRE(bc >= 0 && bc <= 2, "bad boundary condition");
     if (!n) return MSBG_OK;
     set_device(g->ctx);
-    SampleGrid s = sample_grid(g);
+    SampleGrid s = sample_grid(g, true);
     ScratchLayout L;
     size_t op = L.add<float>(3 * n), oo = L.add<float>(n);
     char* base = scratch(g->ctx, L);
@@ -641,7 +652,13 @@ int msbg_sample_linear(msbg_grid* g, const float* pos, size_t n, int align, int 
     float* dout = ScratchLayout::at<float>(base, oo);
     CUDA_CHECK(cudaMemcpyAsync(dp, pos, 12 * n, cudaMemcpyHostToDevice, g->ctx->stream));
     begin_launch(g->ctx);
-    sample_linear_kernel<<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout);
+    switch (g->dtype) {
+        case MSBG_F32: sample_linear_kernel<ElemF32><<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout); break;
+        case MSBG_U16: sample_linear_kernel<ElemU16><<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout); break;
+        case MSBG_BF16: sample_linear_kernel<ElemBF16><<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout); break;
+        case MSBG_U8: sample_linear_kernel<ElemU8><<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout); break;
+        default: sample_linear_kernel<ElemF16><<<grid_for(n), 256, 0, g->ctx->stream>>>(s, dp, n, align, bc, dout); break;
+    }
     after_launch(g->ctx, "sample_linear_kernel");
     CUDA_CHECK(cudaMemcpyAsync(out, dout, 4 * n, cudaMemcpyDeviceToHost, g->ctx->stream));
     sync(g->ctx);
@@ -659,9 +676,15 @@ int msbg_sample_ext_device(msbg_grid* g, const float* d_pos, size_t n, int mode,
     MSBG_REQUIRE(g->bsx >= 4, "cubic sampling needs blocks of at least 4^3 cells");
     if (!n) return MSBG_OK;
     set_device(g->ctx);
-    SampleGrid s = sample_grid(g);
+    SampleGrid s = sample_grid(g, true);
     begin_launch(g->ctx);
-    sample_ext_kernel<<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out);
+    switch (g->dtype) {
+        case MSBG_F32: sample_ext_kernel<ElemF32><<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out); break;
+        case MSBG_U16: sample_ext_kernel<ElemU16><<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out); break;
+        case MSBG_BF16: sample_ext_kernel<ElemBF16><<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out); break;
+        case MSBG_U8: sample_ext_kernel<ElemU8><<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out); break;
+        default: sample_ext_kernel<ElemF16><<<grid_for(n), 128, 0, g->ctx->stream>>>(s, d_pos, n, mode, align, bc, d_out); break;
+    }
     after_launch(g->ctx, "sample_ext_kernel");
     MSBG_API_END
 }

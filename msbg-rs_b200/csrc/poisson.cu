@@ -55,6 +55,7 @@ struct PLevelDev {
     DevBuf diag;     // f32 [cells] s_l (6 - g_l m), 0 for inactive cells; l >= 1 (level 0: 6, all active)
     DevBuf x, b, r, t;  // f32 [cells]
     int cfg_jac = 0, cfg_res = 0;  // launch shapes of the level's Jacobi and residual kernels (autotuned)
+    int slab = 1;                  // tile of the 16^3 kernels: 1 quad tile, else slab z-planes (autotuned)
     int64_t n() const { return (int64_t)bids.size(); }
     int64_t cells() const { return n() * bs * bs * bs; }
 };
@@ -213,29 +214,48 @@ __global__ void pk_jacobi(LevelArgs L, const float* __restrict__ x, const float*
     }
 }
 
-// The 7-point kernels on 16^3 blocks, one CTA per slab of kB16Slab z-planes
-// of a block: thread (x, y) walks its z-column with the planes below and
-// above in registers (the next one prefetched), the current plane and its x/y
-// halo from the face neighbours in shared memory.  Each value of x is read once (plus the block's halo
-// faces), coalesced.  The neighbour sum adds x-1, x+1, y-1, y+1, z-1, z+1 in
-// that order, zeros outside the active blocks, as nb_sum.
+// The 7-point kernels on 16^3 blocks.  Both tile kernels add the neighbours
+// x-1, x+1, y-1, y+1, z-1, z+1 in that order (zeros outside the active
+// blocks, as nb_sum) and round every operation as written (no contraction),
+// so every tile choice gives the same bits:
 // OP 0: weighted Jacobi xn = w (b + s nb) / (6 s) + (1 - w) x (x null: the
 // first sweep from zero); 1: residual r = b - s (6 x - nb); 2: y = s (6 x - nb).
-constexpr int kB16Slab = 4;  // z-planes per CTA (shorter dependent chains, more CTAs)
-
 template <int OP>
+__device__ __forceinline__ float op7(float sn, float cur, float bz, float scale, float omega, float inv_d) {
+    if (OP == 0)
+        return __fadd_rn(__fmul_rn(__fmul_rn(omega, __fadd_rn(bz, __fmul_rn(scale, sn))), inv_d),
+                         __fmul_rn(__fsub_rn(1.0f, omega), cur));
+    if (OP == 1) return __fsub_rn(bz, __fmul_rn(scale, __fsub_rn(__fmul_rn(6.0f, cur), sn)));
+    return __fmul_rn(scale, __fsub_rn(__fmul_rn(6.0f, cur), sn));
+}
+__device__ __forceinline__ float nb6(float xm, float xp, float ym, float yp, float zm, float zp) {
+    float sn = xm;
+    sn = __fadd_rn(sn, xp);
+    sn = __fadd_rn(sn, ym);
+    sn = __fadd_rn(sn, yp);
+    sn = __fadd_rn(sn, zm);
+    return __fadd_rn(sn, zp);
+}
+
+// Slab tile: one 256-thread CTA per slab of SLAB z-planes of a block (2, 4,
+// 8 or 16: shorter dependent chains and more CTAs against more re-read slab
+// boundaries).  Thread (x, y) walks its z-column with the planes below and
+// above in registers (the next one prefetched), the current plane and its
+// x/y halo from the face neighbours in shared memory.
+template <int OP, int SLAB>
 __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __restrict__ x, const float* __restrict__ b,
                                                   float* __restrict__ out, float omega) {
     __shared__ float pl[18][18];
     __shared__ int32_t nb[6];
-    const int64_t k = blockIdx.x / (16 / kB16Slab);
-    const int z0 = (int)(blockIdx.x % (16 / kB16Slab)) * kB16Slab;
+    const int64_t k = blockIdx.x / (16 / SLAB);
+    const int z0 = (int)(blockIdx.x % (16 / SLAB)) * SLAB;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int col = tx + (ty << 4);
     const int64_t base = k << 12;
     const float inv_d = 1.0f / (6.0f * L.scale);
     if (OP == 0 && !x) {
-        for (int z = z0; z < z0 + kB16Slab; ++z) out[base + col + (z << 8)] = omega * b[base + col + (z << 8)] * inv_d;
+        for (int z = z0; z < z0 + SLAB; ++z)
+            out[base + col + (z << 8)] = __fmul_rn(__fmul_rn(omega, b[base + col + (z << 8)]), inv_d);
         return;
     }
     if (threadIdx.x < 6) nb[threadIdx.x] = L.nbr[k * 6 + threadIdx.x];
@@ -248,7 +268,7 @@ __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __re
         return xb[col + (z << 8)];
     };
     float down = plane(z0 - 1), cur = plane(z0), up = plane(z0 + 1);
-    for (int z = z0; z < z0 + kB16Slab; ++z) {
+    for (int z = z0; z < z0 + SLAB; ++z) {
         const float upn = z + 2 <= 16 ? plane(z + 2) : 0.0f;
         const float bz = OP == 2 ? 0.0f : b[base + col + (z << 8)];
         pl[ty + 1][tx + 1] = cur;
@@ -257,17 +277,77 @@ __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __re
         if (ty == 0) pl[0][tx + 1] = nym >= 0 ? x[((int64_t)nym << 12) + tx + (15 << 4) + (z << 8)] : 0.0f;
         if (ty == 15) pl[17][tx + 1] = nyp >= 0 ? x[((int64_t)nyp << 12) + tx + (z << 8)] : 0.0f;
         __syncthreads();
-        float sn = pl[ty + 1][tx];
-        sn += pl[ty + 1][tx + 2];
-        sn += pl[ty][tx + 1];
-        sn += pl[ty + 2][tx + 1];
-        sn += down;
-        sn += up;
-        const int64_t i = base + col + (z << 8);
-        if (OP == 0) out[i] = omega * (bz + L.scale * sn) * inv_d + (1.0f - omega) * cur;
-        else if (OP == 1) out[i] = bz - L.scale * (6.0f * cur - sn);
-        else out[i] = L.scale * (6.0f * cur - sn);
+        const float sn = nb6(pl[ty + 1][tx], pl[ty + 1][tx + 2], pl[ty][tx + 1], pl[ty + 2][tx + 1], down, up);
+        out[base + col + (z << 8)] = op7<OP>(sn, cur, bz, L.scale, omega, inv_d);
         __syncthreads();
+        down = cur;
+        cur = up;
+        up = upn;
+    }
+}
+
+// Quad tile: one 64-thread CTA per block; thread (q, y) owns the four
+// x-consecutive cells 4q..4q+3 of row y and walks all 16 z-planes with the
+// planes below and above in registers as float4 (plane z+2 loaded one step
+// ahead), so each thread keeps two 16-byte loads in flight per plane.  The x
+// neighbours come from the adjacent lanes of the row (shuffles) and, at the
+// block's x faces, from the neighbour blocks; the y neighbours from a
+// double-buffered shared plane whose halo rows the first and last row load
+// from the y neighbour blocks.
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float comp(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+
+template <int OP>
+__global__ void __launch_bounds__(64) pk_quad16(LevelArgs L, const float* __restrict__ x, const float* __restrict__ b,
+                                                float* __restrict__ out, float omega) {
+    __shared__ float4 pl[2][18][4];  // rows y = -1..16 of a plane, four quads each
+    const int64_t k = blockIdx.x;
+    const int q = threadIdx.x & 3, y = threadIdx.x >> 2;
+    const int64_t base = k << 12;
+    const int off = (y << 4) + (q << 2);
+    const float inv_d = 1.0f / (6.0f * L.scale);
+    if (OP == 0 && !x) {
+        for (int z = 0; z < 16; ++z) {
+            const float4 bv = ld4(b + base + off + (z << 8));
+            *reinterpret_cast<float4*>(out + base + off + (z << 8)) =
+                make_float4(__fmul_rn(__fmul_rn(omega, bv.x), inv_d), __fmul_rn(__fmul_rn(omega, bv.y), inv_d),
+                            __fmul_rn(__fmul_rn(omega, bv.z), inv_d), __fmul_rn(__fmul_rn(omega, bv.w), inv_d));
+        }
+        return;
+    }
+    const int32_t* nbr = L.nbr + k * 6;
+    const int32_t nxm = __ldg(nbr), nxp = __ldg(nbr + 1), nym = __ldg(nbr + 2), nyp = __ldg(nbr + 3), nzm = __ldg(nbr + 4),
+                  nzp = __ldg(nbr + 5);
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    auto plane = [&](int z) -> float4 {  // this thread's quad at plane z in [-1, 16]
+        if (z < 0) return nzm >= 0 ? ld4(x + ((int64_t)nzm << 12) + off + (15 << 8)) : zero;
+        if (z > 15) return nzp >= 0 ? ld4(x + ((int64_t)nzp << 12) + off) : zero;
+        return ld4(x + base + off + (z << 8));
+    };
+    float4 down = plane(-1), cur = plane(0), up = plane(1);
+    for (int z = 0; z < 16; ++z) {
+        const int buf = z & 1;
+        const float4 upn = z + 2 <= 16 ? plane(z + 2) : zero;
+        const float4 bz = OP == 2 ? zero : ld4(b + base + off + (z << 8));
+        const float xl = q == 0 && nxm >= 0 ? x[((int64_t)nxm << 12) + 15 + (y << 4) + (z << 8)] : 0.0f;
+        const float xr = q == 3 && nxp >= 0 ? x[((int64_t)nxp << 12) + (y << 4) + (z << 8)] : 0.0f;
+        pl[buf][y + 1][q] = cur;
+        if (y == 0) pl[buf][0][q] = nym >= 0 ? ld4(x + ((int64_t)nym << 12) + (15 << 4) + (q << 2) + (z << 8)) : zero;
+        if (y == 15) pl[buf][17][q] = nyp >= 0 ? ld4(x + ((int64_t)nyp << 12) + (q << 2) + (z << 8)) : zero;
+        float lw = __shfl_up_sync(0xffffffffu, cur.w, 1);
+        float rx = __shfl_down_sync(0xffffffffu, cur.x, 1);
+        if (q == 0) lw = xl;
+        if (q == 3) rx = xr;
+        __syncthreads();  // one barrier per plane: the two buffers alternate
+        const float4 ym = pl[buf][y][q], yp = pl[buf][y + 2][q];
+        float r[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float xm = e == 0 ? lw : comp(cur, e - 1), xp = e == 3 ? rx : comp(cur, e + 1);
+            const float sn = nb6(xm, xp, comp(ym, e), comp(yp, e), comp(down, e), comp(up, e));
+            r[e] = op7<OP>(sn, comp(cur, e), comp(bz, e), L.scale, omega, inv_d);
+        }
+        *reinterpret_cast<float4*>(out + base + off + (z << 8)) = make_float4(r[0], r[1], r[2], r[3]);
         down = cur;
         cur = up;
         up = upn;
@@ -704,11 +784,31 @@ static void build(msbg_poisson* P, uint64_t sx, uint64_t sy, uint64_t sz, int bs
     sync(ctx);
 }
 
+// tile: 1 = the quad tile (one 64-thread CTA per block), 2, 4, 8, 16 = the
+// slab tile with that many z-planes per 256-thread CTA.
+template <int OP>
+static void launch_block16(msbg_ctx* ctx, const PLevelDev& L, int slab, const float* x, const float* b, float* out,
+                           float omega) {
+    const LevelArgs a = level_args(L);
+    if (slab == 1) {
+        pk_quad16<OP><<<(unsigned)L.n(), 64, 0, ctx->stream>>>(a, x, b, out, omega);
+        return;
+    }
+    const unsigned grid = (unsigned)(L.n() * (16 / slab));
+    switch (slab) {
+        case 2: pk_block16<OP, 2><<<grid, 256, 0, ctx->stream>>>(a, x, b, out, omega); break;
+        case 8: pk_block16<OP, 8><<<grid, 256, 0, ctx->stream>>>(a, x, b, out, omega); break;
+        case 16: pk_block16<OP, 16><<<grid, 256, 0, ctx->stream>>>(a, x, b, out, omega); break;
+        default: pk_block16<OP, 4><<<(unsigned)(L.n() * 4), 256, 0, ctx->stream>>>(a, x, b, out, omega); break;
+    }
+}
+static bool uses_block16(const PLevelDev& L) { return L.lg == 4 && !L.diag.p; }
+
 static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
-    if (L.lg == 4 && !L.diag.p) {
-        pk_block16<2><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), x, nullptr, y, 0.0f);
+    if (uses_block16(L)) {
+        launch_block16<2>(P->ctx, L, L.slab, x, nullptr, y, 0.0f);
         after_launch(P->ctx, "pk_block16_matvec");
         return;
     }
@@ -719,8 +819,8 @@ static void launch_matvec(msbg_poisson* P, int l, const float* x, float* y) {
 static void launch_residual(msbg_poisson* P, int l, const float* x, const float* b, float* r) {
     const PLevelDev& L = P->lv[l];
     begin_launch(P->ctx);
-    if (L.lg == 4 && !L.diag.p) {
-        pk_block16<1><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), x, b, r, 0.0f);
+    if (uses_block16(L)) {
+        launch_block16<1>(P->ctx, L, L.slab, x, b, r, 0.0f);
         after_launch(P->ctx, "pk_block16_residual");
         return;
     }
@@ -737,9 +837,8 @@ static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps,
         const float* src = (s % 2 == 0) ? x : t;
         float* dst = (s % 2 == 0) ? t : x;
         begin_launch(P->ctx);
-        if (L.lg == 4 && !L.diag.p) {
-            pk_block16<0><<<(unsigned)(L.n() * (16 / kB16Slab)), 256, 0, P->ctx->stream>>>(level_args(L), (s == 0 && x_zero) ? nullptr : src, b,
-                                                                        dst, omega);
+        if (uses_block16(L)) {
+            launch_block16<0>(P->ctx, L, L.slab, (s == 0 && x_zero) ? nullptr : src, b, dst, omega);
             after_launch(P->ctx, "pk_block16_jacobi");
             continue;
         }
@@ -1456,9 +1555,11 @@ static void batch_cycle(msbg_poisson* P, double* x64, const float* b, int K, dou
     scalars(P, 2, tol);
 }
 
-// Autotuner: for every level but the coarsest, time each launch shape of the
-// Jacobi and residual kernels on the level's own buffers (CUDA events, three
-// launches after one warm-up) and keep the fastest.
+// Autotuner: for every level but the coarsest, time each choice on the
+// level's own buffers (CUDA events, three launches after one warm-up) and keep
+// the fastest: levels of whole 16^3 blocks the tile kernel's slab depth (one
+// Jacobi sweep plus one residual per candidate), the others each launch shape
+// of the Jacobi and residual kernels.
 static void autotune(msbg_poisson* P) {
     msbg_ctx* ctx = P->ctx;
     MSBG_REQUIRE(!ctx->timing, "autotuning needs per-kernel timing off");
@@ -1470,6 +1571,31 @@ static void autotune(msbg_poisson* P) {
         const int64_t cells = L.cells();
         CUDA_CHECK(cudaMemsetAsync(L.x.p, 0, cells * 4, ctx->stream));
         CUDA_CHECK(cudaMemsetAsync(L.b.p, 0, cells * 4, ctx->stream));
+        if (uses_block16(L)) {
+            float best = 1e30f;
+            int best_slab = 4;
+            for (int slab : {1, 2, 4, 8, 16}) {
+                auto run = [&]() {
+                    launch_block16<0>(ctx, L, slab, L.x.as<float>(), L.b.as<float>(), L.t.as<float>(), P->omega);
+                    launch_block16<1>(ctx, L, slab, L.x.as<float>(), L.b.as<float>(), L.r.as<float>(), 0.0f);
+                };
+                run();
+                CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+                for (int rep = 0; rep < 3; ++rep) run();
+                CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+                CUDA_CHECK(cudaEventSynchronize(e1));
+                CUDA_CHECK(cudaGetLastError());
+                float ms = 0.0f;
+                CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                ctx->launches += 8;
+                if (ms < best) {
+                    best = ms;
+                    best_slab = slab;
+                }
+            }
+            L.slab = best_slab;
+            continue;
+        }
         for (int kind = 0; kind < 2; ++kind) {
             float best = 1e30f;
             int best_cfg = 0;
@@ -1506,15 +1632,43 @@ static void autotune(msbg_poisson* P) {
 
 }  // namespace msbg
 
+namespace msbg {
+
+// The convergence test of the device-side solve loop: any problem of any
+// group still active (S_ACTIVE > 0) and fewer than ctrl[1] cycles run sets
+// the loop's condition; `advance` counts the cycle just finished.  One block.
+struct GroupScal {
+    const double* scal;
+    int64_t np;
+};
+__global__ void bk_loop_ctrl(cudaGraphConditionalHandle h, const GroupScal* __restrict__ gt, int ng,
+                             long long* __restrict__ ctrl, int advance) {
+    int any = 0;
+    for (int g = 0; g < ng; ++g)
+        for (int64_t i = threadIdx.x; i < gt[g].np; i += blockDim.x) any |= gt[g].scal[i * S_WIDTH + S_ACTIVE] > 0.0;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const long long c = ctrl[0] + advance;
+        ctrl[0] = c;
+        cudaGraphSetConditional(h, (any && c < ctrl[1]) ? 1u : 0u);
+    }
+}
+
+}  // namespace msbg
+
 // A batch: problems grouped by block size, each group one stacked hierarchy.
+// The solve is one graph: a convergence test, then a device-side while loop
+// whose body is one cycle of every group followed by the test again.
 struct msbg_batch {
     msbg_ctx* ctx = nullptr;
     std::vector<msbg_poisson*> groups;
     std::vector<int> prob_group, prob_index;  // per problem: group and index inside it
     std::vector<msbg::DevBuf> b, x;           // per group: f32 right-hand sides, FP64 solutions
+    msbg::DevBuf gtab;                         // GroupScal per group
+    msbg::DevBuf ctrl;                         // long long [2]: cycles run, cycle limit
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int graph_k = 0, graph_kernels = 0;
+    int graph_k = 0, graph_kernels = 0;  // CG iterations per cycle, kernels per loop iteration
     double graph_tol = 0.0;
     ~msbg_batch() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -1771,9 +1925,28 @@ int msbg_poisson_autotune(msbg_poisson* P, int* cfg_out, size_t cap, size_t* n_l
     set_device(P->ctx);
     autotune(P);
     if (n_levels) *n_levels = P->lv.size();
-    for (size_t l = 0; l < P->lv.size() && cfg_out && 2 * l + 1 < cap; ++l) {
-        cfg_out[2 * l] = P->lv[l].cfg_jac;
-        cfg_out[2 * l + 1] = P->lv[l].cfg_res;
+    for (size_t l = 0; l < P->lv.size() && cfg_out && 3 * l + 2 < cap; ++l) {
+        cfg_out[3 * l] = P->lv[l].cfg_jac;
+        cfg_out[3 * l + 1] = P->lv[l].cfg_res;
+        cfg_out[3 * l + 2] = uses_block16(P->lv[l]) ? P->lv[l].slab : 0;
+    }
+    MSBG_API_END
+}
+
+int msbg_poisson_set_tuning(msbg_poisson* P, const int* cfg, size_t n_levels) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(P && (cfg || !n_levels), "null argument");
+    MSBG_REQUIRE(n_levels <= P->lv.size(), "more levels than the hierarchy has");
+    for (size_t l = 0; l < n_levels; ++l) {
+        const int j = cfg[3 * l], r = cfg[3 * l + 1], t = cfg[3 * l + 2];
+        MSBG_REQUIRE(j >= 0 && j < kNumShapes && r >= 0 && r < kNumShapes, "launch shape index out of range");
+        MSBG_REQUIRE(uses_block16(P->lv[l]) ? (t == 1 || t == 2 || t == 4 || t == 8 || t == 16) : t == 0,
+                     "tile must be 1, 2, 4, 8 or 16 on levels of whole 16^3 blocks and 0 elsewhere");
+    }
+    for (size_t l = 0; l < n_levels; ++l) {
+        P->lv[l].cfg_jac = cfg[3 * l];
+        P->lv[l].cfg_res = cfg[3 * l + 1];
+        if (cfg[3 * l + 2]) P->lv[l].slab = cfg[3 * l + 2];
     }
     MSBG_API_END
 }
@@ -1901,8 +2074,9 @@ int msbg_batch_tuning(const msbg_batch* B, int g, int* cfg_out, uint64_t* cells_
     *n_levels = P->lv.size();
     for (size_t l = 0; l < P->lv.size() && l < cap; ++l) {
         if (cfg_out) {
-            cfg_out[2 * l] = P->lv[l].cfg_jac;
-            cfg_out[2 * l + 1] = P->lv[l].cfg_res;
+            cfg_out[3 * l] = P->lv[l].cfg_jac;
+            cfg_out[3 * l + 1] = P->lv[l].cfg_res;
+            cfg_out[3 * l + 2] = uses_block16(P->lv[l]) ? P->lv[l].slab : 0;
         }
         if (cells_out) cells_out[l] = (uint64_t)P->lv[l].cells();
     }
@@ -1911,8 +2085,10 @@ int msbg_batch_tuning(const msbg_batch* B, int g, int* cfg_out, uint64_t* cells_
 
 // Solves every problem of the batch to relative residual `tol` (true
 // residual of the FP64 solution) from the current solutions (zero_x: from
-// zero).  Each cycle -- iters_per_cycle CG iterations for all problems and
-// the FP64 residual replacement -- is one CUDA graph launch.
+// zero).  A cycle is iters_per_cycle CG iterations for all problems and the
+// FP64 residual replacement; the cycles run in one CUDA graph launch, a
+// device-side while loop that stops once no problem is active or after
+// max_cycles cycles, so the host waits only once, at the end.
 int msbg_batch_solve(msbg_batch* B, double tol, int iters_per_cycle, int max_cycles, int zero_x, int* iters_out,
                      double* rel_out, int* cycles_out) {
     MSBG_API_BEGIN
@@ -1930,47 +2106,86 @@ int msbg_batch_solve(msbg_batch* B, double tol, int iters_per_cycle, int max_cyc
         if (B->graph) cudaGraphDestroy(B->graph);
         B->exec = nullptr;
         B->graph = nullptr;
+        const int ng = (int)B->groups.size();
+        if (!B->gtab.p) {
+            std::vector<GroupScal> gt(ng);
+            for (int g = 0; g < ng; ++g) gt[g] = GroupScal{B->groups[g]->scal.as<double>(), (int64_t)B->groups[g]->np};
+            B->gtab.reserve(sizeof(GroupScal) * ng);
+            B->ctrl.reserve(2 * sizeof(long long));
+            CUDA_CHECK(cudaMemcpyAsync(B->gtab.p, gt.data(), sizeof(GroupScal) * ng, cudaMemcpyHostToDevice, ctx->stream));
+            sync(ctx);
+        }
+        const GroupScal* gt = B->gtab.as<GroupScal>();
+        long long* ctrl = B->ctrl.as<long long>();
+        cudaGraph_t G = nullptr;
+        CUDA_CHECK(cudaGraphCreate(&G, 0));
         const uint64_t l0 = ctx->launches;
-        CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        bool capturing = false;
         try {
-            for (size_t g = 0; g < B->groups.size(); ++g)
+            cudaGraphConditionalHandle h;
+            CUDA_CHECK(cudaGraphConditionalHandleCreate(&h, G, 0, 0));
+            // the test before the loop, captured into G
+            CUDA_CHECK(cudaStreamBeginCaptureToGraph(ctx->stream, G, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            capturing = true;
+            bk_loop_ctrl<<<1, 256, 0, ctx->stream>>>(h, gt, ng, ctrl, 0);
+            CUDA_CHECK(cudaGetLastError());
+            CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &G));
+            capturing = false;
+            size_t nn = 1;
+            cudaGraphNode_t test_node;
+            CUDA_CHECK(cudaGraphGetNodes(G, &test_node, &nn));
+            // the while node after it
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t loop_node;
+            CUDA_CHECK(cudaGraphAddNode(&loop_node, G, &test_node, 1, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            // its body: one cycle of every group, then the test
+            CUDA_CHECK(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            capturing = true;
+            for (int g = 0; g < ng; ++g)
                 batch_cycle(B->groups[g], B->x[g].as<double>(), B->b[g].as<float>(), iters_per_cycle, tol);
+            begin_launch(ctx);
+            bk_loop_ctrl<<<1, 256, 0, ctx->stream>>>(h, gt, ng, ctrl, 1);
+            after_launch(ctx, "bk_loop_ctrl");
+            CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &body));
+            capturing = false;
+            CUDA_CHECK(cudaGraphInstantiate(&B->exec, G, 0));
         } catch (...) {
-            cudaGraph_t tmp = nullptr;
-            cudaStreamEndCapture(ctx->stream, &tmp);
-            if (tmp) cudaGraphDestroy(tmp);
+            if (capturing) {
+                cudaGraph_t tmp = nullptr;
+                cudaStreamEndCapture(ctx->stream, &tmp);
+            }
+            cudaGraphDestroy(G);
             ctx->launches = l0;
             throw;
         }
-        CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &B->graph));
-        CUDA_CHECK(cudaGraphInstantiate(&B->exec, B->graph, 0));
+        B->graph = G;
         B->graph_k = iters_per_cycle;
         B->graph_tol = tol;
         B->graph_kernels = (int)(ctx->launches - l0);
         ctx->launches = l0;
     }
+    // one launch of the whole solve: the host reads the scalars once, after it
+    const long long ctrl_init[2] = {0, (long long)max_cycles};
+    CUDA_CHECK(cudaMemcpyAsync(B->ctrl.p, ctrl_init, sizeof(ctrl_init), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_CHECK(cudaGraphLaunch(B->exec, ctx->stream));
     std::vector<std::vector<double>> sc(B->groups.size());
-    auto read_scalars = [&]() {
-        bool any = false;
+    long long cyc[2] = {0, 0};
+    {
         SmallReads rd(ctx);
         for (size_t g = 0; g < B->groups.size(); ++g) {
             const msbg_poisson* P = B->groups[g];
             sc[g].resize((size_t)P->np * S_WIDTH);
             rd.add(sc[g].data(), P->scal.p, sc[g].size() * 8);
         }
+        rd.add(cyc, B->ctrl.p, sizeof(cyc));
         rd.wait();
-        for (size_t g = 0; g < B->groups.size(); ++g)
-            for (int i = 0; i < B->groups[g]->np; ++i) any |= sc[g][(size_t)i * S_WIDTH + S_ACTIVE] > 0.0;
-        return any;
-    };
-    bool any = read_scalars();
-    int cycles = 0;
-    while (any && cycles < max_cycles) {
-        CUDA_CHECK(cudaGraphLaunch(B->exec, ctx->stream));
-        ctx->launches += (uint64_t)B->graph_kernels;
-        ++cycles;
-        any = read_scalars();
     }
+    const int cycles = (int)cyc[0];
+    ctx->launches += 1 + (uint64_t)cycles * (uint64_t)B->graph_kernels;
     for (size_t p = 0; p < B->prob_group.size(); ++p) {
         const double* S = sc[B->prob_group[p]].data() + (size_t)B->prob_index[p] * S_WIDTH;
         if (iters_out) iters_out[p] = (int)S[S_ITER];

@@ -119,7 +119,7 @@ extern "C" {
 int msbg_regularize_refinement_map_device(msbg_ctx* ctx, uint8_t* d_levels, uint64_t nx, uint64_t ny, uint64_t nz,
                                           int n_levels) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(ctx && (d_levels || !(nx * ny * nz)), "null argument");
+    MSBG_REQUIRE(ctx && (d_levels || nx * ny * nz == 0), "null argument");
     MSBG_REQUIRE(n_levels >= 1 && n_levels <= 255, "n_levels must be 1..255");
     set_device(ctx);
     regularize(ctx, d_levels, (int64_t)nx, (int64_t)ny, (int64_t)nz, n_levels);
@@ -128,7 +128,7 @@ int msbg_regularize_refinement_map_device(msbg_ctx* ctx, uint8_t* d_levels, uint
 
 int msbg_regularize_refinement_map(msbg_ctx* ctx, uint8_t* levels, uint64_t nx, uint64_t ny, uint64_t nz, int n_levels) {
     MSBG_API_BEGIN
-    MSBG_REQUIRE(ctx && (levels || !(nx * ny * nz)), "null argument");
+    MSBG_REQUIRE(ctx && (levels || nx * ny * nz == 0), "null argument");
     MSBG_REQUIRE(n_levels >= 1 && n_levels <= 255, "n_levels must be 1..255");
     set_device(ctx);
     const int64_t n = (int64_t)(nx * ny * nz);

@@ -31,7 +31,7 @@ struct SurfArgs {
     int64_t sx, sy, sz, nx, ny;
     int lg, m, W;
     float r_scan, dmax, inv;
-    int density;               // 1: Density (u16) storage
+    int qmax;                  // stored integer scale: 65535 Density, 255 Density8, 0 f32
     uint32_t full;
 };
 
@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(256) sf_splat_kernel(SurfArgs a) {
                 const float d2 = dx * dx + dyz;
                 if (d2 <= a.dmax) {
                     const float t = d2 * a.inv;
-                    const uint32_t q = a.density ? ((uint32_t)(int32_t)roundf(t * 65535.0f) & 0xffffu) : __float_as_uint(t);
+                    const uint32_t q = a.qmax ? ((uint32_t)(int32_t)roundf(t * (float)a.qmax) & (uint32_t)a.qmax)
+                                              : __float_as_uint(t);
                     atomicMin(win + row + ix, q);
                 }
             }
@@ -150,35 +151,40 @@ __global__ void __launch_bounds__(256) sf_splat_kernel(SurfArgs a) {
     }
 }
 
-// The min field of the listed slots into the grid payload (u16 or f32).
+// The min field of the listed slots into the grid payload (u16, u8 or f32).
 __global__ void sf_writeback_kernel(const uint32_t* __restrict__ f, const int32_t* __restrict__ slots, size_t n_slots,
-                                    int N, int density, void* payload) {
+                                    int N, int qmax, void* payload) {
     const size_t total = n_slots * (size_t)N;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const size_t k = i / N, v = i % N;
         const size_t at = (size_t)slots[k] * N + v;
         const uint32_t x = f[at];
-        if (density) static_cast<uint16_t*>(payload)[at] = (uint16_t)x;
+        if (qmax == 65535) static_cast<uint16_t*>(payload)[at] = (uint16_t)x;
+        else if (qmax == 255) static_cast<uint8_t*>(payload)[at] = (uint8_t)x;
         else static_cast<float*>(payload)[at] = __uint_as_float(x);
     }
 }
 
 // finalize.rs:35-71 on the listed slots, in place: ratio = dequantised value,
 // touched = ratio < 0.999, f = 1 - clamp((sqrt(ratio r^2) - r_p + r_p) /
-// (2 r_p + nb), 0, 1), 0 when untouched; Density stores round(f * 65535).
-__global__ void sf_finalize_kernel(const int32_t* __restrict__ slots, size_t n_slots, int N, int density, void* payload,
-                                   float dmax, float r_particle, float denom) {
+// (2 r_p + nb), 0, 1), 0 when untouched; Density / Density8 read q * inv_q
+// (Quant::dequant_chunk) and store round(f * qmax) (Quant::quant_chunk,
+// channel.rs:303-447).
+__global__ void sf_finalize_kernel(const int32_t* __restrict__ slots, size_t n_slots, int N, int qmax, float inv_q,
+                                   void* payload, float dmax, float r_particle, float denom) {
     const size_t total = n_slots * (size_t)N;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const size_t at = (size_t)slots[i / N] * N + i % N;
-        const float ratio = density ? (float)static_cast<uint16_t*>(payload)[at] * (1.0f / 65535.0f)
-                                    : static_cast<float*>(payload)[at];
+        const float ratio = qmax == 65535 ? __fmul_rn((float)static_cast<uint16_t*>(payload)[at], inv_q)
+                            : qmax == 255 ? __fmul_rn((float)static_cast<uint8_t*>(payload)[at], inv_q)
+                                          : static_cast<float*>(payload)[at];
         const bool touched = ratio < 0.999f;
         const float dist = __fsqrt_rn(ratio * dmax) - r_particle;
         float t = __fdiv_rn(dist + r_particle, denom);
         t = fminf(fmaxf(t, 0.0f), 1.0f);
         const float f = touched ? 1.0f - t : 0.0f;
-        if (density) static_cast<uint16_t*>(payload)[at] = (uint16_t)(int32_t)roundf(f * 65535.0f);
+        if (qmax == 65535) static_cast<uint16_t*>(payload)[at] = (uint16_t)(int32_t)roundf(__fmul_rn(f, 65535.0f));
+        else if (qmax == 255) static_cast<uint8_t*>(payload)[at] = (uint8_t)(int32_t)roundf(__fmul_rn(f, 255.0f));
         else static_cast<float*>(payload)[at] = f;
     }
 }
@@ -240,8 +246,11 @@ static void check(int st) {
     if (st != MSBG_OK) MSBG_THROW(st, msbg_last_error());
 }
 
+static int surface_qmax(const msbg_grid* g) { return g->dtype == MSBG_U16 ? 65535 : g->dtype == MSBG_U8 ? 255 : 0; }
+
 static void surface_checks(msbg_grid* g, float r_particle, float nb_dist) {
-    MSBG_REQUIRE(g->dtype == MSBG_F32 || g->dtype == MSBG_U16, "surface grids hold f32 or Density (u16) values");
+    MSBG_REQUIRE(g->dtype == MSBG_F32 || g->dtype == MSBG_U16 || g->dtype == MSBG_U8,
+                 "surface grids hold f32, Density (u16) or Density8 (u8) values");
     MSBG_REQUIRE(g->sx % g->bsx == 0 && g->sy % g->bsx == 0 && g->sz % g->bsx == 0,
                  "the surface splat needs domain extents that are multiples of bsx");
     MSBG_REQUIRE(r_particle > 0.0f && nb_dist >= 0.0f, "r_particle must be > 0 and nb_dist >= 0");
@@ -316,7 +325,8 @@ static std::vector<uint64_t> surface_splat(msbg_grid* g, const float* d_pos, siz
     ScratchLayout L3 = L2;
     const size_t o_min = L3.add<uint32_t>(g->n_slots() * (size_t)N), o_sl = L3.add<int32_t>(active.size());
     base = scratch(ctx, L3);
-    const uint32_t full = g->dtype == MSBG_U16 ? 65535u : 0x3f800000u;  // Density(u16::MAX) or 1.0f
+    const int qmax = surface_qmax(g);
+    const uint32_t full = qmax ? (uint32_t)qmax : 0x3f800000u;  // Density(u16::MAX), Density8(u8::MAX) or 1.0f
     uint32_t* minfield = ScratchLayout::at<uint32_t>(base, o_min);
     int32_t* d_slots = ScratchLayout::at<int32_t>(base, o_sl);
     CUDA_CHECK(cudaMemcpyAsync(d_slots, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -336,7 +346,7 @@ static std::vector<uint64_t> surface_splat(msbg_grid* g, const float* d_pos, siz
     a.r_scan = r_scan;
     a.dmax = r_scan * r_scan;
     a.inv = 1.0f / a.dmax;
-    a.density = g->dtype == MSBG_U16;
+    a.qmax = qmax;
     a.full = full;
     const size_t smem = (size_t)W * W * W * 4;
     CUDA_CHECK(cudaFuncSetAttribute(sf_splat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -346,7 +356,7 @@ static std::vector<uint64_t> surface_splat(msbg_grid* g, const float* d_pos, siz
     if (!active.empty()) {
         begin_launch(ctx);
         sf_writeback_kernel<<<sf_grid(active.size() * N), 256, 0, ctx->stream>>>(minfield, d_slots, active.size(), N,
-                                                                               a.density, g->payload.p);
+                                                                               a.qmax, g->payload.p);
         after_launch(ctx, "sf_writeback_kernel");
     }
     sync(ctx);  // slots (host) and the scratch layout end here
@@ -371,8 +381,10 @@ static void surface_finalize(msbg_grid* g, const uint64_t* active, size_t n, flo
     const float r_scan = r_particle + nb_dist;
     const int N = g->bsx * g->bsx * g->bsx;
     begin_launch(ctx);
-    sf_finalize_kernel<<<sf_grid(n * N), 256, 0, ctx->stream>>>(d_slots, n, N, g->dtype == MSBG_U16, g->payload.p,
-                                                                r_scan * r_scan, r_particle, 2.0f * r_particle + nb_dist);
+    const int qmax = surface_qmax(g);
+    sf_finalize_kernel<<<sf_grid(n * N), 256, 0, ctx->stream>>>(d_slots, n, N, qmax, qmax ? 1.0f / (float)qmax : 0.0f,
+                                                                g->payload.p, r_scan * r_scan, r_particle,
+                                                                2.0f * r_particle + nb_dist);
     after_launch(ctx, "sf_finalize_kernel");
     sync(ctx);
 }

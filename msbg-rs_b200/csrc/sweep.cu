@@ -92,6 +92,13 @@ struct SweepArgs {
     int32_t sx, sy, sz;
     float empty, full, dt;
     int clamp01;
+    // Density8 stores: lane seeds of the generator, the stream position of
+    // this launch's plan index 0, log2 of the lane count and the generator
+    // step over one z-plane of a block (16807^(bsx^2 / lanes))
+    uint32_t sr_seed[16];
+    uint64_t sr_base;
+    uint32_t sr_zstep;
+    int sr_lg;
 };
 
 template <int BSX> struct Lg { static constexpr int v = BSX == 4 ? 2 : BSX == 8 ? 3 : BSX == 16 ? 4 : 5; };
@@ -106,6 +113,20 @@ template <> struct Quad<ElemU16> {
         const uint2 u = *reinterpret_cast<const uint2*>(p);
         return make_float4(ElemU16::load((uint16_t)(u.x & 0xffff)), ElemU16::load((uint16_t)(u.x >> 16)),
                            ElemU16::load((uint16_t)(u.y & 0xffff)), ElemU16::load((uint16_t)(u.y >> 16)));
+    }
+};
+template <> struct Quad<ElemU8> {
+    __device__ static float4 load(const uint8_t* p) {
+        const uint32_t u = *reinterpret_cast<const uint32_t*>(p);
+        return make_float4(ElemU8::load((uint8_t)(u & 0xff)), ElemU8::load((uint8_t)((u >> 8) & 0xff)),
+                           ElemU8::load((uint8_t)((u >> 16) & 0xff)), ElemU8::load((uint8_t)(u >> 24)));
+    }
+};
+template <> struct Quad<ElemF16> {
+    __device__ static float4 load(const uint16_t* p) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        return make_float4(ElemF16::load((uint16_t)(u.x & 0xffff)), ElemF16::load((uint16_t)(u.x >> 16)),
+                           ElemF16::load((uint16_t)(u.y & 0xffff)), ElemF16::load((uint16_t)(u.y >> 16)));
     }
 };
 template <> struct Quad<ElemBF16> {
@@ -137,7 +158,7 @@ template <int ST> __device__ __forceinline__ bool xhalo_needed(int dx, int dy, i
 // the staged values from shared memory, writes the result in place (and the
 // block's new x-planes to the side buffer).
 template <class E, int BSX, int ST>
-__device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+__device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* __restrict__ h, int slot, int pi, int tid) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
     constexpr int HSX = BSX + 2 * HALO;
     constexpr int RS = Stage<BSX>::RS;
@@ -155,6 +176,15 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
         const int i0 = (HALO * HSX + (y + HALO)) * RS + X0 + x + HALO;  // z = 0
         const float dt = a.dt;
         const int clamp01 = a.clamp01;
+        // generator state of this thread's element at z = 0: the chunk of
+        // element x + y*BSX + z*BSX^2 is that index >> sr_lg, its lane x's
+        // low bits; each z step advances the chunk by BSX^2 >> sr_lg
+        uint32_t st = 0, zs = 0;
+        if constexpr (std::is_same<E, ElemU8>::value) {
+            const uint64_t q0 = (uint64_t)((x + y * BSX) >> a.sr_lg);
+            st = a.sr_seed[x & ((1 << a.sr_lg) - 1)] * sr_pow(a.sr_base + (uint64_t)pi * (uint64_t)(N >> a.sr_lg) + q0 + 1);
+            zs = a.sr_zstep;
+        }
         if (ST == MSBG_LAPLACIAN) {
             // taps along z slide through registers: 5 shared loads per output
             float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
@@ -171,7 +201,8 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
                 const float fx = (rx - lx) * 0.5f, fy = (dyd - dyu) * 0.5f, fz = (zf - zb) * 0.5f;
                 const float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
                 const float nv = fmaf(dt * lap, g, c);
-                const typename E::T sv = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                const typename E::T sv = StoreBack<E>::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv, st);
+                st *= zs;
                 out[z * BSX * BSX] = sv;
                 if (xo) xo[z * BSX] = E::load(sv);
                 zb = c;
@@ -203,7 +234,8 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
                 const float hc = grad > 1e-7f ? hnum / grad : 0.0f;
                 const float d = clampf(dt * hc, -0.1f, 0.1f);
                 const float nv = f0 + d;
-                const typename E::T sv = E::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv);
+                const typename E::T sv = StoreBack<E>::store(clamp01 ? clampf(nv, 0.0f, 1.0f) : nv, st);
+                st *= zs;
                 out[z * BSX * BSX] = sv;
                 if (xo) xo[z * BSX] = E::load(sv);
                 pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
@@ -217,7 +249,8 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
 #pragma unroll 4
             for (int z = 0; z < BSX; ++z) {
                 const int i = i0 + z * PL;
-                const typename E::T sv = E::store(stencil_bilaplacian(h, i, RS, PL, dt, clamp01));
+                const typename E::T sv = StoreBack<E>::store(stencil_bilaplacian(h, i, RS, PL, dt, clamp01), st);
+                st *= zs;
                 out[z * BSX * BSX] = sv;
                 if (xo) xo[z * BSX] = E::load(sv);
             }
@@ -464,7 +497,7 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
             stage_general<E, BSX, ST>(a, h, nb, pi, &ok[0][0], &dd[0][0], &ll[0][0]);
         }
         __syncthreads();
-        sweep_compute<E, BSX, ST>(a, h, nb[13], tid);
+        sweep_compute<E, BSX, ST>(a, h, nb[13], pi, tid);
     }
 }
 
@@ -630,7 +663,7 @@ sweep_pipe_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
         if ((flg[b] >> (HALO - 1)) & 1) cp_async_wait<1>();  // this block's copies have landed
         else stage_general<ElemF32, BSX, ST>(a, hb + b * BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
         __syncthreads();
-        sweep_compute<ElemF32, BSX, ST>(a, hb + b * BUF, nbs[b][13], tid);
+        sweep_compute<ElemF32, BSX, ST>(a, hb + b * BUF, nbs[b][13], 0, tid);
     }
     cp_async_wait<0>();
 }
@@ -1251,10 +1284,14 @@ static SweepPlan* get_plan(msbg_grid* g, msbg_grid* coarse, const uint8_t* level
 }
 
 static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const uint64_t* active, size_t n, int stencil,
-                  float dt, int iterations, int clamp01) {
+                  float dt, int iterations, int clamp01, uint32_t seed = 0xdeadbeefu, int lanes = 16,
+                  uint64_t* stream_pos = nullptr) {
     MSBG_REQUIRE(stencil >= 0 && stencil <= 2, "bad stencil");
     MSBG_REQUIRE(iterations >= 0, "negative iteration count");
     MSBG_REQUIRE(g->bsx >= 4, "sweeps need bsx >= 4");
+    if (g->dtype == MSBG_U8)
+        MSBG_REQUIRE((lanes == 4 || lanes == 8 || lanes == 16) && lanes <= g->bsx,
+                     "Density8 sweeps need 4, 8 or 16 generator lanes, at most the block size");
     if (coarse) {
         MSBG_REQUIRE(g->dtype == MSBG_F32 && coarse->dtype == MSBG_F32, "multiresolution sweep needs f32 levels");
         MSBG_REQUIRE(coarse->bsx * 2 == g->bsx && coarse->nx == g->nx && coarse->ny == g->ny && coarse->nz == g->nz,
@@ -1274,6 +1311,13 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
     a.full = coarse ? 0.0f : quantize_roundtrip(g->dtype, g->full_value);
     a.dt = dt;
     a.clamp01 = clamp01 ? 1 : 0;
+    int lg = 0;
+    while ((1 << lg) < lanes) ++lg;
+    for (int l = 0; l < 16; ++l) a.sr_seed[l] = sr_lane_seed(seed, (uint32_t)l);
+    a.sr_lg = lg;
+    a.sr_zstep = sr_pow((uint64_t)(g->bsx * g->bsx) >> lg);
+    const uint64_t chunks_per_sweep = (uint64_t)plan->n * ((uint64_t)g->block_elems >> lg);
+    const uint64_t pos0 = stream_pos ? *stream_pos : 0;
     // x-plane side buffer: sized for every slot, refreshed from the payload at
     // the start of each call (the payload may have changed in between)
     {
@@ -1285,18 +1329,25 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
         a.xface = plan->xface.as<float>();
         if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
         else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+        else if (g->dtype == MSBG_U8) xface_init<ElemU8>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+        else if (g->dtype == MSBG_F16) xface_init<ElemF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
         else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
     }
     const int32_t* order = plan->order.as<int32_t>();
-    for (int it = 0; it < iterations; ++it)
+    for (int it = 0; it < iterations; ++it) {
+        a.sr_base = pos0 + (uint64_t)it * chunks_per_sweep;
         for (int c = 0; c < 8; ++c) {
             int cnt = plan->color_off[c + 1] - plan->color_off[c];
             if (!cnt) continue;
             const int32_t* o = order + plan->color_off[c];
             if (g->dtype == MSBG_F32) launch_phase_bsx<ElemF32>(g->ctx, g->bsx, stencil, a, o, cnt);
             else if (g->dtype == MSBG_U16) launch_phase_bsx<ElemU16>(g->ctx, g->bsx, stencil, a, o, cnt);
+            else if (g->dtype == MSBG_U8) launch_phase_bsx<ElemU8>(g->ctx, g->bsx, stencil, a, o, cnt);
+            else if (g->dtype == MSBG_F16) launch_phase_bsx<ElemF16>(g->ctx, g->bsx, stencil, a, o, cnt);
             else launch_phase_bsx<ElemBF16>(g->ctx, g->bsx, stencil, a, o, cnt);
         }
+    }
+    if (stream_pos && g->dtype == MSBG_U8) *stream_pos = pos0 + (uint64_t)iterations * chunks_per_sweep;
 }
 
 }  // namespace msbg
@@ -1308,7 +1359,15 @@ extern "C" {
 int msbg_sweep(msbg_grid* g, const uint64_t* active, size_t n, int stencil, float dt, int iterations, int clamp01) {
     MSBG_API_BEGIN
     MSBG_REQUIRE(g && (active || !n), "null argument");
-    sweep(g, nullptr, nullptr, active, n, stencil, dt, iterations, clamp01);
+    sweep(g, nullptr, nullptr, active, n, stencil, dt, iterations, clamp01, 0xdeadbeefu, std::min(16, g->bsx));
+    MSBG_API_END
+}
+
+int msbg_sweep_stochastic(msbg_grid* g, const uint64_t* active, size_t n, int stencil, float dt, int iterations,
+                          int clamp01, uint32_t seed, int lanes, uint64_t* stream_pos) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(g && (active || !n) && stream_pos, "null argument");
+    sweep(g, nullptr, nullptr, active, n, stencil, dt, iterations, clamp01, seed, lanes, stream_pos);
     MSBG_API_END
 }
 

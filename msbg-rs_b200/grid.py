@@ -16,7 +16,8 @@ import numpy as np
 from . import _lib
 from ._lib import call, ptr
 
-DTYPES = {"f32": (_lib.MSBG_F32, np.float32), "u16": (_lib.MSBG_U16, np.uint16), "bf16": (_lib.MSBG_BF16, np.uint16)}
+DTYPES = {"f32": (_lib.MSBG_F32, np.float32), "u16": (_lib.MSBG_U16, np.uint16), "bf16": (_lib.MSBG_BF16, np.uint16),
+          "u8": (_lib.MSBG_U8, np.uint8), "f16": (_lib.MSBG_F16, np.uint16)}
 
 
 def _log2(v: int) -> int:
@@ -96,6 +97,11 @@ class HostGrid:
         if self.dtype == "u16":
             r = np.floor(np.abs(np.float32(v) * np.float32(65535.0)) + 0.5) * np.sign(v)
             return np.uint16(min(max(r, 0.0), 65535.0))
+        if self.dtype == "u8":  # Density8 from_unit (channel.rs:378-382)
+            r = np.floor(np.abs(np.float32(v) * np.float32(255.0)) + 0.5) * np.sign(v)
+            return np.uint8(min(max(r, 0.0), 255.0))
+        if self.dtype == "f16":  # binary16 bits, round to nearest even
+            return np.array([v], np.float32).astype(np.float16).view(np.uint16)[0]
         b = np.array([v], np.float32).view(np.uint32)[0]
         b = (int(b) + 0x7FFF + ((int(b) >> 16) & 1)) >> 16
         return np.uint16(b)

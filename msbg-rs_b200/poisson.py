@@ -37,6 +37,19 @@ class Poisson:
     def set_smoother(self, nu1=2, nu2=2, omega=2.0 / 3.0):
         call("msbg_poisson_set_smoother", self.handle, int(nu1), int(nu2), float(omega))
 
+    def autotune(self) -> np.ndarray:
+        """Times the launch choices of every level but the coarsest and keeps
+        the fastest; per level (Jacobi shape, residual shape, tile or 0)."""
+        cfg = np.zeros(3 * 64, np.int32)
+        n = C.c_size_t()
+        call("msbg_poisson_autotune", self.handle, ptr(cfg), cfg.size, C.byref(n))
+        return cfg[: 3 * n.value].reshape(-1, 3)
+
+    def set_tuning(self, cfg) -> None:
+        """Per level (Jacobi shape, residual shape, tile or 0), as autotune returns it."""
+        c = np.ascontiguousarray(cfg, np.int32).reshape(-1, 3)
+        call("msbg_poisson_set_tuning", self.handle, ptr(c), len(c))
+
     def matvec(self, d_x, d_y):
         call("msbg_poisson_matvec_device", self.handle, ptr(d_x), ptr(d_y))
 

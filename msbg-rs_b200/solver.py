@@ -9,6 +9,7 @@ enqueues the sweep on the grid's context stream and returns.
 """
 from __future__ import annotations
 
+import ctypes as C
 import enum
 from dataclasses import dataclass
 
@@ -48,15 +49,25 @@ class PdeParams:
 class Sweeper:
     """Sweeper::new(grid, num_threads, fence) (solver.rs:154-160)."""
 
-    def __init__(self, grid: SparseGrid, num_threads: int = 0, fence: Fence = Fence.Sfence):
+    def __init__(self, grid: SparseGrid, num_threads: int = 0, fence: Fence = Fence.Sfence,
+                 seed: int = 0xDEADBEEF, lanes: int = 16):
+        """`seed` and `lanes` set the Density8 store's generator: the slot of
+        the reference's first sweeping thread is SimdRng::<LANES>::seed(
+        0xdeadbeef) (solver.rs:109-119), LANES the build's SIMD width."""
         self.grid = grid
         self.fence = fence
+        self.seed = int(seed) & 0xFFFFFFFF
+        self.lanes = int(lanes)
+        self.stream_pos = 0  # generator draws taken so far (Density8 only)
 
     def sweep(self, active, stencil: Stencil, params: PdeParams) -> None:
-        """Sweeper::sweep (solver.rs:166-185)."""
+        """Sweeper::sweep (solver.rs:166-185); a Density8 grid continues this
+        sweeper's generator stream across calls."""
         a = np.ascontiguousarray(active, np.uint64)
-        call("msbg_sweep", self.grid.handle, ptr(a), len(a), int(stencil), float(params.dt), int(params.iterations),
-             int(bool(params.do_constr_zero_one)))
+        pos = C.c_uint64(self.stream_pos)
+        call("msbg_sweep_stochastic", self.grid.handle, ptr(a), len(a), int(stencil), float(params.dt),
+             int(params.iterations), int(bool(params.do_constr_zero_one)), self.seed, self.lanes, C.byref(pos))
+        self.stream_pos = pos.value
 
     def sweep_multires(self, coarse: SparseGrid, levels: np.ndarray, active, stencil: Stencil, params: PdeParams) -> None:
         """Sweep whose halos sample coarser neighbours from `coarse`

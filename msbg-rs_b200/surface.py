@@ -2,7 +2,7 @@
 SurfaceConfig, the instanced placement `place` (particles/sort.rs:31-144),
 the min-splat of normalised squared distances (particles/splat.rs:92-319),
 `finalize` (particles/finalize.rs:35-71) and reconstruct_and_smooth.  The
-density grid is a SparseGrid of Density (u16) or f32 values with empty value
+density grid is a SparseGrid of Density (u16), Density8 (u8) or f32 values with empty value
 0 and full value 1 (the crate's D::empty() and D::full())."""
 from __future__ import annotations
 

@@ -326,7 +326,7 @@ inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
 }
 
 // Storage element conversions (stencil.rs:142-192 StoreBack, sample.rs:45-70 Dequant).
-enum DType { DT_F32 = 0, DT_U16 = 1, DT_BF16 = 2 };
+enum DType { DT_F32 = 0, DT_U16 = 1, DT_BF16 = 2, DT_U8 = 3, DT_F16 = 4 };
 inline float bf16_to_f32(uint16_t b) { uint32_t u = (uint32_t)b << 16; float f; memcpy(&f, &u, 4); return f; }
 inline uint16_t f32_to_bf16_rn(float f) {
     uint32_t u; memcpy(&u, &f, 4);
@@ -343,6 +343,99 @@ inline uint16_t f32_to_density(float v) {
     return (uint16_t)r;
 }
 inline float density_to_f32(uint16_t v) { return (float)v * (1.0f / 65535.0f); }
+
+// Density8 (channel.rs:155-190): read linearly, q / 255 (sample.rs:64-70);
+// a plain write rounds half away from zero and saturates (from_unit,
+// channel.rs:378-382).
+inline float density8_to_f32(uint8_t q) { return (float)q * (1.0f / 255.0f); }
+inline uint8_t f32_to_density8(float v) {
+    float r = roundf(v * 255.0f);
+    if (!(r > 0.0f)) r = 0.0f;
+    if (r > 255.0f) r = 255.0f;
+    return (uint8_t)r;
+}
+// The smoother's Density8 write-back (stencil.rs:176-192): sqrt compression,
+// then floor + 1 when the draw u lies below the fraction.  The float -> i32
+// conversion is the x86 one (NaN or out of range gives INT_MIN) and the
+// i32 -> u8 cast wraps.
+inline uint8_t density8_store_sr(float v, float u) {
+    float vf = sqrtf(v) * 255.0f;
+    float fl = floorf(vf);
+    float frac = vf - fl;
+    float r = u < frac ? fl + 1.0f : fl;
+    int32_t i = (r >= -2147483648.0f && r < 2147483648.0f) ? (int32_t)r : INT32_MIN;
+    return (uint8_t)(i & 0xff);
+}
+
+// SimdRng<W> (stencil.rs:103-132): W lanes seeded by a murmur finaliser of
+// seed ^ lane * 0x9e3779b9 (zero replaced by 0xdeadbeef); each draw
+// multiplies every lane by 16807 and maps state >> 9 into [1, 2), minus 1.
+struct LaneRng {
+    uint32_t s[16];
+    int w;
+    LaneRng(uint32_t seed, int lanes) : w(lanes) {
+        for (int l = 0; l < 16; ++l) {
+            uint32_t h = seed ^ ((uint32_t)l * 0x9e3779b9u);
+            h ^= h >> 16;
+            h *= 0x85ebca6bu;
+            h ^= h >> 13;
+            h *= 0xc2b2ae35u;
+            h ^= h >> 16;
+            s[l] = h ? h : 0xdeadbeefu;
+        }
+    }
+    void next(float* u) {
+        for (int l = 0; l < w; ++l) {
+            s[l] *= 16807u;
+            uint32_t bits = (s[l] >> 9) | 0x3f800000u;
+            float f;
+            memcpy(&f, &bits, 4);
+            u[l] = f - 1.0f;
+        }
+    }
+};
+
+// IEEE 754 binary16, written from the format: 1 sign, 5 exponent (bias 15),
+// 10 fraction bits; conversions from f32 round to nearest, ties to even.
+inline uint16_t f32_to_f16_rn(float f) {
+    uint32_t x;
+    memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u, ax = x & 0x7fffffffu;
+    if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7e00u);   // NaN
+    if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // >= 65520 rounds to infinity
+    if (ax >= 0x38800000u) {                                    // normal: >= 2^-14
+        const uint32_t e = (ax >> 23) - 127 + 15, m = ax & 0x7fffffu;
+        uint32_t h = (e << 10) | (m >> 13);
+        const uint32_t rem = m & 0x1fffu;
+        if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;  // a carry moves into the exponent
+        return (uint16_t)(sign | h);
+    }
+    const uint32_t e = ax >> 23;  // subnormal result, unit 2^-24
+    if (e == 0) return (uint16_t)sign;
+    const uint32_t m = (ax & 0x7fffffu) | 0x800000u;  // value m * 2^(e - 150)
+    const uint32_t shift = 126 - e;                  // m * 2^(e - 126) units; shift >= 14
+    if (shift >= 32) return (uint16_t)sign;
+    uint32_t h = m >> shift;
+    const uint32_t rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+    if (rem > half || (rem == half && (h & 1u))) ++h;
+    return (uint16_t)(sign | h);
+}
+inline float f16_to_f32(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t bits;
+    if (e == 0) {
+        const float v = ldexpf((float)m, -24);
+        memcpy(&bits, &v, 4);
+        bits |= sign;
+    } else if (e == 31) {
+        bits = sign | 0x7f800000u | (m << 13);
+    } else {
+        bits = sign | ((e - 15 + 127) << 23) | (m << 13);
+    }
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
 
 }  // namespace
 
@@ -395,9 +488,10 @@ uint64_t or_morton3(uint64_t x, uint64_t y, uint64_t z) { return morton3(x, y, z
 // elements and the halo dequantizes them (Dequant::copy_row), the store
 // re-quantizes (StoreBack::store_chunk).  `threads` > 1 runs each colour's
 // blocks in parallel (the timed CPU baseline).
-static void sweep_impl(const OracleGrid* og, void* raw, int elem, const int64_t* active,
-                       int64_t n_active, int stencil, float dt, int iterations, int clamp01,
-                       int threads, const OracleGrid* coarse, const uint8_t* levels) {
+static uint64_t sweep_impl(const OracleGrid* og, void* raw, int elem, const int64_t* active,
+                           int64_t n_active, int stencil, float dt, int iterations, int clamp01,
+                           int threads, const OracleGrid* coarse, const uint8_t* levels,
+                           uint32_t seed = 0xdeadbeefu, int lanes = 16, uint64_t stream_pos = 0) {
     Grid g = to_grid(og);
     const int bsx = g.bsx;
     const size_t N = (size_t)bsx * bsx * bsx;
@@ -413,14 +507,28 @@ static void sweep_impl(const OracleGrid* og, void* raw, int elem, const int64_t*
     if (elem != DT_F32) {
         shadow.resize((size_t)n_slots * N);
         for (size_t i = 0; i < shadow.size(); ++i)
-            shadow[i] = elem == DT_U16 ? density_to_f32(((uint16_t*)raw)[i]) : bf16_to_f32(((uint16_t*)raw)[i]);
+            shadow[i] = elem == DT_U16   ? density_to_f32(((uint16_t*)raw)[i])
+                        : elem == DT_U8  ? density8_to_f32(((uint8_t*)raw)[i])
+                        : elem == DT_F16 ? f16_to_f32(((uint16_t*)raw)[i])
+                                         : bf16_to_f32(((uint16_t*)raw)[i]);
         g.data = shadow.data();
     } else {
         g.data = (float*)raw;
     }
     if (elem == DT_U16) g.empty_value = density_to_f32(f32_to_density(g.empty_value)), g.full_value = density_to_f32(f32_to_density(g.full_value));
     if (elem == DT_BF16) g.empty_value = bf16_to_f32(f32_to_bf16_rn(g.empty_value)), g.full_value = bf16_to_f32(f32_to_bf16_rn(g.full_value));
+    if (elem == DT_U8) g.empty_value = density8_to_f32(f32_to_density8(g.empty_value)), g.full_value = density8_to_f32(f32_to_density8(g.full_value));
+    if (elem == DT_F16) g.empty_value = f16_to_f32(f32_to_f16_rn(g.empty_value)), g.full_value = f16_to_f32(f32_to_f16_rn(g.full_value));
     Dummies dm(g);
+    // Density8: the generator of the one sweeping thread (solver.rs:90-119),
+    // advanced to the stream position; its draws follow the serial order of
+    // stores, so the blocks run one after another
+    LaneRng rng(seed, lanes);
+    if (elem == DT_U8) {
+        float u[16];
+        for (uint64_t k = 0; k < stream_pos; ++k) rng.next(u);
+        threads = 1;
+    }
     // A block listed twice would be updated twice by concurrent threads in
     // the reference (a race); every listed block is swept once per phase.
     std::vector<std::vector<int64_t>> buckets(8);
@@ -459,9 +567,24 @@ static void sweep_impl(const OracleGrid* og, void* raw, int elem, const int64_t*
                 else if (stencil == 1) kernel_meancurv(halo.data(), bsx, dt, clamp01 != 0, out.data());
                 else kernel_bilaplacian(halo.data(), bsx, dt, clamp01 != 0, out.data());
                 float* dstf = g.data + (size_t)s * N;
+                float u[16];
                 for (size_t i = 0; i < N; ++i) {
+                    if (elem == DT_U8) {
+                        if (i % (size_t)lanes == 0) {  // one draw per chunk of `lanes`
+                            rng.next(u);
+                            ++stream_pos;
+                        }
+                        uint8_t q = density8_store_sr(out[i], u[i % (size_t)lanes]);
+                        ((uint8_t*)raw)[(size_t)s * N + i] = q;
+                        dstf[i] = density8_to_f32(q);
+                        continue;
+                    }
                     if (elem == DT_F32) {
                         dstf[i] = out[i];
+                    } else if (elem == DT_F16) {
+                        uint16_t q = f32_to_f16_rn(out[i]);
+                        ((uint16_t*)raw)[(size_t)s * N + i] = q;
+                        dstf[i] = f16_to_f32(q);
                     } else if (elem == DT_U16) {
                         uint16_t q = f32_to_density(out[i]);
                         ((uint16_t*)raw)[(size_t)s * N + i] = q;
@@ -474,11 +597,37 @@ static void sweep_impl(const OracleGrid* og, void* raw, int elem, const int64_t*
                 }
             }
         }
+    return stream_pos;
 }
 
 void or_sweep(const OracleGrid* og, void* raw, int elem, const int64_t* active, int64_t n_active,
               int stencil, float dt, int iterations, int clamp01, int threads) {
     sweep_impl(og, raw, elem, active, n_active, stencil, dt, iterations, clamp01, threads, nullptr, nullptr);
+}
+
+// Sweeper::sweep on Density8 storage with an explicit generator (seed, SIMD
+// lane count, draws already taken); returns the draws taken afterwards.
+uint64_t or_sweep_stochastic(const OracleGrid* og, uint8_t* raw, const int64_t* active, int64_t n_active,
+                             int stencil, float dt, int iterations, int clamp01, uint32_t seed, int lanes,
+                             uint64_t stream_pos) {
+    return sweep_impl(og, raw, DT_U8, active, n_active, stencil, dt, iterations, clamp01, 1, nullptr, nullptr,
+                      seed, lanes, stream_pos);
+}
+
+// Element conversions, exported for the tests: binary16 both ways, the
+// Density8 write-back and the lane generator's first draws.
+void or_f32_to_f16(const float* x, int64_t n, uint16_t* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = f32_to_f16_rn(x[i]);
+}
+void or_f16_to_f32(const uint16_t* x, int64_t n, float* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = f16_to_f32(x[i]);
+}
+void or_density8_store_sr(const float* v, const float* u, int64_t n, uint8_t* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = density8_store_sr(v[i], u[i]);
+}
+void or_lane_rng(uint32_t seed, int lanes, int64_t draws, float* out) {
+    LaneRng r(seed, lanes);
+    for (int64_t k = 0; k < draws; ++k) r.next(out + k * lanes);
 }
 
 void or_sweep_multires(const OracleGrid* fine, float* data, const OracleGrid* coarse,
@@ -1569,14 +1718,15 @@ int64_t or_surface_active(const float* pos, int64_t n, int64_t sx, int64_t sy, i
 // floor(p + r - 1/2)] (r = r_scan, clipped to its block's staging window),
 // dist_sq = dx dx + (dz dz + dy dy) with d = voxel - (p - 1/2); where dist_sq
 // <= r^2 the voxel takes min(old, q), q = dist_sq / r^2 (f32 storage) or
-// round(dist_sq / r^2 * 65535) (Density, u16; channel.rs:392-417).  Voxels
+// round(dist_sq / r^2 * qmax) (Density: qmax 65535, channel.rs:392-417;
+// Density8: qmax 255, channel.rs:425-447).  Voxels
 // outside the domain or in blocks outside `active` are skipped (the
 // reference's commit skips them).  The reference stages per block and
 // commits by colour; min is order-independent, so a direct scatter-min gives
-// the same grid.  out is [n_active][bsx^3] f32 (values of u16 as floats
-// when density != 0).
+// the same grid.  out is [n_active][bsx^3] f32 (the stored integers as
+// floats when qmax != 0; qmax 0 is f32 storage).
 void or_density_splat(const float* pos, int64_t n, int64_t sx, int64_t sy, int64_t sz, int bsx, float r_particle,
-                      float nb_dist, int density, const int64_t* active, int64_t n_active, float* out) {
+                      float nb_dist, int qmax, const int64_t* active, int64_t n_active, float* out) {
     const int64_t nx = (sx + bsx - 1) / bsx, ny = (sy + bsx - 1) / bsx, nz = (sz + bsx - 1) / bsx;
     const int lg = ilog2(bsx), msk = bsx - 1;
     const int64_t N = (int64_t)bsx * bsx * bsx;
@@ -1585,7 +1735,7 @@ void or_density_splat(const float* pos, int64_t n, int64_t sx, int64_t sy, int64
     const float r_scan = r_particle + nb_dist;
     const float dmax = r_scan * r_scan, inv = 1.0f / dmax;
     const int m = (int)ceilf(r_scan);
-    std::vector<uint32_t> q((size_t)(n_active * N), density ? 65535u : 0x3f800000u);  // full: u16 max or 1.0f
+    std::vector<uint32_t> q((size_t)(n_active * N), qmax ? (uint32_t)qmax : 0x3f800000u);  // full: MAX or 1.0f
     for (int64_t i = 0; i < n; ++i) {
         const float* p = pos + 3 * i;
         int32_t b0[3];
@@ -1609,7 +1759,7 @@ void or_density_splat(const float* pos, int64_t n, int64_t sx, int64_t sy, int64
                     if (s < 0) continue;
                     const float t = d2 * inv;
                     uint32_t v;
-                    if (density) v = (uint32_t)(int32_t)roundf(t * 65535.0f) & 0xffffu;
+                    if (qmax) v = (uint32_t)(int32_t)roundf(t * (float)qmax) & (uint32_t)qmax;
                     else memcpy(&v, &t, 4);
                     uint32_t& o = q[(size_t)(s * N + ((ix & msk) | ((iy & msk) << lg) | ((iz & msk) << (2 * lg))))];
                     if (v < o) o = v;
@@ -1618,28 +1768,28 @@ void or_density_splat(const float* pos, int64_t n, int64_t sx, int64_t sy, int64
         }
     }
     for (size_t k = 0; k < q.size(); ++k) {
-        if (density) out[k] = (float)q[k];
+        if (qmax) out[k] = (float)q[k];
         else memcpy(&out[k], &q[k], 4);
     }
 }
 
-// particles/finalize.rs:35-71 in place on [n][bsx^3] values (u16 values as
-// floats when density != 0): ratio (dequantised), touched = ratio < 0.999,
-// f = 1 - clamp((sqrt(ratio r^2) - r_p + r_p) / (2 r_p + nb), 0, 1), 0 when
-// untouched; stored back (Density: round(f * 65535)).
-void or_density_finalize(float* vals, int64_t n, int density, float r_particle, float nb_dist) {
+// particles/finalize.rs:35-71 in place on [n][bsx^3] values (the stored
+// integers as floats when qmax != 0): ratio (dequantised, q / qmax),
+// touched = ratio < 0.999, f = 1 - clamp((sqrt(ratio r^2) - r_p + r_p) /
+// (2 r_p + nb), 0, 1), 0 when untouched; stored back (round(f * qmax)).
+void or_density_finalize(float* vals, int64_t n, int qmax, float r_particle, float nb_dist) {
     const float r_scan = r_particle + nb_dist, dmax = r_scan * r_scan;
     const float denom = 2.0f * r_particle + nb_dist;
     for (int64_t k = 0; k < n; ++k) {
-        const float ratio = density ? density_to_f32((uint16_t)vals[k]) : vals[k];
+        const float ratio = qmax ? (float)(uint32_t)vals[k] * (1.0f / (float)qmax) : vals[k];
         const bool touched = ratio < 0.999f;
         const float dist = sqrtf(ratio * dmax) - r_particle;
         float t = (dist + r_particle) / denom;
         t = std::min(std::max(t, 0.0f), 1.0f);
         const float f = touched ? 1.0f - t : 0.0f;
-        if (density) {
-            const float r = roundf(f * 65535.0f);
-            vals[k] = (float)(uint16_t)(int32_t)r;
+        if (qmax) {
+            const float r = roundf(f * (float)qmax);
+            vals[k] = (float)((uint32_t)(int32_t)r & (uint32_t)qmax);
         } else {
             vals[k] = f;
         }

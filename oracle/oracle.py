@@ -88,6 +88,13 @@ def lib() -> C.CDLL:
         _lib.or_poisson_levels.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_void_p]
         _lib.or_poisson_levels.restype = C.c_int
         _lib.or_num_threads.restype = C.c_int
+        _lib.or_sweep_stochastic.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_float, C.c_int,
+                                             C.c_int, C.c_uint32, C.c_int, C.c_uint64]
+        _lib.or_sweep_stochastic.restype = C.c_uint64
+        _lib.or_f32_to_f16.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        _lib.or_f16_to_f32.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        _lib.or_density8_store_sr.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        _lib.or_lane_rng.argtypes = [C.c_uint32, C.c_int, C.c_int64, C.c_void_p]
     return _lib
 
 
@@ -142,7 +149,7 @@ def kernel(stencil: int, halo: np.ndarray, bsx: int, dt: float, clamp01: bool) -
     return out
 
 
-_ELEM = {"f32": 0, "u16": 1, "bf16": 2}
+_ELEM = {"f32": 0, "u16": 1, "bf16": 2, "u8": 3, "f16": 4}
 
 
 def sweep(host, active, stencil: int, dt: float, iterations: int, clamp01: bool, threads: int = 1) -> None:
@@ -152,6 +159,52 @@ def sweep(host, active, stencil: int, dt: float, iterations: int, clamp01: bool,
     lib().or_sweep(v.ref(), _p(v.data), _ELEM[host.dtype], _p(a), len(a), int(stencil), float(dt), int(iterations),
                    int(bool(clamp01)), int(threads))
     v.write_back()
+
+
+def sweep_stochastic(host, active, stencil: int, dt: float, iterations: int, clamp01: bool, seed: int = 0xDEADBEEF,
+                     lanes: int = 16, stream_pos: int = 0) -> int:
+    """Sweeper::sweep on Density8 storage (solver.rs:166-217) with the one
+    sweeping thread's generator SimdRng::<lanes>::seed(seed) after
+    `stream_pos` draws (stencil.rs:103-132, 176-192); in place on host.
+    Returns the draws taken after the call."""
+    assert host.dtype == "u8"
+    v = GridView(host)
+    a = np.ascontiguousarray(active, np.int64)
+    pos = lib().or_sweep_stochastic(v.ref(), _p(v.data), _p(a), len(a), int(stencil), float(dt), int(iterations),
+                                    int(bool(clamp01)), int(seed) & 0xFFFFFFFF, int(lanes), int(stream_pos))
+    v.write_back()
+    return int(pos)
+
+
+def f32_to_f16(x) -> np.ndarray:
+    """IEEE binary16 bits of f32 values, round to nearest even."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty(x.shape, np.uint16)
+    lib().or_f32_to_f16(_p(x), x.size, _p(out))
+    return out
+
+
+def f16_to_f32(bits) -> np.ndarray:
+    b = np.ascontiguousarray(bits, np.uint16)
+    out = np.empty(b.shape, np.float32)
+    lib().or_f16_to_f32(_p(b), b.size, _p(out))
+    return out
+
+
+def density8_store_sr(v, u) -> np.ndarray:
+    """Density8 StoreBack of values v against draws u (stencil.rs:176-192)."""
+    v = np.ascontiguousarray(v, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    out = np.empty(v.shape, np.uint8)
+    lib().or_density8_store_sr(_p(v), _p(u), v.size, _p(out))
+    return out
+
+
+def lane_rng(seed: int, lanes: int, draws: int) -> np.ndarray:
+    """The first `draws` outputs of SimdRng::<lanes>::seed(seed), [draws][lanes]."""
+    out = np.empty((draws, lanes), np.float32)
+    lib().or_lane_rng(int(seed) & 0xFFFFFFFF, int(lanes), int(draws), _p(out))
+    return out
 
 
 def sweep_multires(fine, coarse, levels, active, stencil, dt, iterations, clamp01, threads=1) -> None:
@@ -321,22 +374,37 @@ def surface_active(pos, sx, sy, sz, bsx, r_scan) -> np.ndarray:
     return out
 
 
+_QMAX = {"f32": (0, np.float32), "u16": (65535, np.uint16), "u8": (255, np.uint8)}
+
+
+def _quant(density):
+    """Storage of a surface grid: True/"u16" Density, "u8" Density8, False/"f32"."""
+    if density is True:
+        density = "u16"
+    elif density is False:
+        density = "f32"
+    return _QMAX[density]
+
+
 def density_splat(pos, sx, sy, sz, bsx, r_particle, nb_dist, density, active) -> np.ndarray:
     """particles/splat.rs:92-319 min-splat into the active blocks (filled with
-    the full value first): [n_active][bsx^3], u16 values (density) or f32."""
+    the full value first): [n_active][bsx^3] in the grid's storage type
+    (`density`: True or "u16" Density, "u8" Density8, False or "f32")."""
+    qmax, dt = _quant(density)
     p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
     a = np.ascontiguousarray(active, np.int64)
     out = np.zeros((len(a), bsx ** 3), np.float32)
-    lib().or_density_splat(_p(p), len(p), sx, sy, sz, bsx, float(r_particle), float(nb_dist), int(bool(density)), _p(a),
+    lib().or_density_splat(_p(p), len(p), sx, sy, sz, bsx, float(r_particle), float(nb_dist), qmax, _p(a),
                            len(a), _p(out))
-    return out.astype(np.uint16) if density else out
+    return out.astype(dt)
 
 
 def density_finalize(vals, density, r_particle, nb_dist) -> np.ndarray:
-    """particles/finalize.rs:35-71 on splatted values (u16 or f32)."""
+    """particles/finalize.rs:35-71 on splatted values (storage as in density_splat)."""
+    qmax, dt = _quant(density)
     v = np.ascontiguousarray(vals, np.float32).copy()
-    lib().or_density_finalize(_p(v), v.size, int(bool(density)), float(r_particle), float(nb_dist))
-    return v.astype(np.uint16) if density else v
+    lib().or_density_finalize(_p(v), v.size, qmax, float(r_particle), float(nb_dist))
+    return v.astype(dt)
 
 
 def mac_sample(vx, vy, vz, pos, bc) -> np.ndarray:

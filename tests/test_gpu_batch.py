@@ -1,5 +1,6 @@
-"""Batched Poisson solves (one CUDA graph launch per cycle, per-problem CG
-scalars on the device, autotuned launch shapes) against the FP64 oracle.
+"""Batched Poisson solves (the whole solve one CUDA graph launch with a
+device-side loop over cycles, per-problem CG scalars on the device,
+autotuned launch shapes) against the FP64 oracle.
 
 No reference exists (parity unpinned).  Checked per problem: the solve
 reaches relative residual 1e-8, re-measured in FP64 on the host with the
@@ -48,8 +49,11 @@ def test_tuning_is_reported(solved):
     for g in range(B.n_groups):
         cfg, cells = B.tuning(g)
         assert len(cfg) == len(cells) >= 2
-        assert np.all((cfg >= 0) & (cfg < 8))
+        assert np.all((cfg[:, :2] >= 0) & (cfg[:, :2] < 8))
+        assert np.all(np.isin(cfg[:, 2], [0, 2, 4, 8, 16]))
         assert np.all(np.diff(cells.astype(np.int64)) <= 0)
+    # a group of 16^3 blocks tunes the tile kernel's depth on its finest level
+    assert any(B.tuning(g)[0][0, 2] in (2, 4, 8, 16) for g in range(B.n_groups))
 
 
 def test_problems_are_independent(msbg, ctx, problems, solved):
@@ -72,6 +76,22 @@ def test_second_solve_reuses_graph(problems, solved):
         B.set_rhs(p, rng.uniform(-1, 1, b.size).astype(np.float32))
     its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=8, max_cycles=40)
     assert np.all(rel <= 1e-8) and cyc > 0
+
+
+def test_device_loop_stops_at_the_cycle_limit(msbg, ctx, problems):
+    """The loop's test runs on the device: with a limit of 0 no cycle runs,
+    with a limit of 1 exactly one runs and the problems stay unconverged;
+    the cycles it reports are the ones it ran (a resumed solve finishes)."""
+    B = msbg.Batch(ctx, [(d, bs, a) for d, bs, a, _ in problems], tune=False)
+    for p, (_, _, _, b) in enumerate(problems):
+        B.set_rhs(p, b)
+    its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=2, max_cycles=0)
+    assert cyc == 0 and np.all(rel > 1e-8) and np.all(its == 0)
+    its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=2, max_cycles=1)
+    assert cyc == 1 and np.all(rel > 1e-8) and np.all(its > 0)
+    its, rel, cyc = B.solve(tol=1e-8, iters_per_cycle=2, max_cycles=200, zero_x=False)
+    assert cyc > 1 and np.all(rel <= 1e-8)
+    B.close()
 
 
 def test_single_problem_and_single_block(msbg, ctx, oracle):

@@ -21,6 +21,10 @@ def random_sparse(msbg, sx, sy, sz, bsx, frac, seed, n_full=3, empty=0.25, full=
             g.blocks[int(b)][:] = v
         elif dtype == "u16":
             g.blocks[int(b)][:] = r.integers(0, 65536, g.N)
+        elif dtype == "u8":
+            g.blocks[int(b)][:] = r.integers(0, 256, g.N)
+        elif dtype == "f16":
+            g.blocks[int(b)][:] = v.astype(np.float16).view(np.uint16)
         else:
             g.blocks[int(b)][:] = (v.view(np.uint32) >> 16).astype(np.uint16)
     rest = [b for b in range(g.n_blocks) if b not in g.blocks]
@@ -35,6 +39,11 @@ def quantized_value(dtype, v):
     if dtype == "u16":
         q = np.floor(f(v) * f(65535.0) + f(0.5))
         return float(f(min(max(q, 0.0), 65535.0)) * (f(1.0) / f(65535.0)))
+    if dtype == "u8":
+        q = np.floor(f(v) * f(255.0) + f(0.5))
+        return float(f(min(max(q, 0.0), 255.0)) * (f(1.0) / f(255.0)))
+    if dtype == "f16":
+        return float(np.array([v], f).astype(np.float16).astype(f)[0])
     if dtype == "bf16":
         b = int(np.array([v], f).view(np.uint32)[0])
         b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
@@ -51,6 +60,10 @@ def dequantized(host):
     for b, v in host.blocks.items():
         if host.dtype == "u16":
             g.blocks[b] = (v.astype(np.float32) * (np.float32(1.0) / np.float32(65535.0))).astype(np.float32)
+        elif host.dtype == "u8":
+            g.blocks[b] = (v.astype(np.float32) * (np.float32(1.0) / np.float32(255.0))).astype(np.float32)
+        elif host.dtype == "f16":
+            g.blocks[b] = v.view(np.float16).astype(np.float32)
         else:
             g.blocks[b] = (v.astype(np.uint32) << 16).view(np.float32)
     g.empty_value = quantized_value(host.dtype, host.empty_value)
@@ -72,7 +85,7 @@ def test_sparse_grid_hash_through_device(msbg, ctx, goldens):
     assert h == int(goldens["sparse_grid_hash"]["hash"], 16)
 
 
-@pytest.mark.parametrize("dtype", ["f32", "u16", "bf16"])
+@pytest.mark.parametrize("dtype", ["f32", "u16", "bf16", "u8", "f16"])
 def test_write_read_roundtrip(msbg, ctx, dtype):
     host = random_sparse(msbg, 40, 33, 17, 8, 0.5, 1, dtype=dtype)
     dev = msbg.SparseGrid.from_host(ctx, host)
@@ -106,7 +119,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("case", CASES)
-@pytest.mark.parametrize("dtype", ["f32", "u16", "bf16"])
+@pytest.mark.parametrize("dtype", ["f32", "u16", "bf16", "u8", "f16"])
 def test_halo_gather_matches_oracle(msbg, ctx, oracle, case, dtype):
     sx, sy, sz, bsx, frac = case
     host = random_sparse(msbg, sx, sy, sz, bsx, frac, 11 + bsx, dtype=dtype)

@@ -62,6 +62,38 @@ def test_matvec_and_jacobi_match_oracle(msbg, ctx, oracle, nb, bsx):
     assert np.max(np.abs(dx.cpu().numpy() - want)) <= 2e-6 * max(1.0, np.abs(want).max())
 
 
+def test_tile_choices_give_the_same_bits(msbg, ctx, oracle):
+    """The 16^3 tile kernels (quad tile, slab tiles of 2..16 z-planes) round
+    identically: matvec, residual and Jacobi sweeps agree bit for bit, and
+    the autotuner's choice is one of them."""
+    nb, bsx = 8, 16
+    act = np.sort(shell(nb, bsx))
+    s = nb * bsx
+    P = msbg.Poisson(ctx, s, s, s, bsx, act)
+    r = np.random.default_rng(7)
+    x = torch.from_numpy(r.uniform(-1, 1, P.n).astype(np.float32)).cuda()
+    b = torch.from_numpy(rhs(P.n, 3)).cuda()
+    base = P.autotune()
+    assert base[0, 2] in (1, 2, 4, 8, 16)
+    results = {}
+    for tile in (1, 2, 4, 8, 16):
+        cfg = base.copy()
+        cfg[0, 2] = tile
+        P.set_tuning(cfg)
+        y, rr, xj = torch.empty_like(x), torch.empty_like(x), x.clone()
+        P.matvec(x, y)
+        P.residual(x, b, rr)
+        P.jacobi(xj, b, 2.0 / 3.0, 3)
+        ctx.synchronize()
+        results[tile] = [t.cpu().numpy() for t in (y, rr, xj)]
+    for tile in (2, 4, 8, 16):
+        for a, c in zip(results[1], results[tile]):
+            assert np.array_equal(a, c), tile
+    want = oracle.poisson_matvec(act.astype(np.int64), nb, nb, nb, bsx, x.cpu().numpy().astype(np.float64))
+    assert np.max(np.abs(results[1][0] - want)) <= 2e-6 * 8
+    P.close()
+
+
 @pytest.mark.parametrize("nb,bsx", CASES)
 @pytest.mark.parametrize("method", [0, 1])
 def test_solve_reaches_tolerance(msbg, ctx, oracle, nb, bsx, method):

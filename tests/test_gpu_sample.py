@@ -54,3 +54,21 @@ def test_sample_ext_bit_exact(msbg, ctx, oracle, bsx, bc):
             got = dev.sample_ext(p, mode, align, bc)
             want = oracle.sample_ext(host, p, mode, bc, align)
             assert np.array_equal(got, want), (mode, align)
+
+
+@pytest.mark.parametrize("dtype", ["u16", "bf16", "u8", "f16"])
+def test_sampler_reads_every_storage_type(msbg, ctx, oracle, dtype):
+    """Sampler over quantised storage: every sample is read through Dequant
+    (math/sample.rs:45-70; Density8 linearly), so the device equals the oracle
+    on the dequantised f32 grid."""
+    from test_gpu_grid import dequantized
+    host = random_sparse(msbg, 40, 36, 44, 8, 0.6, seed=9, dtype=dtype)
+    dev = msbg.SparseGrid.from_host(ctx, host)
+    fhost = dequantized(host)
+    r = np.random.default_rng(4)
+    p = np.concatenate([r.uniform(-3, 47, (3000, 3)), r.integers(0, 44, (200, 3)) + 0.5]).astype(np.float32)
+    for mode in range(4):
+        assert np.array_equal(dev.sample_ext(p, mode, 0, msbg.NEUMANN), oracle.sample_ext(fhost, p, mode, msbg.NEUMANN, 0))
+    smp = msbg.Sampler(dev, msbg.CELL_CENTERED, msbg.CLAMP)
+    fdev = msbg.SparseGrid.from_host(ctx, fhost)
+    assert np.array_equal(smp.sample(p), msbg.Sampler(fdev, msbg.CELL_CENTERED, msbg.CLAMP).sample(p))

@@ -3,7 +3,7 @@ particles/mod.rs:279-302): the crate's splat and finalize known answers, and
 bit-exact agreement with the oracle's restatement for random clouds (the
 splat is a minimum, so the order of the particles does not matter), for the
 placement, and for reconstruct_and_smooth (splat, finalize, clamped
-mean-curvature sweeps on Density storage)."""
+mean-curvature sweeps on Density and Density8 storage)."""
 import numpy as np
 import pytest
 import torch
@@ -46,7 +46,7 @@ def test_splat_known_answers(msbg, ctx):
     assert voxel(g, act, 16, 21, 16, 16) == 65535 and voxel(g, act, 16, 20, 16, 16) == 65535
 
 
-@pytest.mark.parametrize("dtype", ["u16", "f32"])
+@pytest.mark.parametrize("dtype", ["u16", "f32", "u8"])
 @pytest.mark.parametrize("bsx,r_particle,nb_dist", [(16, 2.0, 2.0), (8, 1.5, 1.0), (16, 3.0, 4.5)])
 def test_splat_and_finalize_match_oracle(msbg, ctx, oracle, dtype, bsx, r_particle, nb_dist):
     s = 64
@@ -58,31 +58,37 @@ def test_splat_and_finalize_match_oracle(msbg, ctx, oracle, dtype, bsx, r_partic
     g, act, cfg = splat(msbg, ctx, pts, s, dtype, bsx, r_particle, nb_dist)
     want_act = oracle.surface_active(pts, s, s, s, bsx, r_particle + nb_dist)
     assert np.array_equal(act.astype(np.int64), want_act)
-    want = oracle.density_splat(pts, s, s, s, bsx, r_particle, nb_dist, dtype == "u16", want_act)
+    want = oracle.density_splat(pts, s, s, s, bsx, r_particle, nb_dist, dtype, want_act)
     got = g.read_blocks(act)
     assert np.array_equal(got, want)
     msbg.surface.finalize(g, act, cfg)
-    want_f = oracle.density_finalize(want, dtype == "u16", r_particle, nb_dist)
+    want_f = oracle.density_finalize(want, dtype, r_particle, nb_dist)
     assert np.array_equal(g.read_blocks(act), want_f)
 
 
-def test_reconstruct_and_smooth_matches_oracle(msbg, ctx, oracle):
+@pytest.mark.parametrize("dtype", ["u16", "u8"])
+def test_reconstruct_and_smooth_matches_oracle(msbg, ctx, oracle, dtype):
+    """Density8 smooths through the sqrt-compressed stochastic store of a
+    fresh sweeper (seed 0xdeadbeef, 16 lanes)."""
     s, bsx = 64, 16
     r = np.random.default_rng(3)
     # particles on a sphere shell, the kind of cloud the pipeline reconstructs
     d = r.normal(size=(30000, 3))
     pts = (32 + 18 * d / np.linalg.norm(d, axis=1, keepdims=True) + r.uniform(-1, 1, (30000, 3))).astype(np.float32)
-    g = density_grid(msbg, ctx, s, bsx)
+    g = density_grid(msbg, ctx, s, bsx, dtype)
     cfg = msbg.SurfaceConfig(s, s, s, r_particle=2.0, nb_dist=2.0, n_smooth_iters=3, smooth_dt=0.05)
     act = msbg.reconstruct_and_smooth(g, pts, cfg)
     want_act = oracle.surface_active(pts, s, s, s, bsx, cfg.r_scan)
     assert np.array_equal(act.astype(np.int64), want_act)
-    vals = oracle.density_finalize(oracle.density_splat(pts, s, s, s, bsx, 2.0, 2.0, True, want_act), True, 2.0, 2.0)
-    host = msbg.HostGrid("surface", s, s, s, 0.0, 1.0, bsx, "u16")
+    vals = oracle.density_finalize(oracle.density_splat(pts, s, s, s, bsx, 2.0, 2.0, dtype, want_act), dtype, 2.0, 2.0)
+    host = msbg.HostGrid("surface", s, s, s, 0.0, 1.0, bsx, dtype)
     for k, b in enumerate(want_act):
         host.ensure_block(int(b))
         host.blocks[int(b)][:] = vals[k]
-    oracle.sweep(host, want_act, msbg.Stencil.MeanCurvature, cfg.smooth_dt, cfg.n_smooth_iters, True)
+    if dtype == "u8":
+        oracle.sweep_stochastic(host, want_act, msbg.Stencil.MeanCurvature, cfg.smooth_dt, cfg.n_smooth_iters, True)
+    else:
+        oracle.sweep(host, want_act, msbg.Stencil.MeanCurvature, cfg.smooth_dt, cfg.n_smooth_iters, True)
     got = g.read_blocks(act)
     for k, b in enumerate(want_act):
         assert np.array_equal(got[k], host.block_array(int(b))), int(b)

@@ -78,11 +78,11 @@ def test_sweep_matches_oracle_f32(msbg, ctx, oracle, case, stencil, clamp):
     assert_same_blocks(dev, host, np.arange(host.n_blocks))
 
 
-@pytest.mark.parametrize("dtype", ["u16", "bf16"])
+@pytest.mark.parametrize("dtype", ["u16", "bf16", "f16"])
 @pytest.mark.parametrize("stencil", [0, 1, 2])
 def test_sweep_matches_oracle_quantized(msbg, ctx, oracle, dtype, stencil):
-    """Density (u16, round half away) and bf16 storage: dequantise on gather,
-    quantise on store (stencil.rs:142-192)."""
+    """Density (u16, round half away), bf16 and binary16 storage: dequantise
+    on gather, quantise on store (stencil.rs:142-192)."""
     host = random_sparse(msbg, 48, 48, 48, 16, 0.6, 21, empty=0.1, full=0.9, dtype=dtype)
     if dtype == "u16":
         for b in host.blocks:
@@ -90,6 +90,51 @@ def test_sweep_matches_oracle_quantized(msbg, ctx, oracle, dtype, stencil):
     active = list(host.blocks)
     dev = run_device(msbg, ctx, host, active, stencil, 0.05, 2, True)
     oracle.sweep(host, active, stencil, 0.05, 2, True)
+    assert_same_blocks(dev, host, np.arange(host.n_blocks))
+
+
+DENSITY8_CASES = [
+    # sx, bsx, frac, lanes, stencil, clamp
+    (48, 16, 0.6, 16, 0, True),
+    (48, 16, 0.6, 8, 1, True),
+    (48, 16, 0.6, 16, 2, True),
+    (48, 16, 0.6, 16, 0, False),  # out-of-range results take the wrapping u8 cast
+    (40, 8, 0.7, 8, 1, True),
+    (20, 4, 0.7, 4, 2, True),
+]
+
+
+@pytest.mark.parametrize("case", DENSITY8_CASES)
+def test_sweep_density8_stochastic(msbg, ctx, oracle, case):
+    """Density8 storage: linear read, sqrt-compressed stochastic store
+    (stencil.rs:103-132, 176-192), bit for bit against the oracle's serial
+    one-thread generator stream, including a second call that continues the
+    stream."""
+    sx, bsx, frac, lanes, stencil, clamp = case
+    host = random_sparse(msbg, sx, sx, sx, bsx, frac, 5 + bsx, empty=0.1, full=0.9, dtype="u8")
+    active = list(host.blocks)
+    dev = msbg.SparseGrid.from_host(ctx, host)
+    sw = msbg.Sweeper(dev, seed=0x2468ACE1, lanes=lanes)
+    sw.sweep(active, stencil, msbg.PdeParams(0.05, 2, clamp))
+    pos = oracle.sweep_stochastic(host, active, stencil, 0.05, 2, clamp, 0x2468ACE1, lanes, 0)
+    assert sw.stream_pos == pos == 2 * len(active) * host.N // lanes
+    assert_same_blocks(dev, host, np.arange(host.n_blocks))
+    sw.sweep(active, stencil, msbg.PdeParams(0.05, 1, clamp))
+    pos = oracle.sweep_stochastic(host, active, stencil, 0.05, 1, clamp, 0x2468ACE1, lanes, pos)
+    assert sw.stream_pos == pos
+    assert_same_blocks(dev, host, np.arange(host.n_blocks))
+
+
+def test_sweep_density8_plain_entry_is_a_fresh_sweeper(msbg, ctx, oracle):
+    """msbg_sweep on Density8 storage: apply_pde's fresh sweeper, the first
+    rayon slot's generator (seed 0xdeadbeef, 16 lanes, solver.rs:109-119)."""
+    from msbg_rs_b200._lib import call, ptr
+    host = random_sparse(msbg, 48, 48, 48, 16, 0.5, 77, empty=0.0, full=1.0, dtype="u8")
+    active = np.array(sorted(host.blocks), np.uint64)
+    dev = msbg.SparseGrid.from_host(ctx, host)
+    for _ in range(2):  # each call starts the stream again
+        call("msbg_sweep", dev.handle, ptr(active), len(active), 1, 0.05, 1, 1)
+        oracle.sweep_stochastic(host, active.astype(np.int64), 1, 0.05, 1, True, 0xDEADBEEF, 16, 0)
     assert_same_blocks(dev, host, np.arange(host.n_blocks))
 
 
