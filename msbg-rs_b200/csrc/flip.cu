@@ -20,29 +20,23 @@ struct msbg_flip {
     msbg_grid* coarse = nullptr;
     std::vector<uint8_t> levels;  // per block of the MAC grid
     cudaStream_t up = nullptr;    // second upload stream
-    cudaEvent_t start = nullptr, uploaded = nullptr;
+    cudaEvent_t start = nullptr, uploaded = nullptr, downloaded = nullptr;
+    static constexpr int kOutChunks = 8;  // G2P chunks whose results return while the next computes
+    cudaEvent_t chunk_done[kOutChunks] = {};
     msbg::DevBuf buf;
     size_t cap = 0;
     std::vector<uint64_t> fine;
     ~msbg_flip() {
         if (start) cudaEventDestroy(start);
         if (uploaded) cudaEventDestroy(uploaded);
+        if (downloaded) cudaEventDestroy(downloaded);
+        for (cudaEvent_t ev : chunk_done)
+            if (ev) cudaEventDestroy(ev);
         if (up) cudaStreamDestroy(up);
     }
 };
 
 namespace msbg {
-
-// dst[perm[i]] = src[i] for rows of 3 floats (the inverse of the sort's gather).
-__global__ void scatter_rows3_kernel(const uint32_t* __restrict__ perm, size_t n, const float* __restrict__ src,
-                                     float* __restrict__ dst) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const size_t d = perm[i];
-        dst[3 * d] = src[3 * i];
-        dst[3 * d + 1] = src[3 * i + 1];
-        dst[3 * d + 2] = src[3 * i + 2];
-    }
-}
 
 static void check(int st) {
     if (st != MSBG_OK) MSBG_THROW(st, msbg_last_error());
@@ -69,6 +63,9 @@ int msbg_flip_create(msbg_mac* mac, msbg_grid* coarse, const uint8_t* levels, si
     cudaError_t e = cudaStreamCreateWithFlags(&f->up, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->start, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->uploaded, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->downloaded, cudaEventDisableTiming);
+    for (int c = 0; c < msbg_flip::kOutChunks && e == cudaSuccess; ++c)
+        e = cudaEventCreateWithFlags(&f->chunk_done[c], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete f;
         MSBG_THROW(MSBG_ERR_CUDA, std::string("msbg_flip_create: ") + cudaGetErrorString(e));
@@ -108,7 +105,7 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
     float* s_pos = (float*)p;  p += b3;
     float* s_vel = (float*)p;  p += b3;
     float* d_u = (float*)p;    p += b3;
-    float* d_new = (float*)p;  p += b3;
+    p += b3;  // spare
     float* d_out = (float*)p;  p += b3;
     p += b3;  // spare row buffer (keeps the layout 256-byte aligned for any n)
     float* d_mass = (float*)p; p += b1;
@@ -138,12 +135,22 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
         check(msbg_sweep_multires(f->mac->ch[3], f->coarse, f->levels.data(), f->fine.data(), f->fine.size(), stencil, dt,
                                   sweeps, 0));
     }
-    check(msbg_g2p_device(f->mac, s_pos, n, MSBG_CLAMP, d_u));
-    check(msbg_g2p_blend_device(ctx, s_vel, d_u, d_u, n, alpha, d_new));
-    begin_launch(ctx);
-    scatter_rows3_kernel<<<std::min<unsigned>(div_up(n, 256), 148 * 32), 256, 0, ctx->stream>>>(perm, n, d_new, d_out);
-    after_launch(ctx, "scatter_rows3_kernel");
-    CUDA_CHECK(cudaMemcpyAsync(vel_out, d_out, n * 12, cudaMemcpyDeviceToHost, ctx->stream));
+    // G2P and the blend per particle in the caller's order (unsorted
+    // positions and velocities: the same values as the sorted pass, and the
+    // grid, a few tens of MB, sits in L2), in chunks whose new velocities
+    // return to the host on the upload stream while the next chunk computes
+    const size_t per = ((n + msbg_flip::kOutChunks - 1) / msbg_flip::kOutChunks + 255) & ~size_t(255);
+    int used = 0;
+    for (size_t lo = 0; lo < n; lo += per, ++used) {
+        const size_t cnt = std::min(per, n - lo);
+        check(msbg_g2p_device(f->mac, d_pos + 3 * lo, cnt, MSBG_CLAMP, d_u + 3 * lo));
+        check(msbg_g2p_blend_device(ctx, d_vel + 3 * lo, d_u + 3 * lo, d_u + 3 * lo, cnt, alpha, d_out + 3 * lo));
+        CUDA_CHECK(cudaEventRecord(f->chunk_done[used], ctx->stream));
+        CUDA_CHECK(cudaStreamWaitEvent(f->up, f->chunk_done[used], 0));
+        CUDA_CHECK(cudaMemcpyAsync(vel_out + 3 * lo, d_out + 3 * lo, cnt * 12, cudaMemcpyDeviceToHost, f->up));
+    }
+    CUDA_CHECK(cudaEventRecord(f->downloaded, f->up));
+    CUDA_CHECK(cudaStreamWaitEvent(ctx->stream, f->downloaded, 0));
     check_device_status(ctx);
     sync(ctx);
     MSBG_API_END
