@@ -61,19 +61,20 @@ __device__ __forceinline__ float stencil_meancurv(const float* h, int i, int dy,
 }
 
 // bilaplacian.rs:45-92 (25 taps)
-__device__ __forceinline__ float stencil_bilaplacian(const float* h, int i, int dy, int dz, float dt, int clamp01) {
-    float f0 = h[i], f1 = h[i - 1], f2 = h[i + 1], f3 = h[i - dy], f4 = h[i + dy], f5 = h[i - dz], f6 = h[i + dz];
-    float g1 = h[i - 2], g2 = h[i + 2], g3 = h[i - 2 * dy], g4 = h[i + 2 * dy], g5 = h[i - 2 * dz], g6 = h[i + 2 * dz];
+// bilaplacian.rs:40-90 on the 25 values: the centre f0, the face
+// neighbours f1..f6 (x-, x+, y-, y+, z-, z+), the distance-2 neighbours g1..g6
+// in the same order, and the 12 edge diagonals in the reference's order
+// (x+y+, x+y-, x-y+, x-y-, x+z+, x+z-, x-z+, x-z-, y+z+, y+z-, y-z+, y-z-).
+__device__ __forceinline__ float bilaplacian_values(float f0, float f1, float f2, float f3, float f4, float f5, float f6,
+                                                    float g1, float g2, float g3, float g4, float g5, float g6,
+                                                    const float (&e)[12], float dt, int clamp01) {
     float s1 = f1 + f2;
     s1 = s1 + f3; s1 = s1 + f4; s1 = s1 + f5; s1 = s1 + f6;
     float s2 = g1 + g2;
     s2 = s2 + g3; s2 = s2 + g4; s2 = s2 + g5; s2 = s2 + g6;
-    float sd = h[i + 1 + dy] + h[i + 1 - dy];
-    sd = sd + h[i - 1 + dy]; sd = sd + h[i - 1 - dy];
-    sd = sd + h[i + 1 + dz]; sd = sd + h[i + 1 - dz];
-    sd = sd + h[i - 1 + dz]; sd = sd + h[i - 1 - dz];
-    sd = sd + h[i + dy + dz]; sd = sd + h[i + dy - dz];
-    sd = sd + h[i - dy + dz]; sd = sd + h[i - dy - dz];
+    float sd = e[0] + e[1];
+#pragma unroll
+    for (int k = 2; k < 12; ++k) sd = sd + e[k];
     float hv = ((42.0f * f0 - 12.0f * s1) + s2) + 2.0f * sd;
     float fx = (f2 - f1) * 0.5f, fy = (f4 - f3) * 0.5f, fz = (f6 - f5) * 0.5f;
     float g = sqrtf(fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
@@ -83,9 +84,18 @@ __device__ __forceinline__ float stencil_bilaplacian(const float* h, int i, int 
     return clamp01 ? clampf(nv, 0.0f, 1.0f) : nv;
 }
 
+__device__ __forceinline__ float stencil_bilaplacian(const float* h, int i, int dy, int dz, float dt, int clamp01) {
+    const float e[12] = {h[i + 1 + dy], h[i + 1 - dy], h[i - 1 + dy], h[i - 1 - dy], h[i + 1 + dz], h[i + 1 - dz],
+                         h[i - 1 + dz], h[i - 1 - dz], h[i + dy + dz], h[i + dy - dz], h[i - dy + dz], h[i - dy - dz]};
+    return bilaplacian_values(h[i], h[i - 1], h[i + 1], h[i - dy], h[i + dy], h[i - dz], h[i + dz], h[i - 2], h[i + 2],
+                              h[i - 2 * dy], h[i + 2 * dy], h[i - 2 * dz], h[i + 2 * dz], e, dt, clamp01);
+}
+
 struct SweepArgs {
     void* payload;              // fine payload (grid dtype)
-    float* xface;               // [slots][2][bsx^2] stored x-planes of every block ([z][y]), or null
+    float* xface;               // [slots][2 XD][bsx^2] stored x-planes of every block ([z][y]), or null:
+                                // x = 0 .. XD-1, then x = bsx-1 .. bsx-XD (XD = 2 for the 25-tap
+                                // stencil's two-cell halo, else 1)
     const float* coarse;        // coarse payload (f32) for multiresolution halos
     const int32_t* nbr;         // [n][27]
     const int32_t* bxyz;        // [n][4]: block coords + flags (bit h-1: interior for halo h)
@@ -167,12 +177,16 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
     constexpr int N = BSX * BSX * BSX;
     typename E::T* payload = (typename E::T*)a.payload;
     if (tid < BSX * BSX) {
-        const int x = tid % BSX, y = tid / BSX;
+        // 16^3 blocks: each warp takes rows y and y + 2 of the plane, whose
+        // shared-memory rows (pitch RS = 24 floats) fall on disjoint banks
+        const int x = tid % BSX;
+        const int y = BSX == 16 ? (((tid >> 6) << 2) | ((tid >> 5) & 1) | (((tid >> 4) & 1) << 1)) : tid / BSX;
         typename E::T* out = payload + (size_t)slot * N + x + y * BSX;
         // this block's new x-planes go to the side buffer as well
-        float* xo = (a.xface && (x == 0 || x == BSX - 1))
-                        ? a.xface + ((size_t)slot * 2 + (x == 0 ? 0 : 1)) * (BSX * BSX) + y
-                        : nullptr;
+        constexpr int XD = ST == MSBG_BILAPLACIAN ? 2 : 1;
+        float* xo = nullptr;
+        if (a.xface && (x < XD || x >= BSX - XD))
+            xo = a.xface + ((size_t)slot * 2 * XD + (x < XD ? x : XD + (BSX - 1 - x))) * (BSX * BSX) + y;
         const int i0 = (HALO * HSX + (y + HALO)) * RS + X0 + x + HALO;  // z = 0
         const float dt = a.dt;
         const int clamp01 = a.clamp01;
@@ -325,7 +339,7 @@ __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const i
 }
 
 template <class E, int BSX, int ST>
-__global__ void __launch_bounds__(BSX * BSX < 32 ? 32 : BSX * BSX)
+__global__ void __launch_bounds__(BSX * BSX < 32 ? 32 : BSX * BSX, BSX == 16 && ST == MSBG_BILAPLACIAN ? 4 : 1)
 sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
     constexpr int HSX = BSX + 2 * HALO;
@@ -476,10 +490,12 @@ sweep_phase_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
                     }
                 }
                 if (dx[k] >= 0) {
-                    if (c >= 0 && a.xface && (lx == 0 || lx == BSX - 1)) {
+                    constexpr int XD = ST == MSBG_BILAPLACIAN ? 2 : 1;
+                    if (c >= 0 && a.xface && (lx < XD || lx >= BSX - XD)) {
                         // x-plane cells from the side buffer: 16 contiguous
                         // floats per (z) row instead of one sector per cell
-                        vx[k] = a.xface[((size_t)c * 2 + (lx == 0 ? 0 : 1)) * (BSX * BSX) + lz * BSX + ly];
+                        const int pl = lx < XD ? lx : XD + (BSX - 1 - lx);
+                        vx[k] = a.xface[((size_t)c * 2 * XD + pl) * (BSX * BSX) + lz * BSX + ly];
                     } else if (c >= 0) {
                         vx[k] = E::load(payload[(size_t)c * N + lx + (ly << LG) + (lz << (2 * LG))]);
                     } else if (c <= kCodeCoarse0) {
@@ -614,8 +630,10 @@ __device__ __forceinline__ void issue_interior_f32(const SweepArgs& a, float* __
                 dst = ((j + HALO) * HSX + ho) * RS + X0 + hx;
             }
         }
-        if (c >= 0 && a.xface && (lx == 0 || lx == BSX - 1)) {
-            cp_async4(h + dst, a.xface + ((size_t)c * 2 + (lx == 0 ? 0 : 1)) * (BSX * BSX) + lz * BSX + ly);
+        constexpr int XD = ST == MSBG_BILAPLACIAN ? 2 : 1;
+        if (c >= 0 && a.xface && (lx < XD || lx >= BSX - XD)) {
+            const int pl = lx < XD ? lx : XD + (BSX - 1 - lx);
+            cp_async4(h + dst, a.xface + ((size_t)c * 2 * XD + pl) * (BSX * BSX) + lz * BSX + ly);
         } else if (c >= 0) {
             cp_async4(h + dst, payload + (size_t)c * N + lx + (ly << LG) + (lz << (2 * LG)));
         } else if (c <= kCodeCoarse0) {
@@ -1058,37 +1076,38 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     cp_async_wait<0>();
 }
 
-// Copies the x-planes (x = 0 and x = bsx-1) of the listed slots into the side
-// buffer: [slot][plane][z][y].
+// Copies the outer x-planes (x = 0 .. xd-1 and x = bsx-1 .. bsx-xd) of the
+// listed slots into the side buffer: [slot][plane][z][y].
 template <class E, int BSX>
 __global__ void xface_init_kernel(const typename E::T* __restrict__ payload, const int32_t* __restrict__ slots, size_t n,
-                                  float* __restrict__ xface) {
+                                  int xd, float* __restrict__ xface) {
     constexpr int LG = Lg<BSX>::v, N = BSX * BSX * BSX, P = BSX * BSX;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n * 2 * P; e += (size_t)gridDim.x * blockDim.x) {
-        const size_t k = e / (2 * P);
-        const int r = (int)(e % (2 * P)), side = r / P, zy = r % P, z = zy / BSX, y = zy % BSX;
+    const size_t per = (size_t)2 * xd * P;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n * per; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t k = e / per;
+        const int r = (int)(e % per), pl = r / P, zy = r % P, z = zy / BSX, y = zy % BSX;
         const int32_t slot = slots[k];
-        const int x = side ? BSX - 1 : 0;
-        xface[((size_t)slot * 2 + side) * P + zy] = E::load(payload[(size_t)slot * N + x + (y << LG) + (z << (2 * LG))]);
+        const int x = pl < xd ? pl : BSX - 1 - (pl - xd);
+        xface[((size_t)slot * 2 * xd + pl) * P + zy] = E::load(payload[(size_t)slot * N + x + (y << LG) + (z << (2 * LG))]);
     }
 }
 
 template <class E, int BSX>
-static void launch_xface_init(msbg_ctx* ctx, const void* payload, const int32_t* slots, size_t n, float* xface) {
+static void launch_xface_init(msbg_ctx* ctx, const void* payload, const int32_t* slots, size_t n, int xd, float* xface) {
     if (!n) return;
     begin_launch(ctx);
-    xface_init_kernel<E, BSX><<<(unsigned)std::min<size_t>((n * 2 * BSX * BSX + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
-        (const typename E::T*)payload, slots, n, xface);
+    xface_init_kernel<E, BSX><<<(unsigned)std::min<size_t>((n * 2 * xd * BSX * BSX + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
+        (const typename E::T*)payload, slots, n, xd, xface);
     after_launch(ctx, "xface_init_kernel");
 }
 
 template <class E>
-static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_t* slots, size_t n, float* xface) {
+static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_t* slots, size_t n, int xd, float* xface) {
     switch (bsx) {
-        case 4: launch_xface_init<E, 4>(ctx, payload, slots, n, xface); break;
-        case 8: launch_xface_init<E, 8>(ctx, payload, slots, n, xface); break;
-        case 16: launch_xface_init<E, 16>(ctx, payload, slots, n, xface); break;
-        default: launch_xface_init<E, 32>(ctx, payload, slots, n, xface); break;
+        case 4: launch_xface_init<E, 4>(ctx, payload, slots, n, xd, xface); break;
+        case 8: launch_xface_init<E, 8>(ctx, payload, slots, n, xd, xface); break;
+        case 16: launch_xface_init<E, 16>(ctx, payload, slots, n, xd, xface); break;
+        default: launch_xface_init<E, 32>(ctx, payload, slots, n, xd, xface); break;
     }
 }
 
@@ -1322,16 +1341,19 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
     // the start of each call (the payload may have changed in between)
     {
         const size_t slots = g->n_slots();
-        if (plan->xface_slots < slots) {
-            plan->xface.reserve(slots * 2 * g->bsx * g->bsx * sizeof(float));
-            plan->xface_slots = slots;
+        const int xd = stencil == MSBG_BILAPLACIAN ? 2 : 1;  // x-planes per side the stencil's halo reaches
+        if (plan->xface_slots < slots * xd) {
+            plan->xface.reserve(slots * 2 * xd * g->bsx * g->bsx * sizeof(float));
+            plan->xface_slots = slots * xd;
         }
         a.xface = plan->xface.as<float>();
-        if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
-        else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
-        else if (g->dtype == MSBG_U8) xface_init<ElemU8>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
-        else if (g->dtype == MSBG_F16) xface_init<ElemF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
-        else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, plan->xslots.as<int32_t>(), plan->n_xslots, a.xface);
+        const int32_t* xs = plan->xslots.as<int32_t>();
+        const size_t nx = plan->n_xslots;
+        if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
+        else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
+        else if (g->dtype == MSBG_U8) xface_init<ElemU8>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
+        else if (g->dtype == MSBG_F16) xface_init<ElemF16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
+        else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
     }
     const int32_t* order = plan->order.as<int32_t>();
     for (int it = 0; it < iterations; ++it) {

@@ -22,8 +22,8 @@ struct SweepPlan {
     // faces or edges), for the x-face side buffer (see sweep.cu).
     DevBuf xslots;  // int32 [n_xslots]
     size_t n_xslots = 0;
-    DevBuf xface;   // f32 [n_slots][2][bsx^2]: x = 0 and x = bsx-1 planes, [z][y]
-    size_t xface_slots = 0;
+    DevBuf xface;   // f32 [n_slots][2 xd][bsx^2]: the xd outermost x-planes per side, [z][y]
+    size_t xface_slots = 0;  // capacity in slots x xd
 };
 
 }  // namespace msbg
