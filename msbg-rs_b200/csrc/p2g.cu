@@ -180,7 +180,16 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             uint64_t rows = 0;
             for (int dv = 0; dv < WIN; ++dv)
                 if ((run[V][0] >> dv) & 1u) rows |= 1ull << (WIN * dv);
-            const uint64_t m = (uint64_t)run[U][0] * rows | ((uint64_t)run[F][1] << 56);
+            uint64_t m = (uint64_t)run[U][0] * rows | ((uint64_t)run[F][1] << 56);
+            // M = 2: bit 32 when the footprint has the regular r_p = 2 shape
+            // (four rows along U and V starting 2 - s before the cell, s = 0
+            // or 1, and faces -2 .. +1 along F), bits 33 and 34 the shifts
+            // s_U and s_V (the r_p = 2 splat's anchor); lane bits end at 24
+            if (M == 2) {
+                const uint32_t rU = run[U][0], rV = run[V][0], rF = run[F][1];
+                if ((rU == 0x0fu || rU == 0x1eu) && (rV == 0x0fu || rV == 0x1eu) && rF == 0x1eu)
+                    m |= (1ull << 32) | ((uint64_t)(rU == 0x1eu) << 33) | ((uint64_t)(rV == 0x1eu) << 34);
+            }
             lane_mask[(size_t)dir * n + i] = m;
         }
         if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
@@ -508,44 +517,70 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
     for (int i = tid; i < 2 * WW; i += blockDim.x) out[i] = st[i];
 }
 
-// Warps of an r_p = 2 splat CTA and the particles each warp stages at once.
+// Splat for r_p = 2 (M = 2), grouped by footprint anchor.  With r_p = 2 the
+// clipped footprint of a particle in cell c spans, along each lane axis (U,
+// V), the four rows [c - 2 + s, c + 1 + s], s = 0 or 1 by the side of the
+// cell centre the particle lies on, and along the face axis F the four faces
+// [c - 2, c + 1] -- except when a coordinate lies exactly on a cell centre
+// (lane axes) or a face plane (face axis).  Such a "regular" particle's
+// footprint is fixed by its anchor (c_U + s_U, c_V + s_V, c_F): the particles
+// of one anchor, drawn from four cells, share every footprint row, so a warp
+// can keep its lanes' face sums in FP64 registers over all of them and add
+// them into the window once.  The block's anchors (0 .. BSX along U and V,
+// 0 .. BSX-1 along F) are cut into 2x2x2 anchor tiles; a tile draws its
+// particles from 3 x 3 x 2 source cells.  Tile footprints are at most six
+// rows wide, so tiles coloured by tile coordinate mod 3 never overlap within
+// a colour, and the tile-order waits of p2g_cells_kernel apply unchanged.
+// Per tile a warp stages its source cells' particles (each tagged with its
+// anchor inside the tile), then takes the tile's eight anchors in turn: lane
+// (i, j, h) evaluates faces 2h and 2h + 1 of footprint row (i, j) for every
+// particle of the anchor and adds its two sums into the window afterwards.
+// Irregular particles (footprint not of that shape) are tagged with their own
+// cell and go through the lane-bit path of p2g_cells_kernel.  Every term is
+// the reference's f32 operation sequence (p2g.rs:263-330); the sums are FP64
+// in a fixed order (colour, tile, anchor, staging order).
 constexpr int kSplatR2Warps = 20;
-template <int BSX> struct SplatR2Cap {
-    static constexpr int v = SplatCap<BSX, 2>::v;
+template <int BSX> struct SplatR2 {
+    static constexpr int M = 2, W = BSX + 2 * M, WW = W * W * W;
+    static constexpr int NA = BSX / 2 + 1;  // anchor tiles along U and V (anchors 0 .. BSX)
+    static constexpr int NF = BSX / 2;      // anchor tiles along F
+    static constexpr int NT = NA * NA * NF;
+    static constexpr int NSRC = 18;         // source cells of a tile
+    static constexpr int WARPS = NT < kSplatR2Warps ? NT : kSplatR2Warps;
+    // particles a warp stages at once: a whole typical tile (144 at 8 per cell)
+    static constexpr int CAP = 192;
+    // per warp: CAP x (float4 position/mass, float momentum, u8 anchor-sorted
+    // index), source cells (int2), 17 anchor-range offsets and 16 counters
+    static constexpr size_t warp_bytes = (size_t)CAP * (16 + 4 + 1 + 1 + 1) + NSRC * 8 + 17 * 4 + 16 * 4;
+    static constexpr size_t smem_bytes = 2 * sizeof(double) * WW + (size_t)WARPS * ((warp_bytes + 15) / 16 * 16);
+    static_assert(NT < 0xffff, "tile indices must fit 16 bits");
+    static_assert(CAP <= 256 && CAP % 32 == 0, "staging indices must fit a byte");
+    static_assert(BSX <= 16, "source-cell Morton codes take 4 bits per axis");
 };
 
-// Splat for r_p = 2 (M = 2): all three face directions in one launch, CTA
-// 3k + d taking particle block k and direction d, so a block's three CTAs run
-// side by side and read its particles from L2 once.  Tiles, colours, the
-// tile-order waits and the FP64 window are those of p2g_cells_kernel; the
-// per-cell work differs.  With r_p = 2 the clipped footprint of a particle
-// in cell c spans cells [c-2+a, c+1+a] along each lane axis (a = 0 or 1 by
-// the side of the cell centre the particle lies on) and faces [c-2, c+1]
-// along the face axis, except when a coordinate lies exactly on a cell
-// centre (lane axes) or a face plane (face axis).  The cell's regular
-// particles are grouped by (a_U, a_V); within a group the warp takes one
-// particle at a time, lane (i, j, h) evaluating faces 2h and 2h + 1 of
-// footprint row (i, j), so every evaluated term is inside the footprint and
-// every lane owns its faces: each lane keeps its two face sums in FP64
-// registers over the group and adds them into the window after the group.
-// The cell's other particles then go through the lane-bit path
-// of p2g_cells_kernel, adding straight into the window.  Every term is the
-// reference's f32 operation sequence (p2g.rs:263-330); the sums are FP64 in
-// a fixed order.
+// Morton code of a cell inside a block of at most 16^3 cells.
+__device__ __forceinline__ uint32_t morton4(uint32_t x, uint32_t y, uint32_t z) {
+    auto sp = [](uint32_t v) { return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6); };
+    return sp(x) | (sp(y) << 1) | (sp(z) << 2);
+}
+
 template <int BSX, int DIR>
 __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb, double* st, uint32_t* s_done,
                                               const uint16_t* s_order, uint32_t* s_next) {
-    constexpr int M = 2;
-    constexpr int W = BSX + 2 * M;
-    constexpr int WW = W * W * W;
-    constexpr int WIN = 2 * M + 1;
-    constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
-    constexpr int NNB = WIN * WIN * WIN;
-    constexpr int CAP = SplatR2Cap<BSX>::v;
-    constexpr int NR = (NNB + 31) / 32;
+    using S = SplatR2<BSX>;
+    constexpr int M = 2, W = S::W, WW = S::WW, NA = S::NA, NF = S::NF, NT = S::NT, CAP = S::CAP, NSRC = S::NSRC;
+    constexpr int NNB = 125, NR = (NNB + 31) / 32;  // tile offsets in [-2, 2]^3, NR of them per lane
     constexpr int F = DIR, U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2;
-    const int tid = threadIdx.x, lane = tid & 31;
-    float4* wslot = reinterpret_cast<float4*>(st + 2 * WW) + (size_t)(tid >> 5) * 2 * CAP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    char* const wbase = reinterpret_cast<char*>(st + 2 * WW) + (size_t)warp * ((S::warp_bytes + 15) / 16 * 16);
+    float4* const wp = reinterpret_cast<float4*>(wbase);                    // U, V, F coordinates - 0.5, mass
+    float* const wm = reinterpret_cast<float*>(wbase + 16 * CAP);           // momentum m * v[DIR]
+    int2* const wc = reinterpret_cast<int2*>(wbase + 20 * CAP);             // (first staging index, first particle)
+    int* const woff = reinterpret_cast<int*>(wbase + 20 * CAP + NSRC * 8);  // anchor code ranges [16 + 1]
+    int* const wcnt = woff + 17;                                            // per-code counters
+    uint8_t* const wlist = reinterpret_cast<uint8_t*>(wcnt + 16);           // staging indices by anchor code
+    int8_t* const wcode = reinterpret_cast<int8_t*>(wlist + CAP);            // anchor code per staging index
+    uint8_t* const wsrc = reinterpret_cast<uint8_t*>(wcode + CAP);          // source cell per staging index
     const uint64_t key = a.pb_key[k_pb];
     const int32_t b0[3] = {(int32_t)compact3(key) * BSX, (int32_t)compact3(key >> 1) * BSX,
                            (int32_t)compact3(key >> 2) * BSX};
@@ -553,9 +588,10 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
     const int32_t* ce = a.cell_end + (size_t)k_pb * BSX * BSX * BSX;
     const float* __restrict__ pv = a.pv[DIR];
     const uint64_t* __restrict__ lmask = a.lane_mask[DIR];
-    const float inv_r2 = a.inv_r2, r_p = a.r_p;
-    // this lane's footprint row inside a group, (i, j) along (U, V), and
-    // which two of the particle's four faces along F it evaluates
+    const float inv_r2 = a.inv_r2;
+    const uint32_t lt = [] { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }();
+    // this lane's footprint row inside an anchor, (i, j) along (U, V), and
+    // which two of the anchor's four faces along F it evaluates
     const int li = lane & 3, lj = (lane >> 2) & 3, half = lane >> 4;
     while (true) {
         uint32_t q = 0;
@@ -563,24 +599,44 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= (uint32_t)NT) break;
         const int t = s_order[q];
-        const int tc[3] = {t % T, (t / T) % T, t / (T * T)};
-        const int ci = tc[0] % K + K * (tc[1] % K + K * (tc[2] % K));
-        int cbeg = 0, cend = 0;
-        if (lane < 8) {
-            const uint32_t lm = (uint32_t)morton3(2 * tc[0] + (lane & 1), 2 * tc[1] + ((lane >> 1) & 1), 2 * tc[2] + (lane >> 2));
-            cbeg = cb[lm];
-            cend = ce[lm];
+        const int tu = t % NA, tv = (t / NA) % NA, tf = t / (NA * NA);
+        const int ci = tu % 3 + 3 * (tv % 3 + 3 * (tf % 3));
+        // source cells, one per lane: (2tu - 1 + c % 3, 2tv - 1 + (c / 3) % 3, 2tf + c / 9)
+        int n_c = 0, b_c = 0;
+        if (lane < NSRC) {
+            const int cu = 2 * tu - 1 + lane % 3, cv = 2 * tv - 1 + (lane / 3) % 3, cf = 2 * tf + lane / 9;
+            if (cu >= 0 && cu < BSX && cv >= 0 && cv < BSX) {
+                int c3[3];
+                c3[U] = cu;
+                c3[V] = cv;
+                c3[F] = cf;
+                const uint32_t lm = morton4(c3[0], c3[1], c3[2]);
+                b_c = cb[lm];
+                n_c = ce[lm] - b_c;
+            }
         }
-        uint32_t nbi[(NR + 1) / 2];
+        int incl = n_c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();  // the previous tile's readers of wc are done
+        if (lane < NSRC) wc[lane] = make_int2(incl - n_c, b_c);
+        // the overlapping tiles of lower colours: each lane takes up to NR of
+        // them; the warp waits for them before its first shared-memory add
+        // of this tile, drops each as it is seen done, sleeps between rounds
+        uint32_t nbi[(NR + 1) / 2];  // tile indices, two 16-bit fields per word, 0xffff = none
 #pragma unroll
         for (int k = 0; k < (NR + 1) / 2; ++k) nbi[k] = 0xffffffffu;
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
             const int o = lane + 32 * k;
-            const int nx = tc[0] + o % WIN - M, ny = tc[1] + (o / WIN) % WIN - M, nz = tc[2] + o / (WIN * WIN) - M;
-            const bool dep = o < NNB && nx >= 0 && ny >= 0 && nz >= 0 && nx < T && ny < T && nz < T &&
-                             nx % K + K * (ny % K + K * (nz % K)) < ci;
-            if (dep) nbi[k >> 1] &= ~(0xffffu << (16 * (k & 1))) | ((uint32_t)(nx + T * (ny + T * nz)) << (16 * (k & 1)));
+            const int nu = tu + o % 5 - 2, nv = tv + (o / 5) % 5 - 2, nf = tf + o / 25 - 2;
+            const bool dep = o < NNB && nu >= 0 && nv >= 0 && nf >= 0 && nu < NA && nv < NA && nf < NF &&
+                             nu % 3 + 3 * (nv % 3 + 3 * (nf % 3)) < ci;
+            if (dep) nbi[k >> 1] &= ~(0xffffu << (16 * (k & 1))) | ((uint32_t)(nu + NA * (nv + NA * nf)) << (16 * (k & 1)));
         }
         bool deps_pending = true;
         auto wait_deps = [&]() {
@@ -611,157 +667,218 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
             __threadfence_block();
             deps_pending = false;
         };
-        const int e_tile = (int)__reduce_max_sync(0xffffffffu, lane < 8 ? (uint32_t)cend : 0u);
-        int st_lo = 0, st_hi = 0;
-        for (int sub = 0; sub < 8; ++sub) {
-            const int b = __shfl_sync(0xffffffffu, cbeg, sub), e = __shfl_sync(0xffffffffu, cend, sub);
-            if (b >= e) continue;
-            int cell[3];
-            cell[0] = 2 * tc[0] + (sub & 1);
-            cell[1] = 2 * tc[1] + ((sub >> 1) & 1);
-            cell[2] = 2 * tc[2] + (sub >> 2);
-            // this lane's two face positions along F: offsets -2 + 2 half and
-            // -1 + 2 half from the cell
-            const uint64_t gf2 = f2_pack((float)(b0[F] - M + cell[F] + 2 * half), (float)(b0[F] - M + cell[F] + 2 * half + 1));
-            for (int p0 = b; p0 < e;) {
-                if (p0 < st_lo || p0 >= st_hi) {
-                    __syncwarp();
-                    st_lo = p0;
-                    st_hi = min(p0 + CAP, e_tile);
-#pragma unroll
-                    for (int k = 0; k < CAP / 32; ++k) {
-                        const int pl = st_lo + lane + 32 * k;
-                        if (pl < st_hi) {
-                            const uint64_t fb = lmask[pl];
-                            const float m = a.pm[pl];
-                            const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
-                            // footprint starts and ends exactly as the reference computes them
-                            int cat = 4;
-                            {
-                                const int cU = pp[U] > 0.0f ? (int)pp[U] : 0, cV = pp[V] > 0.0f ? (int)pp[V] : 0,
-                                          cF = pp[F] > 0.0f ? (int)pp[F] : 0;
-                                const int sU = (int)ceilf((pp[U] - r_p) - 0.5f), eU = (int)floorf((pp[U] + r_p) - 0.5f);
-                                const int sV = (int)ceilf((pp[V] - r_p) - 0.5f), eV = (int)floorf((pp[V] + r_p) - 0.5f);
-                                const int sF = (int)ceilf((pp[F] - r_p) - 1.0f), eF = (int)floorf((pp[F] + r_p) - 1.0f);
-                                const int aU = sU - cU + 2, aV = sV - cV + 2;
-                                if (eU - sU == 3 && eV - sV == 3 && sF == cF - 2 && eF == cF + 1 && (unsigned)aU <= 1u &&
-                                    (unsigned)aV <= 1u)
-                                    cat = aU | (aV << 1);
-                            }
-                            wslot[pl - st_lo] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
-                            wslot[CAP + pl - st_lo] = make_float4(m * pv[pl], __uint_as_float((uint32_t)fb),
-                                                                  __uint_as_float((uint32_t)(fb >> 32)), __int_as_float(cat));
-                        }
-                    }
-                    __syncwarp();
-                }
-                const int pend = min(e, st_hi);
-                for (int c0 = p0; c0 < pend; c0 += 32) {
-                    const int my = c0 + lane < pend ? __float_as_int(wslot[CAP + c0 + lane - st_lo].w) : 7;
+        for (int s0 = 0; s0 < total; s0 += CAP) {
+            const int ns = min(CAP, total - s0);
+            __syncwarp();  // wc written; the previous chunk's readers of the slots are done
+            if (lane < 16) wcnt[lane] = 0;
+            // source cell of every staging index of the chunk
+            if (lane < NSRC) {
+                const int2 cc = wc[lane];
+                const int lo = max(cc.x, s0), hi = min(cc.x + n_c, s0 + ns);
+                for (int g = lo; g < hi; ++g) wsrc[g - s0] = (uint8_t)lane;
+            }
+            __syncwarp();
 #pragma unroll 1
-                    for (int g = 0; g < 4; ++g) {
-                        uint32_t gm = __ballot_sync(0xffffffffu, my == g);
-                        if (!gm) continue;
-                        // this lane's row: lane-axis offsets -2 + a + (i, j)
-                        // from the cell; its faces: F offsets -2 + 2 half, +1
-                        const int su = cell[U] + (g & 1) + li, sv = cell[V] + (g >> 1) + lj;
-                        const float gu = (float)(b0[U] - M + su), gv = (float)(b0[V] - M + sv);
-                        double am0 = 0.0, am1 = 0.0, av0 = 0.0, av1 = 0.0;
-                        while (gm) {
-                            const int jj = c0 - st_lo + __ffs(gm) - 1;
-                            gm &= gm - 1;
-                            const float4 P = wslot[jj];
-                            const float4 R = wslot[CAP + jj];
-                            const float m_p = P.w, scale_mom = R.x;
-                            const float du = gu - P.x, dv = gv - P.y;
-                            float hoist0 = 0.0f, hoist1 = 0.0f;
-                            if (DIR == 0) hoist0 = dv * dv + du * du;
-                            else { hoist0 = dv * dv; hoist1 = du * du; }
-                            const uint64_t df = f2_sub(gf2, f2_pack(P.z, P.z));
-                            float d0, d1;
-                            f2_unpack(df, d0, d1);
-                            const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
-                            const uint64_t h02 = f2_pack(hoist0, hoist0);
-                            uint64_t dist;
-                            if (DIR == 0) dist = f2_add(sq, h02);
-                            else if (DIR == 1) dist = f2_add(f2_pack(hoist1, hoist1), f2_add(h02, sq));
-                            else dist = f2_add(f2_pack(hoist1, hoist1), f2_add(sq, h02));
-                            const uint64_t df2 = f2_add(f2_add(dist, df), f2_pack(0.25f, 0.25f));
-                            float e0, e1;
-                            f2_unpack(df2, e0, e1);
-                            const uint64_t tt = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
-                            float w0, w1;
-                            f2_unpack(tt, w0, w1);
-                            uint64_t w = f2_pack(fmaxf(w0, 0.0f), fmaxf(w1, 0.0f));
-                            w = f2_mul(f2_mul(w, w), w);
-                            float tm0, tm1, tv0, tv1;
-                            f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
-                            f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
-                            am0 += (double)tm0;
-                            av0 += (double)tv0;
-                            am1 += (double)tm1;
-                            av1 += (double)tv1;
-                        }
-                        if (deps_pending) wait_deps();
-                        {
-                            int sc[3];
-                            sc[F] = cell[F] + 2 * half;  // faces -2 + 2 half: staging cell[F] + M - 2 + 2 half
-                            sc[U] = su;
-                            sc[V] = sv;
-                            const int si = (sc[2] * W + sc[1]) * W + sc[0];
-                            constexpr int step = F == 0 ? 1 : F == 1 ? W : W * W;
-                            st[si] += am0;
-                            st[WW + si] += av0;
-                            st[si + step] += am1;
-                            st[WW + si + step] += av1;
-                        }
-                        __syncwarp();
-                    }
-                    // the chunk's other particles: lanes take the 5 x 5 rows
-                    // around the cell, faces by the lane bits
-                    uint32_t rm = __ballot_sync(0xffffffffu, my == 4);
-                    while (rm) {
-                        const int jr = __ffs(rm) - 1;
-                        rm &= rm - 1;
-                        if (deps_pending) wait_deps();
-                        const float4 P = wslot[c0 + jr - st_lo];
-                        const float4 R = wslot[CAP + c0 + jr - st_lo];
-                        const uint32_t f_lo = __float_as_uint(R.y), f_hi = __float_as_uint(R.z);
-                        const bool on = lane < WIN * WIN;
-                        const uint32_t lanebit = on ? ((f_lo >> lane) & 1u) : 0u;
-                        const uint32_t fbits = (f_hi >> 24) & (0u - lanebit);
-                        const int su = cell[U] + lane % WIN, sv = cell[V] + lane / WIN;
-                        const float du = (float)(b0[U] - M + su) - P.x, dv = (float)(b0[V] - M + sv) - P.y;
-                        float hoist0 = 0.0f, hoist1 = 0.0f;
-                        if (DIR == 0) hoist0 = dv * dv + du * du;
-                        else { hoist0 = dv * dv; hoist1 = du * du; }
-                        if (on) {
+            for (int k = 0; 32 * k < ns; ++k) {
+                const int s = lane + 32 * k;
+                int code = -1;
+                if (s < ns) {
+                    const int c = wsrc[s];
+                    const int2 cc = wc[c];
+                    const int pl = cc.y + (s0 + s - cc.x);
+                    const uint32_t fb = (uint32_t)(lmask[pl] >> 32);
+                    const float m = a.pm[pl];
+                    const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
+                    // the anchor relative to the tile: source cell c sits at
+                    // (c % 3 - 1, c / 3 % 3 - 1, c / 9) from the tile's first
+                    // anchor; a regular particle's anchor is its cell shifted
+                    // by (s_U, s_V), an irregular one's its cell
+                    const bool regular = fb & 1u;
+                    const int du = c % 3 - 1 + (regular ? (int)((fb >> 1) & 1u) : 0);
+                    const int dv = (c / 3) % 3 - 1 + (regular ? (int)((fb >> 2) & 1u) : 0);
+                    const int df = c / 9;
+                    if ((unsigned)du <= 1u && (unsigned)dv <= 1u)
+                        code = du + 2 * dv + 4 * df + (regular ? 0 : 8);
+                    wp[s] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
+                    wm[s] = m * pv[pl];
+                }
+                wcode[s] = (int8_t)code;
+            }
+            // counting sort of the staging indices by anchor code, stable
+            // (staging order inside a code): ranks by lane inside each
+            // 32-particle group, group counts added in order
+            __syncwarp();
+#pragma unroll 1
+            for (int k = 0; 32 * k < ns; ++k) {
+                const int code = wcode[lane + 32 * k];
+                const uint32_t peers = __match_any_sync(0xffffffffu, code);
+                const int before = code >= 0 ? wcnt[code] : 0;
+                __syncwarp();
+                if (code >= 0 && !(peers & lt)) wcnt[code] = before + __popc(peers);
+                __syncwarp();
+            }
+            {
+                const int c = lane < 16 ? wcnt[lane] : 0;
+                int inc = c;
 #pragma unroll
-                            for (int s = 0; s < WIN; ++s) {
-                                const int sf = cell[F] + s - 1;
-                                if (sf < 0 || sf >= W || !((fbits >> s) & 1u)) continue;
-                                const float df = (float)(b0[F] - M + sf) - P.z;
-                                const float sq = df * df;
-                                float dist;
-                                if (DIR == 0) dist = sq + hoist0;
-                                else if (DIR == 1) dist = hoist1 + (hoist0 + sq);
-                                else dist = hoist1 + (sq + hoist0);
-                                const float df2 = (dist + df) + 0.25f;
-                                float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
-                                w = (w * w) * w;
-                                int sc[3];
-                                sc[F] = sf;
-                                sc[U] = su;
-                                sc[V] = sv;
-                                const int si = (sc[2] * W + sc[1]) * W + sc[0];
-                                st[si] += (double)(w * P.w);
-                                st[WW + si] += (double)(w * R.x);
-                            }
-                        }
-                        __syncwarp();
+                for (int o = 1; o < 16; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += v;
+                }
+                if (lane < 16) {
+                    woff[lane + 1] = inc;
+                    wcnt[lane] = inc - c;  // next free position of each code
+                }
+                if (lane == 0) woff[0] = 0;
+            }
+            __syncwarp();
+#pragma unroll 1
+            for (int k = 0; 32 * k < ns; ++k) {
+                const int code = wcode[lane + 32 * k];
+                const uint32_t peers = __match_any_sync(0xffffffffu, code);
+                const int before = code >= 0 ? wcnt[code] : 0;
+                if (code >= 0) wlist[before + __popc(peers & lt)] = (uint8_t)(lane + 32 * k);
+                __syncwarp();
+                if (code >= 0 && !(peers & lt)) wcnt[code] = before + __popc(peers);
+                __syncwarp();
+            }
+#pragma unroll 1
+            for (int al = 0; al < 8; ++al) {
+                const int beg = woff[al], end = woff[al + 1];
+                if (beg == end) continue;
+                const int du = al & 1, dv = (al >> 1) & 1, df = al >> 2;
+                // staging coordinates of this lane's row and of its first face
+                const int su = 2 * tu + du + li, sv = 2 * tv + dv + lj, sf = 2 * tf + df + 2 * half;
+                const uint64_t guv = f2_pack((float)(b0[U] - M + su), (float)(b0[V] - M + sv));
+                const uint64_t gf2 = f2_pack((float)(b0[F] - M + sf), (float)(b0[F] - M + sf + 1));
+                double am0 = 0.0, am1 = 0.0, av0 = 0.0, av1 = 0.0;
+                // the reference's terms of one particle for this lane's two faces
+                auto terms = [&](int i, float& tm0, float& tm1, float& tv0, float& tv1) {
+                    const float4 P = wp[i];
+                    const float m_p = P.w, scale_mom = wm[i];
+                    float duu, dvv;  // du * du, dv * dv (paired)
+                    {
+                        const uint64_t d2 = f2_sub(guv, f2_pack(P.x, P.y));
+                        f2_unpack(f2_mul(d2, d2), duu, dvv);
+                    }
+                    // p2g.rs:287-325: dz2 = dz*dz; dyz = dz2 + dy*dy; dist_sq = dx*dx + dyz,
+                    // with (dx, dy, dz) = (df, du, dv), (du, df, dv) or (du, dv, df)
+                    float hoist0 = 0.0f, hoist1 = 0.0f;
+                    if (DIR == 0) hoist0 = dvv + duu;
+                    else { hoist0 = dvv; hoist1 = duu; }
+                    const uint64_t dff = f2_sub(gf2, f2_pack(P.z, P.z));
+                    float d0, d1;
+                    f2_unpack(dff, d0, d1);
+                    // products that feed a sum stay scalar: a paired product
+                    // feeding a paired sum may be contracted
+                    const uint64_t sq = f2_pack(d0 * d0, d1 * d1);
+                    const uint64_t h02 = f2_pack(hoist0, hoist0);
+                    uint64_t dist;
+                    if (DIR == 0) dist = f2_add(sq, h02);
+                    else if (DIR == 1) dist = f2_add(f2_pack(hoist1, hoist1), f2_add(h02, sq));
+                    else dist = f2_add(f2_pack(hoist1, hoist1), f2_add(sq, h02));
+                    const uint64_t df2 = f2_add(f2_add(dist, dff), f2_pack(0.25f, 0.25f));
+                    float e0, e1;
+                    f2_unpack(df2, e0, e1);
+                    const uint64_t tt = f2_sub(f2_pack(1.0f, 1.0f), f2_pack(e0 * inv_r2, e1 * inv_r2));
+                    float w0, w1;
+                    f2_unpack(tt, w0, w1);
+                    uint64_t w = f2_pack(fmaxf(w0, 0.0f), fmaxf(w1, 0.0f));
+                    w = f2_mul(f2_mul(w, w), w);
+                    f2_unpack(f2_mul(w, f2_pack(m_p, m_p)), tm0, tm1);
+                    f2_unpack(f2_mul(w, f2_pack(scale_mom, scale_mom)), tv0, tv1);
+                };
+                // two particles per round (independent arithmetic), added in
+                // list order
+                int j = beg;
+#pragma unroll 1
+                for (; j + 1 < end; j += 2) {
+                    const int i1 = wlist[j], i2 = wlist[j + 1];
+                    float a0, a1, a2, a3, c0, c1, c2, c3;
+                    terms(i1, a0, a1, a2, a3);
+                    terms(i2, c0, c1, c2, c3);
+                    am0 += (double)a0;
+                    am1 += (double)a1;
+                    av0 += (double)a2;
+                    av1 += (double)a3;
+                    am0 += (double)c0;
+                    am1 += (double)c1;
+                    av0 += (double)c2;
+                    av1 += (double)c3;
+                }
+                if (j < end) {
+                    float a0, a1, a2, a3;
+                    terms(wlist[j], a0, a1, a2, a3);
+                    am0 += (double)a0;
+                    am1 += (double)a1;
+                    av0 += (double)a2;
+                    av1 += (double)a3;
+                }
+                if (deps_pending) wait_deps();
+                {
+                    int sc[3];
+                    sc[F] = sf;
+                    sc[U] = su;
+                    sc[V] = sv;
+                    const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                    constexpr int step = F == 0 ? 1 : F == 1 ? W : W * W;
+                    st[si] += am0;
+                    st[WW + si] += av0;
+                    st[si + step] += am1;
+                    st[WW + si + step] += av1;
+                }
+                __syncwarp();  // anchors of a tile share faces: order their adds
+            }
+            // irregular particles (codes 8 .. 15, their own cell): lanes take
+            // the 5 x 5 rows around the cell, faces by the lane bits
+#pragma unroll 1
+            for (int j = woff[8]; j < woff[16]; ++j) {
+                if (deps_pending) wait_deps();
+                int al = 8;
+                while (woff[al + 1] <= j) ++al;
+                const int jj = wlist[j];
+                const int2 cc = wc[wsrc[jj]];
+                const int pl = cc.y + (s0 + jj - cc.x);
+                const float4 P = wp[jj];
+                const float smom = wm[jj];
+                const uint64_t fb = lmask[pl];
+                const uint32_t f_lo = (uint32_t)fb, f_hi = (uint32_t)(fb >> 32);
+                int cell[3];  // the particle's cell inside the block
+                cell[U] = 2 * tu + (al & 1);
+                cell[V] = 2 * tv + ((al >> 1) & 1);
+                cell[F] = 2 * tf + ((al >> 2) & 1);
+                const bool on = lane < 25;
+                const uint32_t lanebit = on ? ((f_lo >> lane) & 1u) : 0u;
+                const uint32_t fbits = (f_hi >> 24) & (0u - lanebit);
+                const int su = cell[U] + lane % 5, sv = cell[V] + lane / 5;
+                const float du_ = (float)(b0[U] - M + su) - P.x, dv_ = (float)(b0[V] - M + sv) - P.y;
+                float hoist0 = 0.0f, hoist1 = 0.0f;
+                if (DIR == 0) hoist0 = dv_ * dv_ + du_ * du_;
+                else { hoist0 = dv_ * dv_; hoist1 = du_ * du_; }
+                if (on) {
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) {
+                        const int sf = cell[F] + s - 1;
+                        if (sf < 0 || sf >= W || !((fbits >> s) & 1u)) continue;
+                        const float dff = (float)(b0[F] - M + sf) - P.z;
+                        const float sq = dff * dff;
+                        float dist;
+                        if (DIR == 0) dist = sq + hoist0;
+                        else if (DIR == 1) dist = hoist1 + (hoist0 + sq);
+                        else dist = hoist1 + (sq + hoist0);
+                        const float df2 = (dist + dff) + 0.25f;
+                        float w = fmaxf(1.0f - df2 * inv_r2, 0.0f);
+                        w = (w * w) * w;
+                        int sc[3];
+                        sc[F] = sf;
+                        sc[U] = su;
+                        sc[V] = sv;
+                        const int si = (sc[2] * W + sc[1]) * W + sc[0];
+                        st[si] += (double)(w * P.w);
+                        st[WW + si] += (double)(w * smom);
                     }
                 }
-                p0 = pend;
+                __syncwarp();
             }
         }
         __syncwarp();
@@ -775,28 +892,26 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
 
 template <int BSX>
 __global__ void __launch_bounds__(32 * kSplatR2Warps, 1) p2g_r2_kernel(SplatArgs a) {
-    constexpr int M = 2;
-    constexpr int W = BSX + 2 * M;
-    constexpr int WW = W * W * W;
-    constexpr int T = BSX / 2, K = M + 1, NT = T * T * T;
-    extern __shared__ double st[];  // [2][W^3]: mass, momentum; then per-warp particle slots
+    using S = SplatR2<BSX>;
+    constexpr int WW = S::WW, NA = S::NA, NF = S::NF, NT = S::NT;
+    extern __shared__ double st[];  // [2][W^3]: mass, momentum; then per-warp staging slots
     __shared__ uint32_t s_done[NT];
-    __shared__ uint16_t s_order[NT];
+    __shared__ uint16_t s_order[NT];  // anchor tiles in colour-major order
     __shared__ uint32_t s_next;
     const int tid = threadIdx.x;
     for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
     for (int t = tid; t < NT; t += blockDim.x) {
         s_done[t] = 0;
-        const int tx = t % T, ty = (t / T) % T, tz = t / (T * T);
-        const int cx = tx % K, cy = ty % K, cz = tz % K;
-        const int ci = cx + K * (cy + K * cz);
+        const int tu = t % NA, tv = (t / NA) % NA, tf = t / (NA * NA);
+        const int cu = tu % 3, cv = tv % 3, cf = tf % 3;
+        const int ci = cu + 3 * (cv + 3 * cf);
         int base = 0;
         for (int c = 0; c < ci; ++c) {
-            const int ox = c % K, oy = (c / K) % K, oz = c / (K * K);
-            base += ((T - ox + K - 1) / K) * ((T - oy + K - 1) / K) * ((T - oz + K - 1) / K);
+            const int ou = c % 3, ov = (c / 3) % 3, of = c / 9;
+            base += ((NA - ou + 2) / 3) * ((NA - ov + 2) / 3) * ((NF - of + 2) / 3);
         }
-        const int ntx = (T - cx + K - 1) / K, nty = (T - cy + K - 1) / K;
-        s_order[base + (tx / K) + ntx * ((ty / K) + nty * (tz / K))] = (uint16_t)t;
+        const int nu = (NA - cu + 2) / 3, nv = (NA - cv + 2) / 3;
+        s_order[base + tu / 3 + nu * (tv / 3 + nv * (tf / 3))] = (uint16_t)t;
     }
     if (tid == 0) s_next = 0;
     __syncthreads();
@@ -881,10 +996,8 @@ static void launch_splat_dir(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
 template <int BSX, int M>
 static void launch_splat(msbg_ctx* ctx, const SplatArgs& a, size_t npb) {
     if (M == 2 && a.r_p == 2.0f) {
-        constexpr int W = BSX + 2 * 2;
-        constexpr int T = BSX / 2, NT = T * T * T;
-        constexpr int WARPS = NT < kSplatR2Warps ? NT : kSplatR2Warps;
-        const size_t smem = 2 * sizeof(double) * W * W * W + (size_t)WARPS * 2 * SplatR2Cap<BSX>::v * sizeof(float4);
+        constexpr int WARPS = SplatR2<BSX>::WARPS;
+        const size_t smem = SplatR2<BSX>::smem_bytes;
         static bool attr = false;
         if (!attr) {
             CUDA_CHECK(cudaFuncSetAttribute(p2g_r2_kernel<BSX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -127,6 +127,33 @@ def check_p2g(msbg, ctx, oracle, pos, vel, mass, s, bsx, r_p):
     return mac, got
 
 
+@pytest.mark.parametrize("r_p,bsx,seed", [(2.0, 16, 11), (2.0, 8, 12), (1.5, 16, 13), (3.0, 16, 14)])
+def test_p2g_terms_bit_exact(msbg, ctx, oracle, r_p, bsx, seed):
+    """Particles on a lattice 8 cells apart, so no two footprints share a
+    face: every face sum is a single term, and mass and velocity must equal
+    the reference's own staged splat bit for bit.  This pins each term's f32
+    operation sequence, which the summed comparisons allow an ulp of slack
+    on.  A quarter of the particles have a coordinate exactly on a cell
+    centre or a face plane (the footprints of irregular shape)."""
+    s = 64
+    r = np.random.default_rng(seed)
+    lat = np.arange(8) * 8 + 2
+    pos = np.stack(np.meshgrid(lat, lat, lat, indexing="ij"), -1).reshape(-1, 3).astype(np.float32)
+    pos += r.uniform(0, 1, pos.shape).astype(np.float32)
+    n = len(pos)
+    special = r.choice(n, n // 4, replace=False)
+    ax = r.integers(0, 3, len(special))
+    pos[special, ax] = np.floor(pos[special, ax]) + r.choice(np.array([0.0, 0.5], np.float32), len(special))
+    vel = r.normal(size=(n, 3)).astype(np.float32)
+    mass = r.uniform(0.5, 1.5, n).astype(np.float32)
+    mac = msbg.MacGrid(ctx, s, s, s, bsx)
+    msbg.particles_to_grid(mac, pos, vel, mass, r_p)
+    act = mac.active_blocks()
+    _, want = oracle.p2g(pos, vel, mass, s, s, s, bsx, r_p, active=act.astype(np.int64), normalize=True)
+    got = device_channels(mac, act)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 @pytest.mark.parametrize("n,s,bsx,r_p,seed", [
     (1, 32, 16, 2.0, 1), (500, 32, 16, 2.0, 2), (20000, 64, 16, 2.0, 3), (20000, 64, 16, 1.5, 4),
     (8000, 48, 8, 2.0, 5), (5000, 64, 16, 3.0, 6),
