@@ -493,6 +493,8 @@ def algorithmic_bytes(kernel, n, n_fine, n_active, launches):
     written per face-cell of the active blocks for the combine; 12 B read + 12
     B written per particle for G2P; 24 B per element per onesweep radix pass
     (3 passes per sort)."""
+    if kernel == "sweep_wave_kernel":  # every phase of the SWEEPS sweeps in one launch
+        return 8.0 * n_fine * 4096 * SWEEPS * launches
     if kernel in SWEEP_KERNELS:
         return 8.0 * n_fine * 4096 * SWEEPS * launches / 80
     if kernel == "p2g_cells_kernel":
@@ -531,8 +533,9 @@ INST_PER_UNIT = {"p2g_cells_kernel": 575950823 / 5767168,
                  "p2g_r2_kernel": 1182366633 / 5767168}
 
 
-# The smoother's sweep kernels (one of them runs, by element type and halo).
-SWEEP_KERNELS = ("sweep_compact_kernel", "sweep_pipe_kernel", "sweep_phase_kernel")
+# The smoother's sweep kernels (one of them runs, by element type, halo and
+# active-set size).
+SWEEP_KERNELS = ("sweep_compact_kernel", "sweep_pipe_kernel", "sweep_phase_kernel", "sweep_wave_kernel")
 
 
 def sweep_kernel_time(kern):

@@ -143,7 +143,8 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 // The device status word collects bits from bounded waits that gave up: 1 =
 // an mbarrier wait in a tensor-core kernel, 2 = a radix-sort look-back, 4 = a
-// P2G tile-order wait.  Every such wait gives up after kWaitLimitNs.
+// P2G tile-order wait, 8 = a one-launch sweep's wait for its
+// neighbours.  Every such wait gives up after kWaitLimitNs.
 constexpr uint64_t kWaitLimitNs = 1000000000ull;
 // raise_device_status(ctx, word) clears the word and throws when it is
 // non-zero; check_device_status reads it (synchronising) and does the same.

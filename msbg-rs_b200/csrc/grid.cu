@@ -18,6 +18,7 @@ void raise_device_status(msbg_ctx* ctx, int word) {
     if (word & 1) what += "an mbarrier wait inside a tensor-core kernel";
     if (word & 2) what += std::string(what.empty() ? "" : " and ") + "a radix-sort look-back";
     if (word & 4) what += std::string(what.empty() ? "" : " and ") + "a P2G tile-order wait";
+    if (word & 8) what += std::string(what.empty() ? "" : " and ") + "a sweep's wait for its neighbours";
     MSBG_THROW(MSBG_ERR_TIMEOUT, what + " waited past its time limit and gave up");
 }
 

@@ -98,7 +98,7 @@ struct SweepArgs {
                                 // stencil's two-cell halo, else 1)
     const float* coarse;        // coarse payload (f32) for multiresolution halos
     const int32_t* nbr;         // [n][27]
-    const int32_t* bxyz;        // [n][4]: block coords + flags (bit h-1: interior for halo h)
+    const int32_t* bxyz;        // [n][4]: block coords + flags (bit h-1: interior for halo h; bit 4 + k: neighbour k at the domain edge)
     int32_t sx, sy, sz;
     float empty, full, dt;
     int clamp01;
@@ -277,7 +277,10 @@ __device__ __forceinline__ void sweep_compute(const SweepArgs& a, const float* _
 // scratch arrays [3][HSX].
 template <int BSX> struct Compact;
 
-template <class E, int BSX, int ST, bool COMPACT = false>
+// CG: the block's neighbours may be updated by other CTAs of the same launch
+// (sweep_wave_kernel), so their values are read through L2 (L1 is not
+// coherent across SMs).
+template <class E, int BSX, int ST, bool COMPACT = false, bool CG = false>
 __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const int32_t* nb, int pi, int8_t* ok, int8_t* dd,
                               int8_t* ll) {
     constexpr int HALO = ST == MSBG_BILAPLACIAN ? 2 : 1;
@@ -323,7 +326,8 @@ __device__ void stage_general(const SweepArgs& a, float* __restrict__ h, const i
                 const int c = nb[dd[hx] + 3 * dd[HSX + hy] + 9 * dd[2 * HSX + hz]];
                 const int lx = ll[hx], ly = ll[HSX + hy], lz = ll[2 * HSX + hz];
                 if (c >= 0) {
-                    v = E::load(payload[(size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)))]);
+                    const typename E::T* src = payload + (size_t)c * N + (lx | (ly << LG) | (lz << (2 * LG)));
+                    v = E::load(CG ? __ldcg(src) : *src);
                 } else if (c == kCodeFull) {
                     v = a.full;
                 } else if (c <= kCodeCoarse0) {
@@ -706,7 +710,7 @@ template <int BSX> struct Compact {
 };
 
 // Issues the staging of an interior block (one-cell halo) in the compact layout.
-template <int BSX, int ST, int NT = BSX * BSX>
+template <int BSX, int ST, int NT = BSX * BSX, bool CG = false>
 __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
     using CL = Compact<BSX>;
     constexpr int H = CL::H;
@@ -818,7 +822,9 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
                 const int ly = sy < 0 ? BSX - 1 : 0, hy = sy < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
                 float* d = h + CL::MAIN + side * CL::XS + (j + 1) * CL::XP + 3 + hy;
                 if (c >= 0) {
-                    cp_async4(d, a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly);
+                    const float* src = a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly;
+                    if (CG) *d = __ldcg(src);  // the 4-byte cp.async goes through L1
+                    else cp_async4(d, src);
                 } else if (c <= kCodeCoarse0) {
                     constexpr int CLG = LG - 1;
                     const int lx = sx < 0 ? BSX - 1 : 0;
@@ -1076,6 +1082,161 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     cp_async_wait<0>();
 }
 
+// ---- one-launch sweeps for small active sets -------------------------------
+// Every colour phase of every sweep of a call in one launch.  Items are
+// (sweep t, block) pairs.  A block of colour c reads its neighbours of lower
+// colours after their update in sweep t and those of higher colours before
+// it (the crate's colour order, solver.rs:187-217), so item (t, b) waits
+// until every neighbour it reads or is read by has completed t + 1 sweeps
+// (lower colour) or t sweeps (higher colour), and b itself t sweeps:
+// per-slot progress words, each published after the block's stores.  The
+// host orders the items by (k = 8 t + c + bz, higher bz first, colour-major
+// Morton rank): every item an item waits for comes strictly earlier in that
+// order (a dependency at the same or a lower block layer has a smaller k; one
+// a layer up has k at most equal, and then comes first by its layer), and
+// CTAs claim items from a counter in that order, so a waiting item only waits
+// for items already claimed by running CTAs.  The CTAs flow from phase to
+// phase without the launch gap and tail of a kernel per phase, which is what
+// bounds a phase of a few hundred blocks.  (On large sets the chain of
+// dependent phases inside each block layer makes it slower than a kernel per
+// phase, whose next block's staging always overlaps the current stencil.)
+// The next item's staging is issued while the current block is computed when
+// its neighbours are already done, else after the current block is
+// published.  Blocks other CTAs update are read through L2.  A wait that runs
+// past kWaitLimitNs sets bit 8 of the status word, and every CTA stops at its
+// next wait once the bit is set (after its copies in flight have landed); the
+// sweep is then incomplete and the next call that reads the status word
+// reports it.
+
+// Neighbours (of the 27) a stencil's halo reads: faces for the 7-tap stencil,
+// faces and edges for the 19- and 25-tap ones.
+template <int ST> __device__ __forceinline__ bool reads_neighbour(int k) {
+    const int nout = (k % 3 != 1) + ((k / 3) % 3 != 1) + (k / 9 != 1);
+    return ST == MSBG_LAPLACIAN ? nout == 1 : (nout == 1 || nout == 2);
+}
+
+template <int BSX, int ST, bool CLAMP>
+__global__ void __launch_bounds__(CompactThreads<BSX, ST>::v, BSX == 16 ? 4 : 1)
+sweep_wave_kernel(SweepArgs a, const int2* __restrict__ items, int total, int* prog, unsigned int* counter, int* status) {
+    using CL = Compact<BSX>;
+    constexpr int NT = CompactThreads<BSX, ST>::v;
+    extern __shared__ float4 h4[];
+    float* hb = reinterpret_cast<float*>(h4);
+    __shared__ int32_t nbs[2][27];
+    __shared__ int32_t flg[2], pis[2], col[2], swp[2];
+    __shared__ int itm[2];
+    __shared__ int8_t ok[3][BSX + 2], dd[3][BSX + 2], ll[3][BSX + 2];
+    __shared__ int s_stop;
+    const int tid = threadIdx.x;
+    auto claim = [&](int b) {
+        if (tid == 0) itm[b] = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int w = itm[b];
+        if (w < total) {
+            const int2 it = items[w];
+            if (tid < 27) nbs[b][tid] = a.nbr[(size_t)it.y * 27 + tid];
+            if (tid == NT - 1) {
+                const int32_t* bx = a.bxyz + (size_t)it.y * 4;
+                flg[b] = bx[3];
+                pis[b] = it.y;
+                swp[b] = it.x;
+                col[b] = (bx[0] & 1) | ((bx[1] & 1) << 1) | ((bx[2] & 1) << 2);
+            }
+        }
+        __syncthreads();
+    };
+    // every swept neighbour the block reads or is read by, and the block
+    // itself, has completed the sweeps item b needs: the neighbours the
+    // stencil reads, and any of the 26 when either block lies at the domain
+    // edge (the Neumann rule may reflect an edge block's halo into a diagonal
+    // neighbour, which must then also wait for it)
+    auto ready = [&](int b) -> bool {
+        bool good = true;
+        const int fl = flg[b];
+        if (tid < 27 && (tid == 13 || !(fl & 1) || ((fl >> (4 + tid)) & 1) || reads_neighbour<ST>(tid))) {
+            const int c = nbs[b][tid];
+            if (c >= 0) {
+                const int nc = col[b] ^ ((tid % 3 != 1) | (((tid / 3) % 3 != 1) << 1) | ((tid / 9 != 1) << 2));
+                const int need = nc < col[b] ? swp[b] + 1 : swp[b];
+                good = *(volatile int*)(prog + c) >= need;
+            }
+        }
+        __threadfence();
+        return __syncthreads_and(good) != 0;
+    };
+    // false: a wait gave up (here or in another CTA); the kernel then stops
+    auto wait_ready = [&](int b) -> bool {
+        uint64_t t0 = 0;
+        for (uint32_t spins = 0;; ++spins) {
+            if (ready(b)) return true;
+            if (tid == 0) {
+                int stop = (*(volatile int*)status & 8) ? 1 : 0;
+                if (!stop && (spins & 15u) == 15u) {
+                    const uint64_t now = globaltimer_ns();
+                    if (!t0) t0 = now;
+                    else if (now - t0 > kWaitLimitNs) {
+                        atomicOr(status, 8);
+                        stop = 1;
+                    }
+                }
+                s_stop = stop;
+            }
+            __syncthreads();
+            if (s_stop) return false;
+            __nanosleep(64);
+        }
+    };
+    auto stage = [&](int b) {  // issues (interior) or performs (edge) the staging of item b into buffer b
+        if (flg[b] & 1) issue_compact<BSX, ST, NT, true>(a, hb + b * CL::BUF, nbs[b]);
+        else stage_general<ElemF32, BSX, ST, true, true>(a, hb + b * CL::BUF, nbs[b], pis[b], &ok[0][0], &dd[0][0], &ll[0][0]);
+        cp_async_commit();
+    };
+    claim(0);
+    if (itm[0] >= total) return;
+    if (!wait_ready(0)) return;
+    stage(0);
+    int b = 0;
+    while (true) {
+        const int bn = b ^ 1;
+        claim(bn);
+        const bool more = itm[bn] < total;
+        bool early = false;
+        if (more && ready(bn)) {
+            stage(bn);
+            early = true;
+        } else {
+            cp_async_commit();  // an empty group keeps the wait count uniform
+        }
+        cp_async_wait<1>();  // the current block's copies have landed
+        __syncthreads();
+        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(prog + nbs[b][13], swp[b] + 1);
+        }
+        if (!more) break;
+        if (!early) {
+            if (!wait_ready(bn)) break;  // nothing of bn is in flight
+            stage(bn);
+        }
+        b = bn;
+    }
+    cp_async_wait<0>();
+}
+
+// Progress words of a wave sweep: INT_MAX for every slot (blocks that are
+// not swept never hold anything up), then 0 for the swept blocks.
+__global__ void wave_init_kernel(int* prog, size_t n_slots, unsigned int* counter) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_slots; i += (size_t)gridDim.x * blockDim.x)
+        prog[i] = 0x7fffffff;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
+}
+__global__ void wave_zero_kernel(int* prog, const int32_t* __restrict__ nbr, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) prog[nbr[(size_t)i * 27 + 13]] = 0;
+}
+
 // Copies the outer x-planes (x = 0 .. xd-1 and x = bsx-1 .. bsx-xd) of the
 // listed slots into the side buffer: [slot][plane][z][y].
 template <class E, int BSX>
@@ -1130,6 +1291,75 @@ static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* ord
     begin_launch(ctx);
     sweep_compact_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
     after_launch(ctx, "sweep_compact_kernel");
+}
+
+template <int BSX, int ST, bool CLAMP>
+static void launch_wave(msbg_ctx* ctx, const SweepArgs& a, const int2* items, int total, int* prog, unsigned int* counter) {
+    const size_t smem = 2 * sizeof(float) * Compact<BSX>::BUF;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_wave_kernel<BSX, ST, CLAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_wave_kernel<BSX, ST, CLAMP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+        attr = true;
+    }
+    const int threads = CompactThreads<BSX, ST>::v;
+    int per_sm = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_wave_kernel<BSX, ST, CLAMP>, threads, smem));
+    int sms = 0;
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const int grid = std::max(1, std::min(total, std::max(per_sm, 1) * sms));
+    begin_launch(ctx);
+    sweep_wave_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, items, total, prog, counter,
+                                                                                       ctx->status.as<int>());
+    after_launch(ctx, "sweep_wave_kernel");
+}
+
+template <int BSX>
+static void launch_wave_laplacian(msbg_ctx* ctx, const SweepArgs& a, const int2* items, int total, int* prog,
+                                  unsigned int* counter) {
+    if (a.clamp01) launch_wave<BSX, MSBG_LAPLACIAN, true>(ctx, a, items, total, prog, counter);
+    else launch_wave<BSX, MSBG_LAPLACIAN, false>(ctx, a, items, total, prog, counter);
+}
+
+// The one-launch sweep runs the 7-tap stencil on active sets of at most
+// this many blocks (measured on B200, 10 sweeps: 872 blocks 0.21 against
+// 0.51 ms for a kernel per phase, 3,464 blocks 0.47 against 0.66 ms, 14,248
+// blocks 1.67 against 1.70 ms, 56,056 blocks 6.46 against 4.82 ms; the
+// 19-tap stencil gains nothing measurable at any size).
+constexpr size_t kWaveMaxBlocks = 16384;
+
+// The (sweep, plan index) items of `iterations` sweeps in wavefront order:
+// by 8 t + colour + bz, then the higher bz, then plan index (colour-major
+// Morton rank).
+static void wave_items(SweepPlan* plan, msbg_ctx* ctx, int iterations) {
+    if (plan->wave_iters == iterations) return;
+    const size_t n = plan->n;
+    MSBG_REQUIRE(n < (1u << 24), "too many blocks for a one-launch sweep");
+    MSBG_REQUIRE(iterations < (1 << 20), "too many sweeps for a one-launch sweep");
+    std::vector<std::pair<uint64_t, int2>> keyed;
+    keyed.reserve(n * (size_t)iterations);
+    for (int t = 0; t < iterations; ++t) {
+        for (size_t i = 0; i < n; ++i) {
+            const uint64_t bz = (uint64_t)plan->h_bz[i];
+            MSBG_REQUIRE(bz < (1u << 21), "block layer out of range");
+            const uint64_t k = 8 * (uint64_t)t + plan->h_col[i] + bz;
+            // ties of k: the higher block layer first (a dependency one layer
+            // up can tie with its dependant; one at the same layer or below
+            // never does)
+            keyed.push_back({(k << 21) | ((1u << 21) - 1 - bz), make_int2(t, (int)i)});
+        }
+    }
+    std::sort(keyed.begin(), keyed.end(), [](const std::pair<uint64_t, int2>& x, const std::pair<uint64_t, int2>& y) {
+        return x.first != y.first ? x.first < y.first : x.second.y < y.second.y;
+    });
+    std::vector<int2> items(keyed.size());
+    for (size_t i = 0; i < keyed.size(); ++i) items[i] = keyed[i].second;
+    plan->wave_items.reserve(items.size() * sizeof(int2));
+    CUDA_CHECK(cudaMemcpyAsync(plan->wave_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                               ctx->stream));
+    sync(ctx);
+    plan->wave_iters = iterations;
 }
 
 template <class E, int BSX, int ST>
@@ -1252,7 +1482,20 @@ static SweepPlan* get_plan(msbg_grid* g, msbg_grid* coarse, const uint8_t* level
                           (by + 1) * B + hh <= (int64_t)g->sy && (bz + 1) * B + hh <= (int64_t)g->sz;
                 if (in) fl |= 1 << (hh - 1);
             }
+            // bits 4 + k: neighbour k lies at the domain edge (its halo of one
+            // cell leaves the domain, so the Neumann rule may reflect its reads
+            // into any of its 26 neighbours, this block included)
+            for (int k = 0; k < 27; ++k) {
+                const int64_t B = g->bsx, X = bx + k % 3 - 1, Y = by + (k / 3) % 3 - 1, Z = bz + k / 9 - 1;
+                if (k == 13 || X < 0 || Y < 0 || Z < 0 || X >= (int64_t)g->nx || Y >= (int64_t)g->ny || Z >= (int64_t)g->nz)
+                    continue;
+                const bool in = X * B - 1 >= 0 && Y * B - 1 >= 0 && Z * B - 1 >= 0 && (X + 1) * B + 1 <= (int64_t)g->sx &&
+                                (Y + 1) * B + 1 <= (int64_t)g->sy && (Z + 1) * B + 1 <= (int64_t)g->sz;
+                if (!in) fl |= 1 << (4 + k);
+            }
             bxyz.push_back(fl);
+            plan->h_col.push_back((uint8_t)c);
+            plan->h_bz.push_back((int32_t)bz);
             for (int k = 0; k < 27; ++k) {
                 int64_t X = bx + k % 3 - 1, Y = by + (k / 3) % 3 - 1, Z = bz + k / 9 - 1;
                 int32_t code = kCodeEmpty;
@@ -1356,6 +1599,32 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
         else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
     }
     const int32_t* order = plan->order.as<int32_t>();
+    // the 7-tap stencil on f32 8^3 or 16^3 blocks of a small active set:
+    // every colour phase of every sweep in one launch
+    if (g->dtype == MSBG_F32 && (g->bsx == 8 || g->bsx == 16) && stencil == MSBG_LAPLACIAN && plan->n <= kWaveMaxBlocks) {
+        MSBG_REQUIRE((double)plan->n * iterations < 2147483647.0, "too many (sweep, block) items for one launch");
+        wave_items(plan, g->ctx, iterations);
+        const size_t slots = g->n_slots();
+        if (plan->wave_slots < slots) {
+            plan->wave_prog.reserve(slots * 4 + 256);
+            plan->wave_slots = slots;
+        }
+        int* prog = plan->wave_prog.as<int>();
+        unsigned int* counter = reinterpret_cast<unsigned int*>(plan->wave_prog.as<char>() + ((slots * 4 + 127) & ~size_t(127)));
+        begin_launch(g->ctx);
+        wave_init_kernel<<<(unsigned)std::min<size_t>((slots + 255) / 256 + 1, 148 * 8), 256, 0, g->ctx->stream>>>(prog, slots,
+                                                                                                                 counter);
+        after_launch(g->ctx, "wave_init_kernel");
+        begin_launch(g->ctx);
+        wave_zero_kernel<<<(unsigned)std::min<size_t>((plan->n + 255) / 256, 148 * 8), 256, 0, g->ctx->stream>>>(
+            prog, a.nbr, (int)plan->n);
+        after_launch(g->ctx, "wave_zero_kernel");
+        const int total = (int)(plan->n * (size_t)iterations);
+        const int2* items = plan->wave_items.as<int2>();
+        if (g->bsx == 16) launch_wave_laplacian<16>(g->ctx, a, items, total, prog, counter);
+        else launch_wave_laplacian<8>(g->ctx, a, items, total, prog, counter);
+        return;
+    }
     for (int it = 0; it < iterations; ++it) {
         a.sr_base = pos0 + (uint64_t)it * chunks_per_sweep;
         for (int c = 0; c < 8; ++c) {

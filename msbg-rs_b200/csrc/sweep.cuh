@@ -24,6 +24,16 @@ struct SweepPlan {
     size_t n_xslots = 0;
     DevBuf xface;   // f32 [n_slots][2 xd][bsx^2]: the xd outermost x-planes per side, [z][y]
     size_t xface_slots = 0;  // capacity in slots x xd
+    // One-launch sweeps (sweep_wave_kernel): colour and block-layer
+    // coordinate of every plan index (host), the (sweep, plan index) items in
+    // wavefront order for `wave_iters` sweeps, and the per-slot progress
+    // words with the claim counter behind them.
+    std::vector<uint8_t> h_col;
+    std::vector<int32_t> h_bz;
+    DevBuf wave_items;  // int2 [n * wave_iters]
+    int wave_iters = -1;
+    DevBuf wave_prog;   // int32 [slots], then the counter
+    size_t wave_slots = 0;
 };
 
 }  // namespace msbg

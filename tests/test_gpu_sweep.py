@@ -61,6 +61,19 @@ SWEEP_CASES = [
 ]
 
 
+def test_sweep_laplacian_large_active_set(msbg, ctx, oracle):
+    """The 7-tap stencil on more than 16,384 active blocks runs a kernel per
+    colour phase (smaller sets run every phase in one launch): bit-exact
+    against the oracle, on a domain whose last block layer is partial."""
+    host = random_sparse(msbg, 260, 256, 256, 8, 0.55, 31, empty=0.1, full=0.9)
+    active = sorted(host.blocks)
+    assert len(active) > 16384
+    dev = run_device(msbg, ctx, host, active, 0, 0.05, 2, False)
+    oracle.sweep(host, active, 0, 0.05, 2, False)
+    ids = np.array(active)[np.random.default_rng(2).choice(len(active), 2000, replace=False)]
+    assert_same_blocks(dev, host, np.sort(ids))
+
+
 @pytest.mark.parametrize("case", SWEEP_CASES)
 @pytest.mark.parametrize("stencil", [0, 1, 2])
 @pytest.mark.parametrize("clamp", [False, True])
