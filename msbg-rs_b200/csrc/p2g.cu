@@ -551,7 +551,7 @@ template <int BSX> struct SplatR2 {
     static constexpr int CAP = 192;
     // per warp: CAP x (float4 position/mass, float momentum, u8 anchor-sorted
     // index), source cells (int2), 17 anchor-range offsets and 16 counters
-    static constexpr size_t warp_bytes = (size_t)CAP * (16 + 4 + 1 + 1 + 1) + NSRC * 8 + 17 * 4 + 16 * 4;
+    static constexpr size_t warp_bytes = (size_t)CAP * (16 + 4 + 1 + 1 + 1 + 1) + NSRC * 8 + 17 * 4 + 16 * 4;
     static constexpr size_t smem_bytes = 2 * sizeof(double) * WW + (size_t)WARPS * ((warp_bytes + 15) / 16 * 16);
     static_assert(NT < 0xffff, "tile indices must fit 16 bits");
     static_assert(CAP <= 256 && CAP % 32 == 0, "staging indices must fit a byte");
@@ -566,11 +566,12 @@ __device__ __forceinline__ uint32_t morton4(uint32_t x, uint32_t y, uint32_t z) 
 
 template <int BSX, int DIR>
 __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb, double* st, uint32_t* s_done,
-                                              const uint16_t* s_order, uint32_t* s_next) {
+                                              const uint16_t* s_order, uint32_t* s_next, const uint32_t (*s_dep)[4]) {
     using S = SplatR2<BSX>;
     constexpr int M = 2, W = S::W, WW = S::WW, NA = S::NA, NF = S::NF, NT = S::NT, CAP = S::CAP, NSRC = S::NSRC;
     constexpr int NNB = 125, NR = (NNB + 31) / 32;  // tile offsets in [-2, 2]^3, NR of them per lane
     constexpr int F = DIR, U = DIR == 0 ? 1 : 0, V = DIR == 2 ? 1 : 2;
+    constexpr int kStride[3] = {1, W, W * W};  // window index step per axis
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     char* const wbase = reinterpret_cast<char*>(st + 2 * WW) + (size_t)warp * ((S::warp_bytes + 15) / 16 * 16);
     float4* const wp = reinterpret_cast<float4*>(wbase);                    // U, V, F coordinates - 0.5, mass
@@ -581,6 +582,7 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
     uint8_t* const wlist = reinterpret_cast<uint8_t*>(wcnt + 16);           // staging indices by anchor code
     int8_t* const wcode = reinterpret_cast<int8_t*>(wlist + CAP);            // anchor code per staging index
     uint8_t* const wsrc = reinterpret_cast<uint8_t*>(wcode + CAP);          // source cell per staging index
+    uint8_t* const wrank = wsrc + CAP;                                      // rank inside its anchor code
     const uint64_t key = a.pb_key[k_pb];
     const int32_t b0[3] = {(int32_t)compact3(key) * BSX, (int32_t)compact3(key >> 1) * BSX,
                            (int32_t)compact3(key >> 2) * BSX};
@@ -593,6 +595,14 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
     // this lane's footprint row inside an anchor, (i, j) along (U, V), and
     // which two of the anchor's four faces along F it evaluates
     const int li = lane & 3, lj = (lane >> 2) & 3, half = lane >> 4;
+    // this lane's tile offsets o = lane + 32 k in [-2, 2]^3, packed (ou + 2,
+    // ov + 2, of + 2)
+    uint32_t opk[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        const int o = lane + 32 * k;
+        opk[k] = (uint32_t)(o % 5) | ((uint32_t)((o / 5) % 5) << 8) | ((uint32_t)(o / 25) << 16);
+    }
     while (true) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(s_next, 1u);
@@ -632,10 +642,11 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
         for (int k = 0; k < (NR + 1) / 2; ++k) nbi[k] = 0xffffffffu;
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
-            const int o = lane + 32 * k;
-            const int nu = tu + o % 5 - 2, nv = tv + (o / 5) % 5 - 2, nf = tf + o / 25 - 2;
-            const bool dep = o < NNB && nu >= 0 && nv >= 0 && nf >= 0 && nu < NA && nv < NA && nf < NF &&
-                             nu % 3 + 3 * (nv % 3 + 3 * (nf % 3)) < ci;
+            // offsets of lower colour (per colour class, precomputed), inside the tile grid
+            const bool lower = (s_dep[ci][k] >> lane) & 1u;
+            const int nu = tu + (int)(opk[k] & 0xffu) - 2, nv = tv + (int)((opk[k] >> 8) & 0xffu) - 2,
+                      nf = tf + (int)(opk[k] >> 16) - 2;
+            const bool dep = lower && (unsigned)nu < (unsigned)NA && (unsigned)nv < (unsigned)NA && (unsigned)nf < (unsigned)NF;
             if (dep) nbi[k >> 1] &= ~(0xffffu << (16 * (k & 1))) | ((uint32_t)(nu + NA * (nv + NA * nf)) << (16 * (k & 1)));
         }
         bool deps_pending = true;
@@ -667,6 +678,13 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
             __threadfence_block();
             deps_pending = false;
         };
+        // staging coordinates of this lane's row and first face for the
+        // tile's first anchor, their global coordinates in f32, and the
+        // window index
+        const int su0 = 2 * tu + li, sv0 = 2 * tv + lj, sf0 = 2 * tf + 2 * half;
+        const uint64_t guv0 = f2_pack((float)(b0[U] - M + su0), (float)(b0[V] - M + sv0));
+        const uint64_t gf20 = f2_pack((float)(b0[F] - M + sf0), (float)(b0[F] - M + sf0 + 1));
+        const int si0 = su0 * kStride[U] + sv0 * kStride[V] + sf0 * kStride[F];
         for (int s0 = 0; s0 < total; s0 += CAP) {
             const int ns = min(CAP, total - s0);
             __syncwarp();  // wc written; the previous chunk's readers of the slots are done
@@ -678,17 +696,28 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 for (int g = lo; g < hi; ++g) wsrc[g - s0] = (uint8_t)lane;
             }
             __syncwarp();
-#pragma unroll 1
-            for (int k = 0; 32 * k < ns; ++k) {
+            // the anchor code of every staging index (from the lane-mask
+            // shape bits alone) and its rank among the chunk's particles of
+            // that code (staging order: ranks by lane inside each group of
+            // 32, group counts added in order)
+            uint32_t fbk[CAP / 32];  // shape bits of the lane masks, all loads issued at once
+#pragma unroll
+            for (int k = 0; k < CAP / 32; ++k) {
+                const int s = lane + 32 * k;
+                fbk[k] = 0;
+                if (s < ns) {
+                    const int2 cc = wc[wsrc[s]];
+                    fbk[k] = (uint32_t)(lmask[cc.y + (s0 + s - cc.x)] >> 32);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < CAP / 32; ++k) {
+                if (32 * k >= ns) break;
                 const int s = lane + 32 * k;
                 int code = -1;
                 if (s < ns) {
                     const int c = wsrc[s];
-                    const int2 cc = wc[c];
-                    const int pl = cc.y + (s0 + s - cc.x);
-                    const uint32_t fb = (uint32_t)(lmask[pl] >> 32);
-                    const float m = a.pm[pl];
-                    const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
+                    const uint32_t fb = fbk[k];
                     // the anchor relative to the tile: source cell c sits at
                     // (c % 3 - 1, c / 3 % 3 - 1, c / 9) from the tile's first
                     // anchor; a regular particle's anchor is its cell shifted
@@ -696,23 +725,12 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                     const bool regular = fb & 1u;
                     const int du = c % 3 - 1 + (regular ? (int)((fb >> 1) & 1u) : 0);
                     const int dv = (c / 3) % 3 - 1 + (regular ? (int)((fb >> 2) & 1u) : 0);
-                    const int df = c / 9;
-                    if ((unsigned)du <= 1u && (unsigned)dv <= 1u)
-                        code = du + 2 * dv + 4 * df + (regular ? 0 : 8);
-                    wp[s] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
-                    wm[s] = m * pv[pl];
+                    if ((unsigned)du <= 1u && (unsigned)dv <= 1u) code = du + 2 * dv + 4 * (c / 9) + (regular ? 0 : 8);
                 }
-                wcode[s] = (int8_t)code;
-            }
-            // counting sort of the staging indices by anchor code, stable
-            // (staging order inside a code): ranks by lane inside each
-            // 32-particle group, group counts added in order
-            __syncwarp();
-#pragma unroll 1
-            for (int k = 0; 32 * k < ns; ++k) {
-                const int code = wcode[lane + 32 * k];
                 const uint32_t peers = __match_any_sync(0xffffffffu, code);
                 const int before = code >= 0 ? wcnt[code] : 0;
+                wcode[s] = (int8_t)code;
+                wrank[s] = (uint8_t)(before + __popc(peers & lt));
                 __syncwarp();
                 if (code >= 0 && !(peers & lt)) wcnt[code] = before + __popc(peers);
                 __syncwarp();
@@ -725,32 +743,33 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                     const int v = __shfl_up_sync(0xffffffffu, inc, o);
                     if (lane >= o) inc += v;
                 }
-                if (lane < 16) {
-                    woff[lane + 1] = inc;
-                    wcnt[lane] = inc - c;  // next free position of each code
-                }
+                if (lane < 16) woff[lane + 1] = inc;
                 if (lane == 0) woff[0] = 0;
             }
             __syncwarp();
-#pragma unroll 1
-            for (int k = 0; 32 * k < ns; ++k) {
-                const int code = wcode[lane + 32 * k];
-                const uint32_t peers = __match_any_sync(0xffffffffu, code);
-                const int before = code >= 0 ? wcnt[code] : 0;
-                if (code >= 0) wlist[before + __popc(peers & lt)] = (uint8_t)(lane + 32 * k);
-                __syncwarp();
-                if (code >= 0 && !(peers & lt)) wcnt[code] = before + __popc(peers);
-                __syncwarp();
+            // the tile's own particles into their anchor-sorted slots
+#pragma unroll 2
+            for (int s = lane; s < ns; s += 32) {
+                const int code = wcode[s];
+                if (code < 0) continue;
+                const int dst = woff[code] + wrank[s];
+                const int2 cc = wc[wsrc[s]];
+                const int pl = cc.y + (s0 + s - cc.x);
+                const float m = a.pm[pl];
+                const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
+                wp[dst] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
+                wm[dst] = m * pv[pl];
+                wlist[dst] = (uint8_t)s;
             }
+            __syncwarp();
 #pragma unroll 1
             for (int al = 0; al < 8; ++al) {
                 const int beg = woff[al], end = woff[al + 1];
                 if (beg == end) continue;
                 const int du = al & 1, dv = (al >> 1) & 1, df = al >> 2;
-                // staging coordinates of this lane's row and of its first face
-                const int su = 2 * tu + du + li, sv = 2 * tv + dv + lj, sf = 2 * tf + df + 2 * half;
-                const uint64_t guv = f2_pack((float)(b0[U] - M + su), (float)(b0[V] - M + sv));
-                const uint64_t gf2 = f2_pack((float)(b0[F] - M + sf), (float)(b0[F] - M + sf + 1));
+                // this lane's row and first face (exact small integers in f32)
+                const uint64_t guv = f2_add(guv0, f2_pack((float)du, (float)dv));
+                const uint64_t gf2 = f2_add(gf20, f2_pack((float)df, (float)df));
                 double am0 = 0.0, am1 = 0.0, av0 = 0.0, av1 = 0.0;
                 // the reference's terms of one particle for this lane's two faces
                 auto terms = [&](int i, float& tm0, float& tm1, float& tv0, float& tv1) {
@@ -793,10 +812,9 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 int j = beg;
 #pragma unroll 1
                 for (; j + 1 < end; j += 2) {
-                    const int i1 = wlist[j], i2 = wlist[j + 1];
                     float a0, a1, a2, a3, c0, c1, c2, c3;
-                    terms(i1, a0, a1, a2, a3);
-                    terms(i2, c0, c1, c2, c3);
+                    terms(j, a0, a1, a2, a3);
+                    terms(j + 1, c0, c1, c2, c3);
                     am0 += (double)a0;
                     am1 += (double)a1;
                     av0 += (double)a2;
@@ -808,7 +826,7 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 }
                 if (j < end) {
                     float a0, a1, a2, a3;
-                    terms(wlist[j], a0, a1, a2, a3);
+                    terms(j, a0, a1, a2, a3);
                     am0 += (double)a0;
                     am1 += (double)a1;
                     av0 += (double)a2;
@@ -816,12 +834,8 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 }
                 if (deps_pending) wait_deps();
                 {
-                    int sc[3];
-                    sc[F] = sf;
-                    sc[U] = su;
-                    sc[V] = sv;
-                    const int si = (sc[2] * W + sc[1]) * W + sc[0];
-                    constexpr int step = F == 0 ? 1 : F == 1 ? W : W * W;
+                    const int si = si0 + du * kStride[U] + dv * kStride[V] + df * kStride[F];
+                    constexpr int step = kStride[F];
                     st[si] += am0;
                     st[WW + si] += av0;
                     st[si + step] += am1;
@@ -836,11 +850,11 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 if (deps_pending) wait_deps();
                 int al = 8;
                 while (woff[al + 1] <= j) ++al;
-                const int jj = wlist[j];
+                const int jj = wlist[j];  // staging index
                 const int2 cc = wc[wsrc[jj]];
                 const int pl = cc.y + (s0 + jj - cc.x);
-                const float4 P = wp[jj];
-                const float smom = wm[jj];
+                const float4 P = wp[j];
+                const float smom = wm[j];
                 const uint64_t fb = lmask[pl];
                 const uint32_t f_lo = (uint32_t)fb, f_hi = (uint32_t)(fb >> 32);
                 int cell[3];  // the particle's cell inside the block
@@ -897,9 +911,22 @@ __global__ void __launch_bounds__(32 * kSplatR2Warps, 1) p2g_r2_kernel(SplatArgs
     extern __shared__ double st[];  // [2][W^3]: mass, momentum; then per-warp staging slots
     __shared__ uint32_t s_done[NT];
     __shared__ uint16_t s_order[NT];  // anchor tiles in colour-major order
+    __shared__ uint32_t s_dep[27][4];  // per colour class: the tile offsets in [-2, 2]^3 of lower colour
     __shared__ uint32_t s_next;
     const int tid = threadIdx.x;
     for (int i = tid; i < 2 * WW; i += blockDim.x) st[i] = 0.0;
+    for (int i = tid; i < 27 * 4; i += blockDim.x) {
+        const int ci = i / 4, k = i % 4;
+        const int cu = ci % 3, cv = (ci / 3) % 3, cf = ci / 9;
+        uint32_t m = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int o = l + 32 * k;
+            if (o >= 125) break;
+            const int nu = cu + 3 + o % 5 - 2, nv = cv + 3 + (o / 5) % 5 - 2, nf = cf + 3 + o / 25 - 2;
+            if (nu % 3 + 3 * (nv % 3 + 3 * (nf % 3)) < ci) m |= 1u << l;
+        }
+        s_dep[ci][k] = m;
+    }
     for (int t = tid; t < NT; t += blockDim.x) {
         s_done[t] = 0;
         const int tu = t % NA, tv = (t / NA) % NA, tf = t / (NA * NA);
@@ -917,9 +944,9 @@ __global__ void __launch_bounds__(32 * kSplatR2Warps, 1) p2g_r2_kernel(SplatArgs
     __syncthreads();
     const int k_pb = blockIdx.x / 3;
     switch (blockIdx.x % 3) {
-        case 0: splat_r2_body<BSX, 0>(a, k_pb, st, s_done, s_order, &s_next); break;
-        case 1: splat_r2_body<BSX, 1>(a, k_pb, st, s_done, s_order, &s_next); break;
-        default: splat_r2_body<BSX, 2>(a, k_pb, st, s_done, s_order, &s_next); break;
+        case 0: splat_r2_body<BSX, 0>(a, k_pb, st, s_done, s_order, &s_next, s_dep); break;
+        case 1: splat_r2_body<BSX, 1>(a, k_pb, st, s_done, s_order, &s_next, s_dep); break;
+        default: splat_r2_body<BSX, 2>(a, k_pb, st, s_done, s_order, &s_next, s_dep); break;
     }
 }
 
