@@ -47,7 +47,7 @@ phasefield: the full phase-field FLIP step on a 512^3 domain of 16^3 blocks:
   a sphere of radius 0.3 * 512 perturbed by 3-octave value noise (amplitude
   10 cells), 4 levels by distance to the surface, 8 particles per cell in a
   band of width 24 (52.8 M particles), a BF16 phase field on the level-0
-  blocks.  One step = Morton sort + permute, P2G, 10 sweeps of the 25-tap
+  blocks.  One step = Morton sort, P2G, 10 sweeps of the 25-tap
   smoother on the BF16 phase field, divergence, pressure solve to 1e-6
   (learned V-cycle/network/V-cycle CG, timed beside MG-PCG and plain MG),
   G2P + blend.  The BF16 storage error is stated against the same sweeps
@@ -223,7 +223,7 @@ def run_ours(args, world, rank, local):
     fine_set = None
     state = {}
 
-    def step(events=None, after_permute=None, before_blend=None):
+    def step(p=pos, v=vel, m=mass, events=None, before_blend=None):
         def mark(name):
             if events is not None:
                 e = torch.cuda.Event(enable_timing=True)
@@ -231,12 +231,13 @@ def run_ours(args, world, rank, local):
                 events.append((name, e))
 
         mark("start")
-        call("msbg_morton_sort_device", ctx.handle, ptr(pos), n, ptr(keys), ptr(perm))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(pos), ptr(spos))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(vel), ptr(svel))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 1, ptr(mass), ptr(smass))
-        if after_permute is not None:
-            after_permute()  # pos, vel and mass are not read again in this step
+        call("msbg_morton_sort_device", ctx.handle, ptr(p), n, ptr(keys), ptr(perm))
+        # the particles into Morton order: the splat's gather and G2P then read
+        # them in cell order (measured: gathering through the permutation
+        # inside P2G and G2P in the caller's order cost 0.6 ms more a step)
+        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(p), ptr(spos))
+        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(v), ptr(svel))
+        call("msbg_permute_device", ctx.handle, ptr(perm), n, 1, ptr(m), ptr(smass))
         mark("sort")
         msbg.particles_to_grid_sorted_device(mac, spos, svel, smass, keys, n, R_P)
         mark("p2g")
@@ -269,7 +270,7 @@ def run_ours(args, world, rank, local):
     t0.record(stream)
     for _ in range(args.steps):
         ev = []
-        step(ev)
+        step(events=ev)
         all_events.append(ev)
     t1.record(stream)
     ctx.synchronize()
@@ -297,47 +298,48 @@ def run_ours(args, world, rank, local):
     pin_out = torch.empty((n, 3), dtype=torch.float32).pin_memory()
     # Every step copies its inputs from pinned host memory and reads its new
     # velocities back.  The copies run on two copy streams, overlapped with
-    # the device work: the next step's inputs go up as soon as this step's
-    # permutes have read pos, vel and mass, and this step's result comes down
-    # while the next step runs (its blend waits for that read).  The library's
-    # own small reads (status words, counts) bypass the copy engines, so they
-    # do not wait behind these transfers.
+    # the device work: the inputs are double-buffered, so the next step's
+    # inputs go up while this step runs (into the buffers the previous step
+    # has finished with), and this step's result comes down while the next
+    # step runs (its blend waits for that read).  The library's own small
+    # reads (status words, counts) bypass the copy engines, so they do not
+    # wait behind these transfers.
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e2e_steps = max(1, min(args.steps, 10))
     up = torch.cuda.Stream(device=dev)
     down = torch.cuda.Stream(device=dev)
     held = {}
+    sets = [(pos, vel, mass), (torch.empty_like(pos), torch.empty_like(vel), torch.empty_like(mass))]
 
-    def upload():
+    def upload(k):
         with torch.cuda.stream(up):
-            pos.copy_(pin_pos, non_blocking=True)
-            vel.copy_(pin_vel, non_blocking=True)
-            mass.copy_(pin_mass, non_blocking=True)
+            p_, v_, m_ = sets[k % 2]
+            p_.copy_(pin_pos, non_blocking=True)
+            v_.copy_(pin_vel, non_blocking=True)
+            m_.copy_(pin_mass, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(up)
-        held["inputs"] = ev
+        held[("inputs", k)] = ev
 
     e0.record(stream)
     up.wait_event(e0)
-    upload()
+    upload(0)
     for i in range(e2e_steps):
-        stream.wait_event(held["inputs"])
-
-        def after_permute(i=i):
-            if i + 1 < e2e_steps:
-                pe = torch.cuda.Event()
-                pe.record(stream)
-                up.wait_event(pe)
-                upload()
+        stream.wait_event(held[("inputs", i)])
+        if i + 1 < e2e_steps:
+            if "done" in held:
+                up.wait_event(held["done"])  # step i - 1 is done with the buffers of step i + 1
+            upload(i + 1)
 
         def before_blend():
             if "read" in held:
                 stream.wait_event(held["read"])
 
-        step(after_permute=after_permute, before_blend=before_blend)
+        step(*sets[i % 2], before_blend=before_blend)
         oe = torch.cuda.Event()
         oe.record(stream)
+        held["done"] = oe
         down.wait_event(oe)
         with torch.cuda.stream(down):
             pin_out.copy_(u_new, non_blocking=True)
@@ -427,7 +429,7 @@ def run_ours(args, world, rank, local):
                 "pipelined_device_api": {
                     "value": world * n / (e2e_ms * 1e-3), "ms_per_step": e2e_ms,
                     "copies": "the same bytes on two torch copy streams, overlapped with the device work of "
-                              "neighbouring steps (identical inputs every step)"}},
+                              "neighbouring steps (double-buffered inputs; identical inputs every step)"}},
         "gpu_launches": launches,
         "phases_ms": {k: round(v, 4) for k, v in phase_ms.items()},
         "kernels_ms_per_step": {k: round(v[1] / prof_steps, 4) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])},
@@ -440,7 +442,7 @@ def run_ours(args, world, rank, local):
         # the other two parts of the metric, on their own configurations:
         # smoother GB/s on the 2048^3 shell and the pressure solve's time to
         # 1e-6 (plain MG, MG-PCG, learned PCG) on the 256^3 layout
-        del pos, vel, mass, keys, perm, spos, svel, smass, u, u_new
+        del pos, vel, mass, keys, perm, spos, svel, smass, u, u_new, sets
         mac.close()
         coarse.close()
         torch.cuda.empty_cache()
@@ -1139,7 +1141,6 @@ def run_phasefield(args, world, rank, local):
     mass = torch.from_numpy(pf.mass).to(dev)
     keys = torch.empty(n, dtype=torch.int64, device=dev)
     perm = torch.empty(n, dtype=torch.int32, device=dev)
-    spos, svel, smass = torch.empty_like(pos), torch.empty_like(vel), torch.empty_like(mass)
     u, u_new = torch.empty_like(vel), torch.empty_like(vel)
     mac = msbg.MacGrid(ctx, size, size, size, 16)
     sampler = msbg.MacSampler(mac, msbg.CLAMP)
@@ -1172,10 +1173,7 @@ def run_phasefield(args, world, rank, local):
 
         mark("start")
         call("msbg_morton_sort_device", ctx.handle, ptr(pos), n, ptr(keys), ptr(perm))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(pos), ptr(spos))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 3, ptr(vel), ptr(svel))
-        call("msbg_permute_device", ctx.handle, ptr(perm), n, 1, ptr(mass), ptr(smass))
-        msbg.particles_to_grid_sorted_device(mac, spos, svel, smass, keys, n, R_P)
+        msbg.particles_to_grid_permuted_device(mac, pos, vel, mass, keys, perm, n, R_P)
         mark("p2g")
         sweeper.sweep(fine_h, msbg.Stencil.BiLaplacian, params)
         mark("phase")
@@ -1185,8 +1183,8 @@ def run_phasefield(args, world, rank, local):
         x.zero_()
         it, rel, _ = P.solve_device(x, b, method=method, tol=1e-6, max_iter=400)
         mark("pressure")
-        sampler.sample_device(spos, n, u)
-        msbg.g2p_blend_device(ctx, svel, u, u, n, ALPHA, u_new)
+        sampler.sample_device(pos, n, u)
+        msbg.g2p_blend_device(ctx, vel, u, u, n, ALPHA, u_new)
         mark("g2p")
         return it, rel
 

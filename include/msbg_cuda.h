@@ -259,6 +259,14 @@ int msbg_p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const
  * result is identical to msbg_p2g_device on the same particles. */
 int msbg_p2g_sorted_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass,
                            const uint64_t* d_keys, size_t n, float r_p, size_t* n_active_out);
+/* particles_to_grid for particles in the caller's order with the result of a
+ * Morton sort of their positions (msbg_morton_sort_device: d_keys sorted,
+ * d_perm[i] the caller index of sorted particle i).  The gather into the
+ * splat's cell-sorted arrays follows d_perm, so the particle arrays need not
+ * be permuted first.  The result is identical to msbg_p2g_device on the same
+ * particles (fluid/p2g.rs:141-164 buckets the particles itself). */
+int msbg_p2g_permuted_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass,
+                             const uint64_t* d_keys, const uint32_t* d_perm, size_t n, float r_p, size_t* n_active_out);
 /* Active block set of the last P2G (ascending bids). */
 int msbg_mac_active_blocks(const msbg_mac* mac, uint64_t* out, size_t cap, size_t* n_out);
 /* MacGrid::normalize_velocity (mac.rs:106-132) over the listed blocks. */
@@ -374,7 +382,7 @@ int msbg_place_instances(msbg_ctx* ctx, const float* base, size_t n_base, const 
 int msbg_flip_create(msbg_mac* mac, msbg_grid* coarse, const uint8_t* levels, size_t n_levels, msbg_flip** out);
 int msbg_flip_destroy(msbg_flip* f);
 /* One step: pos, vel ([n][3] f32) and mass ([n]) are copied up; the particles
- * are Morton-sorted (msbg_morton_sort_device), splatted (msbg_p2g_sorted_device,
+ * are Morton-sorted (msbg_morton_sort_device), splatted (msbg_p2g_permuted_device,
  * r_p), the x-face mass is smoothed by `sweeps` multires sweeps of `stencil`
  * (dt) over the level-0 blocks of the new active set, velocities are sampled
  * back (Clamp) and blended (alpha), and vel_out[i] ([n][3], host) receives the

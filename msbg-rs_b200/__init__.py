@@ -16,7 +16,8 @@ from .grid import Context, HostGrid, SparseGrid
 from .solver import Fence, PdeParams, Stencil, Sweeper, apply_pde
 from .particles import BucketPlan, bucket_indices, morton3, morton3_host, morton_sort, sort_block_list_morton
 from .fluid import (FlipStep, MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend_device, particles_to_grid,
-                    particles_to_grid_device, particles_to_grid_sorted_device)
+                    particles_to_grid_device, particles_to_grid_sorted_device,
+                    particles_to_grid_permuted_device)
 from .multires import downsample_channel_avg
 from .sampler import CELL_CENTERED, CORNER, CUBIC_BSPLINE, LINEAR, Sampler
 from . import surface
@@ -33,7 +34,7 @@ __all__ = [
     "Context", "HostGrid", "SparseGrid", "Fence", "PdeParams", "Stencil", "Sweeper", "apply_pde",
     "BucketPlan", "bucket_indices", "morton3", "morton3_host", "morton_sort", "sort_block_list_morton",
     "FlipStep", "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
-    "particles_to_grid_device", "particles_to_grid_sorted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
+    "particles_to_grid_device", "particles_to_grid_sorted_device", "particles_to_grid_permuted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
     "surface", "SurfaceConfig", "reconstruct_and_smooth", "Sampler", "LINEAR", "CUBIC_BSPLINE", "CORNER", "CELL_CENTERED",
     "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch", "BlockMap",
 ]

@@ -88,6 +88,7 @@ SIGNATURES = {
     "msbg_p2g": [_P, _P, _P, _P, _SZ, _F, _SZP],
     "msbg_p2g_device": [_P, _P, _P, _P, _SZ, _F, _SZP],
     "msbg_p2g_sorted_device": [_P, _P, _P, _P, _P, _SZ, _F, _SZP],
+    "msbg_p2g_permuted_device": [_P, _P, _P, _P, _P, _P, _SZ, _F, _SZP],
     "msbg_mac_active_blocks": [_P, _P, _SZ, _SZP],
     "msbg_mac_normalize_velocity": [_P, _P, _SZ],
     "msbg_mac_divergence": [_P, _P, _P, _SZ],

@@ -6,10 +6,11 @@
 //
 // The step keeps its device arrays between calls (sized for the largest n
 // seen).  The positions go up first on the context stream; the velocities and
-// masses go up on a second stream while the positions are sorted, and the
-// sort's permutation is applied to them once they have arrived.  The new
-// velocities are scattered back to the caller's particle order on the device,
-// so vel_out[i] belongs to input particle i.
+// masses go up on a second stream while the positions are sorted.  P2G reads
+// the particles in the caller's order through the sort's permutation
+// (msbg_p2g_permuted_device), and G2P and the blend run in the caller's
+// order, so vel_out[i] belongs to input particle i and no particle array is
+// ever permuted.
 #include <algorithm>
 
 #include "mac.cuh"
@@ -96,20 +97,15 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
     if (n > f->cap) {
         sync(ctx);
         f->buf.release();
-        f->buf.reserve(8 * b3 + 2 * b1 + b8 + b1);
+        f->buf.reserve(4 * b3 + 2 * b1 + b8);
         f->cap = n;
     }
     char* p = (char*)f->buf.p;
     float* d_pos = (float*)p;  p += b3;
     float* d_vel = (float*)p;  p += b3;
-    float* s_pos = (float*)p;  p += b3;
-    float* s_vel = (float*)p;  p += b3;
     float* d_u = (float*)p;    p += b3;
-    p += b3;  // spare
     float* d_out = (float*)p;  p += b3;
-    p += b3;  // spare row buffer (keeps the layout 256-byte aligned for any n)
     float* d_mass = (float*)p; p += b1;
-    float* s_mass = (float*)p; p += b1;
     uint64_t* keys = (uint64_t*)p; p += b8;
     uint32_t* perm = (uint32_t*)p;
     // positions on the context stream; velocities and masses beside the sort
@@ -120,11 +116,8 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
     CUDA_CHECK(cudaMemcpyAsync(d_mass, mass, n * 4, cudaMemcpyHostToDevice, f->up));
     CUDA_CHECK(cudaEventRecord(f->uploaded, f->up));
     check(msbg_morton_sort_device(ctx, d_pos, n, keys, perm));
-    check(msbg_permute_device(ctx, perm, n, 3, d_pos, s_pos));
     CUDA_CHECK(cudaStreamWaitEvent(ctx->stream, f->uploaded, 0));
-    check(msbg_permute_device(ctx, perm, n, 3, d_vel, s_vel));
-    check(msbg_permute_device(ctx, perm, n, 1, d_mass, s_mass));
-    check(msbg_p2g_sorted_device(f->mac, s_pos, s_vel, s_mass, keys, n, r_p, nullptr));
+    check(msbg_p2g_permuted_device(f->mac, d_pos, d_vel, d_mass, keys, perm, n, r_p, nullptr));
     // smooth the x-face mass over the level-0 blocks of the new active set,
     // halos of coarser neighbours sampled from its 2^3 downsample
     f->fine.clear();

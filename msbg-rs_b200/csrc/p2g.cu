@@ -1063,10 +1063,13 @@ static void dispatch(msbg_ctx* ctx, int bsx, int M, const SplatArgs* s, size_t n
 
 static size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// d_sorted_keys: optional Morton keys of particles that are already sorted
-// by them (msbg_morton_sort_device + msbg_permute_device); skips the sort.
+// d_sorted_keys: optional sorted Morton keys (msbg_morton_sort_device); the
+// internal sort is skipped.  With d_perm null the particle arrays are already
+// in that order (msbg_permute_device); otherwise they are in the caller's
+// order and d_perm[i] is the caller index of sorted particle i, which the
+// gather follows.
 void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const float* d_mass, size_t n, float r_p,
-                size_t* n_active_out, const uint64_t* d_sorted_keys) {
+                size_t* n_active_out, const uint64_t* d_sorted_keys, const uint32_t* d_perm) {
     msbg_ctx* ctx = mac->ctx;
     msbg_grid* u = mac->ch[0];
     const int bsx = u->bsx, lg = u->lg;
@@ -1107,7 +1110,7 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     CUDA_CHECK(cudaMemsetAsync(bad, 0, 4, ctx->stream));
     if (d_sorted_keys) {
         skeys = d_sorted_keys;
-        perm = nullptr;
+        perm = const_cast<uint32_t*>(d_perm);
     } else {
         morton_keys(ctx, d_pos, n, keys);
         radix_sort_pairs(ctx, keys, nullptr, ScratchLayout::at<uint64_t>(base, o_skeys), perm, n, key_bits,
@@ -1240,7 +1243,7 @@ int msbg_p2g_device(msbg_mac* m, const float* d_pos, const float* d_vel, const f
     MSBG_API_BEGIN
     MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass) || !n), "null argument");
     set_device(m->ctx);
-    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, nullptr);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, nullptr, nullptr);
     MSBG_API_END
 }
 
@@ -1249,7 +1252,16 @@ int msbg_p2g_sorted_device(msbg_mac* m, const float* d_pos, const float* d_vel, 
     MSBG_API_BEGIN
     MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass && d_keys) || !n), "null argument");
     set_device(m->ctx);
-    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, d_keys);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, d_keys, nullptr);
+    MSBG_API_END
+}
+
+int msbg_p2g_permuted_device(msbg_mac* m, const float* d_pos, const float* d_vel, const float* d_mass,
+                             const uint64_t* d_keys, const uint32_t* d_perm, size_t n, float r_p, size_t* n_active_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((d_pos && d_vel && d_mass && d_keys && d_perm) || !n), "null argument");
+    set_device(m->ctx);
+    p2g_device(m, d_pos, d_vel, d_mass, n, r_p, n_active_out, d_keys, d_perm);
     MSBG_API_END
 }
 
@@ -1268,7 +1280,7 @@ int msbg_p2g(msbg_mac* m, const float* pos, const float* vel, const float* mass,
         CUDA_CHECK(cudaMemcpyAsync(dv, vel, n * 12, cudaMemcpyHostToDevice, m->ctx->stream));
         CUDA_CHECK(cudaMemcpyAsync(dm, mass, n * 4, cudaMemcpyHostToDevice, m->ctx->stream));
     }
-    p2g_device(m, dp, dv, dm, n, r_p, n_active_out, nullptr);
+    p2g_device(m, dp, dv, dm, n, r_p, n_active_out, nullptr, nullptr);
     sync(m->ctx);
     MSBG_API_END
 }

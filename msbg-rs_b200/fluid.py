@@ -95,6 +95,15 @@ def particles_to_grid_sorted_device(mac: MacGrid, d_pos, d_vel, d_mass, d_keys, 
     return na.value
 
 
+def particles_to_grid_permuted_device(mac: MacGrid, d_pos, d_vel, d_mass, d_keys, d_perm, n: int, r_p: float) -> int:
+    """particles_to_grid for device arrays in the caller's order, with the sorted
+    keys and the permutation of a Morton sort of their positions."""
+    na = C.c_size_t()
+    call("msbg_p2g_permuted_device", mac.handle, ptr(d_pos), ptr(d_vel), ptr(d_mass), ptr(d_keys), ptr(d_perm), int(n),
+         float(r_p), C.byref(na))
+    return na.value
+
+
 class MacSampler:
     """MacSampler::new(mac, bc) + sample::<Linear> (fluid/g2p.rs:15-32)."""
 

@@ -215,6 +215,26 @@ def test_p2g_sorted_input_identical(msbg, ctx):
     assert np.array_equal(device_channels(mac2, mac2.active_blocks()), ref)
 
 
+def test_p2g_permuted_input_identical(msbg, ctx):
+    """msbg_p2g_permuted_device on particles in the caller's order with the
+    keys and permutation of their Morton sort == msbg_p2g."""
+    import torch
+    pos, vel, mass = make_particles(40000, 64, 14)
+    mac = msbg.MacGrid(ctx, 64, 64, 64, 16)
+    msbg.particles_to_grid(mac, pos, vel, mass, 2.0)
+    ref = device_channels(mac, mac.active_blocks())
+    tp, tv, tm = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (pos, vel, mass))
+    tk = torch.empty(len(pos), dtype=torch.int64, device="cuda")
+    tperm = torch.empty(len(pos), dtype=torch.int32, device="cuda")
+    from msbg_rs_b200._lib import call, ptr
+    call("msbg_morton_sort_device", ctx.handle, ptr(tp), len(pos), ptr(tk), ptr(tperm))
+    mac2 = msbg.MacGrid(ctx, 64, 64, 64, 16)
+    msbg.particles_to_grid_permuted_device(mac2, tp, tv, tm, tk, tperm, len(pos), 2.0)
+    ctx.synchronize()
+    assert np.array_equal(mac2.active_blocks(), mac.active_blocks())
+    assert np.array_equal(device_channels(mac2, mac2.active_blocks()), ref)
+
+
 def test_p2g_rejects_out_of_domain(msbg, ctx):
     mac = msbg.MacGrid(ctx, 32, 32, 32, 16)
     with pytest.raises(msbg.MsbgError):
