@@ -1006,15 +1006,116 @@ __device__ __forceinline__ void compute_compact_pair(const SweepArgs& a, const f
     }
 }
 
-// Threads of a compact-sweep CTA: the 7-tap stencil takes two columns per
-// thread, the 19-tap one a column.
-template <int BSX, int ST> struct CompactThreads {
-    static constexpr bool pair = ST == MSBG_LAPLACIAN && BSX >= 8;
+// The 19-tap stencil over a block staged in the compact layout, two
+// x-columns per thread with paired arithmetic: the same operations in the
+// same order per cell as compute_compact (meancurv.rs:50-101).  Sums whose
+// operands are products are formed in scalar arithmetic (the code generator
+// may contract a paired product feeding a paired sum); 2 f0 is formed as
+// f0 + f0, which is the same value.  For the pair (x, x + 1) the columns L =
+// x - 1, A = x, B = x + 1 and R = x + 2 of a row give the x-neighbour pairs
+// (L, A) and (B, R).
+template <int BSX, bool CLAMP>
+__device__ __forceinline__ void compute_compact_pair_mc(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+    using CL = Compact<BSX>;
+    constexpr int H = CL::H;
+    constexpr int RS = BSX, PL = H * BSX;
+    constexpr int N = BSX * BSX * BSX;
+    float* payload = (float*)a.payload;
+    const int xp = tid % (BSX / 2), y = tid / (BSX / 2), x = 2 * xp;
+    float* out = payload + (size_t)slot * N + x + y * BSX;
+    float* xo0 = x == 0 ? a.xface + ((size_t)slot * 2 + 0) * (BSX * BSX) + y : nullptr;
+    float* xo1 = x + 1 == BSX - 1 ? a.xface + ((size_t)slot * 2 + 1) * (BSX * BSX) + y : nullptr;
+    const int i0 = (1 * H + (y + 1)) * BSX + x;  // z = 0, column x
+    // columns x - 1 and x + 2: block rows or x-halo columns
+    const float* lp = x > 0 ? h + i0 - 1 : h + CL::MAIN + 1 * CL::XP + 3 + (y + 1);
+    const float* rp = x + 2 < BSX ? h + i0 + 2 : h + CL::MAIN + CL::XS + 1 * CL::XP + 3 + (y + 1);
+    const int lsz = x > 0 ? PL : CL::XP, lsy = x > 0 ? RS : 1;
+    const int rsz = x + 2 < BSX ? PL : CL::XP, rsy = x + 2 < BSX ? RS : 1;
+    const uint64_t half2 = sw_pack(0.5f, 0.5f), q2 = sw_pack(0.25f, 0.25f), m2 = sw_pack(-2.0f, -2.0f),
+                   dt2 = sw_pack(a.dt, a.dt);
+    auto lo = [](uint64_t v) { float p, q; sw_unpack(v, p, q); return p; };
+    auto hi = [](uint64_t v) { float p, q; sw_unpack(v, p, q); return q; };
+    // planes z - 1 (p), z (c), z + 1 (n): row y as L, (A, B), R; rows y - 1
+    // and y + 1 as (A, B)
+    float pL = lp[-lsz], pR = rp[-rsz], cL = lp[0], cR = rp[0], nL = lp[lsz], nR = rp[rsz];
+    uint64_t pAB = sw_ld2(h + i0 - PL), pABm = sw_ld2(h + i0 - PL - RS), pABp = sw_ld2(h + i0 - PL + RS);
+    uint64_t cAB = sw_ld2(h + i0), cABm = sw_ld2(h + i0 - RS), cABp = sw_ld2(h + i0 + RS);
+    uint64_t nAB = sw_ld2(h + i0 + PL), nABm = sw_ld2(h + i0 + PL - RS), nABp = sw_ld2(h + i0 + PL + RS);
+#pragma unroll 2
+    for (int z = 0; z < BSX; ++z) {
+        const int i = i0 + z * PL;
+        // plane z's diagonal columns: L and R of rows y - 1 and y + 1
+        const float cLm = lp[z * lsz - lsy], cLp = lp[z * lsz + lsy], cRm = rp[z * rsz - rsy], cRp = rp[z * rsz + rsy];
+        // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
+        const uint64_t f0 = cAB, f1 = sw_pack(cL, lo(cAB)), f2 = sw_pack(hi(cAB), cR);
+        const uint64_t f3 = cABm, f4 = cABp, f5 = pAB, f6 = nAB;
+        const uint64_t fx = sw_mul(sw_sub(f2, f1), half2), fy = sw_mul(sw_sub(f4, f3), half2),
+                       fz = sw_mul(sw_sub(f6, f5), half2);
+        const uint64_t two_f0 = sw_add(f0, f0);
+        const uint64_t fxx = sw_sub(sw_add(f1, f2), two_f0), fyy = sw_sub(sw_add(f3, f4), two_f0),
+                       fzz = sw_sub(sw_add(f5, f6), two_f0);
+        // d1..d4: (x+1, y+1), (x+1, y-1), (x-1, y+1), (x-1, y-1) in plane z
+        const uint64_t d1 = sw_pack(hi(cABp), cRp), d2 = sw_pack(hi(cABm), cRm), d3 = sw_pack(cLp, lo(cABp)),
+                       d4 = sw_pack(cLm, lo(cABm));
+        // d5..d8: (x+1, z+1), (x+1, z-1), (x-1, z+1), (x-1, z-1) in row y
+        const uint64_t d5 = sw_pack(hi(nAB), nR), d6 = sw_pack(hi(pAB), pR), d7 = sw_pack(nL, lo(nAB)),
+                       d8 = sw_pack(pL, lo(pAB));
+        // d9..d12: (y+1, z+1), (y+1, z-1), (y-1, z+1), (y-1, z-1)
+        const uint64_t fyx = sw_mul(sw_add(sw_sub(sw_sub(d1, d2), d3), d4), q2);
+        const uint64_t fzx = sw_mul(sw_add(sw_sub(sw_sub(d5, d6), d7), d8), q2);
+        const uint64_t fzy = sw_mul(sw_add(sw_sub(sw_sub(nABp, pABp), nABm), pABm), q2);
+        // cross = (fx (fy fyx) + fx (fz fzx)) + fy (fz fzy): the inner
+        // products paired, the outer products and their sums scalar
+        const uint64_t i1 = sw_mul(fy, fyx), i2 = sw_mul(fz, fzx), i3 = sw_mul(fz, fzy);
+        const float cr0 = (lo(fx) * lo(i1) + lo(fx) * lo(i2)) + lo(fy) * lo(i3);
+        const float cr1 = (hi(fx) * hi(i1) + hi(fx) * hi(i2)) + hi(fy) * hi(i3);
+        // squares paired, their sums scalar
+        const uint64_t sx = sw_mul(fx, fx), sy = sw_mul(fy, fy), sz = sw_mul(fz, fz);
+        const uint64_t syz = sw_pack(lo(sy) + lo(sz), hi(sy) + hi(sz)), sxz = sw_pack(lo(sx) + lo(sz), hi(sx) + hi(sz)),
+                       sxy = sw_pack(lo(sx) + lo(sy), hi(sx) + hi(sy));
+        const uint64_t hnum = sw_fma(syz, fxx, sw_fma(sxz, fyy, sw_fma(sxy, fzz, sw_mul(m2, sw_pack(cr0, cr1)))));
+        const uint64_t grad = sw_fma(fx, fx, sw_fma(fy, fy, sw_mul(fz, fz)));
+        const float g0 = lo(grad), g1 = hi(grad);
+        const float hc0 = g0 > 1e-7f ? lo(hnum) / g0 : 0.0f, hc1 = g1 > 1e-7f ? hi(hnum) / g1 : 0.0f;
+        float dd0, dd1;
+        sw_unpack(sw_mul(dt2, sw_pack(hc0, hc1)), dd0, dd1);
+        float n0, n1;
+        sw_unpack(sw_add(f0, sw_pack(clampf(dd0, -0.1f, 0.1f), clampf(dd1, -0.1f, 0.1f))), n0, n1);
+        if (CLAMP) {
+            n0 = clampf(n0, 0.0f, 1.0f);
+            n1 = clampf(n1, 0.0f, 1.0f);
+        }
+        *reinterpret_cast<float2*>(out + z * BSX * BSX) = make_float2(n0, n1);
+        if (xo0) xo0[z * BSX] = n0;
+        if (xo1) xo1[z * BSX] = n1;
+        pL = cL; pR = cR; pAB = cAB; pABm = cABm; pABp = cABp;
+        cL = nL; cR = nR; cAB = nAB; cABm = nABm; cABp = nABp;
+        if (z + 1 < BSX) {
+            const int j = i + 2 * PL;
+            nL = lp[(z + 2) * lsz];
+            nR = rp[(z + 2) * rsz];
+            nAB = sw_ld2(h + j);
+            nABm = sw_ld2(h + j - RS);
+            nABp = sw_ld2(h + j + RS);
+        }
+    }
+}
+
+// Threads of a compact-sweep CTA: two columns per thread (PAIR) or one.
+template <int BSX, int ST, bool PAIR = true> struct CompactThreads {
+    static constexpr bool pair = PAIR && (ST == MSBG_LAPLACIAN || ST == MSBG_MEAN_CURVATURE) && BSX >= 8;
     static constexpr int v = pair ? BSX * BSX / 2 : BSX * BSX;
 };
 
-template <int BSX, int ST, bool CLAMP>
-__global__ void __launch_bounds__(CompactThreads<BSX, ST>::v, BSX == 16 ? 4 : 1)
+// The 19-tap stencil takes two columns per thread in colour phases of at
+// least this many blocks (B200, 16^3 blocks: 10 sweeps of 56,056 blocks 9.2
+// against 10.5 ms), one column otherwise: a phase of a few hundred blocks is
+// bound by the latency of one block, which twice the threads shorten (776
+// blocks: 0.87 against 0.99 ms).
+constexpr int kPairMinPhaseBlocks = 1184;
+
+template <int BSX, int ST, bool CLAMP, bool PAIR>
+__global__ void __launch_bounds__(CompactThreads<BSX, ST, PAIR>::v, BSX == 16 ? 4 : 1)
 sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
     using CL = Compact<BSX>;
     extern __shared__ float4 h4[];
@@ -1055,7 +1156,7 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
         if (t + 2 * g < n) pi2 = order[t + 2 * g];
     }
     __syncthreads();
-    constexpr int NT = CompactThreads<BSX, ST>::v;
+    constexpr int NT = CompactThreads<BSX, ST, PAIR>::v;
     if (flg[0] & 1) issue_compact<BSX, ST, NT>(a, hb, nbs[0]);
     cp_async_commit();
     for (int j = 0; t < n; t += g, ++j) {
@@ -1074,7 +1175,8 @@ sweep_compact_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
         if (flg[sl] & 1) cp_async_wait<1>();  // this block's copies have landed
         else stage_general<ElemF32, BSX, ST, true>(a, hb + b * CL::BUF, nbs[sl], pis[sl], &ok[0][0], &dd[0][0], &ll[0][0]);
         __syncthreads();
-        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
+        if (CompactThreads<BSX, ST, PAIR>::pair && ST == MSBG_LAPLACIAN) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
+        else if (CompactThreads<BSX, ST, PAIR>::pair) compute_compact_pair_mc<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
         else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[sl][13], tid);
         if (meta_thread && t2 < n) put_meta(s2, pi2, nb2, fl2);
         pi2 = pi3;
@@ -1209,7 +1311,8 @@ sweep_wave_kernel(SweepArgs a, const int2* __restrict__ items, int total, int* p
         }
         cp_async_wait<1>();  // the current block's copies have landed
         __syncthreads();
-        if (CompactThreads<BSX, ST>::pair) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        if (CompactThreads<BSX, ST>::pair && ST == MSBG_LAPLACIAN) compute_compact_pair<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
+        else if (CompactThreads<BSX, ST>::pair) compute_compact_pair_mc<BSX, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
         else compute_compact<BSX, ST, CLAMP>(a, hb + b * CL::BUF, nbs[b][13], tid);
         __syncthreads();
         if (tid == 0) {
@@ -1272,25 +1375,36 @@ static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_
     }
 }
 
-template <int BSX, int ST, bool CLAMP>
-static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
+template <int BSX, int ST, bool CLAMP, bool PAIR>
+static void launch_compact_v(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
     const size_t smem = 2 * sizeof(float) * Compact<BSX>::BUF;
     static bool attr = false;
     if (!attr) {
-        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_compact_kernel<BSX, ST, CLAMP, PAIR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                         (int)cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
-    const int threads = CompactThreads<BSX, ST>::v;
+    const int threads = CompactThreads<BSX, ST, PAIR>::v;
     int per_sm = 0;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_compact_kernel<BSX, ST, CLAMP>, threads, smem));
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_compact_kernel<BSX, ST, CLAMP, PAIR>, threads, smem));
     int sms = 0;
     CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     const int grid = std::max(1, std::min(n, std::max(per_sm, 1) * sms));
     begin_launch(ctx);
-    sweep_compact_kernel<BSX, ST, CLAMP><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
+    sweep_compact_kernel<BSX, ST, CLAMP, PAIR><<<(unsigned)grid, threads, smem, ctx->stream>>>(a, order, n);
     after_launch(ctx, "sweep_compact_kernel");
+}
+
+template <int BSX, int ST, bool CLAMP>
+static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
+    if constexpr (ST == MSBG_LAPLACIAN) {
+        launch_compact_v<BSX, ST, CLAMP, true>(ctx, a, order, n);
+    } else {
+        if (n >= kPairMinPhaseBlocks) launch_compact_v<BSX, ST, CLAMP, true>(ctx, a, order, n);
+        else launch_compact_v<BSX, ST, CLAMP, false>(ctx, a, order, n);
+    }
 }
 
 template <int BSX, int ST, bool CLAMP>
