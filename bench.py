@@ -525,14 +525,14 @@ P2G_SPLAT_LAUNCHES = 3
 # count, so it is scaled by particles.
 TRAFFIC_PER_UNIT = {"p2g_cells_kernel": (167.28e6 + 3.96e6) / 5767168,
                     # r_p = 2 kernel, all three directions in one launch at 128^3
-                    # (profiles/p2g_r2_kernel_flip128.txt): 309.34 MB read, 47.91 MB written
-                    "p2g_r2_kernel": (309.34e6 + 47.91e6) / 5767168}
+                    # (profiles/p2g_r2_kernel_flip128.txt): 308.83 MB read, 47.21 MB written
+                    "p2g_r2_kernel": (308.83e6 + 47.21e6) / 5767168}
 
 # Warp instructions per unit of work from the same capture (575,950,823 per
 # launch at 128^3): the splat is bound by instruction issue, not by DRAM, so
 # its second roofline is issue slots (4 warp instructions per SM per clock).
 INST_PER_UNIT = {"p2g_cells_kernel": 575950823 / 5767168,
-                 "p2g_r2_kernel": 1067742284 / 5767168}
+                 "p2g_r2_kernel": 1073931570 / 5767168}
 
 
 # The smoother's sweep kernels (one of them runs, by element type, halo and

@@ -539,7 +539,10 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
 // cell and go through the lane-bit path of p2g_cells_kernel.  Every term is
 // the reference's f32 operation sequence (p2g.rs:263-330); the sums are FP64
 // in a fixed order (colour, tile, anchor, staging order).
-constexpr int kSplatR2Warps = 20;
+// 24 warps with 160 staging slots each (a typical tile stages 144 particles)
+// measured fastest on B200 among 16 x 192, 20 x 192, 24 x 160 and 28 x 128
+// (6.02 against 7.02, 6.42 and 6.69 ms at 256^3).
+constexpr int kSplatR2Warps = 24;
 template <int BSX> struct SplatR2 {
     static constexpr int M = 2, W = BSX + 2 * M, WW = W * W * W;
     static constexpr int NA = BSX / 2 + 1;  // anchor tiles along U and V (anchors 0 .. BSX)
@@ -548,7 +551,7 @@ template <int BSX> struct SplatR2 {
     static constexpr int NSRC = 18;         // source cells of a tile
     static constexpr int WARPS = NT < kSplatR2Warps ? NT : kSplatR2Warps;
     // particles a warp stages at once: a whole typical tile (144 at 8 per cell)
-    static constexpr int CAP = 192;
+    static constexpr int CAP = 160;
     // per warp: CAP x (float4 position/mass, float momentum, u8 anchor-sorted
     // index), source cells (int2), 17 anchor-range offsets and 16 counters
     static constexpr size_t warp_bytes = (size_t)CAP * (16 + 4 + 1 + 1 + 1 + 1) + NSRC * 8 + 17 * 4 + 16 * 4;
