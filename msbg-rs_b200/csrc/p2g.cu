@@ -34,7 +34,8 @@
 namespace msbg {
 
 struct SplatArgs {
-    const float *px, *py, *pz, *pm, *pv[3];  // cell-sorted particle SoA
+    const float *px, *py, *pz, *pm, *pv[3];  // cell-sorted particles: x, y, z, velocity
+    int ps;                                  // components at px[i ps] .. pv[d][i ps]; mass at pm[i]
     const int32_t* cell_begin;               // [npb][bsx^3] by local Morton code
     const int32_t* cell_end;
     const uint64_t* pb_key;                  // block Morton key per particle block
@@ -118,7 +119,8 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
     }
 }
 
-// Payload gather into cell-sorted SoA (perm == null: already sorted), each
+// Payload gather into cell-sorted SoA (only for particles in the caller's
+// order, perm != null; sorted particles are read by the splat in place), each
 // particle's block-footprint mask (particles/mod.rs:207-212 footprint_axis
 // with r_scan = (r_p + 1) / bsx, relative to its own block) and, per face
 // direction, its clipped face footprint (p2g.rs:263-270) relative to its own
@@ -132,15 +134,17 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
                                   int lg, int M, float r_p, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz,
                                   float* px, float* py, float* pz, float* pm, float* v0, float* v1, float* v2,
                                   uint32_t* fmask, uint64_t* lane_mask, int* bad) {
-    const float bsx = (float)(1 << lg);
+    const float inv_bsx = 1.0f / (float)(1 << lg);
     const int32_t B = 1 << lg;
     const int WIN = 2 * M + 1;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const size_t s = perm ? perm[i] : i;
         const float x = pos[3 * s], y = pos[3 * s + 1], z = pos[3 * s + 2];
-        px[i] = x; py[i] = y; pz[i] = z;
-        pm[i] = mass[s];
-        v0[i] = vel[3 * s]; v1[i] = vel[3 * s + 1]; v2[i] = vel[3 * s + 2];
+        if (perm) {
+            px[i] = x; py[i] = y; pz[i] = z;
+            pm[i] = mass[s];
+            v0[i] = vel[3 * s]; v1[i] = vel[3 * s + 1]; v2[i] = vel[3 * s + 2];
+        }
         const float p[3] = {x, y, z};
         const int64_t nn[3] = {nx, ny, nz};
         uint32_t lo[3], hi[3];
@@ -150,7 +154,7 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             const int64_t c = p[ax] > 0.0f ? (int64_t)p[ax] : 0;  // the particle's cell (p as usize)
             const int64_t cb = c >> lg;                              // and block
             if (cb >= nn[ax]) out = true;
-            const float b = p[ax] / bsx;
+            const float b = p[ax] * inv_bsx;  // p / bsx: bsx is a power of two, the product is exact
             const int64_t l = max((int64_t)(int32_t)truncf(b - r_scan_bsx), (int64_t)0);
             const int64_t h = min((int64_t)(int32_t)truncf(b + r_scan_bsx), nn[ax] - 1);
             lo[ax] = (uint32_t)(min(max(l - cb, (int64_t)-1), (int64_t)1) + 1);
@@ -193,11 +197,17 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             lane_mask[(size_t)dir * n + i] = m;
         }
         if (out) { atomicExch(bad, 1); fmask[i] = 0; continue; }
-        uint32_t m = 0;
-        for (uint32_t dz = lo[2]; dz <= hi[2]; ++dz)
-            for (uint32_t dy = lo[1]; dy <= hi[1]; ++dy)
-                for (uint32_t dx = lo[0]; dx <= hi[0]; ++dx) m |= 1u << (dx + 3 * dy + 9 * dz);
-        fmask[i] = m;
+        // bit dx + 3 dy + 9 dz for dx, dy, dz in [lo, hi] per axis: the x run
+        // replicated at the y run's and the z run's offsets (products of
+        // disjoint bit patterns, no carries)
+        auto rep = [](uint32_t l, uint32_t h, uint32_t step) {
+            uint32_t r = 0;
+            for (uint32_t d = 0; d < 3; ++d)
+                if (l <= d && d <= h) r |= 1u << (step * d);
+            return r;
+        };
+        const uint32_t xr = ((2u << hi[0]) - 1u) & ~((1u << lo[0]) - 1u);
+        fmask[i] = xr * rep(lo[1], hi[1], 3) * rep(lo[2], hi[2], 9);
     }
 }
 
@@ -416,9 +426,10 @@ __global__ void __launch_bounds__(32 * kSplatWarps, 1) p2g_cells_kernel(SplatArg
                           if (pl < st_hi) {
                               const uint64_t f = lmask[pl];
                               const float m = a.pm[pl];
-                              const float pc[3] = {a.px[pl] - 0.5f, a.py[pl] - 0.5f, a.pz[pl] - 0.5f};
+                              const size_t q = (size_t)pl * a.ps;
+                              const float pc[3] = {a.px[q] - 0.5f, a.py[q] - 0.5f, a.pz[q] - 0.5f};
                               wslot[pl - st_lo] = make_float4(pc[U], pc[V], pc[F], m);
-                              wslot[CAP + pl - st_lo] = make_float4(m * pv[pl], __uint_as_float((uint32_t)f),
+                              wslot[CAP + pl - st_lo] = make_float4(m * pv[q], __uint_as_float((uint32_t)f),
                                                                     __uint_as_float((uint32_t)(f >> 32)), 0.0f);
                           }
                       }
@@ -759,9 +770,10 @@ __device__ __forceinline__ void splat_r2_body(const SplatArgs& a, const int k_pb
                 const int2 cc = wc[wsrc[s]];
                 const int pl = cc.y + (s0 + s - cc.x);
                 const float m = a.pm[pl];
-                const float pp[3] = {a.px[pl], a.py[pl], a.pz[pl]};
+                const size_t q = (size_t)pl * a.ps;
+                const float pp[3] = {a.px[q], a.py[q], a.pz[q]};
                 wp[dst] = make_float4(pp[U] - 0.5f, pp[V] - 0.5f, pp[F] - 0.5f, m);
-                wm[dst] = m * pv[pl];
+                wm[dst] = m * pv[q];
                 wlist[dst] = (uint8_t)s;
             }
             __syncwarp();
@@ -1094,8 +1106,10 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     }
     // ---- phase 1: sort, gather, particle blocks -------------------------------
     ScratchLayout L1;
+    // the cell-sorted SoA copy exists only for particles in the caller's order
+    const bool sorted_in_place = d_sorted_keys && !d_perm;
     const size_t o_keys = L1.add<uint64_t>(n), o_skeys = L1.add<uint64_t>(n), o_perm = L1.add<uint32_t>(n),
-                 o_soa = L1.add<float>(7 * n), o_fm = L1.add<uint32_t>(n), o_fp = L1.add<uint64_t>(3 * n),
+                 o_soa = L1.add<float>(sorted_in_place ? 1 : 7 * n), o_fm = L1.add<uint32_t>(n), o_fp = L1.add<uint64_t>(3 * n),
                  o_pbk = L1.add<uint64_t>(n + 1),
                  o_pbs = L1.add<uint64_t>(n + 2), o_tmp = L1.add<char>(std::max(radix_sort_scratch_bytes(n), segment_scratch_bytes(n))),
                  o_bad = L1.add<int>(4);
@@ -1206,8 +1220,15 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
                                                                   (int64_t)u->nz, nbr_rank);
     after_launch(ctx, "active_nbr_kernel");
     SplatArgs s;
-    s.px = px; s.py = py; s.pz = pz; s.pm = pm;
-    s.pv[0] = v0; s.pv[1] = v1; s.pv[2] = v2;
+    if (perm) {  // the gathered cell-sorted SoA
+        s.px = px; s.py = py; s.pz = pz; s.pm = pm;
+        s.pv[0] = v0; s.pv[1] = v1; s.pv[2] = v2;
+        s.ps = 1;
+    } else {  // already sorted: the caller's arrays in place
+        s.px = d_pos; s.py = d_pos + 1; s.pz = d_pos + 2; s.pm = d_mass;
+        s.pv[0] = d_vel; s.pv[1] = d_vel + 1; s.pv[2] = d_vel + 2;
+        s.ps = 3;
+    }
     s.cell_begin = cell_begin;
     s.cell_end = cell_end;
     s.pb_key = pb_key;
