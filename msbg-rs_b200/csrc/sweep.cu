@@ -17,6 +17,7 @@
 // where the reference calls mul_add.  Results are bit-identical to the CPU
 // restatement in oracle/.
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 
 #include "sweep.cuh"
@@ -710,8 +711,12 @@ template <int BSX> struct Compact {
 };
 
 // Issues the staging of an interior block (one-cell halo) in the compact layout.
-template <int BSX, int ST, int NT = BSX * BSX, bool CG = false>
-__device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb) {
+// SLAB: only the cells of halo planes hz0 .. hz1 (the z-slab of one CTA of a
+// cluster that shares the block).
+template <int BSX, int ST, int NT = BSX * BSX, bool CG = false, bool SLAB = false>
+__device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restrict__ h, const int32_t* nb, int hz0 = 0,
+                                              int hz1 = BSX + 1) {
+    auto in = [&](int hz) { return !SLAB || (hz >= hz0 && hz <= hz1); };
     using CL = Compact<BSX>;
     constexpr int H = CL::H;
     constexpr int LG = Lg<BSX>::v;
@@ -726,13 +731,13 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
     for (int k = 0; k < N / 4 / NT; ++k) {
         const int it = tid + k * NT;
         const int q = it % QR, r = it / QR, y = r & (BSX - 1), z = r >> LG;
-        cp_async16(h + ((z + 1) * H + y + 1) * BSX + 4 * q, payload + (size_t)c13 * N + 4 * it);
+        if (in(z + 1)) cp_async16(h + ((z + 1) * H + y + 1) * BSX + 4 * q, payload + (size_t)c13 * N + 4 * it);
     }
     // y and z face rows (and the four x-edge rows of the 19-tap stencil)
     constexpr int NFACE = 4 * BSX * QR;
     constexpr int NEDGE = ST == MSBG_LAPLACIAN ? 0 : 4 * QR;
     for (int it = tid; it < NFACE + NEDGE; it += NT) {
-        int c, dst, srcoff, ly, lz;
+        int c, dst, srcoff, ly, lz, hz;
         if (it < NFACE) {
             const int q = it % QR, rr = it / QR, row = rr % BSX, pd = rr / BSX;  // pd: y-, y+, z-, z+
             const int side = (pd & 1) ? 1 : -1, l = side < 0 ? BSX - 1 : 0, hh = side < 0 ? 0 : H - 1;
@@ -741,11 +746,13 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
                 ly = l;
                 lz = row;
                 dst = ((row + 1) * H + hh) * BSX + 4 * q;
+                hz = row + 1;
             } else {
                 c = nb[13 + 9 * side];
                 ly = row;
                 lz = l;
                 dst = (hh * H + row + 1) * BSX + 4 * q;
+                hz = hh;
             }
             srcoff = (ly << LG) + (lz << (2 * LG)) + 4 * q;
         } else {
@@ -756,7 +763,9 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
             c = nb[13 + 3 * sy + 9 * sz];
             dst = ((sz < 0 ? 0 : H - 1) * H + (sy < 0 ? 0 : H - 1)) * BSX + 4 * q;
             srcoff = (ly << LG) + (lz << (2 * LG)) + 4 * q;
+            hz = sz < 0 ? 0 : H - 1;
         }
+        if (!in(hz)) continue;
         if (c >= 0) {
             cp_async16(h + dst, payload + (size_t)c * N + srcoff);
         } else if (c <= kCodeCoarse0) {
@@ -774,6 +783,7 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
     constexpr int NXR = 2 * BSX * QR;
     for (int it = tid; it < NXR; it += NT) {
         const int q = it % QR, z = (it / QR) % BSX, side = it / (QR * BSX);  // side 0: x = -1, 1: x = BSX
+        if (!in(z + 1)) continue;
         const int c = nb[13 + (side ? 1 : -1)];
         float* d = h + CL::MAIN + side * CL::XS + (z + 1) * CL::XP + 4 + 4 * q;
         if (c >= 0) {
@@ -800,6 +810,7 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
                 const int sx = (kind & 1) ? 1 : -1, sz = (kind & 2) ? 1 : -1;
                 const int c = nb[13 + sx + 9 * sz];
                 const int lz = sz < 0 ? BSX - 1 : 0, hz = sz < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
+                if (!in(hz)) continue;
                 float* d = h + CL::MAIN + side * CL::XS + hz * CL::XP + 4 + 4 * q;
                 if (c >= 0) {
                     cp_async16(d, a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + lz * BSX + 4 * q);
@@ -820,6 +831,7 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
                 const int sx = (kind & 1) ? 1 : -1, sy = (kind & 2) ? 1 : -1;
                 const int c = nb[13 + sx + 3 * sy];
                 const int ly = sy < 0 ? BSX - 1 : 0, hy = sy < 0 ? 0 : H - 1, side = sx < 0 ? 0 : 1;
+                if (!in(j + 1)) continue;
                 float* d = h + CL::MAIN + side * CL::XS + (j + 1) * CL::XP + 3 + hy;
                 if (c >= 0) {
                     const float* src = a.xface + ((size_t)c * 2 + (sx < 0 ? 1 : 0)) * (BSX * BSX) + j * BSX + ly;
@@ -840,8 +852,13 @@ __device__ __forceinline__ void issue_compact(const SweepArgs& a, float* __restr
 // The stencil over a block staged in the compact layout (thread (x, y) walks
 // its z-column).  x-1 and x+1 come through per-thread accessors: from the
 // block rows, or from the x-halo columns for x = 0 and x = BSX-1.
-template <int BSX, int ST, bool CLAMP>
-__device__ __forceinline__ void compute_compact(const SweepArgs& a, const float* __restrict__ h, int slot, int tid) {
+// ZS < BSX: only planes z0 .. z0 + ZS - 1 (the z-slab of one CTA of a
+// cluster that shares the block; the slab's planes and one halo plane on
+// either side are staged).
+template <int BSX, int ST, bool CLAMP, int ZS = BSX>
+__device__ __forceinline__ void compute_compact(const SweepArgs& a, const float* __restrict__ h, int slot, int tid,
+                                                int z0_ = 0) {
+    const int z0 = ZS == BSX ? 0 : z0_, z1 = z0 + ZS;
     using CL = Compact<BSX>;
     constexpr int H = CL::H;
     constexpr int RS = BSX, PL = H * BSX;
@@ -858,9 +875,9 @@ __device__ __forceinline__ void compute_compact(const SweepArgs& a, const float*
     const int rsz = x < BSX - 1 ? PL : CL::XP, rsy = x < BSX - 1 ? RS : 1;
     const float dt = a.dt;
     if (ST == MSBG_LAPLACIAN) {
-        float zb = h[i0 - PL], c = h[i0], zf = h[i0 + PL];
+        float zb = h[i0 + (z0 - 1) * PL], c = h[i0 + z0 * PL], zf = h[i0 + (z0 + 1) * PL];
 #pragma unroll 4
-        for (int z = 0; z < BSX; ++z) {
+        for (int z = z0; z < z1; ++z) {
             const int i = i0 + z * PL;
             const float lx = lp[z * lsz], rx = rp[z * rsz], dyu = h[i - RS], dyd = h[i + RS];
             float nbs = lx + rx;
@@ -877,15 +894,16 @@ __device__ __forceinline__ void compute_compact(const SweepArgs& a, const float*
             if (xo) xo[z * BSX] = nv;
             zb = c;
             c = zf;
-            if (z + 1 < BSX) zf = h[i + 2 * PL];
+            if (z + 1 < z1) zf = h[i + 2 * PL];
         }
     } else {
         // plane z-1: cross (c, x-, x+, y-, y+); plane z: 3x3; plane z+1: cross
-        float pc = h[i0 - PL], pxm = lp[-lsz], pxp = rp[-rsz], pym = h[i0 - PL - RS], pyp = h[i0 - PL + RS];
-        float c = h[i0], cxm = lp[0], cxp = rp[0], cym = h[i0 - RS], cyp = h[i0 + RS];
-        float nc = h[i0 + PL], nxm = lp[lsz], nxp = rp[rsz], nym = h[i0 + PL - RS], nyp = h[i0 + PL + RS];
+        const int j0 = i0 + z0 * PL;
+        float pc = h[j0 - PL], pxm = lp[(z0 - 1) * lsz], pxp = rp[(z0 - 1) * rsz], pym = h[j0 - PL - RS], pyp = h[j0 - PL + RS];
+        float c = h[j0], cxm = lp[z0 * lsz], cxp = rp[z0 * rsz], cym = h[j0 - RS], cyp = h[j0 + RS];
+        float nc = h[j0 + PL], nxm = lp[(z0 + 1) * lsz], nxp = rp[(z0 + 1) * rsz], nym = h[j0 + PL - RS], nyp = h[j0 + PL + RS];
 #pragma unroll 2
-        for (int z = 0; z < BSX; ++z) {
+        for (int z = z0; z < z1; ++z) {
             const int i = i0 + z * PL;
             const float xpyp = rp[z * rsz + rsy], xpym = rp[z * rsz - rsy], xmyp = lp[z * lsz + lsy], xmym = lp[z * lsz - lsy];
             // meancurv.rs:50-101 with f1..f6 = x-, x+, y-, y+, z-, z+
@@ -909,7 +927,7 @@ __device__ __forceinline__ void compute_compact(const SweepArgs& a, const float*
             if (xo) xo[z * BSX] = nv;
             pc = c; pxm = cxm; pxp = cxp; pym = cym; pyp = cyp;
             c = nc; cxm = nxm; cxp = nxp; cym = nym; cyp = nyp;
-            if (z + 1 < BSX) {
+            if (z + 1 < z1) {
                 const int j = i + 2 * PL;
                 nc = h[j]; nxm = lp[(z + 2) * lsz]; nxp = rp[(z + 2) * rsz]; nym = h[j - RS]; nyp = h[j + RS];
             }
@@ -1375,6 +1393,78 @@ static void xface_init(msbg_ctx* ctx, int bsx, const void* payload, const int32_
     }
 }
 
+// ---- small colour phases: one block per thread-block cluster ---------------
+// A phase of a few hundred blocks leaves most SMs idle with one CTA per
+// block and takes one block's latency.  Here a cluster of BSX / ZS CTAs
+// shares a block: each stages the planes of its z-slab (and one halo plane
+// on either side), the cluster barrier orders every CTA's reads of the block
+// before any CTA's in-place writes (the stencil reads the block's values from
+// before the phase, as with one CTA), and each computes its ZS planes.
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <int BSX, int ST, bool CLAMP, int ZS>
+__global__ void __launch_bounds__(BSX * BSX) sweep_cluster_kernel(SweepArgs a, const int32_t* __restrict__ order, int n) {
+    using CL = Compact<BSX>;
+    constexpr int NS = BSX / ZS;  // CTAs of a cluster, one block
+    extern __shared__ float4 h4[];
+    float* hb = reinterpret_cast<float*>(h4);
+    __shared__ int32_t nbs[27];
+    __shared__ int32_t flg, pis;
+    __shared__ int8_t ok[3][BSX + 2], dd[3][BSX + 2], ll[3][BSX + 2];
+    const int tid = threadIdx.x;
+    const int t = blockIdx.x / NS, z0 = (int)(blockIdx.x % NS) * ZS;
+    const int pi = order[t];
+    if (tid < 27) nbs[tid] = a.nbr[(size_t)pi * 27 + tid];
+    if (tid == BSX * BSX - 1) {
+        flg = a.bxyz[(size_t)pi * 4 + 3];
+        pis = pi;
+    }
+    __syncthreads();
+    if (flg & 1) {
+        issue_compact<BSX, ST, BSX * BSX, false, true>(a, hb, nbs, z0, z0 + ZS + 1);
+        cp_async_commit();
+        cp_async_wait<0>();
+    } else {
+        stage_general<ElemF32, BSX, ST, true>(a, hb, nbs, pis, &ok[0][0], &dd[0][0], &ll[0][0]);
+    }
+    __syncthreads();
+    cluster_barrier();  // every CTA of the block has read it
+    compute_compact<BSX, ST, CLAMP, ZS>(a, hb, nbs[13], tid, z0);
+}
+
+// Colour phases of at most this many blocks run one block per cluster of 4
+// CTAs (16^3 blocks, one-cell halos).
+constexpr int kClusterMaxPhaseBlocks = 296;
+
+template <int BSX, int ST, bool CLAMP>
+static void launch_cluster(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
+    constexpr int ZS = 4, NS = BSX / ZS;
+    const size_t smem = sizeof(float) * Compact<BSX>::BUF;
+    static bool attr = false;
+    if (!attr) {
+        CUDA_CHECK(cudaFuncSetAttribute(sweep_cluster_kernel<BSX, ST, CLAMP, ZS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+        attr = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n * NS));
+    cfg.blockDim = dim3(BSX * BSX);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = NS;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    begin_launch(ctx);
+    CUDA_CHECK(cudaLaunchKernelEx(&cfg, sweep_cluster_kernel<BSX, ST, CLAMP, ZS>, a, order, n));
+    after_launch(ctx, "sweep_cluster_kernel");
+}
+
 template <int BSX, int ST, bool CLAMP, bool PAIR>
 static void launch_compact_v(msbg_ctx* ctx, const SweepArgs& a, const int32_t* order, int n) {
     const size_t smem = 2 * sizeof(float) * Compact<BSX>::BUF;
@@ -1402,8 +1492,17 @@ static void launch_compact(msbg_ctx* ctx, const SweepArgs& a, const int32_t* ord
     if constexpr (ST == MSBG_LAPLACIAN) {
         launch_compact_v<BSX, ST, CLAMP, true>(ctx, a, order, n);
     } else {
-        if (n >= kPairMinPhaseBlocks) launch_compact_v<BSX, ST, CLAMP, true>(ctx, a, order, n);
-        else launch_compact_v<BSX, ST, CLAMP, false>(ctx, a, order, n);
+        if (n >= kPairMinPhaseBlocks) {
+            launch_compact_v<BSX, ST, CLAMP, true>(ctx, a, order, n);
+            return;
+        }
+        if constexpr (BSX == 16 && ST == MSBG_MEAN_CURVATURE) {
+            if (n <= kClusterMaxPhaseBlocks) {
+                launch_cluster<BSX, ST, CLAMP>(ctx, a, order, n);
+                return;
+            }
+        }
+        launch_compact_v<BSX, ST, CLAMP, false>(ctx, a, order, n);
     }
 }
 
@@ -1654,6 +1753,7 @@ static SweepPlan* get_plan(msbg_grid* g, msbg_grid* coarse, const uint8_t* level
         CUDA_CHECK(cudaMemcpyAsync(plan->order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, g->ctx->stream));
         sync(g->ctx);
     }
+    if (g->plan && !g->plan->graphs.empty()) sync(g->ctx);  // its graphs may still run
     delete g->plan;
     g->plan = plan;
     return plan;
@@ -1694,65 +1794,118 @@ static void sweep(msbg_grid* g, msbg_grid* coarse, const uint8_t* levels, const 
     a.sr_zstep = sr_pow((uint64_t)(g->bsx * g->bsx) >> lg);
     const uint64_t chunks_per_sweep = (uint64_t)plan->n * ((uint64_t)g->block_elems >> lg);
     const uint64_t pos0 = stream_pos ? *stream_pos : 0;
-    // x-plane side buffer: sized for every slot, refreshed from the payload at
+    // x-plane side buffer: sized for every slot (here, before any launch: a
+    // graph capture below must not allocate), refreshed from the payload at
     // the start of each call (the payload may have changed in between)
-    {
-        const size_t slots = g->n_slots();
-        const int xd = stencil == MSBG_BILAPLACIAN ? 2 : 1;  // x-planes per side the stencil's halo reaches
-        if (plan->xface_slots < slots * xd) {
-            plan->xface.reserve(slots * 2 * xd * g->bsx * g->bsx * sizeof(float));
-            plan->xface_slots = slots * xd;
-        }
-        a.xface = plan->xface.as<float>();
-        const int32_t* xs = plan->xslots.as<int32_t>();
-        const size_t nx = plan->n_xslots;
-        if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
-        else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
-        else if (g->dtype == MSBG_U8) xface_init<ElemU8>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
-        else if (g->dtype == MSBG_F16) xface_init<ElemF16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
-        else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, xs, nx, xd, a.xface);
+    const size_t slots = g->n_slots();
+    const int xd = stencil == MSBG_BILAPLACIAN ? 2 : 1;  // x-planes per side the stencil's halo reaches
+    if (plan->xface_slots < slots * xd) {
+        plan->xface.reserve(slots * 2 * xd * g->bsx * g->bsx * sizeof(float));
+        plan->xface_slots = slots * xd;
     }
+    a.xface = plan->xface.as<float>();
     const int32_t* order = plan->order.as<int32_t>();
     // the 7-tap stencil on f32 8^3 or 16^3 blocks of a small active set:
     // every colour phase of every sweep in one launch
-    if (g->dtype == MSBG_F32 && (g->bsx == 8 || g->bsx == 16) && stencil == MSBG_LAPLACIAN && plan->n <= kWaveMaxBlocks) {
+    const bool wave =
+        g->dtype == MSBG_F32 && (g->bsx == 8 || g->bsx == 16) && stencil == MSBG_LAPLACIAN && plan->n <= kWaveMaxBlocks;
+    int* prog = nullptr;
+    unsigned int* counter = nullptr;
+    if (wave) {
         MSBG_REQUIRE((double)plan->n * iterations < 2147483647.0, "too many (sweep, block) items for one launch");
         wave_items(plan, g->ctx, iterations);
-        const size_t slots = g->n_slots();
         if (plan->wave_slots < slots) {
             plan->wave_prog.reserve(slots * 4 + 256);
             plan->wave_slots = slots;
         }
-        int* prog = plan->wave_prog.as<int>();
-        unsigned int* counter = reinterpret_cast<unsigned int*>(plan->wave_prog.as<char>() + ((slots * 4 + 127) & ~size_t(127)));
-        begin_launch(g->ctx);
-        wave_init_kernel<<<(unsigned)std::min<size_t>((slots + 255) / 256 + 1, 148 * 8), 256, 0, g->ctx->stream>>>(prog, slots,
-                                                                                                                 counter);
-        after_launch(g->ctx, "wave_init_kernel");
-        begin_launch(g->ctx);
-        wave_zero_kernel<<<(unsigned)std::min<size_t>((plan->n + 255) / 256, 148 * 8), 256, 0, g->ctx->stream>>>(
-            prog, a.nbr, (int)plan->n);
-        after_launch(g->ctx, "wave_zero_kernel");
-        const int total = (int)(plan->n * (size_t)iterations);
-        const int2* items = plan->wave_items.as<int2>();
-        if (g->bsx == 16) launch_wave_laplacian<16>(g->ctx, a, items, total, prog, counter);
-        else launch_wave_laplacian<8>(g->ctx, a, items, total, prog, counter);
+        prog = plan->wave_prog.as<int>();
+        counter = reinterpret_cast<unsigned int*>(plan->wave_prog.as<char>() + ((slots * 4 + 127) & ~size_t(127)));
+    }
+    auto issue = [&]() {
+        const int32_t* xs = plan->xslots.as<int32_t>();
+        const size_t nxs = plan->n_xslots;
+        if (g->dtype == MSBG_F32) xface_init<ElemF32>(g->ctx, g->bsx, g->payload.p, xs, nxs, xd, a.xface);
+        else if (g->dtype == MSBG_U16) xface_init<ElemU16>(g->ctx, g->bsx, g->payload.p, xs, nxs, xd, a.xface);
+        else if (g->dtype == MSBG_U8) xface_init<ElemU8>(g->ctx, g->bsx, g->payload.p, xs, nxs, xd, a.xface);
+        else if (g->dtype == MSBG_F16) xface_init<ElemF16>(g->ctx, g->bsx, g->payload.p, xs, nxs, xd, a.xface);
+        else xface_init<ElemBF16>(g->ctx, g->bsx, g->payload.p, xs, nxs, xd, a.xface);
+        if (wave) {
+            begin_launch(g->ctx);
+            wave_init_kernel<<<(unsigned)std::min<size_t>((slots + 255) / 256 + 1, 148 * 8), 256, 0, g->ctx->stream>>>(
+                prog, slots, counter);
+            after_launch(g->ctx, "wave_init_kernel");
+            begin_launch(g->ctx);
+            wave_zero_kernel<<<(unsigned)std::min<size_t>((plan->n + 255) / 256, 148 * 8), 256, 0, g->ctx->stream>>>(
+                prog, a.nbr, (int)plan->n);
+            after_launch(g->ctx, "wave_zero_kernel");
+            const int total = (int)(plan->n * (size_t)iterations);
+            const int2* items = plan->wave_items.as<int2>();
+            if (g->bsx == 16) launch_wave_laplacian<16>(g->ctx, a, items, total, prog, counter);
+            else launch_wave_laplacian<8>(g->ctx, a, items, total, prog, counter);
+            return;
+        }
+        for (int it = 0; it < iterations; ++it) {
+            a.sr_base = pos0 + (uint64_t)it * chunks_per_sweep;
+            for (int c = 0; c < 8; ++c) {
+                int cnt = plan->color_off[c + 1] - plan->color_off[c];
+                if (!cnt) continue;
+                const int32_t* o = order + plan->color_off[c];
+                if (g->dtype == MSBG_F32) launch_phase_bsx<ElemF32>(g->ctx, g->bsx, stencil, a, o, cnt);
+                else if (g->dtype == MSBG_U16) launch_phase_bsx<ElemU16>(g->ctx, g->bsx, stencil, a, o, cnt);
+                else if (g->dtype == MSBG_U8) launch_phase_bsx<ElemU8>(g->ctx, g->bsx, stencil, a, o, cnt);
+                else if (g->dtype == MSBG_F16) launch_phase_bsx<ElemF16>(g->ctx, g->bsx, stencil, a, o, cnt);
+                else launch_phase_bsx<ElemBF16>(g->ctx, g->bsx, stencil, a, o, cnt);
+            }
+        }
+    };
+    // f32 sweeps: the call's launches (a kernel per colour phase: 80 for 10
+    // sweeps) are captured once into a graph and replayed by later calls with
+    // the same plan, arguments and buffers, so a phase of a few hundred
+    // blocks costs a graph node rather than a host launch.  (Per-kernel
+    // timing launches directly; Density8 sweeps advance the generator
+    // stream every call.)
+    if (g->dtype != MSBG_F32 || g->ctx->timing) {
+        issue();
+        if (stream_pos && g->dtype == MSBG_U8) *stream_pos = pos0 + (uint64_t)iterations * chunks_per_sweep;
         return;
     }
-    for (int it = 0; it < iterations; ++it) {
-        a.sr_base = pos0 + (uint64_t)it * chunks_per_sweep;
-        for (int c = 0; c < 8; ++c) {
-            int cnt = plan->color_off[c + 1] - plan->color_off[c];
-            if (!cnt) continue;
-            const int32_t* o = order + plan->color_off[c];
-            if (g->dtype == MSBG_F32) launch_phase_bsx<ElemF32>(g->ctx, g->bsx, stencil, a, o, cnt);
-            else if (g->dtype == MSBG_U16) launch_phase_bsx<ElemU16>(g->ctx, g->bsx, stencil, a, o, cnt);
-            else if (g->dtype == MSBG_U8) launch_phase_bsx<ElemU8>(g->ctx, g->bsx, stencil, a, o, cnt);
-            else if (g->dtype == MSBG_F16) launch_phase_bsx<ElemF16>(g->ctx, g->bsx, stencil, a, o, cnt);
-            else launch_phase_bsx<ElemBF16>(g->ctx, g->bsx, stencil, a, o, cnt);
+    uint64_t key = 0xcbf29ce484222325ULL;
+    auto bits = [](float f) { uint32_t u; memcpy(&u, &f, 4); return (uint64_t)u; };
+    for (uint64_t v : {(uint64_t)iterations, (uint64_t)stencil, bits(dt), (uint64_t)a.clamp01, (uint64_t)(uintptr_t)a.payload,
+                       (uint64_t)(uintptr_t)a.coarse, (uint64_t)(uintptr_t)a.xface, (uint64_t)(uintptr_t)prog, bits(a.empty),
+                       bits(a.full)})
+        key = fnv(key, v);
+    SweepPlan::Graph* sg = nullptr;
+    for (auto& q : plan->graphs)
+        if (q.key == key) sg = &q;
+    if (!sg) {
+        msbg_ctx* ctx = g->ctx;
+        const uint64_t l0 = ctx->launches;
+        cudaGraph_t graph = nullptr;
+        CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            issue();
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            ctx->launches = l0;
+            throw;
         }
+        CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &graph));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) MSBG_THROW(MSBG_ERR_CUDA, std::string("sweep graph: ") + cudaGetErrorString(e));
+        if (plan->graphs.size() >= 8) {  // keep the most recent few
+            cudaGraphExecDestroy(plan->graphs.front().exec);
+            plan->graphs.erase(plan->graphs.begin());
+        }
+        plan->graphs.push_back({key, exec, (int)(ctx->launches - l0)});
+        ctx->launches = l0;
+        sg = &plan->graphs.back();
     }
-    if (stream_pos && g->dtype == MSBG_U8) *stream_pos = pos0 + (uint64_t)iterations * chunks_per_sweep;
+    CUDA_CHECK(cudaGraphLaunch(sg->exec, g->ctx->stream));
+    g->ctx->launches += (uint64_t)sg->kernels;
 }
 
 }  // namespace msbg

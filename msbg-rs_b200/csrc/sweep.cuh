@@ -34,6 +34,20 @@ struct SweepPlan {
     int wave_iters = -1;
     DevBuf wave_prog;   // int32 [slots], then the counter
     size_t wave_slots = 0;
+    // Captured launches of earlier f32 calls on this plan, keyed by the
+    // arguments and buffers they bake in.
+    struct Graph {
+        uint64_t key;
+        cudaGraphExec_t exec;
+        int kernels;
+    };
+    std::vector<Graph> graphs;
+    SweepPlan() = default;
+    SweepPlan(const SweepPlan&) = delete;
+    SweepPlan& operator=(const SweepPlan&) = delete;
+    ~SweepPlan() {
+        for (auto& q : graphs) cudaGraphExecDestroy(q.exec);
+    }
 };
 
 }  // namespace msbg
