@@ -441,6 +441,92 @@ __global__ void pk_prolong(TransferArgs T, const float* __restrict__ xc, float* 
     }
 }
 
+// The transfers between two levels on one block grid (the fine block size
+// twice the coarse one, coarse block k the parent of fine block k), one CTA
+// per block: the block and a one-cell halo from its neighbours (zeros where
+// a neighbour is absent) staged in shared memory, then pk_restrict's and
+// pk_prolong's sums in the same order.
+template <int LGF>
+__global__ void __launch_bounds__(256) pk_restrict_tile(TransferArgs T, const float* __restrict__ r, float* __restrict__ bc) {
+    constexpr int BF = 1 << LGF, BC = BF / 2, LGC = LGF - 1, W = BF + 2, NC = BC * BC * BC;
+    __shared__ float f[W * W * W];  // fine cells -1 .. BF of the fine block under coarse block k
+    __shared__ int32_t fs[27];
+    const int64_t k = blockIdx.x;
+    if (threadIdx.x < 27) {
+        // fine block at offset (t % 3, t / 3 % 3, t / 9) - 1; the restriction table starts at offset -1
+        const int t = threadIdx.x;
+        fs[t] = T.nb[k * 64 + (t % 3) + 4 * ((t / 3) % 3) + 16 * (t / 9)];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < W * W * W; e += blockDim.x) {
+        const int lx = e % W - 1, ly = (e / W) % W - 1, lz = e / (W * W) - 1;
+        const int ox = lx < 0 ? 0 : lx >= BF ? 2 : 1, oy = ly < 0 ? 0 : ly >= BF ? 2 : 1, oz = lz < 0 ? 0 : lz >= BF ? 2 : 1;
+        const int32_t sl = fs[ox + 3 * oy + 9 * oz];
+        f[e] = sl >= 0 ? r[((int64_t)sl << (3 * LGF)) + ((lx & (BF - 1)) | ((ly & (BF - 1)) << LGF) | ((lz & (BF - 1)) << (2 * LGF)))]
+                       : 0.0f;
+    }
+    __syncthreads();
+    const float w1[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+    for (int v = threadIdx.x; v < NC; v += blockDim.x) {
+        const int64_t i = (k << (3 * LGC)) + v;
+        if (T.diag && !(T.diag[i] > 0.0f)) {
+            bc[i] = 0.0f;
+            continue;
+        }
+        const int qx = v & (BC - 1), qy = (v >> LGC) & (BC - 1), qz = v >> (2 * LGC);
+        const float* fb = f + 2 * qx + W * (2 * qy + W * 2 * qz);  // fine cell 2q - 1 + t sits at window index 2q + t
+        float s = 0.0f;
+#pragma unroll
+        for (int tz = 0; tz < 4; ++tz) {
+#pragma unroll
+            for (int ty = 0; ty < 4; ++ty) {
+                float row = 0.0f;
+#pragma unroll
+                for (int tx = 0; tx < 4; ++tx) row += w1[tx] * fb[tx + W * (ty + W * tz)];
+                s += (w1[ty] * w1[tz]) * row;
+            }
+        }
+        bc[i] = s * 0.125f;
+    }
+}
+
+template <int LGF>
+__global__ void __launch_bounds__(256) pk_prolong_tile(TransferArgs T, const float* __restrict__ xc, float* __restrict__ xf) {
+    constexpr int BF = 1 << LGF, BC = BF / 2, LGC = LGF - 1, W = BC + 2, NF = BF * BF * BF;
+    __shared__ float c[W * W * W];  // coarse cells -1 .. BC of fine block k's parent
+    __shared__ int32_t cs[27];
+    const int64_t k = blockIdx.x;
+    if (threadIdx.x < 27) cs[threadIdx.x] = T.nb[k * 27 + threadIdx.x];
+    __syncthreads();
+    for (int e = threadIdx.x; e < W * W * W; e += blockDim.x) {
+        const int lx = e % W - 1, ly = (e / W) % W - 1, lz = e / (W * W) - 1;
+        const int ox = lx < 0 ? 0 : lx >= BC ? 2 : 1, oy = ly < 0 ? 0 : ly >= BC ? 2 : 1, oz = lz < 0 ? 0 : lz >= BC ? 2 : 1;
+        const int32_t sl = cs[ox + 3 * oy + 9 * oz];
+        c[e] = sl >= 0 ? xc[((int64_t)sl << (3 * LGC)) + ((lx & (BC - 1)) | ((ly & (BC - 1)) << LGC) | ((lz & (BC - 1)) << (2 * LGC)))]
+                       : 0.0f;
+    }
+    __syncthreads();
+    for (int v = threadIdx.x; v < NF; v += blockDim.x) {
+        const int64_t i = (k << (3 * LGF)) + v;
+        if (T.diag && !(T.diag[i] > 0.0f)) continue;
+        const int g[3] = {v & (BF - 1), (v >> LGF) & (BF - 1), v >> (2 * LGF)};
+        int near[3], far[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            near[a] = g[a] >> 1;
+            far[a] = near[a] + ((g[a] & 1) ? 1 : -1);
+        }
+        float s = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int cx = (q & 1) ? far[0] : near[0], cy = (q & 2) ? far[1] : near[1], cz = (q & 4) ? far[2] : near[2];
+            const float w = ((q & 1) ? 0.25f : 0.75f) * ((q & 2) ? 0.25f : 0.75f) * ((q & 4) ? 0.25f : 0.75f);
+            s += w * c[(cx + 1) + W * ((cy + 1) + W * (cz + 1))];
+        }
+        xf[i] += s;
+    }
+}
+
 // x_c = A^-1 b_c with the FP64 inverse, one warp per row.  The inverse of
 // the symmetric operator is symmetric, so row i is column i: its n entries
 // are contiguous and the warp reads them coalesced.  Lane partial sums are
@@ -861,16 +947,34 @@ static void vcycle(msbg_poisson* P, int l, float* x, const float* b, bool x_zero
     PLevelDev& C = P->lv[l + 1];
     jacobi(P, l, x, b, P->nu1, P->omega, x_zero);
     launch_residual(P, l, x, b, F.r.as<float>());
+    // the fine block size twice the coarse one: coarse block k is fine block k's parent
+    const bool same_grid = F.bs == 2 * C.bs && F.lg >= 2 && F.lg <= 4;
     TransferArgs R{C.coords.as<int32_t>(), C.rnb.as<int32_t>(), nullptr, nullptr, C.diag.as<float>(), F.lg, C.lg, C.cells()};
     begin_launch(P->ctx);
-    pk_restrict<<<grid_for(C.cells()), 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
-    after_launch(P->ctx, "pk_restrict");
+    if (same_grid) {
+        const unsigned nb = (unsigned)C.n();
+        if (F.lg == 4) pk_restrict_tile<4><<<nb, 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        else if (F.lg == 3) pk_restrict_tile<3><<<nb, 128, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        else pk_restrict_tile<2><<<nb, 64, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        after_launch(P->ctx, "pk_restrict_tile");
+    } else {
+        pk_restrict<<<grid_for(C.cells()), 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        after_launch(P->ctx, "pk_restrict");
+    }
     vcycle(P, l + 1, C.x.as<float>(), C.b.as<float>(), true);
     TransferArgs T{F.coords.as<int32_t>(), F.pnb.as<int32_t>(), C.coords.as<int32_t>(), F.parent.as<int32_t>(),
                    F.diag.p ? F.diag.as<float>() : nullptr, F.lg, C.lg, F.cells()};
     begin_launch(P->ctx);
-    pk_prolong<<<grid_for(F.cells()), 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
-    after_launch(P->ctx, "pk_prolong");
+    if (same_grid) {
+        const unsigned nb = (unsigned)F.n();
+        if (F.lg == 4) pk_prolong_tile<4><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        else if (F.lg == 3) pk_prolong_tile<3><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        else pk_prolong_tile<2><<<nb, 64, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        after_launch(P->ctx, "pk_prolong_tile");
+    } else {
+        pk_prolong<<<grid_for(F.cells()), 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        after_launch(P->ctx, "pk_prolong");
+    }
     jacobi(P, l, x, b, P->nu2, P->omega, false);
 }
 
