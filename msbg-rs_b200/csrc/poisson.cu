@@ -94,8 +94,22 @@ struct msbg_poisson {
         int kernels;
     };
     std::vector<VGraph> vgraphs;
+    // Captured solve loops of methods 0 and 1 (iterations in a device-side
+    // while loop, no host read between them), one per (method, b, x64).
+    struct SGraph {
+        int method;
+        const float* b;
+        const double* x64;
+        cudaGraphExec_t exec;
+        int kernels_first, kernels_body;  // launches before the loop and per loop iteration
+    };
+    std::vector<SGraph> sgraphs;
+    msbg::DevBuf sctl;   // SolveCtl of the captured loops
+    msbg::DevBuf shist;  // f64 [capacity] relative residual per iteration
     ~msbg_poisson() {
         for (auto& g : vgraphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        for (auto& g : sgraphs)
             if (g.exec) cudaGraphExecDestroy(g.exec);
     }
 };
@@ -111,9 +125,10 @@ struct LevelArgs {
     const float* diag;  // per-cell diagonal (0: inactive cell), or null: 6 s, every cell active
 };
 
-// Sum of the 6 face neighbours of cell i (zero outside the active blocks).
-template <typename T>
-__device__ __forceinline__ T nb_sum(const LevelArgs& L, const T* __restrict__ x, int64_t i) {
+// Sum of the 6 face neighbours of cell i (zero outside the active blocks),
+// the value at cell index j given by get(j).
+template <typename T, typename G>
+__device__ __forceinline__ T nb_sum_of(const LevelArgs& L, int64_t i, G get) {
     const int bs = 1 << L.lg, m = bs - 1;
     const int64_t k = i >> (3 * L.lg);
     const int v = (int)(i & ((1 << (3 * L.lg)) - 1));
@@ -122,29 +137,33 @@ __device__ __forceinline__ T nb_sum(const LevelArgs& L, const T* __restrict__ x,
     T s;
     {
         const int32_t kk = cx > 0 ? (int32_t)k : nb[0];
-        s = kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + (v & ~m) + ((cx - 1) & m)] : T(0);
+        s = kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + (v & ~m) + ((cx - 1) & m)) : T(0);
     }
     {
         const int32_t kk = cx < m ? (int32_t)k : nb[1];
-        s += kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + (v & ~m) + ((cx + 1) & m)] : T(0);
+        s += kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + (v & ~m) + ((cx + 1) & m)) : T(0);
     }
     {
         const int32_t kk = cy > 0 ? (int32_t)k : nb[2];
-        s += kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + cx + (((cy - 1) & m) << L.lg) + (cz << (2 * L.lg))] : T(0);
+        s += kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + cx + (((cy - 1) & m) << L.lg) + (cz << (2 * L.lg))) : T(0);
     }
     {
         const int32_t kk = cy < m ? (int32_t)k : nb[3];
-        s += kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + cx + (((cy + 1) & m) << L.lg) + (cz << (2 * L.lg))] : T(0);
+        s += kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + cx + (((cy + 1) & m) << L.lg) + (cz << (2 * L.lg))) : T(0);
     }
     {
         const int32_t kk = cz > 0 ? (int32_t)k : nb[4];
-        s += kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + cx + (cy << L.lg) + (((cz - 1) & m) << (2 * L.lg))] : T(0);
+        s += kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + cx + (cy << L.lg) + (((cz - 1) & m) << (2 * L.lg))) : T(0);
     }
     {
         const int32_t kk = cz < m ? (int32_t)k : nb[5];
-        s += kk >= 0 ? x[((int64_t)kk << (3 * L.lg)) + cx + (cy << L.lg) + (((cz + 1) & m) << (2 * L.lg))] : T(0);
+        s += kk >= 0 ? get(((int64_t)kk << (3 * L.lg)) + cx + (cy << L.lg) + (((cz + 1) & m) << (2 * L.lg))) : T(0);
     }
     return s;
+}
+template <typename T>
+__device__ __forceinline__ T nb_sum(const LevelArgs& L, const T* __restrict__ x, int64_t i) {
+    return nb_sum_of<T>(L, i, [x](int64_t j) { return x[j]; });
 }
 
 // y = A x
@@ -214,15 +233,40 @@ __global__ void pk_jacobi(LevelArgs L, const float* __restrict__ x, const float*
     }
 }
 
+// The first two weighted Jacobi sweeps from x = 0 in one pass: the first
+// sweep's x1 = w b / (6 s) (w b / d with a diagonal; 0 at inactive cells) is
+// formed where the second sweep reads it, with pk_jacobi's operations, so the
+// result is the two sweeps' bits (x1's products rounded on their own, as
+// when x1 is stored, not fused into the neighbour sum).
+__global__ void pk_jacobi_zero2(LevelArgs L, const float* __restrict__ b, float* __restrict__ xn, float omega) {
+    const float inv_d = 1.0f / (6.0f * L.scale);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L.cells; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!L.diag) {
+            auto x1 = [&](int64_t j) { return __fmul_rn(__fmul_rn(omega, b[j]), inv_d); };
+            xn[i] = omega * (b[i] + L.scale * nb_sum_of<float>(L, i, x1)) * inv_d + (1.0f - omega) * x1(i);
+        } else {
+            const float d = L.diag[i];
+            auto x1 = [&](int64_t j) {
+                const float dj = L.diag[j];
+                return !(dj > 0.0f) ? 0.0f : __fdiv_rn(__fmul_rn(omega, b[j]), dj);
+            };
+            if (!(d > 0.0f)) xn[i] = 0.0f;
+            else xn[i] = omega * (b[i] + L.scale * nb_sum_of<float>(L, i, x1)) / d + (1.0f - omega) * x1(i);
+        }
+    }
+}
+
 // The 7-point kernels on 16^3 blocks.  Both tile kernels add the neighbours
 // x-1, x+1, y-1, y+1, z-1, z+1 in that order (zeros outside the active
 // blocks, as nb_sum) and round every operation as written (no contraction),
 // so every tile choice gives the same bits:
 // OP 0: weighted Jacobi xn = w (b + s nb) / (6 s) + (1 - w) x (x null: the
-// first sweep from zero); 1: residual r = b - s (6 x - nb); 2: y = s (6 x - nb).
+// first sweep from zero); 1: residual r = b - s (6 x - nb); 2: y = s (6 x - nb);
+// 3: OP 0 on x1 = w b / (6 s), the first sweep from zero formed from b where
+// it is read (x is b): the first two sweeps from zero in one pass, bit for bit.
 template <int OP>
 __device__ __forceinline__ float op7(float sn, float cur, float bz, float scale, float omega, float inv_d) {
-    if (OP == 0)
+    if (OP == 0 || OP == 3)
         return __fadd_rn(__fmul_rn(__fmul_rn(omega, __fadd_rn(bz, __fmul_rn(scale, sn))), inv_d),
                          __fmul_rn(__fsub_rn(1.0f, omega), cur));
     if (OP == 1) return __fsub_rn(bz, __fmul_rn(scale, __fsub_rn(__fmul_rn(6.0f, cur), sn)));
@@ -261,21 +305,22 @@ __global__ void __launch_bounds__(256) pk_block16(LevelArgs L, const float* __re
     if (threadIdx.x < 6) nb[threadIdx.x] = L.nbr[k * 6 + threadIdx.x];
     __syncthreads();
     const int32_t nxm = nb[0], nxp = nb[1], nym = nb[2], nyp = nb[3], nzm = nb[4], nzp = nb[5];
-    const float* xb = x + base;
+    // the value the sweep reads at x[j]: x1 = w b inv_d for OP 3
+    auto xv = [&](int64_t j) -> float { return OP == 3 ? __fmul_rn(__fmul_rn(omega, x[j]), inv_d) : x[j]; };
     auto plane = [&](int z) -> float {  // this column's value at plane z in [-1, 16]
-        if (z < 0) return nzm >= 0 ? x[((int64_t)nzm << 12) + col + (15 << 8)] : 0.0f;
-        if (z > 15) return nzp >= 0 ? x[((int64_t)nzp << 12) + col] : 0.0f;
-        return xb[col + (z << 8)];
+        if (z < 0) return nzm >= 0 ? xv(((int64_t)nzm << 12) + col + (15 << 8)) : 0.0f;
+        if (z > 15) return nzp >= 0 ? xv(((int64_t)nzp << 12) + col) : 0.0f;
+        return xv(base + col + (z << 8));
     };
     float down = plane(z0 - 1), cur = plane(z0), up = plane(z0 + 1);
     for (int z = z0; z < z0 + SLAB; ++z) {
         const float upn = z + 2 <= 16 ? plane(z + 2) : 0.0f;
         const float bz = OP == 2 ? 0.0f : b[base + col + (z << 8)];
         pl[ty + 1][tx + 1] = cur;
-        if (tx == 0) pl[ty + 1][0] = nxm >= 0 ? x[((int64_t)nxm << 12) + 15 + (ty << 4) + (z << 8)] : 0.0f;
-        if (tx == 15) pl[ty + 1][17] = nxp >= 0 ? x[((int64_t)nxp << 12) + (ty << 4) + (z << 8)] : 0.0f;
-        if (ty == 0) pl[0][tx + 1] = nym >= 0 ? x[((int64_t)nym << 12) + tx + (15 << 4) + (z << 8)] : 0.0f;
-        if (ty == 15) pl[17][tx + 1] = nyp >= 0 ? x[((int64_t)nyp << 12) + tx + (z << 8)] : 0.0f;
+        if (tx == 0) pl[ty + 1][0] = nxm >= 0 ? xv(((int64_t)nxm << 12) + 15 + (ty << 4) + (z << 8)) : 0.0f;
+        if (tx == 15) pl[ty + 1][17] = nxp >= 0 ? xv(((int64_t)nxp << 12) + (ty << 4) + (z << 8)) : 0.0f;
+        if (ty == 0) pl[0][tx + 1] = nym >= 0 ? xv(((int64_t)nym << 12) + tx + (15 << 4) + (z << 8)) : 0.0f;
+        if (ty == 15) pl[17][tx + 1] = nyp >= 0 ? xv(((int64_t)nyp << 12) + tx + (z << 8)) : 0.0f;
         __syncthreads();
         const float sn = nb6(pl[ty + 1][tx], pl[ty + 1][tx + 2], pl[ty][tx + 1], pl[ty + 2][tx + 1], down, up);
         out[base + col + (z << 8)] = op7<OP>(sn, cur, bz, L.scale, omega, inv_d);
@@ -319,21 +364,27 @@ __global__ void __launch_bounds__(64) pk_quad16(LevelArgs L, const float* __rest
     const int32_t nxm = __ldg(nbr), nxp = __ldg(nbr + 1), nym = __ldg(nbr + 2), nyp = __ldg(nbr + 3), nzm = __ldg(nbr + 4),
                   nzp = __ldg(nbr + 5);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // the values the sweep reads: x1 = w b inv_d for OP 3
+    auto tr = [&](float v) -> float { return OP == 3 ? __fmul_rn(__fmul_rn(omega, v), inv_d) : v; };
+    auto xv4 = [&](const float* p) -> float4 {
+        const float4 v = ld4(p);
+        return make_float4(tr(v.x), tr(v.y), tr(v.z), tr(v.w));
+    };
     auto plane = [&](int z) -> float4 {  // this thread's quad at plane z in [-1, 16]
-        if (z < 0) return nzm >= 0 ? ld4(x + ((int64_t)nzm << 12) + off + (15 << 8)) : zero;
-        if (z > 15) return nzp >= 0 ? ld4(x + ((int64_t)nzp << 12) + off) : zero;
-        return ld4(x + base + off + (z << 8));
+        if (z < 0) return nzm >= 0 ? xv4(x + ((int64_t)nzm << 12) + off + (15 << 8)) : zero;
+        if (z > 15) return nzp >= 0 ? xv4(x + ((int64_t)nzp << 12) + off) : zero;
+        return xv4(x + base + off + (z << 8));
     };
     float4 down = plane(-1), cur = plane(0), up = plane(1);
     for (int z = 0; z < 16; ++z) {
         const int buf = z & 1;
         const float4 upn = z + 2 <= 16 ? plane(z + 2) : zero;
         const float4 bz = OP == 2 ? zero : ld4(b + base + off + (z << 8));
-        const float xl = q == 0 && nxm >= 0 ? x[((int64_t)nxm << 12) + 15 + (y << 4) + (z << 8)] : 0.0f;
-        const float xr = q == 3 && nxp >= 0 ? x[((int64_t)nxp << 12) + (y << 4) + (z << 8)] : 0.0f;
+        const float xl = q == 0 && nxm >= 0 ? tr(x[((int64_t)nxm << 12) + 15 + (y << 4) + (z << 8)]) : 0.0f;
+        const float xr = q == 3 && nxp >= 0 ? tr(x[((int64_t)nxp << 12) + (y << 4) + (z << 8)]) : 0.0f;
         pl[buf][y + 1][q] = cur;
-        if (y == 0) pl[buf][0][q] = nym >= 0 ? ld4(x + ((int64_t)nym << 12) + (15 << 4) + (q << 2) + (z << 8)) : zero;
-        if (y == 15) pl[buf][17][q] = nyp >= 0 ? ld4(x + ((int64_t)nyp << 12) + (q << 2) + (z << 8)) : zero;
+        if (y == 0) pl[buf][0][q] = nym >= 0 ? xv4(x + ((int64_t)nym << 12) + (15 << 4) + (q << 2) + (z << 8)) : zero;
+        if (y == 15) pl[buf][17][q] = nyp >= 0 ? xv4(x + ((int64_t)nyp << 12) + (q << 2) + (z << 8)) : zero;
         float lw = __shfl_up_sync(0xffffffffu, cur.w, 1);
         float rx = __shfl_down_sync(0xffffffffu, cur.x, 1);
         if (q == 0) lw = xl;
@@ -446,8 +497,10 @@ __global__ void pk_prolong(TransferArgs T, const float* __restrict__ xc, float* 
 // per block: the block and a one-cell halo from its neighbours (zeros where
 // a neighbour is absent) staged in shared memory, then pk_restrict's and
 // pk_prolong's sums in the same order.
-template <int LGF>
-__global__ void __launch_bounds__(256) pk_restrict_tile(TransferArgs T, const float* __restrict__ r, float* __restrict__ bc) {
+// NT threads a CTA; the staging loops are unrolled so that a thread's loads
+// are in flight together.
+template <int LGF, int NT>
+__global__ void __launch_bounds__(NT) pk_restrict_tile(TransferArgs T, const float* __restrict__ r, float* __restrict__ bc) {
     constexpr int BF = 1 << LGF, BC = BF / 2, LGC = LGF - 1, W = BF + 2, NC = BC * BC * BC;
     __shared__ float f[W * W * W];  // fine cells -1 .. BF of the fine block under coarse block k
     __shared__ int32_t fs[27];
@@ -458,7 +511,10 @@ __global__ void __launch_bounds__(256) pk_restrict_tile(TransferArgs T, const fl
         fs[t] = T.nb[k * 64 + (t % 3) + 4 * ((t / 3) % 3) + 16 * (t / 9)];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < W * W * W; e += blockDim.x) {
+#pragma unroll
+    for (int e0 = 0; e0 < W * W * W; e0 += NT) {
+        const int e = e0 + (int)threadIdx.x;
+        if (e >= W * W * W) break;
         const int lx = e % W - 1, ly = (e / W) % W - 1, lz = e / (W * W) - 1;
         const int ox = lx < 0 ? 0 : lx >= BF ? 2 : 1, oy = ly < 0 ? 0 : ly >= BF ? 2 : 1, oz = lz < 0 ? 0 : lz >= BF ? 2 : 1;
         const int32_t sl = fs[ox + 3 * oy + 9 * oz];
@@ -467,7 +523,7 @@ __global__ void __launch_bounds__(256) pk_restrict_tile(TransferArgs T, const fl
     }
     __syncthreads();
     const float w1[4] = {0.25f, 0.75f, 0.75f, 0.25f};
-    for (int v = threadIdx.x; v < NC; v += blockDim.x) {
+    for (int v = threadIdx.x; v < NC; v += NT) {
         const int64_t i = (k << (3 * LGC)) + v;
         if (T.diag && !(T.diag[i] > 0.0f)) {
             bc[i] = 0.0f;
@@ -490,15 +546,18 @@ __global__ void __launch_bounds__(256) pk_restrict_tile(TransferArgs T, const fl
     }
 }
 
-template <int LGF>
-__global__ void __launch_bounds__(256) pk_prolong_tile(TransferArgs T, const float* __restrict__ xc, float* __restrict__ xf) {
+template <int LGF, int NT>
+__global__ void __launch_bounds__(NT) pk_prolong_tile(TransferArgs T, const float* __restrict__ xc, float* __restrict__ xf) {
     constexpr int BF = 1 << LGF, BC = BF / 2, LGC = LGF - 1, W = BC + 2, NF = BF * BF * BF;
     __shared__ float c[W * W * W];  // coarse cells -1 .. BC of fine block k's parent
     __shared__ int32_t cs[27];
     const int64_t k = blockIdx.x;
     if (threadIdx.x < 27) cs[threadIdx.x] = T.nb[k * 27 + threadIdx.x];
     __syncthreads();
-    for (int e = threadIdx.x; e < W * W * W; e += blockDim.x) {
+#pragma unroll
+    for (int e0 = 0; e0 < W * W * W; e0 += NT) {
+        const int e = e0 + (int)threadIdx.x;
+        if (e >= W * W * W) break;
         const int lx = e % W - 1, ly = (e / W) % W - 1, lz = e / (W * W) - 1;
         const int ox = lx < 0 ? 0 : lx >= BC ? 2 : 1, oy = ly < 0 ? 0 : ly >= BC ? 2 : 1, oz = lz < 0 ? 0 : lz >= BC ? 2 : 1;
         const int32_t sl = cs[ox + 3 * oy + 9 * oz];
@@ -506,7 +565,8 @@ __global__ void __launch_bounds__(256) pk_prolong_tile(TransferArgs T, const flo
                        : 0.0f;
     }
     __syncthreads();
-    for (int v = threadIdx.x; v < NF; v += blockDim.x) {
+#pragma unroll 4
+    for (int v = threadIdx.x; v < NF; v += NT) {
         const int64_t i = (k << (3 * LGF)) + v;
         if (T.diag && !(T.diag[i] > 0.0f)) continue;
         const int g[3] = {v & (BF - 1), (v >> LGF) & (BF - 1), v >> (2 * LGF)};
@@ -656,6 +716,26 @@ static dim3 shape_grid(int cfg, int64_t n) {
 
 static LevelArgs level_args(const PLevelDev& L) {
     return LevelArgs{L.nbr.as<int32_t>(), L.lg, L.cells(), L.scale, L.diag.p ? L.diag.as<float>() : nullptr};
+}
+
+// Control block of a captured solve loop: iterations run, the limit, the
+// stopping threshold tol |b| and |b|.
+struct SolveCtl {
+    long long it, max_iter;
+    double thr, bn;
+};
+
+// The test at the end of a captured solve iteration: counts it, records
+// |r| / |b| and keeps the loop running while |r| > tol |b|, the limit is not
+// reached and (check_bad) CG saw no breakdown.  One thread.
+__global__ void pk_solve_test(cudaGraphConditionalHandle h, const double* __restrict__ sc, SolveCtl* __restrict__ c,
+                              double* __restrict__ hist, int check_bad) {
+    const long long it = c->it + 1;
+    c->it = it;
+    const double rn = sqrt(sc[SC_RR]);
+    hist[it - 1] = rn / c->bn;
+    const bool bad = check_bad && sc[SC_BAD] != 0.0;
+    cudaGraphSetConditional(h, (rn > c->thr && it < c->max_iter && !bad) ? 1u : 0u);
 }
 
 static void upload(msbg_ctx* ctx, DevBuf& d, const void* h, size_t bytes) {
@@ -919,7 +999,21 @@ static void launch_residual(msbg_poisson* P, int l, const float* x, const float*
 static void jacobi(msbg_poisson* P, int l, float* x, const float* b, int sweeps, float omega, bool x_zero) {
     PLevelDev& L = P->lv[l];
     float* t = L.t.as<float>();
-    for (int s = 0; s < sweeps; ++s) {
+    int s = 0;
+    if (x_zero && sweeps >= 2) {
+        // the first two sweeps from zero in one pass, into x (where the second sweep writes)
+        begin_launch(P->ctx);
+        if (uses_block16(L)) {
+            launch_block16<3>(P->ctx, L, L.slab, b, b, x, omega);
+            after_launch(P->ctx, "pk_block16_jacobi0");
+        } else {
+            pk_jacobi_zero2<<<shape_grid(L.cfg_jac, L.cells()), kShapes[L.cfg_jac].threads, 0, P->ctx->stream>>>(
+                level_args(L), b, x, omega);
+            after_launch(P->ctx, "pk_jacobi_zero2");
+        }
+        s = 2;
+    }
+    for (; s < sweeps; ++s) {
         const float* src = (s % 2 == 0) ? x : t;
         float* dst = (s % 2 == 0) ? t : x;
         begin_launch(P->ctx);
@@ -953,9 +1047,9 @@ static void vcycle(msbg_poisson* P, int l, float* x, const float* b, bool x_zero
     begin_launch(P->ctx);
     if (same_grid) {
         const unsigned nb = (unsigned)C.n();
-        if (F.lg == 4) pk_restrict_tile<4><<<nb, 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
-        else if (F.lg == 3) pk_restrict_tile<3><<<nb, 128, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
-        else pk_restrict_tile<2><<<nb, 64, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        if (F.lg == 4) pk_restrict_tile<4, 256><<<nb, 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        else if (F.lg == 3) pk_restrict_tile<3, 128><<<nb, 128, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
+        else pk_restrict_tile<2, 64><<<nb, 64, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
         after_launch(P->ctx, "pk_restrict_tile");
     } else {
         pk_restrict<<<grid_for(C.cells()), 256, 0, P->ctx->stream>>>(R, F.r.as<float>(), C.b.as<float>());
@@ -967,9 +1061,9 @@ static void vcycle(msbg_poisson* P, int l, float* x, const float* b, bool x_zero
     begin_launch(P->ctx);
     if (same_grid) {
         const unsigned nb = (unsigned)F.n();
-        if (F.lg == 4) pk_prolong_tile<4><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
-        else if (F.lg == 3) pk_prolong_tile<3><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
-        else pk_prolong_tile<2><<<nb, 64, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        if (F.lg == 4) pk_prolong_tile<4, 256><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        else if (F.lg == 3) pk_prolong_tile<3, 256><<<nb, 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
+        else pk_prolong_tile<2, 64><<<nb, 64, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
         after_launch(P->ctx, "pk_prolong_tile");
     } else {
         pk_prolong<<<grid_for(F.cells()), 256, 0, P->ctx->stream>>>(T, C.x.as<float>(), x);
@@ -1072,6 +1166,155 @@ static void vcycle_top(msbg_poisson* P, float* x, const float* b) {
     ctx->launches += (uint64_t)g->kernels;
 }
 
+// Releases the captured V-cycles and solve loops: they bake in the smoother
+// parameters, the launch shapes and the buffers.
+static void drop_graphs(msbg_poisson* P) {
+    if (P->vgraphs.empty() && P->sgraphs.empty()) return;
+    sync(P->ctx);
+    for (auto& g : P->vgraphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& g : P->sgraphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    P->vgraphs.clear();
+    P->sgraphs.clear();
+}
+
+// Iterations of method 0 (z = V r, x += z, r = b - A x) or of method 1 (MG-
+// PCG from a restart: z = V r, p = z, then CG steps) in one graph launch: a
+// device-side while loop whose test (pk_solve_test) ends every iteration, so
+// the host waits once instead of once per iteration.  The kernels and their
+// order are those of the host loop in solve().  Captured on the first use of
+// each (method, b, x64).  Returns the iterations the launch ran; sc_out gets
+// the CG scalar block after it.
+static int solve_loop(msbg_poisson* P, int method, const float* b, double* x64, float* r, float* z, float* p, float* q,
+                      long long it0, long long max_iter, double thr, double bn, double* sc_out) {
+    msbg_ctx* ctx = P->ctx;
+    const int64_t n = P->lv[0].cells();
+    if (P->shist.bytes < (size_t)max_iter * 8) {
+        drop_graphs(P);  // the graphs bake in the history buffer
+        P->shist.reserve((size_t)max_iter * 8);
+    }
+    if (!P->sctl.p) P->sctl.reserve(sizeof(SolveCtl));
+    double* sc = cg_scalars(P);
+    SolveCtl* ctl = P->sctl.as<SolveCtl>();
+    double* hist = P->shist.as<double>();
+    msbg_poisson::SGraph* g = nullptr;
+    for (auto& v : P->sgraphs)
+        if (v.method == method && v.b == b && v.x64 == x64) g = &v;
+    if (!g) {
+        auto cg_step = [&](cudaGraphConditionalHandle h) {  // q = A p, alpha, x += alpha p, r -= alpha q, r.r, test
+            launch_matvec(P, 0, p, q);
+            dot_dev(P, p, q, n, SC_PQ);
+            begin_launch(ctx);
+            pk_cg_update<<<grid_for(n), 256, 0, ctx->stream>>>(n, sc, p, q, x64, r);
+            after_launch(ctx, "pk_cg_update");
+            dot_dev(P, r, r, n, SC_RR);
+            begin_launch(ctx);
+            pk_solve_test<<<1, 1, 0, ctx->stream>>>(h, sc, ctl, hist, 1);
+            after_launch(ctx, "pk_solve_test");
+        };
+        cudaGraph_t G = nullptr;
+        CUDA_CHECK(cudaGraphCreate(&G, 0));
+        const uint64_t l0 = ctx->launches;
+        bool capturing = false;
+        int k_first = 0, k_body = 0;
+        cudaGraphExec_t exec = nullptr;
+        try {
+            // method 0 enters the loop at once (the host has tested |r|);
+            // method 1 runs the restart and its first CG step before the loop
+            cudaGraphConditionalHandle h;
+            CUDA_CHECK(cudaGraphConditionalHandleCreate(&h, G, method == 0 ? 1u : 0u,
+                                                        method == 0 ? cudaGraphCondAssignDefault : 0u));
+            cudaGraphNode_t tail = nullptr;
+            if (method == 1) {
+                CUDA_CHECK(cudaStreamBeginCaptureToGraph(ctx->stream, G, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+                capturing = true;
+                vcycle(P, 0, z, r, true);
+                CUDA_CHECK(cudaMemcpyAsync(p, z, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+                dot_dev(P, r, z, n, SC_RZ);
+                cg_step(h);
+                CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &G));
+                capturing = false;
+                k_first = (int)(ctx->launches - l0);
+                // the captured chain's last node
+                size_t nn = 0;
+                CUDA_CHECK(cudaGraphGetNodes(G, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                CUDA_CHECK(cudaGraphGetNodes(G, nodes.data(), &nn));
+                for (cudaGraphNode_t nd : nodes) {
+                    size_t nout = 0;
+                    CUDA_CHECK(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+                    if (nout == 0) tail = nd;
+                }
+                MSBG_REQUIRE(tail != nullptr, "captured solve: no last node");
+            }
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t loop_node;
+            CUDA_CHECK(cudaGraphAddNode(&loop_node, G, tail ? &tail : nullptr, tail ? 1 : 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const uint64_t l1 = ctx->launches;
+            CUDA_CHECK(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            capturing = true;
+            vcycle(P, 0, z, r, true);
+            if (method == 0) {
+                add64(P, n, 1.0, z, x64);
+                launch_residual64(P, x64, b, r);
+                dot_dev(P, r, r, n, SC_RR);
+                begin_launch(ctx);
+                pk_solve_test<<<1, 1, 0, ctx->stream>>>(h, sc, ctl, hist, 0);
+                after_launch(ctx, "pk_solve_test");
+            } else {
+                dot_dev(P, r, z, n, SC_RZ2);
+                begin_launch(ctx);
+                pk_cg_beta<<<1, 1, 0, ctx->stream>>>(sc, 0);
+                after_launch(ctx, "pk_cg_beta");
+                begin_launch(ctx);
+                pk_cg_direction<<<grid_for(n), 256, 0, ctx->stream>>>(n, sc, z, p);
+                after_launch(ctx, "pk_cg_direction");
+                cg_step(h);
+            }
+            CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &body));
+            capturing = false;
+            k_body = (int)(ctx->launches - l1);
+            CUDA_CHECK(cudaGraphInstantiate(&exec, G, 0));
+        } catch (...) {
+            if (capturing) {
+                cudaGraph_t tmp = nullptr;
+                cudaStreamEndCapture(ctx->stream, &tmp);
+            }
+            cudaGraphDestroy(G);
+            ctx->launches = l0;
+            throw;
+        }
+        cudaGraphDestroy(G);
+        ctx->launches = l0;
+        P->sgraphs.push_back({method, b, x64, exec, k_first, k_body});
+        g = &P->sgraphs.back();
+    }
+    const SolveCtl c0{it0, max_iter, thr, bn};
+    CUDA_CHECK(cudaMemcpyAsync(ctl, &c0, sizeof(c0), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_CHECK(cudaGraphLaunch(g->exec, ctx->stream));
+    SolveCtl c1;
+    {
+        SmallReads rd(ctx);
+        rd.add(&c1, ctl, sizeof(c1));
+        rd.add(sc_out, sc, SC_COUNT * 8);
+        rd.wait();
+    }
+    const int ran = (int)(c1.it - it0);
+    // method 1: the first iteration is the part before the loop
+    ctx->launches += (uint64_t)g->kernels_first + (uint64_t)(method == 1 ? ran - 1 : ran) * (uint64_t)g->kernels_body;
+    return ran;
+}
+
+// Relative residuals of iterations [from, to) of the last captured solve loop.
+static void loop_history(msbg_poisson* P, double* hist, long long from, long long to) {
+    if (hist && to > from) read_small(P->ctx, hist + from, P->shist.as<double>() + from, (size_t)(to - from) * 8);
+}
+
 // Preconditioners of the CG solve.
 enum { PC_MG = 0, PC_NET = 1, PC_HYBRID = 2 };
 
@@ -1147,6 +1390,14 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
         // V when an iteration fails to halve the residual
         bool learned = method == 4;
         double rn_prev = rn;
+        if (method == 0 && !P->ctx->timing && rn > tol * bn && it < max_iter) {
+            double hs[SC_COUNT];
+            it = solve_loop(P, 0, b, x64, r, z, nullptr, nullptr, 0, max_iter, tol * bn, bn, hs);
+            P->n_vcycle += it;
+            loop_history(P, hist, 0, it);
+            rn = std::sqrt(hs[SC_RR]);
+            if (!std::isfinite(rn)) MSBG_THROW(MSBG_ERR_NUMERIC, "multigrid residual is not finite");
+        }
         while (rn > tol * bn && it < max_iter) {
             if (learned) {
                 learned_cycle(P, z, r, sv, uv);
@@ -1209,71 +1460,90 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
             since = 0;
         };
         rn_hist.push_back(rn);  // the window below always holds the start
-        restart();
-        if (flexible && !(rz > 0.0)) fall_back(3);
-        while (rn > tol * bn && it < max_iter) {
-            // q = A p, alpha = r.z / p.Ap, x += alpha p, r -= alpha q and r.r
-            // run back to back on the device; the host reads the scalars once
-            launch_matvec(P, 0, p, q);
-            dot_dev(P, p, q, n, SC_PQ);
-            if (flexible) CUDA_CHECK(cudaMemcpyAsync(r_old, r, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
-            begin_launch(P->ctx);
-            pk_cg_update<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, p, q, x64, r);
-            after_launch(P->ctx, "pk_cg_update");
-            dot_dev(P, r, r, n, SC_RR);
-            read_scalars(P, hs);
-            if (hs[SC_BAD] != 0.0) {  // p.Ap <= 0: x and r were left as they were
-                if (flexible && pc != PC_MG) {
-                    fall_back(2);
-                    continue;
+        if (method == 1 && !P->ctx->timing) {
+            // the captured loop: a restart and CG steps until |r| <= tol |b|,
+            // the limit or a breakdown; then the host loop's checks
+            while (rn > tol * bn && it < max_iter) {
+                const int ran = solve_loop(P, 1, b, x64, r, z, p, q, it, max_iter, tol * bn, bn, hs);
+                P->n_vcycle += ran;
+                loop_history(P, hist, it, it + ran);
+                it += ran;
+                if (hs[SC_BAD] != 0.0) MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
+                rn = std::sqrt(hs[SC_RR]);
+                if (rn <= tol * bn) {
+                    // the true residual decides; above tol the loop restarts from it
+                    launch_residual64(P, x64, b, r);
+                    rn = std::sqrt(dot(P, r, r, n));
+                    if (hist) hist[it - 1] = rn / bn;
                 }
-                MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
             }
-            rn = std::sqrt(hs[SC_RR]);
-            ++it;
-            if (rn <= tol * bn) {
-                launch_residual64(P, x64, b, r);
-                rn = std::sqrt(dot(P, r, r, n));
-                if (hist) hist[it - 1] = rn / bn;
-                if (rn <= tol * bn) break;
-                restart();
-                since = 0;
-                continue;
-            }
-            if (hist) hist[it - 1] = rn / bn;
-            rn_hist.push_back(rn);
-            ++since;
-            // stall: the residual norm of CG is not monotone, so the test is
-            // over a window: less than a halving in the last 4 iterations
-            if (flexible && pc != PC_MG && since >= 4 && rn > 0.5 * rn_hist[rn_hist.size() - 5]) {
-                fall_back(1);
-                continue;
-            }
-            if (lead > 0 && pc == PC_HYBRID && P->n_net >= lead) {
-                // method 5: the lead is over; CG restarts from the current
-                // iterate with the fixed V-cycle preconditioner
-                pc = PC_MG;
-                flexible = false;
-                restart();
-                since = 0;
-                continue;
-            }
-            precondition(r, z);
-            dot_dev(P, r, z, n, SC_RZ2);
-            if (flexible) dot_dev(P, z, r_old, n, SC_ZR);
-            begin_launch(P->ctx);
-            pk_cg_beta<<<1, 1, 0, P->ctx->stream>>>(sc, flexible ? 1 : 0);
-            after_launch(P->ctx, "pk_cg_beta");
-            if (flexible && pc != PC_MG) {
+        } else {
+            restart();
+            if (flexible && !(rz > 0.0)) fall_back(3);
+            while (rn > tol * bn && it < max_iter) {
+                // q = A p, alpha = r.z / p.Ap, x += alpha p, r -= alpha q and r.r
+                // run back to back on the device; the host reads the scalars once
+                launch_matvec(P, 0, p, q);
+                dot_dev(P, p, q, n, SC_PQ);
+                if (flexible) CUDA_CHECK(cudaMemcpyAsync(r_old, r, n * 4, cudaMemcpyDeviceToDevice, P->ctx->stream));
+                begin_launch(P->ctx);
+                pk_cg_update<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, p, q, x64, r);
+                after_launch(P->ctx, "pk_cg_update");
+                dot_dev(P, r, r, n, SC_RR);
                 read_scalars(P, hs);
-                if (!(hs[SC_RZ] > 0.0)) {  // the new r.z
-                    fall_back(3);
+                if (hs[SC_BAD] != 0.0) {  // p.Ap <= 0: x and r were left as they were
+                    if (flexible && pc != PC_MG) {
+                        fall_back(2);
+                        continue;
+                    }
+                    MSBG_THROW(MSBG_ERR_NUMERIC, "PCG breakdown (p.Ap <= 0)");
+                }
+                rn = std::sqrt(hs[SC_RR]);
+                ++it;
+                if (rn <= tol * bn) {
+                    launch_residual64(P, x64, b, r);
+                    rn = std::sqrt(dot(P, r, r, n));
+                    if (hist) hist[it - 1] = rn / bn;
+                    if (rn <= tol * bn) break;
+                    restart();
+                    since = 0;
                     continue;
                 }
+                if (hist) hist[it - 1] = rn / bn;
+                rn_hist.push_back(rn);
+                ++since;
+                // stall: the residual norm of CG is not monotone, so the test is
+                // over a window: less than a halving in the last 4 iterations
+                if (flexible && pc != PC_MG && since >= 4 && rn > 0.5 * rn_hist[rn_hist.size() - 5]) {
+                    fall_back(1);
+                    continue;
+                }
+                if (lead > 0 && pc == PC_HYBRID && P->n_net >= lead) {
+                    // method 5: the lead is over; CG restarts from the current
+                    // iterate with the fixed V-cycle preconditioner
+                    pc = PC_MG;
+                    flexible = false;
+                    restart();
+                    since = 0;
+                    continue;
+                }
+                precondition(r, z);
+                dot_dev(P, r, z, n, SC_RZ2);
+                if (flexible) dot_dev(P, z, r_old, n, SC_ZR);
+                begin_launch(P->ctx);
+                pk_cg_beta<<<1, 1, 0, P->ctx->stream>>>(sc, flexible ? 1 : 0);
+                after_launch(P->ctx, "pk_cg_beta");
+                if (flexible && pc != PC_MG) {
+                    read_scalars(P, hs);
+                    if (!(hs[SC_RZ] > 0.0)) {  // the new r.z
+                        fall_back(3);
+                        continue;
+                    }
+                }
+                begin_launch(P->ctx);
+                pk_cg_direction<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, z, p);
+                after_launch(P->ctx, "pk_cg_direction");
             }
-            begin_launch(P->ctx);
-            pk_cg_direction<<<grid_for(n), 256, 0, P->ctx->stream>>>(n, sc, z, p);
-            after_launch(P->ctx, "pk_cg_direction");
         }
     }
     if (!x64_ext) {
@@ -1667,6 +1937,7 @@ static void batch_cycle(msbg_poisson* P, double* x64, const float* b, int K, dou
 static void autotune(msbg_poisson* P) {
     msbg_ctx* ctx = P->ctx;
     MSBG_REQUIRE(!ctx->timing, "autotuning needs per-kernel timing off");
+    drop_graphs(P);
     cudaEvent_t e0, e1;
     CUDA_CHECK(cudaEventCreate(&e0));
     CUDA_CHECK(cudaEventCreate(&e1));
@@ -1876,6 +2147,8 @@ int msbg_poisson_levels(const msbg_poisson* P, uint64_t* cells_out, size_t cap, 
 int msbg_poisson_set_smoother(msbg_poisson* P, int nu1, int nu2, float omega) {
     MSBG_API_BEGIN
     MSBG_REQUIRE(P && nu1 >= 0 && nu2 >= 0 && omega > 0.0f && omega < 2.0f, "bad smoother parameters");
+    set_device(P->ctx);
+    drop_graphs(P);
     P->nu1 = nu1;
     P->nu2 = nu2;
     P->omega = omega;
@@ -2047,6 +2320,8 @@ int msbg_poisson_set_tuning(msbg_poisson* P, const int* cfg, size_t n_levels) {
         MSBG_REQUIRE(uses_block16(P->lv[l]) ? (t == 1 || t == 2 || t == 4 || t == 8 || t == 16) : t == 0,
                      "tile must be 1, 2, 4, 8 or 16 on levels of whole 16^3 blocks and 0 elsewhere");
     }
+    set_device(P->ctx);
+    drop_graphs(P);
     for (size_t l = 0; l < n_levels; ++l) {
         P->lv[l].cfg_jac = cfg[3 * l];
         P->lv[l].cfg_res = cfg[3 * l + 1];

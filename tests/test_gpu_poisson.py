@@ -95,6 +95,32 @@ def test_tile_choices_give_the_same_bits(msbg, ctx, oracle):
 
 
 @pytest.mark.parametrize("nb,bsx", CASES)
+def test_zero_start_sweeps_give_the_same_bits(msbg, ctx, nb, bsx):
+    """A V-cycle from x = 0 runs its first two pre-smoothing sweeps as one
+    pass (the first sweep's w b / (6 s) formed where the second reads it).
+    One plain V-cycle iteration of a solve from x = 0 (fused on level 0) equals
+    a V-cycle applied to an explicit zero vector (two sweeps on level 0) bit
+    for bit, for every tile choice of the 16^3 kernels."""
+    act = np.sort(shell(nb, bsx))
+    s = nb * bsx
+    P = msbg.Poisson(ctx, s, s, s, bsx, act)
+    b = rhs(P.n, 11)
+    db = torch.from_numpy(b).cuda()
+    base = P.autotune()
+    for tile in ((1, 2, 4, 8, 16) if bsx == 16 else (int(base[0, 2]),)):
+        cfg = base.copy()
+        cfg[0, 2] = tile
+        P.set_tuning(cfg)
+        x = torch.zeros(P.n, device="cuda")
+        P.vcycle(x, db)
+        ctx.synchronize()
+        xs, it, _, _ = P.solve(b, method=0, tol=1e-30, max_iter=1)
+        assert it == 1
+        assert np.array_equal(x.cpu().numpy(), xs), tile
+    P.close()
+
+
+@pytest.mark.parametrize("nb,bsx", CASES)
 @pytest.mark.parametrize("method", [0, 1])
 def test_solve_reaches_tolerance(msbg, ctx, oracle, nb, bsx, method):
     act = np.sort(shell(nb, bsx))
