@@ -1460,9 +1460,10 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
             since = 0;
         };
         rn_hist.push_back(rn);  // the window below always holds the start
-        if (method == 1 && !P->ctx->timing) {
-            // the captured loop: a restart and CG steps until |r| <= tol |b|,
-            // the limit or a breakdown; then the host loop's checks
+        // MG-PCG from a restart at the current iterate as captured loops: a
+        // restart and CG steps until |r| <= tol |b|, the limit or a
+        // breakdown; then the host loop's checks
+        auto captured_mg_pcg = [&]() {
             while (rn > tol * bn && it < max_iter) {
                 const int ran = solve_loop(P, 1, b, x64, r, z, p, q, it, max_iter, tol * bn, bn, hs);
                 P->n_vcycle += ran;
@@ -1477,6 +1478,9 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                     if (hist) hist[it - 1] = rn / bn;
                 }
             }
+        };
+        if (method == 1 && !P->ctx->timing) {
+            captured_mg_pcg();
         } else {
             restart();
             if (flexible && !(rz > 0.0)) fall_back(3);
@@ -1523,6 +1527,10 @@ static int solve(msbg_poisson* P, int method, float* x, const float* b, double t
                     // iterate with the fixed V-cycle preconditioner
                     pc = PC_MG;
                     flexible = false;
+                    if (!P->ctx->timing) {
+                        captured_mg_pcg();
+                        break;
+                    }
                     restart();
                     since = 0;
                     continue;
