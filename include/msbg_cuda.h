@@ -200,11 +200,10 @@ int msbg_morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_
  * reserved up front).  Its temporaries live in a fixed scratch array built
  * into the library (about 5 MB, held by every device that loads the library
  * until exit), so n is limited to 262144 particles; larger n returns
- * MSBG_ERR_ARG.  The first call on a device looks up the array's device
- * address: make it before any stream capture.  Each call blocks the host
+ * MSBG_ERR_ARG.  Each call blocks the host
  * until its stream reaches the end of the sort: it reads the largest key (to
- * choose the number of digit passes) and the bounded-wait status word back.
- * Calls share the array, so calls whose GPU work overlaps in time race;
+ * choose the number of digit passes) and the bounded-wait status word back,
+ * so no call can be captured into a CUDA graph.  Calls share the array, so calls whose GPU work overlaps in time race;
  * calls ordered on one stream do not.  The device address is looked up once
  * per device and kept, so a cudaDeviceReset while the library is loaded is
  * not supported.  Returns MSBG_ERR_STATE while per-kernel timing is enabled
