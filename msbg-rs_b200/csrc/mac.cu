@@ -298,35 +298,60 @@ __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, s
     }
 }
 
+// Block code lookups of the G2P interior path: the dense table's one load
+// inline, the hash probe out of line (grids too large for a dense table), so
+// the kernel's 24 lookup sites stay small.
+__device__ __noinline__ int32_t block_code_hashed(const DevHash h, uint64_t bid) { return hash_find(h, bid); }
+__device__ __forceinline__ int32_t block_code_g2p(const SampleGrid& g, uint64_t bid) {
+    return g.dense ? __ldg(g.dense + bid) : block_code_hashed(g.hash, bid);
+}
+
 // One component's sample when its 2x2x2 corners lie inside the domain
-// (gather_map's interior case, no boundary condition applies): the code of
-// the block of corner (0, 0, 0) and, for corners in the next block along an
-// axis, that block's code (looked up only where the corners cross).
+// (gather_map's interior case, no boundary condition applies).  Corner s =
+// (i, j, k) sits at local index vid0 + i dv[0] + j dv[1] + k dv[2] (a step
+// that wraps to the next block's first cell where the corner crosses) in the
+// block of code code[s]: the code of corner (0, 0, 0)'s block, or where the
+// corner crosses along some axes, the code of the block across them (looked
+// up only for the crossings a sample has).
 struct InteriorCorners {
     int32_t code[8];
-    int32_t vid[8];
-    float x, y, z;
+    int32_t vid0, dv[3];
+    float u, v, w;  // x - floor(x), ...
     bool ok;
 };
 
 __device__ __forceinline__ InteriorCorners interior_corners(const SampleGrid& g, float x, float y, float z) {
     InteriorCorners f;
-    f.x = x; f.y = y; f.z = z;
     const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
-    const int32_t ix0 = (int32_t)floorf(x), iy0 = (int32_t)floorf(y), iz0 = (int32_t)floorf(z);
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    f.u = x - fx;
+    f.v = y - fy;
+    f.w = z - fz;
+    const int32_t ix0 = (int32_t)fx, iy0 = (int32_t)fy, iz0 = (int32_t)fz;
     f.ok = ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + 1 < g.sx && iy0 + 1 < g.sy && iz0 + 1 < g.sz;
     const int32_t jx0 = f.ok ? ix0 : 0, jy0 = f.ok ? iy0 : 0, jz0 = f.ok ? iz0 : 0;
+    const int lx = jx0 & mask, ly = jy0 & mask, lz = jz0 & mask;
+    const bool crx = lx == mask, cry = ly == mask, crz = lz == mask;
+    f.vid0 = lx | (ly << lg) | (lz << (2 * lg));
+    f.dv[0] = crx ? -mask : 1;
+    f.dv[1] = cry ? -(mask << lg) : bsx;
+    f.dv[2] = crz ? -(mask << (2 * lg)) : bsx << lg;
     const uint64_t sy = (uint64_t)g.nx, sz = (uint64_t)g.nx * g.ny;
     const uint64_t bid0 = (uint64_t)(jx0 >> lg) + (uint64_t)(jy0 >> lg) * sy + (uint64_t)(jz0 >> lg) * sz;
-    const int32_t c0 = f.ok ? block_code(g, bid0) : kCodeEmpty;
-    const bool crx = (jx0 & mask) == mask, cry = (jy0 & mask) == mask, crz = (jz0 & mask) == mask;
+    const int32_t c0 = f.ok ? block_code_g2p(g, bid0) : kCodeEmpty;
+    // the blocks across the crossed axes (x, y, xy, z, xz, yz, xyz)
+    int32_t cc[8];
+    cc[0] = c0;
+#pragma unroll
+    for (int s = 1; s < 8; ++s) {
+        const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
+        cc[s] = need ? block_code_g2p(g, bid0 + (uint64_t)(s & 1) + ((s & 2) ? sy : 0) + ((s & 4) ? sz : 0)) : c0;
+    }
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        const int i = s & 1, j = (s >> 1) & 1, k = s >> 2;
-        const bool other = (i && crx) || (j && cry) || (k && crz);
-        const uint64_t bid = bid0 + (uint64_t)(i && crx) + (j && cry ? sy : 0) + (k && crz ? sz : 0);
-        f.code[s] = f.ok && other ? block_code(g, bid) : c0;
-        f.vid[s] = ((jx0 + i) & mask) | (((jy0 + j) & mask) << lg) | (((jz0 + k) & mask) << (2 * lg));
+        // the axes corner s crosses
+        const int x = (s & 1) && crx ? 1 : 0, y = (s & 2) && cry ? 2 : 0, z = (s & 4) && crz ? 4 : 0;
+        f.code[s] = cc[x | y | z];
     }
     return f;
 }
@@ -336,22 +361,29 @@ __device__ __forceinline__ InteriorCorners interior_corners(const SampleGrid& g,
 __device__ __forceinline__ float interior_sample(const SampleGrid& g, const InteriorCorners& f) {
     float c[8];
 #pragma unroll
-    for (int s = 0; s < 8; ++s)
-        c[s] = f.code[s] >= 0 ? __ldg(g.payload + ((size_t)f.code[s] << (3 * g.lg)) + f.vid[s])
+    for (int s = 0; s < 8; ++s) {
+        const int32_t vid = f.vid0 + ((s & 1) ? f.dv[0] : 0) + ((s & 2) ? f.dv[1] : 0) + ((s & 4) ? f.dv[2] : 0);
+        c[s] = f.code[s] >= 0 ? __ldg(g.payload + ((size_t)f.code[s] << (3 * g.lg)) + vid)
                               : (f.code[s] == kCodeFull ? g.full : g.empty);
-    const float fx = floorf(f.x), fy = floorf(f.y), fz = floorf(f.z);
-    const float u = f.x - fx, v = f.y - fy, w = f.z - fz;
-    const float c00 = lerpf(c[0], c[1], u), c10 = lerpf(c[2], c[3], u), c01 = lerpf(c[4], c[5], u),
-                c11 = lerpf(c[6], c[7], u);
-    const float c0 = lerpf(c00, c10, v), c1 = lerpf(c01, c11, v);
-    return lerpf(c0, c1, w);
+    }
+    const float c00 = lerpf(c[0], c[1], f.u), c10 = lerpf(c[2], c[3], f.u), c01 = lerpf(c[4], c[5], f.u),
+                c11 = lerpf(c[6], c[7], f.u);
+    const float c0 = lerpf(c00, c10, f.v), c1 = lerpf(c01, c11, f.v);
+    return lerpf(c0, c1, f.w);
+}
+
+// The general gather (boundary conditions) out of line: rare, and large.
+__device__ __noinline__ float sample_linear_boundary(const SampleGrid g, float x, float y, float z, int bc) {
+    return sample_linear_dev(g, x, y, z, bc);
 }
 
 // MacSampler::sample::<Linear> (fluid/g2p.rs:26-32): component a is a
 // cell-centred sample of velocity[a] at p - 1/2 e_a.  One thread per
 // particle; the block lookups, then the 24 corner loads, are issued
 // together; only samples whose corners leave the domain take the general
-// gather (boundary conditions).
+// gather (boundary conditions), after the interior samples are stored.
+// (One thread per particle and component measured slower: 1.34 against
+// 0.95 ms at 25.4 M particles.)
 __global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz,
                                                   const float* __restrict__ pos, size_t n, int bc, float* __restrict__ out) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -362,9 +394,14 @@ __global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, 
     const InteriorCorners f0 = interior_corners(gx, x0, cy, cz);
     const InteriorCorners f1 = interior_corners(gy, cx, y1, cz);
     const InteriorCorners f2 = interior_corners(gz, cx, cy, z2);
-    out[3 * i + 0] = f0.ok ? interior_sample(gx, f0) : sample_linear_dev(gx, x0, cy, cz, bc);
-    out[3 * i + 1] = f1.ok ? interior_sample(gy, f1) : sample_linear_dev(gy, cx, y1, cz, bc);
-    out[3 * i + 2] = f2.ok ? interior_sample(gz, f2) : sample_linear_dev(gz, cx, cy, z2, bc);
+    const bool ok0 = f0.ok, ok1 = f1.ok, ok2 = f2.ok;
+    if (ok0) out[3 * i + 0] = interior_sample(gx, f0);
+    if (ok1) out[3 * i + 1] = interior_sample(gy, f1);
+    if (ok2) out[3 * i + 2] = interior_sample(gz, f2);
+    // the general gathers last, with little live across their calls
+    if (!ok0) out[3 * i + 0] = sample_linear_boundary(gx, x0, cy, cz, bc);
+    if (!ok1) out[3 * i + 1] = sample_linear_boundary(gy, cx, y1, cz, bc);
+    if (!ok2) out[3 * i + 2] = sample_linear_boundary(gz, cx, cy, z2, bc);
 }
 
 // g2p_blend (fluid/g2p.rs:42-45), component-wise.
