@@ -130,10 +130,13 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
 // footprint (offset 0.5) holds the lane's row, at cell offsets du - M and
 // dv - M along U and V, and bit 56 + s (s in [0, 2M]) when the face
 // footprint (offset 1.0) along F holds cell offset s - 1 - M.
+// MT > 0 fixes M = MT at compile time (the footprint loops unrolled).
+template <int MT>
 __global__ void p2g_gather_kernel(const float* pos, const float* vel, const float* mass, const uint32_t* perm, size_t n,
-                                  int lg, int M, float r_p, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz,
+                                  int lg, int M_, float r_p, float r_scan_bsx, int64_t nx, int64_t ny, int64_t nz,
                                   float* px, float* py, float* pz, float* pm, float* v0, float* v1, float* v2,
                                   uint32_t* fmask, uint64_t* lane_mask, int* bad) {
+    const int M = MT > 0 ? MT : M_;
     const float inv_bsx = 1.0f / (float)(1 << lg);
     const int32_t B = 1 << lg;
     const int WIN = 2 * M + 1;
@@ -146,21 +149,27 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
             v0[i] = vel[3 * s]; v1[i] = vel[3 * s + 1]; v2[i] = vel[3 * s + 2];
         }
         const float p[3] = {x, y, z};
-        const int64_t nn[3] = {nx, ny, nz};
+        // block counts per axis are below 2^21 (Morton keys take 21 bits per
+        // axis), so the cell and block arithmetic fits 32 bits; a coordinate
+        // beyond the int32 range converts to INT_MAX, whose block is out of
+        // range as well
+        const int32_t nn[3] = {(int32_t)nx, (int32_t)ny, (int32_t)nz};
         uint32_t lo[3], hi[3];
         int32_t a1[3][2], a2[3][2], cell[3];
         bool out = false;
+#pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-            const int64_t c = p[ax] > 0.0f ? (int64_t)p[ax] : 0;  // the particle's cell (p as usize)
-            const int64_t cb = c >> lg;                              // and block
+            const int32_t c = p[ax] > 0.0f ? (int32_t)p[ax] : 0;  // the particle's cell (p as usize)
+            const int32_t cb = c >> lg;                              // and block
             if (cb >= nn[ax]) out = true;
             const float b = p[ax] * inv_bsx;  // p / bsx: bsx is a power of two, the product is exact
-            const int64_t l = max((int64_t)(int32_t)truncf(b - r_scan_bsx), (int64_t)0);
-            const int64_t h = min((int64_t)(int32_t)truncf(b + r_scan_bsx), nn[ax] - 1);
-            lo[ax] = (uint32_t)(min(max(l - cb, (int64_t)-1), (int64_t)1) + 1);
-            hi[ax] = (uint32_t)(min(max(h - cb, (int64_t)-1), (int64_t)1) + 1);
-            const int32_t b0 = (int32_t)cb * B;
-            cell[ax] = (int32_t)(c - (int64_t)b0);
+            const int32_t l = max((int32_t)truncf(b - r_scan_bsx), 0);
+            const int32_t h = min((int32_t)truncf(b + r_scan_bsx), nn[ax] - 1);
+            lo[ax] = (uint32_t)(min(max(l - cb, -1), 1) + 1);
+            hi[ax] = (uint32_t)(min(max(h - cb, -1), 1) + 1);
+            const int32_t b0 = cb * B;
+            cell[ax] = c - b0;
+#pragma unroll
             for (int face = 0; face < 2; ++face) {
                 // staging coordinates (global - (b0 - M)) of the clipped footprint
                 const float of = face ? 1.0f : 0.5f;
@@ -172,16 +181,20 @@ __global__ void p2g_gather_kernel(const float* pos, const float* vel, const floa
         // cell + k (cell-centred, face 0) or cell + k - 1 (faces, face 1)
         // lies in the clipped footprint: a contiguous run of bits
         uint32_t run[3][2];
+#pragma unroll
         for (int ax = 0; ax < 3; ++ax)
+#pragma unroll
             for (int face = 0; face < 2; ++face) {
                 const int lo = max(a1[ax][face] - cell[ax] + face, 0), hi = min(a2[ax][face] - cell[ax] + face, WIN - 1);
                 run[ax][face] = lo > hi ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
             }
+#pragma unroll
         for (int dir = 0; dir < 3; ++dir) {
             const int F = dir, U = dir == 0 ? 1 : 0, V = dir == 2 ? 1 : 2;
             // lane bit du + WIN dv for du in run U, dv in run V: the U run
             // repeated at the V run's rows (one product, no carries)
             uint64_t rows = 0;
+#pragma unroll
             for (int dv = 0; dv < WIN; ++dv)
                 if ((run[V][0] >> dv) & 1u) rows |= 1ull << (WIN * dv);
             uint64_t m = (uint64_t)run[U][0] * rows | ((uint64_t)run[F][1] << 56);
@@ -1135,9 +1148,14 @@ void p2g_device(msbg_mac* mac, const float* d_pos, const float* d_vel, const flo
     }
     float *px = soa, *py = soa + n, *pz = soa + 2 * n, *pm = soa + 3 * n, *v0 = soa + 4 * n, *v1 = soa + 5 * n, *v2 = soa + 6 * n;
     begin_launch(ctx);
-    p2g_gather_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, M, r_p,
-                                                            (r_p + 1.0f) / (float)bsx, (int64_t)u->nx, (int64_t)u->ny,
-                                                            (int64_t)u->nz, px, py, pz, pm, v0, v1, v2, fmask, fpk, bad);
+    if (M == 2)
+        p2g_gather_kernel<2><<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, M, r_p,
+                                                                   (r_p + 1.0f) / (float)bsx, (int64_t)u->nx, (int64_t)u->ny,
+                                                                   (int64_t)u->nz, px, py, pz, pm, v0, v1, v2, fmask, fpk, bad);
+    else
+        p2g_gather_kernel<0><<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, d_vel, d_mass, perm, n, lg, M, r_p,
+                                                                   (r_p + 1.0f) / (float)bsx, (int64_t)u->nx, (int64_t)u->ny,
+                                                                   (int64_t)u->nz, px, py, pz, pm, v0, v1, v2, fmask, fpk, bad);
     after_launch(ctx, "p2g_gather_kernel");
     const size_t npb = sorted_segments(ctx, skeys, n, (uint64_t)(3 * lg), pb_key, pb_starts, ScratchLayout::at<char>(base, o_tmp));
     int hbad = 0, hstatus = 0;
