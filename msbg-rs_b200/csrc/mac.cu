@@ -298,13 +298,10 @@ __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, s
     }
 }
 
-// Block code lookups of the G2P interior path: the dense table's one load
-// inline, the hash probe out of line (grids too large for a dense table), so
-// the kernel's 24 lookup sites stay small.
+// Block code lookups of the G2P interior path through the hash (grids too
+// large for a dense table) out of line, so the kernel's lookup sites stay
+// small.
 __device__ __noinline__ int32_t block_code_hashed(const DevHash h, uint64_t bid) { return hash_find(h, bid); }
-__device__ __forceinline__ int32_t block_code_g2p(const SampleGrid& g, uint64_t bid) {
-    return g.dense ? __ldg(g.dense + bid) : block_code_hashed(g.hash, bid);
-}
 
 // One component's sample when its 2x2x2 corners lie inside the domain
 // (gather_map's interior case, no boundary condition applies).  Corner s =
@@ -336,16 +333,29 @@ __device__ __forceinline__ InteriorCorners interior_corners(const SampleGrid& g,
     f.dv[0] = crx ? -mask : 1;
     f.dv[1] = cry ? -(mask << lg) : bsx;
     f.dv[2] = crz ? -(mask << (2 * lg)) : bsx << lg;
-    const uint64_t sy = (uint64_t)g.nx, sz = (uint64_t)g.nx * g.ny;
-    const uint64_t bid0 = (uint64_t)(jx0 >> lg) + (uint64_t)(jy0 >> lg) * sy + (uint64_t)(jz0 >> lg) * sz;
-    const int32_t c0 = f.ok ? block_code_g2p(g, bid0) : kCodeEmpty;
-    // the blocks across the crossed axes (x, y, xy, z, xz, yz, xyz)
+    // the code of corner (0, 0, 0)'s block, then of the blocks across the
+    // crossed axes (x, y, xy, z, xz, yz, xyz); a dense table has at most
+    // 2^24 entries, so its index arithmetic is 32-bit
     int32_t cc[8];
-    cc[0] = c0;
+    if (g.dense) {
+        const uint32_t sy = (uint32_t)g.nx, sz = (uint32_t)(g.nx * g.ny);
+        const uint32_t bid0 = (uint32_t)(jx0 >> lg) + (uint32_t)(jy0 >> lg) * sy + (uint32_t)(jz0 >> lg) * sz;
+        cc[0] = f.ok ? __ldg(g.dense + bid0) : kCodeEmpty;
 #pragma unroll
-    for (int s = 1; s < 8; ++s) {
-        const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
-        cc[s] = need ? block_code_g2p(g, bid0 + (uint64_t)(s & 1) + ((s & 2) ? sy : 0) + ((s & 4) ? sz : 0)) : c0;
+        for (int s = 1; s < 8; ++s) {
+            const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
+            cc[s] = need ? __ldg(g.dense + (bid0 + (uint32_t)(s & 1) + ((s & 2) ? sy : 0u) + ((s & 4) ? sz : 0u))) : cc[0];
+        }
+    } else {
+        const uint64_t sy = (uint64_t)g.nx, sz = (uint64_t)g.nx * g.ny;
+        const uint64_t bid0 = (uint64_t)(jx0 >> lg) + (uint64_t)(jy0 >> lg) * sy + (uint64_t)(jz0 >> lg) * sz;
+        cc[0] = f.ok ? block_code_hashed(g.hash, bid0) : kCodeEmpty;
+#pragma unroll
+        for (int s = 1; s < 8; ++s) {
+            const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
+            cc[s] = need ? block_code_hashed(g.hash, bid0 + (uint64_t)(s & 1) + ((s & 2) ? sy : 0) + ((s & 4) ? sz : 0))
+                         : cc[0];
+        }
     }
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
