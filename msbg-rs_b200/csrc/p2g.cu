@@ -111,11 +111,14 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
     int32_t* ce = cell_end + (size_t)k * n_cells;
     for (int i = threadIdx.x; i < n_cells; i += blockDim.x) cb[i] = ce[i] = 0;
     __syncthreads();
-    const int64_t s = (int64_t)pb_starts[k], e = (int64_t)pb_starts[k + 1];
-    for (int64_t i = s + threadIdx.x; i < e; i += blockDim.x) {
-        const uint64_t c = skeys[i] & cmask;
-        if (i == s || (skeys[i - 1] & cmask) != c) cb[c] = (int32_t)i;
-        if (i == e - 1 || (skeys[i + 1] & cmask) != c) ce[c] = (int32_t)(i + 1);
+    // particle indices fit int32 (the CSR stores them as int32)
+    const int32_t s = (int32_t)pb_starts[k], e = (int32_t)pb_starts[k + 1];
+    const uint32_t cm = (uint32_t)cmask;
+#pragma unroll 4
+    for (int32_t i = s + (int32_t)threadIdx.x; i < e; i += (int32_t)blockDim.x) {
+        const uint32_t c = (uint32_t)skeys[i] & cm;
+        if (i == s || ((uint32_t)skeys[i - 1] & cm) != c) cb[c] = i;
+        if (i == e - 1 || ((uint32_t)skeys[i + 1] & cm) != c) ce[c] = i + 1;
     }
 }
 
@@ -984,7 +987,10 @@ __global__ void pb_candidates_kernel(const uint32_t* fmask, const uint64_t* pb_s
                                      int64_t nx, int64_t ny, int64_t nz, uint64_t* cand) {
     for (size_t k = blockIdx.x; k < npb; k += gridDim.x) {
         uint32_t m = 0;
-        for (uint64_t i = pb_starts[k] + threadIdx.x; i < pb_starts[k + 1]; i += blockDim.x) m |= fmask[i];
+        const uint32_t* f = fmask + pb_starts[k];
+        const uint32_t cnt = (uint32_t)(pb_starts[k + 1] - pb_starts[k]);  // particles of one block
+#pragma unroll 4
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) m |= f[i];
         for (int o = 16; o; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
         __shared__ uint32_t wm[32];
         if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;

@@ -428,20 +428,63 @@ int key_bits(msbg_ctx* ctx, const uint64_t* d_keys, size_t n, void* tmp8) {
     return b;
 }
 
-__global__ void seg_flags_kernel(const uint64_t* k, size_t n, uint64_t shift, uint32_t* f) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        f[i] = (i == 0 || (k[i] >> shift) != (k[i - 1] >> shift)) ? 1u : 0u;
+// Runs of equal key >> shift in sorted keys, in two passes over the keys:
+// each tile of SEG_TILE keys counts its run starts, the counts are scanned,
+// then each tile writes its runs' keys and start indices in index order
+// (warp w of a tile owns the tile's w-th range of 32 * SEG_ITEMS keys and
+// walks it in rounds of 32).
+constexpr int SEG_THREADS = 256, SEG_ITEMS = 16, SEG_TILE = SEG_THREADS * SEG_ITEMS;
+
+__device__ __forceinline__ bool seg_start(const uint64_t* k, size_t i, uint64_t shift) {
+    return i == 0 || (k[i] >> shift) != (k[i - 1] >> shift);
 }
 
-__global__ void seg_write_kernel(const uint64_t* k, size_t n, uint64_t shift, const uint32_t* f, const uint32_t* idx,
-                                 uint64_t* uniq, uint64_t* starts, const uint32_t* count) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (f[i]) {
-            uniq[idx[i]] = k[i] >> shift;
-            starts[idx[i]] = i;
-        }
-        if (i == 0) starts[*count] = n;
+__global__ void __launch_bounds__(SEG_THREADS) seg_count_kernel(const uint64_t* __restrict__ k, size_t n, uint64_t shift,
+                                                                uint32_t* __restrict__ tile_cnt) {
+    const size_t base = (size_t)blockIdx.x * SEG_TILE;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < SEG_ITEMS; ++j) {
+        const size_t i = base + (size_t)j * SEG_THREADS + threadIdx.x;
+        if (i < n && seg_start(k, i, shift)) ++c;
     }
+    uint32_t total;
+    block_exclusive_scan(c, &total);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SEG_THREADS) seg_emit_kernel(const uint64_t* __restrict__ k, size_t n, uint64_t shift,
+                                                               const uint32_t* __restrict__ tile_off,
+                                                               uint64_t* __restrict__ uniq, uint64_t* __restrict__ starts,
+                                                               const uint32_t* __restrict__ count) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const size_t wbase = (size_t)blockIdx.x * SEG_TILE + (size_t)w * 32 * SEG_ITEMS;
+    uint32_t fl = 0;  // bit j: item wbase + 32 j + lane starts a run
+    uint32_t wc = 0;  // run starts in the warp's range
+#pragma unroll
+    for (int j = 0; j < SEG_ITEMS; ++j) {
+        const size_t i = wbase + 32 * j + lane;
+        const bool st = i < n && seg_start(k, i, shift);
+        fl |= (uint32_t)st << j;
+        wc += __popc(__ballot_sync(0xffffffffu, st));
+    }
+    uint32_t total;
+    uint32_t off = block_exclusive_scan(lane == 0 ? wc : 0u, &total);
+    off = __shfl_sync(0xffffffffu, off, 0) + tile_off[blockIdx.x];
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < SEG_ITEMS; ++j) {
+        const bool st = (fl >> j) & 1u;
+        const uint32_t b = __ballot_sync(0xffffffffu, st);
+        if (st) {
+            const size_t i = wbase + 32 * j + lane;
+            const uint32_t d = off + __popc(b & lt);
+            uniq[d] = k[i] >> shift;
+            starts[d] = i;
+        }
+        off += __popc(b);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) starts[*count] = n;
 }
 
 size_t segment_scratch_bytes(size_t n) { return align256(n * 4) * 2 + scan_scratch_bytes(n) + 256; }
@@ -454,21 +497,21 @@ size_t sorted_segments(msbg_ctx* ctx, const uint64_t* d_sorted, size_t n, uint64
         sync(ctx);
         return 0;
     }
+    const size_t tiles = div_up(n, (size_t)SEG_TILE);
     char* t = (char*)tmp;
-    uint32_t* f = (uint32_t*)t;
-    t += align256(n * 4);
-    uint32_t* idx = (uint32_t*)t;
-    t += align256(n * 4);
+    uint32_t* tile_cnt = (uint32_t*)t;
+    t += align256(tiles * 4);
+    uint32_t* tile_off = (uint32_t*)t;
+    t += align256(tiles * 4);
     uint32_t* count = (uint32_t*)t;
     t += 256;
-    unsigned g = std::min<size_t>(div_up(n, 256), 8192);
     begin_launch(ctx);
-    seg_flags_kernel<<<g, 256, 0, ctx->stream>>>(d_sorted, n, shift, f);
-    after_launch(ctx, "seg_flags_kernel");
-    exclusive_scan_u32(ctx, f, idx, n, count, t);
+    seg_count_kernel<<<(unsigned)tiles, SEG_THREADS, 0, ctx->stream>>>(d_sorted, n, shift, tile_cnt);
+    after_launch(ctx, "seg_count_kernel");
+    exclusive_scan_u32(ctx, tile_cnt, tile_off, tiles, count, t);
     begin_launch(ctx);
-    seg_write_kernel<<<g, 256, 0, ctx->stream>>>(d_sorted, n, shift, f, idx, d_uniq, d_starts, count);
-    after_launch(ctx, "seg_write_kernel");
+    seg_emit_kernel<<<(unsigned)tiles, SEG_THREADS, 0, ctx->stream>>>(d_sorted, n, shift, tile_off, d_uniq, d_starts, count);
+    after_launch(ctx, "seg_emit_kernel");
     uint32_t c = 0;
     read_small(ctx, &c, count, 4);
     return c;
