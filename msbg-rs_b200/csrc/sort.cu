@@ -526,6 +526,19 @@ __global__ void morton_keys_kernel(const float* pos, size_t n, uint64_t* keys) {
         keys[i] = morton3(trunc_coord(pos[3 * i]), trunc_coord(pos[3 * i + 1]), trunc_coord(pos[3 * i + 2]));
 }
 
+// The same keys and their maximum (atomicMax into *kmax, zeroed before), so
+// the sort learns its digit count without a second pass over the keys.
+__global__ void morton_keys_max_kernel(const float* pos, size_t n, uint64_t* keys, unsigned long long* kmax) {
+    unsigned long long m = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t k = morton3(trunc_coord(pos[3 * i]), trunc_coord(pos[3 * i + 1]), trunc_coord(pos[3 * i + 2]));
+        keys[i] = k;
+        m = max(m, (unsigned long long)k);
+    }
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(kmax, m);
+}
+
 __global__ void morton3_kernel(const uint64_t* xyz, size_t n, uint64_t* keys) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         keys[i] = morton3(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
@@ -591,8 +604,15 @@ void morton_sort_device(msbg_ctx* ctx, const float* d_pos, size_t n, uint64_t* d
     size_t ok = L.add<uint64_t>(n), ot = L.add<char>(radix_sort_scratch_bytes(n)), o8 = L.add<uint64_t>(1);
     char* base = scratch(ctx, L);
     uint64_t* keys = ScratchLayout::at<uint64_t>(base, ok);
-    morton_keys(ctx, d_pos, n, keys);
-    int bits = key_bits(ctx, keys, n, ScratchLayout::at<char>(base, o8));
+    unsigned long long* kmax = ScratchLayout::at<unsigned long long>(base, o8);
+    CUDA_CHECK(cudaMemsetAsync(kmax, 0, 8, ctx->stream));
+    begin_launch(ctx);
+    morton_keys_max_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(d_pos, n, keys, kmax);
+    after_launch(ctx, "morton_keys_kernel");
+    uint64_t m = 0;
+    read_small(ctx, &m, kmax, 8);
+    int bits = 0;
+    while (bits < 64 && (m >> bits)) ++bits;
     radix_sort_pairs(ctx, keys, nullptr, d_keys_out, d_perm_out, n, bits, ScratchLayout::at<char>(base, ot));
 }
 
