@@ -247,10 +247,10 @@ def run_ours(args, world, rank, local):
         msbg.downsample_channel_avg(coarse, mac.mass(0))
         sweeper.sweep_multires(coarse, levels, fine, msbg.Stencil.MeanCurvature, msbg.PdeParams(DT, SWEEPS, False))
         mark("smooth")
-        sampler.sample_device(spos, n, u)
         if before_blend is not None:
             before_blend()  # u_new of the previous step has been read back
-        msbg.g2p_blend_device(ctx, svel, u, u, n, ALPHA, u_new)
+        # MacSampler::sample and g2p_blend in one pass (u_tilde = the sample)
+        msbg.g2p_flip_device(sampler, spos, n, svel, ALPHA, u_new)
         mark("g2p")
 
     # warm-up

@@ -281,6 +281,14 @@ int msbg_g2p_device(msbg_mac* mac, const float* d_pos, size_t n, int bc, float* 
 /* g2p_blend (fluid/g2p.rs:42-45) on [n][3] arrays. */
 int msbg_g2p_blend_device(msbg_ctx* ctx, const float* d_u_old, const float* d_u, const float* d_u_tilde,
                           size_t n, float alpha, float* d_out);
+/* msbg_g2p_device followed by msbg_g2p_blend_device in one pass, the
+ * samples never stored: d_out[i] = (u_old[i] + (u[i] - u_tilde[i])) alpha +
+ * u[i] (1 - alpha) with u the velocity sampled at d_pos[i] (MacSampler::sample,
+ * fluid/g2p.rs:26-32; g2p_blend, fluid/g2p.rs:42-45).  d_u_tilde null: u_tilde
+ * is the sample itself (the grid unchanged between the two samples).  Bit for
+ * bit the two calls' result.  d_out may not alias an input. */
+int msbg_g2p_flip_device(msbg_mac* mac, const float* d_pos, size_t n, int bc, const float* d_u_old,
+                         const float* d_u_tilde, float alpha, float* d_out);
 /* Scalar trilinear Sampler::sample::<Linear> (math/sample.rs:494-512);
  * align 0 = Corner, 1 = CellCentered.  Any storage type: samples are read
  * through Dequant (math/sample.rs:45-70; Density8 linearly, q / 255). */

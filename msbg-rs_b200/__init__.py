@@ -15,8 +15,8 @@ from . import _lib
 from .grid import Context, HostGrid, SparseGrid
 from .solver import Fence, PdeParams, Stencil, Sweeper, apply_pde
 from .particles import BucketPlan, bucket_indices, morton3, morton3_host, morton_sort, sort_block_list_morton
-from .fluid import (FlipStep, MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend_device, particles_to_grid,
-                    particles_to_grid_device, particles_to_grid_sorted_device,
+from .fluid import (FlipStep, MacGrid, MacSampler, X, Y, Z, g2p_blend, g2p_blend_device, g2p_flip_device,
+                    particles_to_grid, particles_to_grid_device, particles_to_grid_sorted_device,
                     particles_to_grid_permuted_device)
 from .multires import downsample_channel_avg
 from .sampler import CELL_CENTERED, CORNER, CUBIC_BSPLINE, LINEAR, Sampler
@@ -33,7 +33,8 @@ CLAMP, NEUMANN, DIRICHLET = _lib.MSBG_CLAMP, _lib.MSBG_NEUMANN, _lib.MSBG_DIRICH
 __all__ = [
     "Context", "HostGrid", "SparseGrid", "Fence", "PdeParams", "Stencil", "Sweeper", "apply_pde",
     "BucketPlan", "bucket_indices", "morton3", "morton3_host", "morton_sort", "sort_block_list_morton",
-    "FlipStep", "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "particles_to_grid",
+    "FlipStep", "MacGrid", "MacSampler", "X", "Y", "Z", "g2p_blend", "g2p_blend_device", "g2p_flip_device",
+    "particles_to_grid",
     "particles_to_grid_device", "particles_to_grid_sorted_device", "particles_to_grid_permuted_device", "downsample_channel_avg", "MsbgError", "CLAMP", "NEUMANN", "DIRICHLET",
     "surface", "SurfaceConfig", "reconstruct_and_smooth", "Sampler", "LINEAR", "CUBIC_BSPLINE", "CORNER", "CELL_CENTERED",
     "Poisson", "MG", "PCG", "LEARNED", "HYBRID", "LEARNED_MG", "LEARNED_LEAD", "UNet", "Batch", "BlockMap",

@@ -95,6 +95,7 @@ SIGNATURES = {
     "msbg_g2p": [_P, _P, _SZ, _I, _P],
     "msbg_g2p_device": [_P, _P, _SZ, _I, _P],
     "msbg_g2p_blend_device": [_P, _P, _P, _P, _SZ, _F, _P],
+    "msbg_g2p_flip_device": [_P, _P, _SZ, _I, _P, _P, _F, _P],
     "msbg_sample_linear": [_P, _P, _SZ, _I, _I, _P],
     "msbg_sample_ext": [_P, _P, _SZ, _I, _I, _I, _P],
     "msbg_sample_ext_device": [_P, _P, _SZ, _I, _I, _I, _P],

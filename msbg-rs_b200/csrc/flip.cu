@@ -97,13 +97,12 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
     if (n > f->cap) {
         sync(ctx);
         f->buf.release();
-        f->buf.reserve(4 * b3 + 2 * b1 + b8);
+        f->buf.reserve(3 * b3 + 2 * b1 + b8);
         f->cap = n;
     }
     char* p = (char*)f->buf.p;
     float* d_pos = (float*)p;  p += b3;
     float* d_vel = (float*)p;  p += b3;
-    float* d_u = (float*)p;    p += b3;
     float* d_out = (float*)p;  p += b3;
     float* d_mass = (float*)p; p += b1;
     uint64_t* keys = (uint64_t*)p; p += b8;
@@ -136,8 +135,7 @@ int msbg_flip_step(msbg_flip* f, const float* pos, const float* vel, const float
     int used = 0;
     for (size_t lo = 0; lo < n; lo += per, ++used) {
         const size_t cnt = std::min(per, n - lo);
-        check(msbg_g2p_device(f->mac, d_pos + 3 * lo, cnt, MSBG_CLAMP, d_u + 3 * lo));
-        check(msbg_g2p_blend_device(ctx, d_vel + 3 * lo, d_u + 3 * lo, d_u + 3 * lo, cnt, alpha, d_out + 3 * lo));
+        check(msbg_g2p_flip_device(f->mac, d_pos + 3 * lo, cnt, MSBG_CLAMP, d_vel + 3 * lo, nullptr, alpha, d_out + 3 * lo));
         CUDA_CHECK(cudaEventRecord(f->chunk_done[used], ctx->stream));
         CUDA_CHECK(cudaStreamWaitEvent(f->up, f->chunk_done[used], 0));
         CUDA_CHECK(cudaMemcpyAsync(vel_out + 3 * lo, d_out + 3 * lo, cnt * 12, cudaMemcpyDeviceToHost, f->up));

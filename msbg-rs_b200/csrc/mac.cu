@@ -394,24 +394,48 @@ __device__ __noinline__ float sample_linear_boundary(const SampleGrid g, float x
 // gather (boundary conditions), after the interior samples are stored.
 // (One thread per particle and component measured slower: 1.34 against
 // 0.95 ms at 25.4 M particles.)
+//
+// BLEND 1 writes g2p_blend (fluid/g2p.rs:42-45) of the sample instead:
+// (u_old + (u - u_tilde)) alpha + u (1 - alpha), with u_tilde the caller's
+// array, or the sample itself where u_tilde is null (no grid change between
+// the two samples); the same operations as g2p_blend_kernel, so the result
+// equals the sample-then-blend pair bit for bit without the round trip of
+// the samples through memory.
+struct BlendArgs {
+    const float* u_old;
+    const float* u_tilde;
+    float alpha;
+};
+
+template <int BLEND>
 __global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz,
-                                                  const float* __restrict__ pos, size_t n, int bc, float* __restrict__ out) {
+                                                  const float* __restrict__ pos, size_t n, int bc, BlendArgs bl,
+                                                  float* __restrict__ out) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
     const float cx = px - 0.5f, cy = py - 0.5f, cz = pz - 0.5f;
     const float x0 = (px - 0.5f) - 0.5f, y1 = (py - 0.5f) - 0.5f, z2 = (pz - 0.5f) - 0.5f;
+    auto emit = [&](int c, float u) {
+        if (BLEND) {
+            const float ut = bl.u_tilde ? bl.u_tilde[3 * i + c] : u;
+            const float delta = u - ut;
+            out[3 * i + c] = (bl.u_old[3 * i + c] + delta) * bl.alpha + u * (1.0f - bl.alpha);
+        } else {
+            out[3 * i + c] = u;
+        }
+    };
     const InteriorCorners f0 = interior_corners(gx, x0, cy, cz);
     const InteriorCorners f1 = interior_corners(gy, cx, y1, cz);
     const InteriorCorners f2 = interior_corners(gz, cx, cy, z2);
     const bool ok0 = f0.ok, ok1 = f1.ok, ok2 = f2.ok;
-    if (ok0) out[3 * i + 0] = interior_sample(gx, f0);
-    if (ok1) out[3 * i + 1] = interior_sample(gy, f1);
-    if (ok2) out[3 * i + 2] = interior_sample(gz, f2);
+    if (ok0) emit(0, interior_sample(gx, f0));
+    if (ok1) emit(1, interior_sample(gy, f1));
+    if (ok2) emit(2, interior_sample(gz, f2));
     // the general gathers last, with little live across their calls
-    if (!ok0) out[3 * i + 0] = sample_linear_boundary(gx, x0, cy, cz, bc);
-    if (!ok1) out[3 * i + 1] = sample_linear_boundary(gy, cx, y1, cz, bc);
-    if (!ok2) out[3 * i + 2] = sample_linear_boundary(gz, cx, cy, z2, bc);
+    if (!ok0) emit(0, sample_linear_boundary(gx, x0, cy, cz, bc));
+    if (!ok1) emit(1, sample_linear_boundary(gy, cx, y1, cz, bc));
+    if (!ok2) emit(2, sample_linear_boundary(gz, cx, cy, z2, bc));
 }
 
 // g2p_blend (fluid/g2p.rs:42-45), component-wise.
@@ -505,12 +529,16 @@ __global__ void downsample_kernel(const float* src, const int32_t* src_slots, fl
 
 static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>(std::max<size_t>(div_up(n, 256), 1), 8192); }
 
-void g2p_device(msbg_mac* m, const float* d_pos, size_t n, int bc, float* d_out) {
+// d_u_old non-null: the blended velocities (g2p_kernel<1>) instead of the samples.
+void g2p_device(msbg_mac* m, const float* d_pos, size_t n, int bc, float* d_out, const float* d_u_old = nullptr,
+                const float* d_u_tilde = nullptr, float alpha = 0.0f) {
     MSBG_REQUIRE(bc >= 0 && bc <= 2, "bad boundary condition");
     if (!n) return;
     SampleGrid gx = sample_grid(m->ch[0]), gy = sample_grid(m->ch[1]), gz = sample_grid(m->ch[2]);
+    const BlendArgs bl{d_u_old, d_u_tilde, alpha};
     begin_launch(m->ctx);
-    g2p_kernel<<<(unsigned)div_up(n, 256), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, d_out);
+    if (d_u_old) g2p_kernel<1><<<(unsigned)div_up(n, 256), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, bl, d_out);
+    else g2p_kernel<0><<<(unsigned)div_up(n, 256), 256, 0, m->ctx->stream>>>(gx, gy, gz, d_pos, n, bc, bl, d_out);
     after_launch(m->ctx, "g2p_kernel");
 }
 
@@ -669,6 +697,16 @@ int msbg_g2p(msbg_mac* m, const float* pos, size_t n, int bc, float* vel_out) {
     g2p_device(m, dp, n, bc, dv);
     CUDA_CHECK(cudaMemcpyAsync(vel_out, dv, n * 12, cudaMemcpyDeviceToHost, m->ctx->stream));
     sync(m->ctx);
+    MSBG_API_END
+}
+
+int msbg_g2p_flip_device(msbg_mac* m, const float* d_pos, size_t n, int bc, const float* d_u_old, const float* d_u_tilde,
+                         float alpha, float* d_out) {
+    MSBG_API_BEGIN
+    MSBG_REQUIRE(m && ((d_pos && d_u_old && d_out) || !n), "null argument");
+    MSBG_REQUIRE(d_out != d_pos && d_out != d_u_old && d_out != d_u_tilde, "the output cannot alias an input");
+    set_device(m->ctx);
+    g2p_device(m, d_pos, n, bc, d_out, d_u_old, d_u_tilde, alpha);
     MSBG_API_END
 }
 

@@ -121,6 +121,13 @@ class MacSampler:
         call("msbg_g2p_device", self.mac.handle, ptr(d_pos), int(n), self.bc, ptr(d_out))
 
 
+def g2p_flip_device(sampler: "MacSampler", d_pos, n: int, d_u_old, alpha: float, d_out, d_u_tilde=None) -> None:
+    """MacSampler::sample then g2p_blend (fluid/g2p.rs:26-45) in one pass on
+    device [n][3] arrays; d_u_tilde None: the sample is its own u_tilde."""
+    call("msbg_g2p_flip_device", sampler.mac.handle, ptr(d_pos), int(n), sampler.bc, ptr(d_u_old), ptr(d_u_tilde),
+         float(alpha), ptr(d_out))
+
+
 def g2p_blend_device(ctx: Context, d_u_old, d_u, d_u_tilde, n: int, alpha: float, d_out) -> None:
     """g2p_blend (fluid/g2p.rs:42-45) on device [n][3] arrays."""
     call("msbg_g2p_blend_device", ctx.handle, ptr(d_u_old), ptr(d_u), ptr(d_u_tilde), int(n), float(alpha), ptr(d_out))

@@ -323,3 +323,31 @@ def test_divergence_and_downsample(msbg, ctx, oracle):
     coarse = msbg.SparseGrid(ctx, s // 2, s // 2, s // 2, 0.0, 0.0, 8)
     msbg.downsample_channel_avg(coarse, div)
     assert np.array_equal(coarse.read_blocks(act), oracle.downsample_avg(want, 16))
+
+
+@pytest.mark.parametrize("with_tilde", [False, True])
+def test_g2p_flip_device_equals_sample_then_blend(msbg, ctx, with_tilde):
+    """msbg_g2p_flip_device (sample and blend in one pass) gives the bits of
+    msbg_g2p_device followed by msbg_g2p_blend_device, with u_tilde the
+    sample itself (null) or a caller array; samples outside the domain (the
+    boundary gather) included."""
+    import torch
+    s, bsx = 48, 16
+    pos, vel, mass = make_particles(20000, s, 5)
+    mac = msbg.MacGrid(ctx, s, s, s, bsx)
+    msbg.particles_to_grid(mac, pos, vel, mass, 2.0)
+    q = np.concatenate([pos, np.random.default_rng(2).uniform(-3, s + 3, (3000, 3)).astype(np.float32)])
+    n = len(q)
+    rng = np.random.default_rng(3)
+    d_q = torch.from_numpy(q).cuda()
+    d_old = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).cuda()
+    d_ut = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).cuda() if with_tilde else None
+    sampler = msbg.MacSampler(mac, msbg.CLAMP)
+    u = torch.empty_like(d_old)
+    want = torch.empty_like(d_old)
+    sampler.sample_device(d_q, n, u)
+    msbg.g2p_blend_device(ctx, d_old, u, d_ut if with_tilde else u, n, 0.95, want)
+    got = torch.full_like(d_old, 7.0)
+    msbg.g2p_flip_device(sampler, d_q, n, d_old, 0.95, got, d_ut)
+    ctx.synchronize()
+    assert np.array_equal(got.cpu().numpy().view(np.uint32), want.cpu().numpy().view(np.uint32))
