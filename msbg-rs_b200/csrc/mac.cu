@@ -304,82 +304,105 @@ __global__ void sample_ext_kernel(SampleGrid g, const float* __restrict__ pos, s
 __device__ __noinline__ int32_t block_code_hashed(const DevHash h, uint64_t bid) { return hash_find(h, bid); }
 
 // One component's sample when its 2x2x2 corners lie inside the domain
-// (gather_map's interior case, no boundary condition applies).  Corner s =
-// (i, j, k) sits at local index vid0 + i dv[0] + j dv[1] + k dv[2] (a step
-// that wraps to the next block's first cell where the corner crosses) in the
-// block of code code[s]: the code of corner (0, 0, 0)'s block, or where the
-// corner crosses along some axes, the code of the block across them (looked
-// up only for the crossings a sample has).
-struct InteriorCorners {
-    int32_t code[8];
-    int32_t vid0, dv[3];
+// (gather_map's interior case, no boundary condition applies).  CornerBase:
+// the sample's corner (0, 0, 0), its block's code c0 and the axes along
+// which the +1 corners cross into the next block.
+struct CornerBase {
+    int32_t jx0, jy0, jz0;  // corner (0, 0, 0), 0 where not ok
+    int32_t c0, vid0;
     float u, v, w;  // x - floor(x), ...
-    bool ok;
+    bool ok, crx, cry, crz;
 };
 
-__device__ __forceinline__ InteriorCorners interior_corners(const SampleGrid& g, float x, float y, float z) {
-    InteriorCorners f;
-    const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
+__device__ __forceinline__ CornerBase corner_base(const SampleGrid& g, float x, float y, float z) {
+    CornerBase b;
+    const int mask = (1 << g.lg) - 1, lg = g.lg;
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-    f.u = x - fx;
-    f.v = y - fy;
-    f.w = z - fz;
+    b.u = x - fx;
+    b.v = y - fy;
+    b.w = z - fz;
     const int32_t ix0 = (int32_t)fx, iy0 = (int32_t)fy, iz0 = (int32_t)fz;
-    f.ok = ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + 1 < g.sx && iy0 + 1 < g.sy && iz0 + 1 < g.sz;
-    const int32_t jx0 = f.ok ? ix0 : 0, jy0 = f.ok ? iy0 : 0, jz0 = f.ok ? iz0 : 0;
-    const int lx = jx0 & mask, ly = jy0 & mask, lz = jz0 & mask;
-    const bool crx = lx == mask, cry = ly == mask, crz = lz == mask;
-    f.vid0 = lx | (ly << lg) | (lz << (2 * lg));
-    f.dv[0] = crx ? -mask : 1;
-    f.dv[1] = cry ? -(mask << lg) : bsx;
-    f.dv[2] = crz ? -(mask << (2 * lg)) : bsx << lg;
-    // the code of corner (0, 0, 0)'s block, then of the blocks across the
-    // crossed axes (x, y, xy, z, xz, yz, xyz); a dense table has at most
-    // 2^24 entries, so its index arithmetic is 32-bit
+    b.ok = ix0 >= 0 && iy0 >= 0 && iz0 >= 0 && ix0 + 1 < g.sx && iy0 + 1 < g.sy && iz0 + 1 < g.sz;
+    b.jx0 = b.ok ? ix0 : 0;
+    b.jy0 = b.ok ? iy0 : 0;
+    b.jz0 = b.ok ? iz0 : 0;
+    const int lx = b.jx0 & mask, ly = b.jy0 & mask, lz = b.jz0 & mask;
+    b.crx = lx == mask;
+    b.cry = ly == mask;
+    b.crz = lz == mask;
+    b.vid0 = lx | (ly << lg) | (lz << (2 * lg));
+    // a dense table has at most 2^24 entries, so its index arithmetic is 32-bit
+    if (g.dense) {
+        const uint32_t bid0 = (uint32_t)(b.jx0 >> lg) + (uint32_t)(b.jy0 >> lg) * (uint32_t)g.nx +
+                              (uint32_t)(b.jz0 >> lg) * (uint32_t)(g.nx * g.ny);
+        b.c0 = b.ok ? __ldg(g.dense + bid0) : kCodeEmpty;
+    } else {
+        const uint64_t bid0 = (uint64_t)(b.jx0 >> lg) + (uint64_t)(b.jy0 >> lg) * (uint64_t)g.nx +
+                              (uint64_t)(b.jz0 >> lg) * (uint64_t)g.nx * g.ny;
+        b.c0 = b.ok ? block_code_hashed(g.hash, bid0) : kCodeEmpty;
+    }
+    return b;
+}
+
+// The eight corner values when no corner crosses a block: c0's block at
+// constant offsets from corner (0, 0, 0) (corner s = (i, j, k) at
+// vid0 + i + j bsx + k bsx^2).
+__device__ __forceinline__ void corners_one_block(const SampleGrid& g, const CornerBase& b, float c[8]) {
+    const int bs = 1 << g.lg;
+    if (b.c0 >= 0) {
+        const float* p = g.payload + ((size_t)b.c0 << (3 * g.lg)) + b.vid0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) c[s] = __ldg(p + ((s & 1) ? 1 : 0) + ((s & 2) ? bs : 0) + ((s & 4) ? bs * bs : 0));
+    } else {
+        const float v = b.c0 == kCodeFull ? g.full : g.empty;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) c[s] = v;
+    }
+}
+
+// The eight corner values in general: corner s = (i, j, k) at local index
+// vid0 + i dv[0] + j dv[1] + k dv[2] (a step that wraps to the next block's
+// first cell where the corner crosses) in the block across the axes it
+// crosses (looked up only for the crossings a sample has).
+__device__ __forceinline__ void corners_general(const SampleGrid& g, const CornerBase& b, float c[8]) {
+    const int bsx = 1 << g.lg, mask = bsx - 1, lg = g.lg;
+    const int32_t dv0 = b.crx ? -mask : 1, dv1 = b.cry ? -(mask << lg) : bsx, dv2 = b.crz ? -(mask << (2 * lg)) : bsx << lg;
+    // the codes of the blocks across the crossed axes (x, y, xy, z, xz, yz, xyz)
     int32_t cc[8];
+    cc[0] = b.c0;
     if (g.dense) {
         const uint32_t sy = (uint32_t)g.nx, sz = (uint32_t)(g.nx * g.ny);
-        const uint32_t bid0 = (uint32_t)(jx0 >> lg) + (uint32_t)(jy0 >> lg) * sy + (uint32_t)(jz0 >> lg) * sz;
-        cc[0] = f.ok ? __ldg(g.dense + bid0) : kCodeEmpty;
+        const uint32_t bid0 = (uint32_t)(b.jx0 >> lg) + (uint32_t)(b.jy0 >> lg) * sy + (uint32_t)(b.jz0 >> lg) * sz;
 #pragma unroll
         for (int s = 1; s < 8; ++s) {
-            const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
-            cc[s] = need ? __ldg(g.dense + (bid0 + (uint32_t)(s & 1) + ((s & 2) ? sy : 0u) + ((s & 4) ? sz : 0u))) : cc[0];
+            const bool need = b.ok && (!(s & 1) || b.crx) && (!(s & 2) || b.cry) && (!(s & 4) || b.crz);
+            cc[s] = need ? __ldg(g.dense + (bid0 + (uint32_t)(s & 1) + ((s & 2) ? sy : 0u) + ((s & 4) ? sz : 0u))) : b.c0;
         }
     } else {
         const uint64_t sy = (uint64_t)g.nx, sz = (uint64_t)g.nx * g.ny;
-        const uint64_t bid0 = (uint64_t)(jx0 >> lg) + (uint64_t)(jy0 >> lg) * sy + (uint64_t)(jz0 >> lg) * sz;
-        cc[0] = f.ok ? block_code_hashed(g.hash, bid0) : kCodeEmpty;
+        const uint64_t bid0 = (uint64_t)(b.jx0 >> lg) + (uint64_t)(b.jy0 >> lg) * sy + (uint64_t)(b.jz0 >> lg) * sz;
 #pragma unroll
         for (int s = 1; s < 8; ++s) {
-            const bool need = f.ok && (!(s & 1) || crx) && (!(s & 2) || cry) && (!(s & 4) || crz);
+            const bool need = b.ok && (!(s & 1) || b.crx) && (!(s & 2) || b.cry) && (!(s & 4) || b.crz);
             cc[s] = need ? block_code_hashed(g.hash, bid0 + (uint64_t)(s & 1) + ((s & 2) ? sy : 0) + ((s & 4) ? sz : 0))
-                         : cc[0];
+                         : b.c0;
         }
     }
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        // the axes corner s crosses
-        const int x = (s & 1) && crx ? 1 : 0, y = (s & 2) && cry ? 2 : 0, z = (s & 4) && crz ? 4 : 0;
-        f.code[s] = cc[x | y | z];
+        const int x = (s & 1) && b.crx ? 1 : 0, y = (s & 2) && b.cry ? 2 : 0, z = (s & 4) && b.crz ? 4 : 0;
+        const int32_t code = cc[x | y | z];
+        const int32_t vid = b.vid0 + ((s & 1) ? dv0 : 0) + ((s & 2) ? dv1 : 0) + ((s & 4) ? dv2 : 0);
+        c[s] = code >= 0 ? __ldg(g.payload + ((size_t)code << (3 * g.lg)) + vid) : (code == kCodeFull ? g.full : g.empty);
     }
-    return f;
 }
 
-// The eight corners of an interior sample, loaded together, then the same
-// three-level lerp as sample_linear_dev.
-__device__ __forceinline__ float interior_sample(const SampleGrid& g, const InteriorCorners& f) {
-    float c[8];
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const int32_t vid = f.vid0 + ((s & 1) ? f.dv[0] : 0) + ((s & 2) ? f.dv[1] : 0) + ((s & 4) ? f.dv[2] : 0);
-        c[s] = f.code[s] >= 0 ? __ldg(g.payload + ((size_t)f.code[s] << (3 * g.lg)) + vid)
-                              : (f.code[s] == kCodeFull ? g.full : g.empty);
-    }
-    const float c00 = lerpf(c[0], c[1], f.u), c10 = lerpf(c[2], c[3], f.u), c01 = lerpf(c[4], c[5], f.u),
-                c11 = lerpf(c[6], c[7], f.u);
-    const float c0 = lerpf(c00, c10, f.v), c1 = lerpf(c01, c11, f.v);
-    return lerpf(c0, c1, f.w);
+// The same three-level lerp as sample_linear_dev.
+__device__ __forceinline__ float lerp_corners(const float c[8], const CornerBase& b) {
+    const float c00 = lerpf(c[0], c[1], b.u), c10 = lerpf(c[2], c[3], b.u), c01 = lerpf(c[4], c[5], b.u),
+                c11 = lerpf(c[6], c[7], b.u);
+    const float c0 = lerpf(c00, c10, b.v), c1 = lerpf(c01, c11, b.v);
+    return lerpf(c0, c1, b.w);
 }
 
 // The general gather (boundary conditions) out of line: rare, and large.
@@ -425,13 +448,22 @@ __global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, 
             out[3 * i + c] = u;
         }
     };
-    const InteriorCorners f0 = interior_corners(gx, x0, cy, cz);
-    const InteriorCorners f1 = interior_corners(gy, cx, y1, cz);
-    const InteriorCorners f2 = interior_corners(gz, cx, cy, z2);
-    const bool ok0 = f0.ok, ok1 = f1.ok, ok2 = f2.ok;
-    if (ok0) emit(0, interior_sample(gx, f0));
-    if (ok1) emit(1, interior_sample(gy, f1));
-    if (ok2) emit(2, interior_sample(gz, f2));
+    const CornerBase b0 = corner_base(gx, x0, cy, cz), b1 = corner_base(gy, cx, y1, cz), b2 = corner_base(gz, cx, cy, z2);
+    // a component whose samples in the whole warp are interior and cross no
+    // block takes the one-block path (most of them, for Morton-sorted
+    // particles); the 24 corner loads are issued before any lerp
+    const unsigned am = __activemask();
+    float c0[8], c1[8], c2[8];
+    if (__all_sync(am, b0.ok && !(b0.crx || b0.cry || b0.crz))) corners_one_block(gx, b0, c0);
+    else corners_general(gx, b0, c0);
+    if (__all_sync(am, b1.ok && !(b1.crx || b1.cry || b1.crz))) corners_one_block(gy, b1, c1);
+    else corners_general(gy, b1, c1);
+    if (__all_sync(am, b2.ok && !(b2.crx || b2.cry || b2.crz))) corners_one_block(gz, b2, c2);
+    else corners_general(gz, b2, c2);
+    const bool ok0 = b0.ok, ok1 = b1.ok, ok2 = b2.ok;
+    if (ok0) emit(0, lerp_corners(c0, b0));
+    if (ok1) emit(1, lerp_corners(c1, b1));
+    if (ok2) emit(2, lerp_corners(c2, b2));
     // the general gathers last, with little live across their calls
     if (!ok0) emit(0, sample_linear_boundary(gx, x0, cy, cz, bc));
     if (!ok1) emit(1, sample_linear_boundary(gy, cx, y1, cz, bc));
