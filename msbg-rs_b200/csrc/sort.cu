@@ -77,7 +77,7 @@ constexpr int OH_ITEMS = 8;
 constexpr int OS_LOOKBACK = 8;  // predecessor tiles read per look-back round
 constexpr uint64_t OS_AGGREGATE = 1ull << 32;  // word holds this tile's own count
 constexpr uint64_t OS_INCLUSIVE = 2ull << 32;  // word holds the count of tiles 0..k
-constexpr size_t OS_PASS_SMEM = (size_t)OS_TILE * (8 + 4);
+constexpr size_t OS_PASS_SMEM = (size_t)OS_TILE * (8 + 4);  // 64-bit keys; 32-bit ones use OS_TILE * 8
 
 __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
     uint64_t v;
@@ -140,15 +140,18 @@ __global__ void __launch_bounds__(256) os_hist_kernel(const uint64_t* __restrict
 // is zeroed here, tile by tile.  A look-back that waits more than limit_ns
 // (one second in a sort) sets bit 2 of *err and carries on with what it has
 // (the result is then wrong and the host reports the error), so no CTA can
-// spin forever.
+// spin forever.  KI, KO: the key types read and written; KS: the type a key
+// has inside the pass (32 bits when every key fits: half the shared-memory
+// and global traffic of the keys in the passes between the first and last).
+template <class KI, class KO, class KS>
 __global__ void __launch_bounds__(OS_THREADS, 4)
-    os_pass_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+    os_pass_kernel(const KI* __restrict__ kin, const uint32_t* __restrict__ vin, KO* __restrict__ kout,
                    uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist,
                    uint64_t* status, uint64_t* __restrict__ status_next, uint32_t* tile_counter, int* err,
                    uint64_t limit_ns) {
     extern __shared__ __align__(16) unsigned char os_smem[];
-    uint64_t* s_keys = reinterpret_cast<uint64_t*>(os_smem);
-    uint32_t* s_vals = reinterpret_cast<uint32_t*>(os_smem + (size_t)OS_TILE * 8);
+    KS* s_keys = reinterpret_cast<KS*>(os_smem);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(os_smem + (size_t)OS_TILE * sizeof(KS));
     __shared__ uint32_t s_wc[OS_WARPS][256];    // per-warp digit counts, then offsets
     __shared__ uint32_t s_match[OS_WARPS][256];  // per-warp lane masks of one round
     __shared__ uint32_t s_base[256];
@@ -169,9 +172,9 @@ __global__ void __launch_bounds__(OS_THREADS, 4)
 
     // keys of this warp still inside the array (0 for warps past the end)
     const int rem = wbase >= n ? 0 : (n - wbase >= (size_t)(32 * OS_ITEMS) ? 32 * OS_ITEMS : (int)(n - wbase));
-    uint64_t key[OS_ITEMS];
+    KS key[OS_ITEMS];
 #pragma unroll
-    for (int j = 0; j < OS_ITEMS; ++j) key[j] = j * 32 + lane < rem ? kin[wbase + lane + j * 32] : 0;
+    for (int j = 0; j < OS_ITEMS; ++j) key[j] = j * 32 + lane < rem ? (KS)kin[wbase + lane + j * 32] : (KS)0;
     // warp-level stable ranking, one round per item: every lane ORs its bit
     // into its digit's mask, so the mask read back holds the lanes with the
     // same digit; the lowest of them adds the group's size to the warp's
@@ -276,10 +279,10 @@ __global__ void __launch_bounds__(OS_THREADS, 4)
 
     const int in_tile = n - tile_base < (size_t)OS_TILE ? (int)(n - tile_base) : OS_TILE;
     for (int i = tid; i < in_tile; i += OS_THREADS) {
-        const uint64_t k = s_keys[i];
+        const KS k = s_keys[i];
         const uint32_t dst = s_base[(uint32_t)(k >> shift) & 255u] + (uint32_t)i;  // modulo 2^32, as s_base is
         if (dst < n) {  // always true unless a look-back gave up
-            kout[dst] = k;
+            kout[dst] = (KO)k;
             vout[dst] = s_vals[i];
         }
     }
@@ -331,17 +334,28 @@ void radix_sort_pairs(msbg_ctx* ctx, const uint64_t* keys_in, const uint32_t* va
     os_hist_kernel<<<(unsigned)std::min<size_t>(div_up(n, 256 * OH_ITEMS), 148 * 8), 256, 0, ctx->stream>>>(
         keys_in, n, passes, hist, status[0], tiles * 256);
     after_launch(ctx, "os_hist_kernel");
-    CUDA_CHECK(cudaFuncSetAttribute(os_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OS_PASS_SMEM));
-    const uint64_t* ki = keys_in;
+    // keys of at most 32 bits move as 32-bit words between the passes (the
+    // first pass narrows, the last widens); the ping-pong buffers hold either
+    const bool narrow = end_bit <= 32;
+    const void* ki = keys_in;
     const uint32_t* vi = vals_in;
     for (int p = 0; p < passes; ++p) {
         const bool to_out = ((passes - 1 - p) % 2) == 0;
-        uint64_t* ko = to_out ? keys_out : kt;
+        void* ko = to_out ? (void*)keys_out : (void*)kt;
         uint32_t* vo = to_out ? vals_out : vt;
+        const bool first = p == 0, last = p + 1 == passes;
+        uint64_t* st_next = p + 1 < passes ? status[(p + 1) & 1] : nullptr;
         begin_launch(ctx);
-        os_pass_kernel<<<(unsigned)tiles, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(
-            ki, vi, ko, vo, n, 8 * p, hist + p * 256, status[p & 1], p + 1 < passes ? status[(p + 1) & 1] : nullptr,
-            counters + p, ctx->status.as<int>(), kWaitLimitNs);
+#define OS_PASS(KI, KO, KS)                                                                                              \
+    os_pass_kernel<KI, KO, KS><<<(unsigned)tiles, OS_THREADS, (size_t)OS_TILE * (sizeof(KS) + 4), ctx->stream>>>(     \
+        (const KI*)ki, vi, (KO*)ko, vo, n, 8 * p, hist + p * 256, status[p & 1], st_next, counters + p,                 \
+        ctx->status.as<int>(), kWaitLimitNs)
+        if (!narrow) OS_PASS(uint64_t, uint64_t, uint64_t);
+        else if (first && last) OS_PASS(uint64_t, uint64_t, uint32_t);
+        else if (first) OS_PASS(uint64_t, uint32_t, uint32_t);
+        else if (last) OS_PASS(uint32_t, uint64_t, uint32_t);
+        else OS_PASS(uint32_t, uint32_t, uint32_t);
+#undef OS_PASS
         after_launch(ctx, "os_pass_kernel");
         ki = ko;
         vi = vo;
@@ -800,11 +814,10 @@ int msbg_test_sort_lookback_timeout(msbg_ctx* ctx, uint64_t limit_ns) {
     CUDA_CHECK(cudaMemsetAsync(status, 0, 2 * 256 * 8, ctx->stream));
     const uint32_t one = 1;  // the CTA's tile id: tile 0 never runs
     CUDA_CHECK(cudaMemcpyAsync(counter, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_CHECK(cudaFuncSetAttribute(os_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OS_PASS_SMEM));
     begin_launch(ctx);
-    os_pass_kernel<<<1, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(keys, nullptr, ScratchLayout::at<uint64_t>(base, oko),
-                                                                ScratchLayout::at<uint32_t>(base, ovo), n, 0, hist, status,
-                                                                nullptr, counter, ctx->status.as<int>(), limit_ns);
+    os_pass_kernel<uint64_t, uint64_t, uint64_t><<<1, OS_THREADS, OS_PASS_SMEM, ctx->stream>>>(
+        keys, nullptr, ScratchLayout::at<uint64_t>(base, oko), ScratchLayout::at<uint32_t>(base, ovo), n, 0, hist, status,
+        nullptr, counter, ctx->status.as<int>(), limit_ns);
     after_launch(ctx, "os_pass_kernel");
     check_device_status(ctx);
     MSBG_API_END
