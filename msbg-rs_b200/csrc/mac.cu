@@ -431,7 +431,7 @@ struct BlendArgs {
 };
 
 template <int BLEND>
-__global__ void __launch_bounds__(256) g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz,
+__global__ void __launch_bounds__(256, 4) g2p_kernel(SampleGrid gx, SampleGrid gy, SampleGrid gz,
                                                   const float* __restrict__ pos, size_t n, int bc, BlendArgs bl,
                                                   float* __restrict__ out) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
