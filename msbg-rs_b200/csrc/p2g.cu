@@ -71,6 +71,11 @@ __global__ void __launch_bounds__(256) p2g_combine_kernel(CombineArgs a) {
     __syncthreads();
     const int px = (int)(bx & 1), py = (int)(by & 1), pz = (int)(bz & 1);
     const int32_t slot = a.slots[j];
+    // this direction's output block (selected once: a dynamically indexed
+    // parameter array is read through local memory)
+    float* const mout = (dir == 0 ? a.mass[0] : dir == 1 ? a.mass[1] : a.mass[2]) + (size_t)slot * N;
+    float* const vout = (dir == 0 ? a.vel[0] : dir == 1 ? a.vel[1] : a.vel[2]) + (size_t)slot * N;
+    const double* const part = a.partial + (size_t)dir * 2 * WW;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         const int lx = i & (BSX - 1), ly = (i >> LG) & (BSX - 1), lz = i >> (2 * LG);
         // Contributions are added in the colour order of the contributing
@@ -90,13 +95,13 @@ __global__ void __launch_bounds__(256) p2g_combine_kernel(CombineArgs a) {
             const int r = rank[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
             if (r < 0) continue;
             const int sx = lx - BSX * ox + M, sy = ly - BSX * oy + M, sz = lz - BSX * oz + M;
-            const double* p = a.partial + ((size_t)r * 3 + dir) * 2 * WW + (sz * W + sy) * W + sx;
+            const double* p = part + (size_t)r * 3 * 2 * WW + (sz * W + sy) * W + sx;
             sm += p[0];
             sv += p[WW];
         }
         const float mf = (float)sm, pf = (float)sv;
-        a.mass[dir][(size_t)slot * N + i] = mf;
-        a.vel[dir][(size_t)slot * N + i] = mf > 0.0f ? pf / mf : 0.0f;
+        mout[i] = mf;
+        vout[i] = mf > 0.0f ? pf / mf : 0.0f;
     }
 }
 

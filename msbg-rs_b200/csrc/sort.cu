@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) os_hist_kernel(const uint64_t* __restrict
 // has inside the pass (32 bits when every key fits: half the shared-memory
 // and global traffic of the keys in the passes between the first and last).
 template <class KI, class KO, class KS>
-__global__ void __launch_bounds__(OS_THREADS, 4)
+__global__ void __launch_bounds__(OS_THREADS, 5)
     os_pass_kernel(const KI* __restrict__ kin, const uint32_t* __restrict__ vin, KO* __restrict__ kout,
                    uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist,
                    uint64_t* status, uint64_t* __restrict__ status_next, uint32_t* tile_counter, int* err,
