@@ -116,14 +116,23 @@ __global__ void cell_csr_kernel(const uint64_t* skeys, const uint64_t* pb_starts
     int32_t* ce = cell_end + (size_t)k * n_cells;
     for (int i = threadIdx.x; i < n_cells; i += blockDim.x) cb[i] = ce[i] = 0;
     __syncthreads();
-    // particle indices fit int32 (the CSR stores them as int32)
+    // particle indices fit int32 (the CSR stores them as int32); a key's
+    // neighbours come from the adjacent lanes (the warp's end lanes load
+    // theirs), every lane of the CTA taking the same rounds
     const int32_t s = (int32_t)pb_starts[k], e = (int32_t)pb_starts[k + 1];
     const uint32_t cm = (uint32_t)cmask;
-#pragma unroll 4
-    for (int32_t i = s + (int32_t)threadIdx.x; i < e; i += (int32_t)blockDim.x) {
-        const uint32_t c = (uint32_t)skeys[i] & cm;
-        if (i == s || ((uint32_t)skeys[i - 1] & cm) != c) cb[c] = i;
-        if (i == e - 1 || ((uint32_t)skeys[i + 1] & cm) != c) ce[c] = i + 1;
+    const int lane = threadIdx.x & 31;
+    for (int32_t r = s; r < e; r += (int32_t)blockDim.x) {
+        const int32_t i = r + (int32_t)threadIdx.x;
+        const bool in = i < e;
+        const uint32_t c = in ? (uint32_t)skeys[i] & cm : 0u;
+        uint32_t prev = __shfl_up_sync(0xffffffffu, c, 1), next = __shfl_down_sync(0xffffffffu, c, 1);
+        if (lane == 0 && in && i > s) prev = (uint32_t)skeys[i - 1] & cm;
+        if (lane == 31 && i + 1 < e) next = (uint32_t)skeys[i + 1] & cm;
+        if (in) {
+            if (i == s || prev != c) cb[c] = i;
+            if (i == e - 1 || next != c) ce[c] = i + 1;
+        }
     }
 }
 
